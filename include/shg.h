@@ -1,0 +1,166 @@
+/*
+ * shg.h — C ABI of the B200-native focused-beam SHG solver (libshg_b200.so).
+ *
+ * This is the drop-in boundary for the split-step Fourier (SSFM) march of the
+ * coupled pump / second-harmonic (SH) fields and the 3D Jacobi heat solve of
+ * alfredos84/cuSHG.  The reference exposes that path as one C++ method with its
+ * parameters split between compile-time constants and arguments:
+ *
+ *   Solver::run(Power, waist, focalpoint, Temp, T_inf, Tpeltier,
+ *               save_only_last, save_temperature)      src/headers/Solver.h:149,311
+ *   NX, NY, NZ                                          src/cuSHG.cu:11-13
+ *   crystal / beam constants                            src/headers/Crystal.h:19-52
+ *   -DTHERMAL                                           src/headers/Solver.h:32,321
+ *   outputs Pump_out_{r,i}.dat, Signal_out_{r,i}.dat    src/headers/Solver.h:283-286
+ *   temperature tensor Tfinal_<z>.dat                   src/headers/Solver.h:372-373
+ *
+ * Here every one of those is a runtime field of shg_params, the fields come back
+ * in caller-owned buffers as interleaved complex (re, im) in the reference's
+ * row-major layout (x fastest: index y*nx + x, src/headers/Common.h:88-90), and
+ * errors come back as a status code instead of exit(1) (src/headers/Common.h:10-20).
+ *
+ * Element types: precision 64 -> double (re, im pairs, like cufftDoubleComplex),
+ * precision 32 -> float (like cufftComplex).  Real 3D arrays (temperature) use
+ * the same scalar type, index z*nx*ny + y*nx + x.
+ *
+ * Units follow the reference: lengths in µm, time in ps, power in W,
+ * temperatures in °C.
+ */
+#ifndef CUSHG_B200_SHG_H
+#define CUSHG_B200_SHG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum shg_status {
+    SHG_OK = 0,
+    SHG_ERR_INVALID = 1,       /* a parameter is out of range, NaN, or a pointer is NULL */
+    SHG_ERR_UNSUPPORTED = 2,   /* grid size / precision combination not built */
+    SHG_ERR_CUDA = 3,          /* a CUDA runtime call failed; see shg_last_error() */
+    SHG_ERR_NOMEM = 4,         /* device or host allocation failed */
+    SHG_ERR_NOT_CONVERGED = 5, /* Jacobi hit max_sweeps before its tolerance */
+    SHG_ERR_NO_DEVICE = 6      /* no CUDA device is visible */
+} shg_status;
+
+/* Heat-equation boundary models (src/headers/Tfield.h). */
+enum {
+    SHG_BOUNDARY_TOP_OPEN = 0,        /* kernelHeatEquationTopOpen, Tfield.h:93-201:
+                                         y=0 face Dirichlet at t_peltier, Robin elsewhere */
+    SHG_BOUNDARY_OVEN_SURROUNDED = 1  /* kernelHeatEquationOvenSurrounded, Tfield.h:205-240:
+                                         4 lateral faces at t_peltier, Robin on z faces */
+};
+
+/* Jacobi stopping rules. */
+enum {
+    SHG_CONV_REFERENCE = 0, /* sqrt(sum (Tf-Ti)^2)/TSIZE < tol, checked every check_every
+                               sweeps, stagnation exit (Solver.h:332-351) */
+    SHG_CONV_MAXABS = 1     /* max |Tf-Ti| < tol, checked every check_every sweeps */
+};
+
+/* Crystals (Sellmeier equations). */
+enum {
+    SHG_CRYSTAL_MGO_SPPLT = 0 /* Bruner et al., src/headers/Crystal.h:54-70 */
+};
+
+typedef struct shg_params {
+    /* grid: src/cuSHG.cu:11-13 (NX, NY, NZ).  nx == ny, even. */
+    int32_t nx, ny, nz;
+    int32_t precision;      /* 64 (double) or 32 (float): src/cuSHG.cu:7-8 */
+    /* window and crystal [µm]: Crystal.h:31-33 (LX, LY, LZ); dx = lx/(nx-1) */
+    double lx, ly, lz;
+    double lambda_p;        /* pump wavelength [µm], SH at lambda_p/2: Crystal.h:27-28 */
+    double deff;            /* effective nonlinearity [µm/V]: Crystal.h:40 */
+    double period;          /* QPM grating period Λ [µm]: Crystal.h:42 */
+    double alpha_p;         /* pump linear absorption [1/µm]: Crystal.h:43 */
+    double alpha_s;         /* SH linear absorption [1/µm]: Crystal.h:44 */
+    double beta_s;          /* SH two-photon absorption [µm/W]: Crystal.h:45 */
+    double rho_p, rho_s;    /* walk-off angles [rad]: Crystal.h:46-47 */
+    double kappa;           /* thermal conductivity [W/(µm K)]: Crystal.h:51 */
+    double h_conv;          /* heat transfer coefficient [W/(µm² K)]: Crystal.h:52 */
+    /* Solver::run arguments: Solver.h:311 and cuSHG.cu:46-53 */
+    double power;           /* pump power [W] */
+    double waist;           /* beam waist radius [µm] */
+    double focus;           /* focal position from the input face [µm] */
+    double temp;            /* initial / phase-matching temperature [°C] */
+    double t_inf;           /* environment temperature [°C] (25 in cuSHG.cu:52) */
+    double t_peltier;       /* oven temperature [°C] */
+    int32_t thermal;        /* 0: plain run; 1: -DTHERMAL outer optical-thermal loop */
+    int32_t boundary;       /* SHG_BOUNDARY_* */
+    int32_t max_outer;      /* outer iterations, 20 in Solver.h:325 */
+    int32_t check_every;    /* Jacobi check period, 5000 in Solver.h:342 */
+    int32_t conv_rule;      /* SHG_CONV_* */
+    int32_t crystal;        /* SHG_CRYSTAL_* */
+    double jacobi_tol;      /* <= 0 selects the reference tolerance 5e-4/TSIZE (Solver.h:332) */
+    int64_t max_sweeps;     /* Jacobi sweep cap per outer iteration (<= 0: 2^40) */
+} shg_params;
+
+/* Per-call report. */
+typedef struct shg_stats {
+    double sh_power;          /* SH output power [W]: sum 0.5*eps0*c*n_s*|S|^2*dx*dy */
+    double pump_power;        /* pump output power [W], same normalisation */
+    int64_t jacobi_sweeps;    /* total Jacobi sweeps over all outer iterations */
+    int32_t outer_iterations; /* outer optical-thermal iterations run */
+    int32_t steps;            /* SSFM steps marched per optical pass */
+    double last_residual;     /* last Jacobi convergence value */
+    double device_ms;         /* device time of the call (CUDA events) */
+} shg_stats;
+
+/* Fill *p with the reference's compile-time defaults (cuSHG.cu:11-13, Crystal.h:19-52,
+ * cuSHG.cu:46-53 with argv = 30 W, 29 µm, 55.66 °C from cuSHG.sh:43-45). */
+void shg_default_params(shg_params* p);
+
+/* Validate a parameter set; SHG_OK or SHG_ERR_INVALID / SHG_ERR_UNSUPPORTED. */
+shg_status shg_check_params(const shg_params* p);
+
+/* Number of SSFM steps a plain optical pass marches for these parameters: the
+ * reference records the fields before its last step (Solver.h:283-286), so a
+ * plain pass marches nz-1 steps and a thermal pass nz (its last step feeds Q). */
+int32_t shg_steps(const shg_params* p);
+
+/*
+ * Solve one instance.  Replaces Solver::run (Solver.h:311-390) with
+ * save_only_last = true.  Host buffers, synchronous.
+ *   signal_in   nx*ny complex or NULL.  NULL starts the SH at zero; the reference
+ *               starts from clock-seeded N(0,1e-20) noise (Efields.h:144-168).
+ *   pump_out, signal_out   nx*ny complex each (Pump_out / Signal_out), may be NULL.
+ *   temperature_out        nx*ny*nz reals (Tfinal), thermal runs only, may be NULL.
+ *   stats                  may be NULL.
+ */
+shg_status shg_solve(const shg_params* p, const void* signal_in, void* pump_out,
+                     void* signal_out, void* temperature_out, shg_stats* stats);
+
+/* The same with device buffers on a caller stream (a cudaStream_t, NULL = legacy
+ * default stream).  Plain runs are asynchronous; thermal runs synchronise at each
+ * Jacobi convergence check.  stats, if given, is filled after a synchronise. */
+shg_status shg_solve_device(const shg_params* p, const void* signal_in_dev,
+                            void* pump_out_dev, void* signal_out_dev,
+                            void* temperature_out_dev, shg_stats* stats, void* stream);
+
+/*
+ * Batched plain runs: `count` independent instances, each with its own parameter
+ * set (grid size, nz, crystal, beam), in one persistent launch per grid-size class
+ * fed by a device work queue.  Replaces the one-process-per-point sweep of
+ * src/cuSHG.sh:58-94.  All instances must share `precision` and have thermal == 0.
+ * pump_out[i] / signal_out[i]: device buffers (nx_i*ny_i complex) or NULL entries.
+ * sh_power_out: host array of `count` doubles or NULL.
+ */
+shg_status shg_solve_batch_device(const shg_params* params, int32_t count,
+                                  void* const* pump_out_dev, void* const* signal_out_dev,
+                                  double* sh_power_out, void* stream);
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* shg_last_error(void);
+const char* shg_status_string(int32_t status);
+
+/* Library version string. */
+const char* shg_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUSHG_B200_SHG_H */

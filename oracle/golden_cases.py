@@ -1,0 +1,77 @@
+"""Golden cases: parameter sets run through the reference program (oracle/ref_build.py,
+oracle/make_golden.py) to pin the CPU oracle and the CUDA path.
+
+TEST INFRASTRUCTURE ONLY.
+
+The reference takes its inputs as compile-time constants plus argv (src/cuSHG.cu:46-58):
+argv = power, waist, oven temperature, save_only_last, save_temperature, with the
+Peltier temperature equal to the oven temperature (src/cuSHG.cu:53), so every case here
+has t_peltier == temp.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+from cushg_b200 import params as P  # noqa: E402
+
+
+def _d(p: P.ShgParams) -> dict:
+    return p.as_dict()
+
+
+def _plain_c1() -> P.ShgParams:
+    return P.config_plain_64()
+
+
+def _plain_96_walkoff() -> P.ShgParams:
+    # 96 = 3 * 32 exercises a radix-3 transform; lx != ly gives dx != dy; walk-off on.
+    p = P.workload(96, 40, 8000.0, 12.0, 25.0, 0.5 * 8000.0, 33.0, precision=64)
+    p.lx, p.ly = 400.0, 330.0
+    p.rho_p, p.rho_s = 0.004, 0.006
+    p.period = 8.0
+    return p
+
+
+def _plain_128_offfocus() -> P.ShgParams:
+    p = P.workload(128, 60, 20000.0, 30.0, 35.0, 0.5 * 20000.0, 29.0, precision=64)
+    return p
+
+
+def _thermal_small() -> P.ShgParams:
+    # small thermal grid with strong absorption so the optical-thermal coupling is visible
+    p = P.workload(24, 12, 4000.0, 20.0, 25.0, 2000.0, 30.0, precision=64, thermal=1)
+    p.alpha_p, p.alpha_s, p.beta_s = 2e-5, 1e-4, 1e-3
+    p.max_outer = 3
+    p.check_every = 5000
+    p.conv_rule = P.SHG_CONV_REFERENCE
+    p.jacobi_tol = 0.0
+    return p
+
+
+def _thermal_small_oven() -> P.ShgParams:
+    p = _thermal_small()
+    p.boundary = P.SHG_BOUNDARY_OVEN_SURROUNDED
+    return p
+
+
+def _plain_c1_f32() -> P.ShgParams:
+    return P.config_plain_64().replace(precision=32)
+
+
+CASES = {
+    "plain64_c1": {"precision": 64, "params": _d(_plain_c1())},
+    "plain64_n96_walkoff": {"precision": 64, "params": _d(_plain_96_walkoff())},
+    "plain64_n128": {"precision": 64, "params": _d(_plain_128_offfocus())},
+    "thermal64_small": {"precision": 64, "params": _d(_thermal_small())},
+    "thermal64_small_oven": {"precision": 64, "params": _d(_thermal_small_oven()), "oven_surrounded": True},
+    "plain32_c1": {"precision": 32, "params": _d(_plain_c1_f32())},
+}
+
+
+def params_of(name: str) -> P.ShgParams:
+    p = P.ShgParams()
+    for k, v in CASES[name]["params"].items():
+        setattr(p, k, v)
+    return p

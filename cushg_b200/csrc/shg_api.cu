@@ -1,0 +1,287 @@
+// shg_api.cu — host side of libshg_b200: the C ABI of include/shg.h.
+//
+// This is the C++ counterpart of the reference's Solver::run (src/headers/Solver.h:311-390)
+// and of the argv / compile-time configuration of src/cuSHG.cu:11-58: it validates a
+// runtime shg_params, derives every per-instance constant in FP64 with the reference's
+// formulas, and drives the fused kernels.  Errors are returned as shg_status codes; the
+// message of the last failure on the calling thread is kept for shg_last_error().
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/shg.h"
+#include "shg_host.h"
+#include "shg_internal.h"
+#include "ssfm_variants.h"
+
+namespace shg {
+
+static thread_local std::string g_last_error;
+
+shg_status fail(shg_status st, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return st;
+}
+
+shg_status cuda_fail(cudaError_t e, const char* what) {
+    return fail(SHG_ERR_CUDA, "%s: %s (%d)", what, cudaGetErrorString(e), (int)e);
+}
+
+void clear_error() { g_last_error.clear(); }
+
+// Physical constants, src/headers/Crystal.h:19-21 (µm, ps, W, V).
+const double kPi = 3.14159265358979323846;
+const double kC = 299792458 * 1E6 / 1E12;
+const double kEps0 = 8.8541878128E-12 * 1E12 / 1E6;
+
+// Sellmeier equation of MgO:sPPLT (Bruner et al.), src/headers/Crystal.h:54-70.
+double sellmeier(double L, double T) {
+    const double A = 4.502483, B = 0.007294, C = 0.185087, D = -0.02357;
+    const double E = 0.073423, F = 0.199595, G = 0.001, H = 7.99724;
+    const double TK = T + 273.15;
+    const double b = 3.483933e-8 * (TK * TK);
+    const double c = 1.607839e-8 * (TK * TK);
+    const double L2 = L * L;
+    return std::sqrt(A + (B + b) / (L2 - (C + c) * (C + c)) + E / (L2 - F * F) + G / (L2 - H * H) + D * L2);
+}
+
+// Δk at temperature T with the grating's thermal expansion (PhaseMatching.h:47-85).
+double delta_k(const shg_params& p, double T) {
+    const double lp = p.lambda_p, ls = 0.5 * lp;
+    const double a = 2.2e-6, b = -5.9e-9, d = T - 25.;
+    return 2 * kPi * (2 * sellmeier(lp, T) / lp - sellmeier(ls, T) / ls + 1 / (p.period * (1. + a * d + b * (d * d))));
+}
+
+// Constants of one plain optical pass at uniform temperature Tc (the reference reads
+// T at voxel (NX/2, NY/2, 0) for the pump and propagators, Efields.h:88,124).
+InstDesc make_plain_desc(const shg_params& p, double Tc, double T_dk) {
+    InstDesc d;
+    std::memset(&d, 0, sizeof(d));
+    const double dx = p.lx / (p.nx - 1), dy = p.ly / (p.ny - 1), dz = p.lz / (p.nz - 1);
+    const double lp = p.lambda_p, ls = 0.5 * lp;
+    const double dQ = 2.0 * p.deff / kPi;
+    const double np = sellmeier(lp, Tc), ns = sellmeier(ls, Tc);
+    d.n = p.nx;
+    d.nsteps = shg_steps(&p);
+    d.dz = dz;
+    d.dk = delta_k(p, T_dk);
+    d.kap_p = 1 * kPi * dQ / (np * lp);
+    d.kap_s = 0.5 * kPi * dQ / (ns * ls);
+    d.hap = 0.5 * p.alpha_p;
+    d.has = 0.5 * p.alpha_s;
+    d.qs = 0.5 * (p.beta_s * 0.5 * kC * kEps0 * ns);
+    // setPump, Efields.h:92-110
+    const double wX2 = p.waist * p.waist;
+    const double zRX = kPi * np * wX2 / lp;
+    const double Ap0 = std::sqrt(4 * p.power / (kEps0 * kC * kPi * np * wX2));
+    const double etaX = p.focus / zRX;
+    const double mre = 1.0, mim = -etaX;  // MX = 1 - i etaX
+    const double den = mre * mre + mim * mim;
+    d.amp_re = (Ap0 * mre) / den;
+    d.amp_im = (-Ap0 * mim) / den;
+    d.den_re = wX2 * mre;
+    d.den_im = wX2 * mim;
+    d.ux = 0.5 * p.nx;
+    d.uy = 0.5 * p.ny;
+    d.dx = dx;
+    d.dy = dy;
+    // beamPropagator, Efields.h:124-137
+    const double kp = 2 * kPi * np / lp, ks = 2 * kPi * ns / ls;
+    d.dfx = 1 / dx / p.nx;
+    d.dfy = 1 / dy / p.ny;
+    d.a_p = 2 * (kPi * kPi) / kp;
+    d.a_s = 2 * (kPi * kPi) / ks;
+    d.b_p = 2 * kPi * d.dfx * std::tan(p.rho_p);
+    d.b_s = 2 * kPi * d.dfx * std::tan(p.rho_s);
+    d.pw_s = 0.5 * kEps0 * kC * ns * dx * dy;
+    d.pw_p = 0.5 * kEps0 * kC * np * dx * dy;
+    return d;
+}
+
+size_t complex_bytes(const shg_params& p) { return p.precision == 32 ? 8 : 16; }
+
+}  // namespace shg
+
+using namespace shg;
+
+extern "C" {
+
+void shg_default_params(shg_params* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->nx = p->ny = 128;
+    p->nz = 100;
+    p->precision = 32;
+    p->lx = 2000.0;
+    p->ly = 1000.0;
+    p->lz = 30000.0;
+    p->lambda_p = 1.064;
+    p->deff = 11.00e-6;
+    p->period = 7.97;
+    p->alpha_p = 0.17e-6;
+    p->alpha_s = 1.57e-6;
+    p->beta_s = 5e-5;
+    p->rho_p = p->rho_s = 0.0;
+    p->kappa = 8.4e-6;
+    p->h_conv = 10e-12;
+    p->power = 30.0;
+    p->waist = 29.0;
+    p->focus = 0.5 * 30000.0;
+    p->temp = 55.66;
+    p->t_inf = 25.0;
+    p->t_peltier = 55.66;
+    p->thermal = 0;
+    p->boundary = SHG_BOUNDARY_TOP_OPEN;
+    p->max_outer = 20;
+    p->check_every = 5000;
+    p->conv_rule = SHG_CONV_REFERENCE;
+    p->crystal = SHG_CRYSTAL_MGO_SPPLT;
+    p->jacobi_tol = 0.0;
+    p->max_sweeps = 0;
+}
+
+static bool finite_all(const shg_params* p) {
+    const double v[] = {p->lx, p->ly, p->lz, p->lambda_p, p->deff, p->period, p->alpha_p, p->alpha_s, p->beta_s,
+                        p->rho_p, p->rho_s, p->kappa, p->h_conv, p->power, p->waist, p->focus, p->temp, p->t_inf,
+                        p->t_peltier, p->jacobi_tol};
+    for (double x : v)
+        if (!std::isfinite(x)) return false;
+    return true;
+}
+
+shg_status shg_check_params(const shg_params* p) {
+    clear_error();
+    if (!p) return fail(SHG_ERR_INVALID, "params is NULL");
+    if (!finite_all(p)) return fail(SHG_ERR_INVALID, "a parameter is NaN or infinite");
+    if (p->precision != 32 && p->precision != 64) return fail(SHG_ERR_INVALID, "precision must be 32 or 64");
+    if (p->nx != p->ny) return fail(SHG_ERR_INVALID, "nx (%d) must equal ny (%d)", p->nx, p->ny);
+    if (p->nx < 2 || (p->nx & 1)) return fail(SHG_ERR_INVALID, "grid side %d must be even and >= 2", p->nx);
+    if (p->nz < 2) return fail(SHG_ERR_INVALID, "nz must be >= 2 (dz = lz/(nz-1))");
+    if (!(p->lx > 0 && p->ly > 0 && p->lz > 0)) return fail(SHG_ERR_INVALID, "lx, ly, lz must be > 0");
+    if (!(p->lambda_p > 0.3 && p->lambda_p < 6.0)) return fail(SHG_ERR_INVALID, "lambda_p out of range");
+    if (!(p->waist > 0) || p->power < 0 || !(p->period > 0)) return fail(SHG_ERR_INVALID, "waist/power/period");
+    if (p->alpha_p < 0 || p->alpha_s < 0 || p->beta_s < 0) return fail(SHG_ERR_INVALID, "negative absorption");
+    if (p->crystal != SHG_CRYSTAL_MGO_SPPLT) return fail(SHG_ERR_UNSUPPORTED, "unknown crystal %d", p->crystal);
+    if (p->thermal) {
+        if (!(p->kappa > 0) || p->h_conv < 0) return fail(SHG_ERR_INVALID, "kappa must be > 0, h_conv >= 0");
+        if (p->boundary != SHG_BOUNDARY_TOP_OPEN && p->boundary != SHG_BOUNDARY_OVEN_SURROUNDED)
+            return fail(SHG_ERR_INVALID, "unknown boundary %d", p->boundary);
+        if (p->conv_rule != SHG_CONV_REFERENCE && p->conv_rule != SHG_CONV_MAXABS)
+            return fail(SHG_ERR_INVALID, "unknown conv_rule %d", p->conv_rule);
+        if (p->nz < 3 || p->nx < 3) return fail(SHG_ERR_INVALID, "thermal grid needs nx, nz >= 3");
+    }
+    if (!find_plain_variant(p->precision, p->nx))
+        return fail(SHG_ERR_UNSUPPORTED, "no kernel built for grid side %d at precision %d", p->nx, p->precision);
+    return SHG_OK;
+}
+
+int32_t shg_steps(const shg_params* p) {
+    if (!p) return 0;
+    return p->thermal ? p->nz : p->nz - 1;
+}
+
+const char* shg_last_error(void) { return g_last_error.c_str(); }
+
+const char* shg_status_string(int32_t s) {
+    switch (s) {
+        case SHG_OK: return "ok";
+        case SHG_ERR_INVALID: return "invalid argument";
+        case SHG_ERR_UNSUPPORTED: return "unsupported configuration";
+        case SHG_ERR_CUDA: return "CUDA error";
+        case SHG_ERR_NOMEM: return "out of memory";
+        case SHG_ERR_NOT_CONVERGED: return "Jacobi did not converge";
+        case SHG_ERR_NO_DEVICE: return "no CUDA device";
+        default: return "unknown status";
+    }
+}
+
+const char* shg_version(void) { return "libshg_b200 0.1 (sm_100a)"; }
+
+shg_status shg_solve_device(const shg_params* p, const void* signal_in_dev, void* pump_out_dev, void* signal_out_dev,
+                            void* temperature_out_dev, shg_stats* stats, void* stream_) {
+    shg_status st = shg_check_params(p);
+    if (st != SHG_OK) return st;
+    cudaStream_t stream = (cudaStream_t)stream_;
+    if (p->thermal) return thermal_solve_device(*p, signal_in_dev, pump_out_dev, signal_out_dev, temperature_out_dev, stats, stream);
+    return plain_solve_device(*p, signal_in_dev, pump_out_dev, signal_out_dev, stats, stream);
+}
+
+shg_status shg_solve(const shg_params* p, const void* signal_in, void* pump_out, void* signal_out,
+                     void* temperature_out, shg_stats* stats) {
+    shg_status st = shg_check_params(p);
+    if (st != SHG_OK) return st;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(SHG_ERR_NO_DEVICE, "no CUDA device visible");
+    }
+    const size_t plane = (size_t)p->nx * p->ny * complex_bytes(*p);
+    const size_t tbytes = (size_t)p->nx * p->ny * p->nz * (p->precision == 32 ? 4 : 8);
+    cudaStream_t s = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
+    void *din = nullptr, *dp = nullptr, *ds = nullptr, *dT = nullptr;
+    shg_status rc = SHG_OK;
+    do {
+        if (signal_in && (e = cudaMallocAsync(&din, plane, s)) != cudaSuccess) { rc = cuda_fail(e, "cudaMallocAsync"); break; }
+        if ((e = cudaMallocAsync(&dp, plane, s)) != cudaSuccess) { rc = cuda_fail(e, "cudaMallocAsync"); break; }
+        if ((e = cudaMallocAsync(&ds, plane, s)) != cudaSuccess) { rc = cuda_fail(e, "cudaMallocAsync"); break; }
+        if (temperature_out && p->thermal && (e = cudaMallocAsync(&dT, tbytes, s)) != cudaSuccess) {
+            rc = cuda_fail(e, "cudaMallocAsync");
+            break;
+        }
+        if (din && (e = cudaMemcpyAsync(din, signal_in, plane, cudaMemcpyHostToDevice, s)) != cudaSuccess) {
+            rc = cuda_fail(e, "cudaMemcpyAsync H2D");
+            break;
+        }
+        rc = shg_solve_device(p, din, dp, ds, dT, stats, s);
+        if (rc != SHG_OK) break;
+        if (pump_out && (e = cudaMemcpyAsync(pump_out, dp, plane, cudaMemcpyDeviceToHost, s)) != cudaSuccess) {
+            rc = cuda_fail(e, "cudaMemcpyAsync D2H");
+            break;
+        }
+        if (signal_out && (e = cudaMemcpyAsync(signal_out, ds, plane, cudaMemcpyDeviceToHost, s)) != cudaSuccess) {
+            rc = cuda_fail(e, "cudaMemcpyAsync D2H");
+            break;
+        }
+        if (dT && (e = cudaMemcpyAsync(temperature_out, dT, tbytes, cudaMemcpyDeviceToHost, s)) != cudaSuccess) {
+            rc = cuda_fail(e, "cudaMemcpyAsync D2H");
+            break;
+        }
+        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) { rc = cuda_fail(e, "cudaStreamSynchronize"); break; }
+    } while (0);
+    if (din) cudaFreeAsync(din, s);
+    if (dp) cudaFreeAsync(dp, s);
+    if (ds) cudaFreeAsync(ds, s);
+    if (dT) cudaFreeAsync(dT, s);
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+    return rc;
+}
+
+shg_status shg_solve_batch_device(const shg_params* params, int32_t count, void* const* pump_out_dev,
+                                  void* const* signal_out_dev, double* sh_power_out, void* stream_) {
+    clear_error();
+    if (!params || count < 0) return fail(SHG_ERR_INVALID, "params is NULL or count < 0");
+    for (int i = 0; i < count; ++i) {
+        shg_status st = shg_check_params(&params[i]);
+        if (st != SHG_OK) return fail(st, "instance %d: %s", i, g_last_error.c_str());
+        if (params[i].thermal) return fail(SHG_ERR_UNSUPPORTED, "instance %d: batched runs are plain (thermal == 0)", i);
+        if (params[i].precision != params[0].precision)
+            return fail(SHG_ERR_INVALID, "instance %d: all instances must share one precision", i);
+    }
+    return plain_solve_batch(params, count, pump_out_dev, signal_out_dev, sh_power_out, (cudaStream_t)stream_);
+}
+
+}  // extern "C"

@@ -1,0 +1,35 @@
+// shg_internal.h — structures shared by the host driver and the kernels of
+// libshg_b200 (not part of the public C ABI).
+#pragma once
+
+#include <stdint.h>
+
+namespace shg {
+
+// Per-instance constants of one plain optical pass.  The host fills them in FP64
+// from shg_params with the reference's formulas (src/headers/Solver.h:57-80,
+// Efields.h:84-141, PhaseMatching.h:68-85, Crystal.h:34-41); the kernels round to
+// the working precision only where a value enters field arithmetic.
+struct InstDesc {
+    int32_t n;             // grid side (nx == ny)
+    int32_t nsteps;        // SSFM steps to march
+    int32_t has_signal_in; // 1: SH starts from signal_in, 0: from zero
+    int32_t slot;          // output slot (batch index)
+    double dz;             // LZ/(NZ-1)
+    double dk;             // phase mismatch Δk at the (uniform) temperature
+    double kap_p, kap_s;   // π dQ/(n_p λp), 0.5 π dQ/(n_s λs)
+    double hap, has, qs;   // 0.5 αp, 0.5 αs, 0.5 βs 0.5 c ε0 n_s
+    // pump at z = 0: P = amp * exp(-(ax^2 + ay^2) / den), ax = (x - ux) dx
+    double amp_re, amp_im, den_re, den_im;
+    double ux, uy, dx, dy;
+    // propagator phase θ = -dz (a (dfx^2 sx^2 + dfy^2 sy^2) + b sx) per field,
+    // sx, sy the signed FFT frequency indices
+    double a_p, b_p, a_s, b_s, dfx, dfy;
+    double pw_s, pw_p;     // power = pw * sum |A|^2  (0.5 eps0 c n dx dy)
+    const void* signal_in; // device, n*n complex (natural layout) or null
+    void* pump_out;        // device, n*n complex or null
+    void* signal_out;      // device, n*n complex or null
+    double* power_out;     // device, [2] = {SH power, pump power} or null
+};
+
+}  // namespace shg

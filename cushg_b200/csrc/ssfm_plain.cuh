@@ -1,0 +1,408 @@
+// ssfm_plain.cuh — the fused, persistent SSFM march of a plain (non-thermal) run.
+//
+// One thread-block cluster of C CTAs owns one instance for its whole z-march.  The
+// pump and SH planes never leave on-chip memory between steps: CTA c holds the global
+// rows y ≡ c (mod C) of both fields in shared memory, and every SSFM step
+//
+//     RK4(z) -> FFT2 -> × propagator -> IFFT2 -> RK4(z)        (Solver.h:267-273)
+//
+// runs as seven shared-memory passes with no HBM traffic and no kernel launch:
+//
+//   RA  rows, DFT over n2 (R2 points) + twiddle, fused with the RK4 half-steps
+//   RB  rows, DFT over n1 (16 points)
+//   CA  columns, DFT over n2 + twiddle           (rows of this CTA only)
+//   CB  columns, DFT over n1, propagator, IDFT   (reads / writes the cluster's DSMEM)
+//   CA' columns, conj twiddle + IDFT over n2
+//   RB' rows, IDFT over n1
+//   RA' rows, conj twiddle + IDFT, RK4(z_s), RK4(z_{s+1}), then RA of the next step
+//
+// The transverse transform is a four-step FFT with N = 16 * R2: x = n1 + 16 n2 and
+// frequency k = k2 + R2 k1 stored at position k1 + 16 k2 (digit-reversed); the
+// propagator is applied in that order and the inverse undoes it, so no reordering
+// pass exists.  Rows are XOR-swizzled so every pass is free of bank conflicts.
+//
+// Reference counterparts: Solver::solverRK4 / dAdz / linealCombination / kernelRK4
+// (src/headers/Solver.h:33-113,189-264), Solver::diffraction with cuFFT,
+// kernelComplexProduct and cuFFTscale (Solver.h:17-30,153-186, Efields.h:15-29),
+// the propagators and their fftshift (Efields.h:32-81,122-141), setPump
+// (Efields.h:84-119) and the z-loop of Solver::CWES (Solver.h:276-308).
+#pragma once
+
+#include <cooperative_groups.h>
+
+#include <type_traits>
+
+#include "dft.cuh"
+#include "shg_internal.h"
+
+namespace shg {
+
+namespace cg = cooperative_groups;
+
+template <typename T, int N, int C, int NT>
+struct PlainCfg {
+    static constexpr int R1 = 16;
+    static constexpr int R2 = N / 16;
+    static constexpr int RL = N / C;           // rows per CTA
+    static constexpr int SW = sizeof(T) == 4 ? 16 : 8;  // complex slots per 128 B
+    static constexpr int JA = RL * 16;         // RA jobs: (row, n1)
+    static constexpr int JB = RL * R2;         // RB jobs: (row, k2)
+    static constexpr int JCA = N * (16 / C);   // CA jobs: (column, n1 of this CTA)
+    static constexpr int JCB = N * R2 / C;     // CB jobs: (column, k2)
+    static constexpr int PLANE = RL * N;       // complex elements per field per CTA
+    static_assert(N % 16 == 0 && 16 % C == 0 && RL * C == N, "bad grid / cluster split");
+    // dynamic shared memory: P, S planes, twiddles + 4 propagator vectors (multiplier
+    // tables), 2x6 coefficients, reduction scratch
+    static constexpr size_t smem_bytes = sizeof(cx<T>) * (2 * (size_t)PLANE + 12) + sizeof(mult<T>) * 5 * (size_t)N +
+                                         sizeof(double) * (2 * (NT / 32) + 4);
+};
+
+// physical offset of logical position p of local row lr
+template <int N, int R2, int SW>
+__device__ __forceinline__ int sidx(int lr, int p) {
+    return lr * N + (p ^ (((p >> 4) + lr * R2) & (SW - 1)));
+}
+
+// dA/dz of the coupled equations at one point (Solver.h:57-80):
+//   dP = cP * S * conj(P) - 0.5 αp P,   cP = i κp e^{-iφ}
+//   dS = cS * P^2 - 0.5 (αs + βs 0.5 c ε0 n_s |S|^2) S,   cS = i κs e^{+iφ}
+template <typename T>
+__device__ __forceinline__ void dadz(cx<T> p, cx<T> s, cx<T> cP, cx<T> cS, T hap, T has, T qs, cx<T>& dp,
+                                     cx<T>& ds) {
+    cx<T> sp = mulc<T>(s, p);
+    cx<T> tp = mul<T>(cP, sp);
+    dp = mk<T>(tp.x - hap * p.x, tp.y - hap * p.y);
+    cx<T> pp = mk<T>(p.x * p.x - p.y * p.y, (T)2 * p.x * p.y);
+    cx<T> ts = mul<T>(cS, pp);
+    T g = has + qs * (s.x * s.x + s.y * s.y);
+    ds = mk<T>(ts.x - g * s.x, ts.y - g * s.y);
+}
+
+// One application of the reference's RK4 scheme (Solver.h:231-259): stage inputs
+// A + 0.5 k1, A + 0.5 k2, A + k3 (no dz factor), stage phases at z, z + dz/4 (twice)
+// and z + dz/2; A += (k1 + 2 k2 + 2 k3 + k4) dz / 6.  cf[0..2] = cP of the three
+// phases, cf[3..5] = cS.
+template <typename T>
+__device__ __forceinline__ void rk4_point(cx<T>& P, cx<T>& S, const cx<T>* cf, T hap, T has, T qs, T dz6) {
+    cx<T> p = P, s = S, kp, ks, ap, as;
+    dadz<T>(p, s, cf[0], cf[3], hap, has, qs, kp, ks);
+    ap = kp; as = ks;
+    dadz<T>(mk<T>(p.x + (T)0.5 * kp.x, p.y + (T)0.5 * kp.y), mk<T>(s.x + (T)0.5 * ks.x, s.y + (T)0.5 * ks.y), cf[1],
+            cf[4], hap, has, qs, kp, ks);
+    ap = mk<T>(ap.x + (T)2 * kp.x, ap.y + (T)2 * kp.y);
+    as = mk<T>(as.x + (T)2 * ks.x, as.y + (T)2 * ks.y);
+    dadz<T>(mk<T>(p.x + (T)0.5 * kp.x, p.y + (T)0.5 * kp.y), mk<T>(s.x + (T)0.5 * ks.x, s.y + (T)0.5 * ks.y), cf[1],
+            cf[4], hap, has, qs, kp, ks);
+    ap = mk<T>(ap.x + (T)2 * kp.x, ap.y + (T)2 * kp.y);
+    as = mk<T>(as.x + (T)2 * ks.x, as.y + (T)2 * ks.y);
+    dadz<T>(add<T>(p, kp), add<T>(s, ks), cf[2], cf[5], hap, has, qs, kp, ks);
+    ap = add<T>(ap, kp);
+    as = add<T>(as, ks);
+    P = mk<T>(p.x + ap.x * dz6, p.y + ap.y * dz6);
+    S = mk<T>(s.x + as.x * dz6, s.y + as.y * dz6);
+}
+
+// stage coefficients of the plain dAdz at position z: phases (z + dz*{0, 1/4, 1/2}) Δk,
+// computed in FP64 (Solver.h:68-74 with increment 0.5*{0, 0.5, 1})
+template <typename T>
+__device__ __forceinline__ void stage_coef(const InstDesc& d, double z, int j, cx<T>* cf) {
+    const double inc = j == 0 ? 0.0 : (j == 1 ? 0.25 : 0.5);
+    const double phi = (z + d.dz * inc) * d.dk;
+    double sn, cs;
+    sincos(phi, &sn, &cs);
+    // i κ e^{-iφ} = κ (sin φ, cos φ);  i κ e^{+iφ} = κ (-sin φ, cos φ)
+    cf[j] = mk<T>((T)(d.kap_p * sn), (T)(d.kap_p * cs));
+    cf[3 + j] = mk<T>((T)(-d.kap_s * sn), (T)(d.kap_s * cs));
+}
+
+template <typename T, int N, int C, int NT>
+__global__ void __launch_bounds__(NT, 1) ssfm_plain_kernel(const InstDesc* __restrict__ descs) {
+    using Cfg = PlainCfg<T, N, C, NT>;
+    constexpr int R2 = Cfg::R2, RL = Cfg::RL, SW = Cfg::SW;
+    constexpr int JA = Cfg::JA, JB = Cfg::JB, JCA = Cfg::JCA, JCB = Cfg::JCB;
+    constexpr int CPR = 16 / C;  // column sub-rows per n1 of this CTA
+    using V = cx<T>;
+
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* Ps = reinterpret_cast<V*>(smem_raw);
+    V* Ss = Ps + Cfg::PLANE;
+    using W = mult<T>;
+    V* coef = Ss + Cfg::PLANE;   // [2][6] RK4 stage coefficients
+    W* tw = reinterpret_cast<W*>(coef + 12);  // tw[k*16 + n1] = W_N^{n1 k}, forward sign
+    W* pxp = tw + N;             // pump propagator, x factor, by physical column position
+    W* pxs = pxp + N;            // SH   propagator, x factor
+    W* pyp = pxs + N;            // pump propagator, y factor by frequency, × 1/N^2
+    W* pys = pyp + N;            // SH   propagator, y factor
+    double* red = reinterpret_cast<double*>(pys + N);  // [2*(NT/32)] + [4]
+
+    const int tid = threadIdx.x;
+    const int inst = blockIdx.x / C;
+    const int crank = (C > 1) ? (int)cg::this_cluster().block_rank() : 0;
+    const InstDesc d = descs[inst];
+    const int nsteps = d.nsteps;
+
+    auto cluster_sync = [&]() {
+        if constexpr (C > 1) cg::this_cluster().sync();
+        else __syncthreads();
+    };
+
+    // ---- tables -----------------------------------------------------------------
+    for (int j = tid; j < N; j += NT) {
+        double sn, cs;
+        sincospi(-2.0 * (double)((j & 15) * (j >> 4)) / (double)N, &sn, &cs);
+        tw[j] = make_mult<T>(cs, sn);
+        // x factor at physical column position j: frequency perm(j) = (j>>4) + R2*(j&15)
+        const int fx = (j >> 4) + R2 * (j & 15);
+        const double sx = (double)(fx < N / 2 ? fx : fx - N);
+        const double thxp = -d.dz * (d.a_p * (d.dfx * d.dfx * (sx * sx)) + d.b_p * sx);
+        const double thxs = -d.dz * (d.a_s * (d.dfx * d.dfx * (sx * sx)) + d.b_s * sx);
+        sincos(thxp, &sn, &cs);
+        pxp[j] = make_mult<T>(cs, sn);
+        sincos(thxs, &sn, &cs);
+        pxs[j] = make_mult<T>(cs, sn);
+        // y factor at frequency j, with the 1/(NX*NY) of the inverse FFT folded in
+        const double sy = (double)(j < N / 2 ? j : j - N);
+        const double inv = 1.0 / ((double)N * (double)N);
+        const double thyp = -d.dz * (d.a_p * (d.dfy * d.dfy * (sy * sy)));
+        const double thys = -d.dz * (d.a_s * (d.dfy * d.dfy * (sy * sy)));
+        sincos(thyp, &sn, &cs);
+        pyp[j] = make_mult<T>(cs * inv, sn * inv);
+        sincos(thys, &sn, &cs);
+        pys[j] = make_mult<T>(cs * inv, sn * inv);
+    }
+    if (tid < 3) stage_coef<T>(d, 0.0, tid, coef);
+
+    // ---- initial fields: setPump (Efields.h:84-119), SH = 0 or given ---------------
+    const V* sin_g = reinterpret_cast<const V*>(d.signal_in);
+    for (int e = tid; e < Cfg::PLANE; e += NT) {
+        const int lr = e / N, x = e % N;
+        const int y = crank + C * lr;
+        const double ax = ((double)x - d.ux) * d.dx, ay = ((double)y - d.uy) * d.dy;
+        const double num = -(ax * ax) - (ay * ay);
+        const double dd = d.den_re * d.den_re + d.den_im * d.den_im;
+        const double are = (num * d.den_re) / dd, aim = (-num * d.den_im) / dd;
+        const double ex = exp(are);
+        double sn, cs;
+        sincos(aim, &sn, &cs);
+        const double er = ex * cs, ei = ex * sn;
+        Ps[sidx<N, R2, SW>(lr, x)] = mk<T>((T)(d.amp_re * er - d.amp_im * ei), (T)(d.amp_re * ei + d.amp_im * er));
+        Ss[sidx<N, R2, SW>(lr, x)] = d.has_signal_in ? sin_g[(size_t)y * N + x] : mk<T>((T)0, (T)0);
+    }
+    __syncthreads();
+
+    const T hap = (T)d.hap, has = (T)d.has, qs = (T)d.qs, dz6 = (T)(d.dz / 6.0);
+
+    // nsteps >= 1 (the host rejects nz < 2)
+    // ---- RA: rows, (inverse tail of the previous step), RK4, DFT over n2 -----------
+    // mode 0: first (natural in), 1: middle, 2: last (writes the outputs)
+    auto pass_ra = [&](int mode, const V* cf_prev, const V* cf_next, double& acc_s, double& acc_p) {
+        for (int j = tid; j < JA; j += NT) {
+            const int n1 = j & 15, lr = j >> 4;
+            V vp[R2], vs[R2];
+#pragma unroll
+            for (int k = 0; k < R2; ++k) {
+                const int o = sidx<N, R2, SW>(lr, n1 + 16 * k);
+                vp[k] = Ps[o];
+                vs[k] = Ss[o];
+            }
+            if (mode != 0) {
+#pragma unroll
+                for (int k = 1; k < R2; ++k) {
+                    const W w = tw[k * 16 + n1];
+                    vp[k] = mulwc(vp[k], w);
+                    vs[k] = mulwc(vs[k], w);
+                }
+                Dft<R2, +1, T>::run(vp);
+                Dft<R2, +1, T>::run(vs);
+#pragma unroll
+                for (int k = 0; k < R2; ++k) rk4_point<T>(vp[k], vs[k], cf_prev, hap, has, qs, dz6);
+            }
+            if (mode != 2) {
+#pragma unroll
+                for (int k = 0; k < R2; ++k) rk4_point<T>(vp[k], vs[k], cf_next, hap, has, qs, dz6);
+                Dft<R2, -1, T>::run(vp);
+                Dft<R2, -1, T>::run(vs);
+#pragma unroll
+                for (int k = 0; k < R2; ++k) {
+                    const W w = tw[k * 16 + n1];
+                    const int o = sidx<N, R2, SW>(lr, n1 + 16 * k);
+                    Ps[o] = k ? mulw(vp[k], w) : vp[k];
+                    Ss[o] = k ? mulw(vs[k], w) : vs[k];
+                }
+            } else {
+                const int y = crank + C * lr;
+                V* po = reinterpret_cast<V*>(d.pump_out);
+                V* so = reinterpret_cast<V*>(d.signal_out);
+#pragma unroll
+                for (int k = 0; k < R2; ++k) {
+                    const size_t g = (size_t)y * N + n1 + 16 * k;
+                    if (po) po[g] = vp[k];
+                    if (so) so[g] = vs[k];
+                    acc_s += (double)vs[k].x * (double)vs[k].x + (double)vs[k].y * (double)vs[k].y;
+                    acc_p += (double)vp[k].x * (double)vp[k].x + (double)vp[k].y * (double)vp[k].y;
+                }
+            }
+        }
+    };
+
+    // ---- RB: rows, 16-point DFT over n1 (in place, digit-reversed output) ----------
+    auto pass_rb = [&](auto sign_tag) {
+        constexpr int SG = decltype(sign_tag)::value;
+        for (int j = tid; j < JB; j += NT) {
+            const int k2 = j % R2, lr = j / R2;
+            V u[16], v[16];
+#pragma unroll
+            for (int n = 0; n < 16; ++n) {
+                const int o = sidx<N, R2, SW>(lr, n + 16 * k2);
+                u[n] = Ps[o];
+                v[n] = Ss[o];
+            }
+            Dft<16, SG, T>::run(u);
+            Dft<16, SG, T>::run(v);
+#pragma unroll
+            for (int n = 0; n < 16; ++n) {
+                const int o = sidx<N, R2, SW>(lr, n + 16 * k2);
+                Ps[o] = u[n];
+                Ss[o] = v[n];
+            }
+        }
+    };
+
+    // ---- CA: columns, DFT over n2 on this CTA's rows --------------------------------
+    auto pass_ca = [&](auto sign_tag) {
+        constexpr int SG = decltype(sign_tag)::value;
+        for (int j = tid; j < JCA; j += NT) {
+            const int x = j % N, n1l = j / N;
+            const int n1 = crank + C * n1l;
+            V u[R2], v[R2];
+#pragma unroll
+            for (int k = 0; k < R2; ++k) {
+                const int o = sidx<N, R2, SW>(n1l + CPR * k, x);
+                u[k] = Ps[o];
+                v[k] = Ss[o];
+            }
+            if (SG < 0) {
+                Dft<R2, -1, T>::run(u);
+                Dft<R2, -1, T>::run(v);
+#pragma unroll
+                for (int k = 1; k < R2; ++k) {
+                    const W w = tw[k * 16 + n1];
+                    u[k] = mulw(u[k], w);
+                    v[k] = mulw(v[k], w);
+                }
+            } else {
+#pragma unroll
+                for (int k = 1; k < R2; ++k) {
+                    const W w = tw[k * 16 + n1];
+                    u[k] = mulwc(u[k], w);
+                    v[k] = mulwc(v[k], w);
+                }
+                Dft<R2, +1, T>::run(u);
+                Dft<R2, +1, T>::run(v);
+            }
+#pragma unroll
+            for (int k = 0; k < R2; ++k) {
+                const int o = sidx<N, R2, SW>(n1l + CPR * k, x);
+                Ps[o] = u[k];
+                Ss[o] = v[k];
+            }
+        }
+    };
+
+    // ---- CB: columns, DFT over n1 across the cluster, propagator, IDFT ----------------
+    auto pass_cb = [&]() {
+        V* rP[C];
+        V* rS[C];
+#pragma unroll
+        for (int r = 0; r < C; ++r) {
+            if constexpr (C > 1) {
+                rP[r] = cg::this_cluster().map_shared_rank(Ps, r);
+                rS[r] = cg::this_cluster().map_shared_rank(Ss, r);
+            } else {
+                rP[r] = Ps;
+                rS[r] = Ss;
+            }
+        }
+        for (int j = tid; j < JCB; j += NT) {
+            const int xl = j % (N / C), k2 = j / (N / C);
+            const int x = crank * (N / C) + xl;
+#pragma unroll
+            for (int f = 0; f < 2; ++f) {
+                V* const* R = f ? rS : rP;
+                const W px = f ? pxs[x] : pxp[x];
+                const W* py = f ? pys : pyp;
+                V u[16];
+#pragma unroll
+                for (int n = 0; n < 16; ++n) u[n] = R[n % C][sidx<N, R2, SW>(n / C + CPR * k2, x)];
+                Dft<16, -1, T>::run(u);
+#pragma unroll
+                for (int k1 = 0; k1 < 16; ++k1) u[k1] = mulw(mulw(u[k1], py[k2 + R2 * k1]), px);
+                Dft<16, +1, T>::run(u);
+#pragma unroll
+                for (int n = 0; n < 16; ++n) R[n % C][sidx<N, R2, SW>(n / C + CPR * k2, x)] = u[n];
+            }
+        }
+    };
+
+    using Neg = std::integral_constant<int, -1>;
+    using Pos = std::integral_constant<int, +1>;
+
+    double acc_s = 0.0, acc_p = 0.0;
+    pass_ra(0, coef, coef, acc_s, acc_p);
+    __syncthreads();
+
+    double z = 0.0;
+    for (int s = 0; s < nsteps; ++s) {
+        V* cf_cur = coef + 6 * (s & 1);
+        V* cf_nxt = coef + 6 * ((s + 1) & 1);
+        pass_rb(Neg{});
+        __syncthreads();
+        pass_ca(Neg{});
+        cluster_sync();
+        if (tid < 3 && s + 1 < nsteps) stage_coef<T>(d, z + d.dz, tid, cf_nxt);
+        pass_cb();
+        cluster_sync();
+        pass_ca(Pos{});
+        __syncthreads();
+        pass_rb(Pos{});
+        __syncthreads();
+        pass_ra(s + 1 < nsteps ? 1 : 2, cf_cur, cf_nxt, acc_s, acc_p);
+        __syncthreads();
+        z += d.dz;
+    }
+
+    // ---- SH and pump power: deterministic block + cluster reduction --------------------
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        acc_s += __shfl_down_sync(0xffffffffu, acc_s, o);
+        acc_p += __shfl_down_sync(0xffffffffu, acc_p, o);
+    }
+    const int warp = tid >> 5, lane = tid & 31;
+    if (lane == 0) {
+        red[2 * warp] = acc_s;
+        red[2 * warp + 1] = acc_p;
+    }
+    __syncthreads();
+    double* part = red + 2 * (NT / 32);
+    if (tid == 0) {
+        double a = 0.0, b = 0.0;
+        for (int w = 0; w < NT / 32; ++w) { a += red[2 * w]; b += red[2 * w + 1]; }
+        part[0] = a;
+        part[1] = b;
+    }
+    cluster_sync();
+    if (crank == 0 && tid == 0 && d.power_out) {
+        double a = 0.0, b = 0.0;
+        for (int r = 0; r < C; ++r) {
+            const double* pr = part;
+            if constexpr (C > 1) pr = cg::this_cluster().map_shared_rank(part, r);
+            a += pr[0];
+            b += pr[1];
+        }
+        d.power_out[0] = a * d.pw_s;
+        d.power_out[1] = b * d.pw_p;
+    }
+    cluster_sync();
+}
+
+}  // namespace shg

@@ -1,0 +1,151 @@
+"""Python mirror of the reference's solver interface over the C ABI of libshg_b200.so.
+
+The reference runs one parameter point per process: ``Solver::run(Power, waist, focalpoint,
+Temp, T_inf, Tpeltier, save_only_last, save_temperature)`` (src/headers/Solver.h:311) with
+grid and crystal constants compiled in, writing ``Pump_out`` / ``Signal_out`` .dat files.
+Here :func:`run` takes the same arguments plus a runtime :class:`ShgParams`, and returns the
+fields as arrays; :func:`solve_batch` runs many points in one persistent launch.
+
+Everything goes through ``libshg_b200.so`` (include/shg.h).  There is no CPU path: if the
+library or a CUDA device is missing, the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from .params import ShgParams, ShgStats, Result, SHG_OK
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libshg_b200.so")
+
+# every entry point declared in include/shg.h
+EXPORTS = (
+    "shg_default_params", "shg_check_params", "shg_steps", "shg_solve", "shg_solve_device",
+    "shg_solve_batch_device", "shg_last_error", "shg_status_string", "shg_version",
+)
+
+
+class ShgError(RuntimeError):
+    """A non-zero shg_status from the library."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"shg status {status}: {message}")
+        self.status = status
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load libshg_b200.so (built by ``python -m cushg_b200.build``)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m cushg_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        P = ctypes.POINTER(ShgParams)
+        vp = ctypes.c_void_p
+        L.shg_default_params.argtypes = [P]
+        L.shg_default_params.restype = None
+        L.shg_check_params.argtypes = [P]
+        L.shg_check_params.restype = ctypes.c_int
+        L.shg_steps.argtypes = [P]
+        L.shg_steps.restype = ctypes.c_int32
+        L.shg_solve.argtypes = [P, vp, vp, vp, vp, ctypes.POINTER(ShgStats)]
+        L.shg_solve.restype = ctypes.c_int
+        L.shg_solve_device.argtypes = [P, vp, vp, vp, vp, ctypes.POINTER(ShgStats), vp]
+        L.shg_solve_device.restype = ctypes.c_int
+        L.shg_solve_batch_device.argtypes = [P, ctypes.c_int32, ctypes.POINTER(vp), ctypes.POINTER(vp),
+                                             ctypes.POINTER(ctypes.c_double), vp]
+        L.shg_solve_batch_device.restype = ctypes.c_int
+        L.shg_last_error.restype = ctypes.c_char_p
+        L.shg_status_string.argtypes = [ctypes.c_int32]
+        L.shg_status_string.restype = ctypes.c_char_p
+        L.shg_version.restype = ctypes.c_char_p
+        _lib = L
+    return _lib
+
+
+def _check(rc: int) -> None:
+    if rc != SHG_OK:
+        raise ShgError(rc, lib().shg_last_error().decode())
+
+
+def default_params() -> ShgParams:
+    p = ShgParams()
+    lib().shg_default_params(ctypes.byref(p))
+    return p
+
+
+def check_params(p: ShgParams) -> int:
+    return int(lib().shg_check_params(ctypes.byref(p)))
+
+
+def steps(p: ShgParams) -> int:
+    return int(lib().shg_steps(ctypes.byref(p)))
+
+
+def last_error() -> str:
+    return lib().shg_last_error().decode()
+
+
+def _ptr(a):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+def solve(p: ShgParams, signal_in: np.ndarray | None = None, want_temperature: bool = False) -> Result:
+    """One instance with host buffers (shg_solve)."""
+    cdt = p.complex_dtype
+    pump = np.empty((p.ny, p.nx), dtype=cdt)
+    sig = np.empty((p.ny, p.nx), dtype=cdt)
+    T = np.empty((p.nz, p.ny, p.nx), dtype=p.real_dtype) if (want_temperature and p.thermal) else None
+    sin = None if signal_in is None else np.ascontiguousarray(np.asarray(signal_in, dtype=cdt).reshape(p.ny, p.nx))
+    st = ShgStats()
+    _check(lib().shg_solve(ctypes.byref(p), _ptr(sin), _ptr(pump), _ptr(sig), _ptr(T), ctypes.byref(st)))
+    return Result(pump=pump, signal=sig, stats=st, temperature=T)
+
+
+def run(power: float, waist: float, focalpoint: float, temp: float, t_inf: float, t_peltier: float,
+        params: ShgParams | None = None, save_temperature: bool = False) -> Result:
+    """``Solver::run`` (src/headers/Solver.h:311) with the crystal / grid of ``params``
+    (default: the reference's compile-time configuration)."""
+    p = (params or default_params()).copy()
+    p.power, p.waist, p.focus = power, waist, focalpoint
+    p.temp, p.t_inf, p.t_peltier = temp, t_inf, t_peltier
+    return solve(p, want_temperature=save_temperature)
+
+
+def solve_device(p: ShgParams, pump_out, signal_out, signal_in=None, temperature_out=None, stream=None,
+                 stats: bool = True) -> ShgStats | None:
+    """One instance on device tensors (torch, complex64/complex128, contiguous)."""
+    st = ShgStats() if stats else None
+
+    def dp(t):
+        return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+    s = None if stream is None else ctypes.c_void_p(stream)
+    _check(lib().shg_solve_device(ctypes.byref(p), dp(signal_in), dp(pump_out), dp(signal_out),
+                                  dp(temperature_out), ctypes.byref(st) if st is not None else None, s))
+    return st
+
+
+def solve_batch_device(ps: list[ShgParams], pump_outs=None, signal_outs=None, stream=None,
+                       want_power: bool = True) -> np.ndarray | None:
+    """Batch of plain instances (shg_solve_batch_device); outputs are device tensors."""
+    n = len(ps)
+    arr = (ShgParams * n)(*ps)
+    vp = ctypes.c_void_p
+
+    def ptrs(ts):
+        if ts is None:
+            return None
+        return (vp * n)(*[vp(t.data_ptr()) if t is not None else None for t in ts])
+
+    power = np.zeros(n, dtype=np.float64) if want_power else None
+    pp = power.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if power is not None else None
+    s = None if stream is None else vp(stream)
+    _check(lib().shg_solve_batch_device(arr, n, ptrs(pump_outs), ptrs(signal_outs), pp, s))
+    return power

@@ -32,6 +32,12 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#if defined(__GNUC__)
+#define SHG_API __attribute__((visibility("default")))
+#else
+#define SHG_API
+#endif
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -111,15 +117,15 @@ typedef struct shg_stats {
 
 /* Fill *p with the reference's compile-time defaults (cuSHG.cu:11-13, Crystal.h:19-52,
  * cuSHG.cu:46-53 with argv = 30 W, 29 µm, 55.66 °C from cuSHG.sh:43-45). */
-void shg_default_params(shg_params* p);
+SHG_API void shg_default_params(shg_params* p);
 
 /* Validate a parameter set; SHG_OK or SHG_ERR_INVALID / SHG_ERR_UNSUPPORTED. */
-shg_status shg_check_params(const shg_params* p);
+SHG_API shg_status shg_check_params(const shg_params* p);
 
 /* Number of SSFM steps a plain optical pass marches for these parameters: the
  * reference records the fields before its last step (Solver.h:283-286), so a
  * plain pass marches nz-1 steps and a thermal pass nz (its last step feeds Q). */
-int32_t shg_steps(const shg_params* p);
+SHG_API int32_t shg_steps(const shg_params* p);
 
 /*
  * Solve one instance.  Replaces Solver::run (Solver.h:311-390) with
@@ -130,13 +136,13 @@ int32_t shg_steps(const shg_params* p);
  *   temperature_out        nx*ny*nz reals (Tfinal), thermal runs only, may be NULL.
  *   stats                  may be NULL.
  */
-shg_status shg_solve(const shg_params* p, const void* signal_in, void* pump_out,
+SHG_API shg_status shg_solve(const shg_params* p, const void* signal_in, void* pump_out,
                      void* signal_out, void* temperature_out, shg_stats* stats);
 
 /* The same with device buffers on a caller stream (a cudaStream_t, NULL = legacy
  * default stream).  Plain runs are asynchronous; thermal runs synchronise at each
  * Jacobi convergence check.  stats, if given, is filled after a synchronise. */
-shg_status shg_solve_device(const shg_params* p, const void* signal_in_dev,
+SHG_API shg_status shg_solve_device(const shg_params* p, const void* signal_in_dev,
                             void* pump_out_dev, void* signal_out_dev,
                             void* temperature_out_dev, shg_stats* stats, void* stream);
 
@@ -148,16 +154,16 @@ shg_status shg_solve_device(const shg_params* p, const void* signal_in_dev,
  * pump_out[i] / signal_out[i]: device buffers (nx_i*ny_i complex) or NULL entries.
  * sh_power_out: host array of `count` doubles or NULL.
  */
-shg_status shg_solve_batch_device(const shg_params* params, int32_t count,
+SHG_API shg_status shg_solve_batch_device(const shg_params* params, int32_t count,
                                   void* const* pump_out_dev, void* const* signal_out_dev,
                                   double* sh_power_out, void* stream);
 
 /* Message of the last failing call on this thread ("" if none). */
-const char* shg_last_error(void);
-const char* shg_status_string(int32_t status);
+SHG_API const char* shg_last_error(void);
+SHG_API const char* shg_status_string(int32_t status);
 
 /* Library version string. */
-const char* shg_version(void);
+SHG_API const char* shg_version(void);
 
 #ifdef __cplusplus
 }

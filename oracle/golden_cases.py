@@ -56,6 +56,23 @@ def _thermal_small_oven() -> P.ShgParams:
     return p
 
 
+def _thermal_n32() -> P.ShgParams:
+    # 32 x 32 x 16 thermal case on a grid the fused kernels support (side a multiple of 16)
+    p = P.workload(32, 16, 5000.0, 25.0, 28.0, 2500.0, 31.0, precision=64, thermal=1)
+    p.alpha_p, p.alpha_s, p.beta_s = 2e-5, 1e-4, 1e-3
+    p.max_outer = 3
+    p.check_every = 5000
+    p.conv_rule = P.SHG_CONV_REFERENCE
+    p.jacobi_tol = 0.0
+    return p
+
+
+def _thermal_n32_oven() -> P.ShgParams:
+    p = _thermal_n32()
+    p.boundary = P.SHG_BOUNDARY_OVEN_SURROUNDED
+    return p
+
+
 def _plain_c1_f32() -> P.ShgParams:
     return P.config_plain_64().replace(precision=32)
 
@@ -67,6 +84,8 @@ CASES = {
     "thermal64_small": {"precision": 64, "params": _d(_thermal_small())},
     "thermal64_small_oven": {"precision": 64, "params": _d(_thermal_small_oven()), "oven_surrounded": True},
     "plain32_c1": {"precision": 32, "params": _d(_plain_c1_f32())},
+    "thermal64_n32": {"precision": 64, "params": _d(_thermal_n32())},
+    "thermal64_n32_oven": {"precision": 64, "params": _d(_thermal_n32_oven()), "oven_surrounded": True},
 }
 
 

@@ -1,0 +1,76 @@
+"""C-ABI checks that need no GPU: the library loads, exports every entry point that
+include/shg.h declares, and validates parameters like the reference's constraints."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from conftest import ROOT
+from cushg_b200 import params as P
+from cushg_b200 import shg
+
+
+def declared_entry_points():
+    text = open(os.path.join(ROOT, "include", "shg.h")).read()
+    return sorted(set(re.findall(r"SHG_API\s+[\w\s\*]+?\b(shg_\w+)\s*\(", text)))
+
+
+def test_header_and_binding_agree():
+    assert sorted(shg.EXPORTS) == declared_entry_points()
+
+
+def test_library_exports_every_declared_symbol():
+    L = shg.lib()
+    for name in declared_entry_points():
+        assert hasattr(L, name), name
+
+
+def test_default_params_are_the_reference_configuration():
+    d = shg.default_params()
+    r = P.reference_defaults()
+    assert d.as_dict() == r.as_dict()
+    assert (d.nx, d.ny, d.nz) == (128, 128, 100)          # src/cuSHG.cu:11-13
+    assert (d.lx, d.ly, d.lz) == (2000.0, 1000.0, 30000.0)  # Crystal.h:31-33
+    assert d.focus == 0.5 * d.lz                            # cuSHG.cu:48
+
+
+def test_steps_follow_the_output_slice_rule():
+    p = P.config_plain_64()
+    assert shg.steps(p) == p.nz - 1
+    assert shg.steps(p.replace(thermal=1)) == p.nz
+
+
+@pytest.mark.parametrize("field,value", [
+    ("nx", 63), ("nz", 1), ("precision", 16), ("waist", 0.0), ("lx", -1.0), ("alpha_p", -1e-6),
+    ("power", float("nan")), ("lambda_p", 0.0),
+])
+def test_invalid_params_are_rejected(field, value):
+    p = P.config_plain_64().replace(**{field: value})
+    assert shg.check_params(p) == P.SHG_ERR_INVALID
+    assert shg.last_error() != ""
+
+
+def test_unbuilt_grid_is_unsupported():
+    p = P.config_plain_64().replace(nx=100, ny=100)
+    assert shg.check_params(p) == P.SHG_ERR_UNSUPPORTED
+
+
+def test_valid_params_pass():
+    for p in [P.config_plain_64(), P.config_thermal_128(), *P.config_sweep(16)]:
+        assert shg.check_params(p) == P.SHG_OK, shg.last_error()
+
+
+def test_solve_without_device_fails_loudly():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(shg.ShgError) as e:
+        shg.solve(P.config_plain_64())
+    assert e.value.status == P.SHG_ERR_NO_DEVICE
+
+
+def test_status_strings():
+    L = shg.lib()
+    assert L.shg_status_string(0) == b"ok"
+    assert L.shg_version().startswith(b"libshg_b200")

@@ -1,0 +1,122 @@
+"""Parity of the fused plain SSFM march (libshg_b200, called through the C ABI) with the
+reference's own FP64 outputs (tests/golden/) and with the CPU oracle.
+
+Tolerances: plain FP64 output fields relative L2 <= 1e-10 and SH power relative error
+<= 1e-12; FP32 SH power relative error against the FP64 oracle <= 1e-5 (fields 1e-4).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from cushg_b200 import params as P
+from cushg_b200 import shg
+from oracle import golden_cases as G
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+PLAIN_FP64_GOLDEN = [n for n, c in G.CASES.items() if c["precision"] == 64 and not c["params"]["thermal"]]
+SIDES = [32, 48, 64, 96, 128, 192, 256]
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.complex128) - b) / np.linalg.norm(b))
+
+
+@pytest.mark.parametrize("name", PLAIN_FP64_GOLDEN)
+def test_plain_fp64_matches_reference(name):
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    p = G.params_of(name)
+    r = shg.solve(p)
+    assert rel_l2(r.pump, z["pump"]) <= 1e-10
+    assert rel_l2(r.signal, z["signal"]) <= 1e-10
+    ref_power = P.sh_power_of(p, z["signal"])
+    assert abs(r.sh_power - ref_power) / ref_power <= 1e-12
+    assert r.stats.steps == p.nz - 1
+
+
+def small_case(n, precision=64, nz=12, seed=0):
+    rng = np.random.default_rng(seed + n)
+    waist = float(rng.uniform(15, 40))
+    lz = float(rng.choice([4000.0, 8000.0]))
+    p = P.workload(n, nz, lz, float(rng.uniform(2, 30)), waist, float(rng.uniform(0, lz)),
+                   float(rng.uniform(25, 45)), precision=precision)
+    p.rho_p = float(rng.uniform(0, 0.01))
+    p.rho_s = float(rng.uniform(0, 0.01))
+    p.ly = p.lx * float(rng.uniform(0.8, 1.2))
+    return p
+
+
+@pytest.mark.parametrize("n", SIDES)
+def test_plain_fp64_every_grid_side_matches_oracle(n):
+    p = small_case(n)
+    r = shg.solve(p)
+    rc, pump, sig, st, _ = O.solve(p)
+    assert rc == 0
+    assert rel_l2(r.pump, pump) <= 1e-10
+    assert rel_l2(r.signal, sig) <= 1e-10
+    assert abs(r.sh_power - st.sh_power) / st.sh_power <= 1e-12
+
+
+def test_plain_fp64_given_signal_in():
+    p = small_case(64, nz=8)
+    rng = np.random.default_rng(5)
+    s0 = (rng.standard_normal((64, 64)) + 1j * rng.standard_normal((64, 64))) * 1e-3
+    r = shg.solve(p, signal_in=s0)
+    rc, pump, sig, st, _ = O.solve(p, signal_in=s0)
+    assert rel_l2(r.signal, sig) <= 1e-10
+    assert rel_l2(r.pump, pump) <= 1e-10
+
+
+@pytest.mark.parametrize("n", SIDES)
+def test_plain_fp32_error_against_fp64_oracle(n):
+    p64 = small_case(n, nz=40)
+    rc, pump, sig, st, _ = O.solve(p64)
+    r = shg.solve(p64.replace(precision=32))
+    assert r.pump.dtype == np.complex64
+    assert rel_l2(r.signal, sig) <= 1e-4
+    assert rel_l2(r.pump, pump) <= 1e-5
+    assert abs(r.sh_power - st.sh_power) / st.sh_power <= 1e-5
+
+
+def test_c1_fp32_against_reference_fp64():
+    z = np.load(os.path.join(GOLDEN, "plain64_c1.npz"))
+    p = G.params_of("plain64_c1").replace(precision=32)
+    r = shg.solve(p)
+    ref_power = P.sh_power_of(p, z["signal"])
+    assert abs(r.sh_power - ref_power) / ref_power <= 1e-5
+    assert rel_l2(r.signal, z["signal"]) <= 1e-4
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_batch_equals_single_runs(precision):
+    import torch
+    ps = [small_case(n, precision=precision, nz=6 + i, seed=i) for i, n in enumerate([64, 128, 64, 256, 96, 192, 32, 128])]
+    dt = torch.complex128 if precision == 64 else torch.complex64
+    pumps = [torch.empty((p.ny, p.nx), dtype=dt, device="cuda") for p in ps]
+    sigs = [torch.empty((p.ny, p.nx), dtype=dt, device="cuda") for p in ps]
+    power = shg.solve_batch_device(ps, pumps, sigs)
+    torch.cuda.synchronize()
+    for i, p in enumerate(ps):
+        r = shg.solve(p)
+        assert np.array_equal(sigs[i].cpu().numpy(), r.signal)
+        assert np.array_equal(pumps[i].cpu().numpy(), r.pump)
+        assert power[i] == r.sh_power
+
+
+def test_device_entry_point_on_torch_stream():
+    import torch
+    p = small_case(128, nz=10)
+    pump = torch.empty((128, 128), dtype=torch.complex128, device="cuda")
+    sig = torch.empty_like(pump)
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        st = shg.solve_device(p, pump, sig, stream=s.cuda_stream)
+    s.synchronize()
+    r = shg.solve(p)
+    assert np.array_equal(sig.cpu().numpy(), r.signal)
+    assert st.sh_power == r.sh_power
+    assert st.device_ms > 0

@@ -24,7 +24,8 @@ LIB_PATH = os.path.join(PKG, "libshg_b200.so")
 # every entry point declared in include/shg.h
 EXPORTS = (
     "shg_default_params", "shg_check_params", "shg_steps", "shg_solve", "shg_solve_device",
-    "shg_solve_batch_device", "shg_last_error", "shg_status_string", "shg_version",
+    "shg_solve_batch_device", "shg_solve_batch_device_noalloc", "shg_last_error", "shg_status_string",
+    "shg_version",
 )
 
 
@@ -61,6 +62,8 @@ def lib() -> ctypes.CDLL:
         L.shg_solve_batch_device.argtypes = [P, ctypes.c_int32, ctypes.POINTER(vp), ctypes.POINTER(vp),
                                              ctypes.POINTER(ctypes.c_double), vp]
         L.shg_solve_batch_device.restype = ctypes.c_int
+        L.shg_solve_batch_device_noalloc.argtypes = L.shg_solve_batch_device.argtypes
+        L.shg_solve_batch_device_noalloc.restype = ctypes.c_int
         L.shg_last_error.restype = ctypes.c_char_p
         L.shg_status_string.argtypes = [ctypes.c_int32]
         L.shg_status_string.restype = ctypes.c_char_p
@@ -148,4 +151,29 @@ def solve_batch_device(ps: list[ShgParams], pump_outs=None, signal_outs=None, st
     pp = power.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if power is not None else None
     s = None if stream is None else vp(stream)
     _check(lib().shg_solve_batch_device(arr, n, ptrs(pump_outs), ptrs(signal_outs), pp, s))
+    return power
+
+
+NOALLOC_MAX_INSTANCES = 64
+
+
+def solve_batch_device_noalloc(ps: list[ShgParams], pump_outs=None, signal_outs=None, stream=None,
+                               want_power: bool = True) -> np.ndarray | None:
+    """shg_solve_batch_device_noalloc: the batched march with no device allocation, for
+    callers that cannot allocate while they run.  Its scratch is a fixed array inside the
+    library shared by all calls: at most 64 instances per call, and calls that overlap on the
+    GPU race.  Outputs are device tensors."""
+    n = len(ps)
+    arr = (ShgParams * n)(*ps)
+    vp = ctypes.c_void_p
+
+    def ptrs(ts):
+        if ts is None:
+            return None
+        return (vp * n)(*[vp(t.data_ptr()) if t is not None else None for t in ts])
+
+    power = np.zeros(n, dtype=np.float64) if want_power else None
+    pp = power.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if power is not None else None
+    s = None if stream is None else vp(stream)
+    _check(lib().shg_solve_batch_device_noalloc(arr, n, ptrs(pump_outs), ptrs(signal_outs), pp, s))
     return power

@@ -158,6 +158,22 @@ SHG_API shg_status shg_solve_batch_device(const shg_params* params, int32_t coun
                                   void* const* pump_out_dev, void* const* signal_out_dev,
                                   double* sh_power_out, void* stream);
 
+/*
+ * The batched plain march of shg_solve_batch_device without any device allocation.  This
+ * entry point has no counterpart in the reference.  It is for callers that cannot allocate
+ * device memory while they run (hosts that give all free memory to their own allocator,
+ * latency-bound loops where an allocation may block or synchronise, plugin hosts that forbid
+ * it): its scratch (instance descriptors, power slots) is a fixed ~16 KB __device__ array of
+ * the library, held by every GPU that loads it until exit.  Limit: count <= 64 instances
+ * (larger counts return SHG_ERR_INVALID).  The first call on a device looks up that array's
+ * address and should come before any stream capture.  Calls share the array: calls that
+ * overlap on the GPU (other streams, other threads) race and must be serialised.
+ * Arguments as shg_solve_batch_device; sh_power_out (host, may be NULL) synchronises.
+ */
+SHG_API shg_status shg_solve_batch_device_noalloc(const shg_params* params, int32_t count,
+                                                  void* const* pump_out_dev, void* const* signal_out_dev,
+                                                  double* sh_power_out, void* stream);
+
 /* Message of the last failing call on this thread ("" if none). */
 SHG_API const char* shg_last_error(void);
 SHG_API const char* shg_status_string(int32_t status);

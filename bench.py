@@ -55,6 +55,17 @@ def algorithmic_flops(ps) -> float:
     return float(sum(p.nx * p.ny * (p.nz - 1) * flops_per_point_step(p.nx) for p in ps))
 
 
+def workload_params(args, rank: int):
+    """The sweep (default) or, with --class-side, `--class-count` copies of one grid-size class
+    (a small case for profiling one kernel variant)."""
+    if args.class_side:
+        base = P.config_sweep(256, seed=rank, precision=args.precision)
+        pick = [p for p in base if p.nx == args.class_side] or [P.workload(args.class_side, 100, 20000.0, 20.0, 30.0,
+                                                                             10000.0, 40.0, precision=args.precision)]
+        return [pick[i % len(pick)].replace(nz=args.class_nz) for i in range(args.class_count)]
+    return P.config_sweep(256, seed=rank, precision=args.precision)
+
+
 def sample_stride(ps, count: int):
     step = max(1, len(ps) // count)
     return ps[::step][:count]
@@ -124,7 +135,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
 
-    ps = P.config_sweep(256, seed=rank, precision=args.precision)
+    ps = workload_params(args, rank)
     cdt = torch.complex64 if args.precision == 32 else torch.complex128
     pumps = [torch.empty((p.ny, p.nx), dtype=cdt, device=dev) for p in ps]
     sigs = [torch.empty((p.ny, p.nx), dtype=cdt, device=dev) for p in ps]
@@ -208,7 +219,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
 
     # accuracy of this precision against the FP64 path on the same sweep
     err = None
-    if args.precision == 32:
+    if args.precision == 32 and not args.class_side:
         ps64 = [p.replace(precision=64) for p in ps]
         p32 = shg.solve_batch_device(ps, None, None, stream=sptr)
         p64 = shg.solve_batch_device(ps64, None, None, stream=sptr)
@@ -247,6 +258,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     }
     if err is not None:
         out["fp32_error_vs_fp64"] = err
+    if args.class_side:
+        out["config"]["workload"] = f"{len(ps)} instances of {args.class_side}x{args.class_side}, nz = {args.class_nz}"
     if not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(ps, args.precision)
     return out
@@ -310,6 +323,9 @@ def main() -> int:
     ap.add_argument("--precision", type=int, default=32, choices=[32, 64])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--class-side", type=int, default=0, help="profile case: one grid-size class only")
+    ap.add_argument("--class-count", type=int, default=18)
+    ap.add_argument("--class-nz", type=int, default=24)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank = int(os.environ.get("RANK", "0"))

@@ -39,23 +39,40 @@ static cudaError_t launch_plain(const InstDesc* descs, int count, cudaStream_t s
 #define SHG_PLAIN(T, PREC, N, C, NT) \
     {PREC, N, C, NT, PlainCfg<T, N, C, NT>::smem_bytes, &launch_plain<T, N, C, NT>}
 
+// Threads per CTA of each variant (tuning knobs, overridable at build time).
+#ifndef SHG_NT_F32_SMALL
+#define SHG_NT_F32_SMALL 512
+#endif
+#ifndef SHG_NT_F32_128
+#define SHG_NT_F32_128 512
+#endif
+#ifndef SHG_NT_F32_192
+#define SHG_NT_F32_192 384
+#endif
+#ifndef SHG_NT_F32_256
+#define SHG_NT_F32_256 256
+#endif
+#ifndef SHG_NT_F64
+#define SHG_NT_F64 256
+#endif
+
 // (precision, grid side) -> cluster size and threads per CTA.  The cluster size keeps
 // both planes of one instance in at most ~150 KB of shared memory per CTA.
 static const PlainVariant kPlainVariants[] = {
     SHG_PLAIN(float, 32, 32, 1, 128),
     SHG_PLAIN(float, 32, 48, 1, 192),
-    SHG_PLAIN(float, 32, 64, 1, 256),
+    SHG_PLAIN(float, 32, 64, 1, SHG_NT_F32_SMALL),
     SHG_PLAIN(float, 32, 96, 1, 192),
-    SHG_PLAIN(float, 32, 128, 2, 256),
-    SHG_PLAIN(float, 32, 192, 4, 192),
-    SHG_PLAIN(float, 32, 256, 8, 256),
+    SHG_PLAIN(float, 32, 128, 2, SHG_NT_F32_128),
+    SHG_PLAIN(float, 32, 192, 4, SHG_NT_F32_192),
+    SHG_PLAIN(float, 32, 256, 8, SHG_NT_F32_256),
     SHG_PLAIN(double, 64, 32, 1, 128),
     SHG_PLAIN(double, 64, 48, 1, 192),
-    SHG_PLAIN(double, 64, 64, 1, 256),
+    SHG_PLAIN(double, 64, 64, 1, SHG_NT_F64),
     SHG_PLAIN(double, 64, 96, 2, 192),
-    SHG_PLAIN(double, 64, 128, 4, 256),
+    SHG_PLAIN(double, 64, 128, 4, SHG_NT_F64),
     SHG_PLAIN(double, 64, 192, 8, 192),
-    SHG_PLAIN(double, 64, 256, 16, 256),
+    SHG_PLAIN(double, 64, 256, 16, SHG_NT_F64),
 };
 
 const PlainVariant* find_plain_variant(int precision, int n) {

@@ -30,7 +30,6 @@
 
 #include <cooperative_groups.h>
 
-#include <type_traits>
 
 #include "dft.cuh"
 #include "shg_internal.h"
@@ -193,118 +192,115 @@ __global__ void __launch_bounds__(NT, 1) ssfm_plain_kernel(const InstDesc* __res
     const T hap = (T)d.hap, has = (T)d.has, qs = (T)d.qs, dz6 = (T)(d.dz / 6.0);
 
     // nsteps >= 1 (the host rejects nz < 2)
-    // ---- RA: rows, (inverse tail of the previous step), RK4, DFT over n2 -----------
-    // mode 0: first (natural in), 1: middle, 2: last (writes the outputs)
+    //
+    // Code size matters more than instruction count here: the step loop cycles through
+    // every pass, so each pass keeps a single copy of its transform (the inverse is computed
+    // as conj(DFT(conj(x))) with the forward body) and the two fields go through it in a
+    // rolled loop.  Forward R2 stage: DFT then twiddle W_N^{n1 k}; inverse: conj twiddle then
+    // IDFT, i.e. conj(DFT(conj(x) W)).
+    auto cj = [](V a) { return mk<T>(a.x, -a.y); };
+
+    // ---- RA: rows, R2-point stage of (row lr, n1) and the pointwise RK4 half-steps -----
+    // mode 0: first (natural order in: RK4(z_0), forward), 1: middle (inverse, RK4(z_s),
+    // RK4(z_{s+1}), forward), 2: last (inverse, RK4(z_s), outputs)
     auto pass_ra = [&](int mode, const V* cf_prev, const V* cf_next, double& acc_s, double& acc_p) {
         for (int j = tid; j < JA; j += NT) {
             const int n1 = j & 15, lr = j >> 4;
-            V vp[R2], vs[R2];
-#pragma unroll
-            for (int k = 0; k < R2; ++k) {
-                const int o = sidx<N, R2, SW>(lr, n1 + 16 * k);
-                vp[k] = Ps[o];
-                vs[k] = Ss[o];
-            }
-            if (mode != 0) {
-#pragma unroll
-                for (int k = 1; k < R2; ++k) {
-                    const W w = tw[k * 16 + n1];
-                    vp[k] = mulwc(vp[k], w);
-                    vs[k] = mulwc(vs[k], w);
+#pragma unroll 1
+            for (int ph = 0; ph < 5; ++ph) {
+                if (ph == 2) {
+                    // pointwise: the two RK4 applications around the step boundary
+                    const int h0 = mode == 0 ? 1 : 0, h1 = mode == 2 ? 1 : 2;
+#pragma unroll 1
+                    for (int k = 0; k < R2; ++k) {
+                        const int o = sidx<N, R2, SW>(lr, n1 + 16 * k);
+                        V p = Ps[o], q = Ss[o];
+#pragma unroll 1
+                        for (int h = h0; h < h1; ++h) rk4_point<T>(p, q, h ? cf_next : cf_prev, hap, has, qs, dz6);
+                        if (mode == 2) {
+                            const size_t g = (size_t)(crank + C * lr) * N + n1 + 16 * k;
+                            if (d.pump_out) reinterpret_cast<V*>(d.pump_out)[g] = p;
+                            if (d.signal_out) reinterpret_cast<V*>(d.signal_out)[g] = q;
+                            acc_s += (double)q.x * (double)q.x + (double)q.y * (double)q.y;
+                            acc_p += (double)p.x * (double)p.x + (double)p.y * (double)p.y;
+                        } else {
+                            Ps[o] = p;
+                            Ss[o] = q;
+                        }
+                    }
+                    continue;
                 }
-                Dft<R2, +1, T>::run(vp);
-                Dft<R2, +1, T>::run(vs);
+                const bool inv = ph < 2;
+                if ((inv && mode == 0) || (!inv && mode == 2)) continue;
+                V* F = (ph == 1 || ph == 3) ? Ss : Ps;
+                V v[R2];
 #pragma unroll
-                for (int k = 0; k < R2; ++k) rk4_point<T>(vp[k], vs[k], cf_prev, hap, has, qs, dz6);
-            }
-            if (mode != 2) {
+                for (int k = 0; k < R2; ++k) v[k] = F[sidx<N, R2, SW>(lr, n1 + 16 * k)];
+                if (inv) {
+                    v[0] = cj(v[0]);
 #pragma unroll
-                for (int k = 0; k < R2; ++k) rk4_point<T>(vp[k], vs[k], cf_next, hap, has, qs, dz6);
-                Dft<R2, -1, T>::run(vp);
-                Dft<R2, -1, T>::run(vs);
-#pragma unroll
-                for (int k = 0; k < R2; ++k) {
-                    const W w = tw[k * 16 + n1];
-                    const int o = sidx<N, R2, SW>(lr, n1 + 16 * k);
-                    Ps[o] = k ? mulw(vp[k], w) : vp[k];
-                    Ss[o] = k ? mulw(vs[k], w) : vs[k];
+                    for (int k = 1; k < R2; ++k) v[k] = mulw(cj(v[k]), tw[k * 16 + n1]);
                 }
-            } else {
-                const int y = crank + C * lr;
-                V* po = reinterpret_cast<V*>(d.pump_out);
-                V* so = reinterpret_cast<V*>(d.signal_out);
+                Dft<R2, -1, T>::run(v);
+                if (inv) {
 #pragma unroll
-                for (int k = 0; k < R2; ++k) {
-                    const size_t g = (size_t)y * N + n1 + 16 * k;
-                    if (po) po[g] = vp[k];
-                    if (so) so[g] = vs[k];
-                    acc_s += (double)vs[k].x * (double)vs[k].x + (double)vs[k].y * (double)vs[k].y;
-                    acc_p += (double)vp[k].x * (double)vp[k].x + (double)vp[k].y * (double)vp[k].y;
+                    for (int k = 0; k < R2; ++k) v[k] = cj(v[k]);
+                } else {
+#pragma unroll
+                    for (int k = 1; k < R2; ++k) v[k] = mulw(v[k], tw[k * 16 + n1]);
                 }
+#pragma unroll
+                for (int k = 0; k < R2; ++k) F[sidx<N, R2, SW>(lr, n1 + 16 * k)] = v[k];
             }
         }
     };
 
     // ---- RB: rows, 16-point DFT over n1 (in place, digit-reversed output) ----------
-    auto pass_rb = [&](auto sign_tag) {
-        constexpr int SG = decltype(sign_tag)::value;
+    auto pass_rb = [&](bool inv) {
         for (int j = tid; j < JB; j += NT) {
             const int k2 = j % R2, lr = j / R2;
-            V u[16], v[16];
+#pragma unroll 1
+            for (int f = 0; f < 2; ++f) {
+                V* F = f ? Ss : Ps;
+                V u[16];
 #pragma unroll
-            for (int n = 0; n < 16; ++n) {
-                const int o = sidx<N, R2, SW>(lr, n + 16 * k2);
-                u[n] = Ps[o];
-                v[n] = Ss[o];
-            }
-            Dft<16, SG, T>::run(u);
-            Dft<16, SG, T>::run(v);
+                for (int n = 0; n < 16; ++n) {
+                    u[n] = F[sidx<N, R2, SW>(lr, n + 16 * k2)];
+                    if (inv) u[n] = cj(u[n]);
+                }
+                Dft<16, -1, T>::run(u);
 #pragma unroll
-            for (int n = 0; n < 16; ++n) {
-                const int o = sidx<N, R2, SW>(lr, n + 16 * k2);
-                Ps[o] = u[n];
-                Ss[o] = v[n];
+                for (int n = 0; n < 16; ++n) F[sidx<N, R2, SW>(lr, n + 16 * k2)] = inv ? cj(u[n]) : u[n];
             }
         }
     };
 
-    // ---- CA: columns, DFT over n2 on this CTA's rows --------------------------------
-    auto pass_ca = [&](auto sign_tag) {
-        constexpr int SG = decltype(sign_tag)::value;
+    // ---- CA: columns, R2-point stage over n2 on this CTA's rows ----------------------
+    auto pass_ca = [&](bool inv) {
         for (int j = tid; j < JCA; j += NT) {
             const int x = j % N, n1l = j / N;
             const int n1 = crank + C * n1l;
-            V u[R2], v[R2];
+#pragma unroll 1
+            for (int f = 0; f < 2; ++f) {
+                V* F = f ? Ss : Ps;
+                V v[R2];
 #pragma unroll
-            for (int k = 0; k < R2; ++k) {
-                const int o = sidx<N, R2, SW>(n1l + CPR * k, x);
-                u[k] = Ps[o];
-                v[k] = Ss[o];
-            }
-            if (SG < 0) {
-                Dft<R2, -1, T>::run(u);
+                for (int k = 0; k < R2; ++k) v[k] = F[sidx<N, R2, SW>(n1l + CPR * k, x)];
+                if (inv) {
+                    v[0] = cj(v[0]);
+#pragma unroll
+                    for (int k = 1; k < R2; ++k) v[k] = mulw(cj(v[k]), tw[k * 16 + n1]);
+                }
                 Dft<R2, -1, T>::run(v);
+                if (inv) {
 #pragma unroll
-                for (int k = 1; k < R2; ++k) {
-                    const W w = tw[k * 16 + n1];
-                    u[k] = mulw(u[k], w);
-                    v[k] = mulw(v[k], w);
+                    for (int k = 0; k < R2; ++k) v[k] = cj(v[k]);
+                } else {
+#pragma unroll
+                    for (int k = 1; k < R2; ++k) v[k] = mulw(v[k], tw[k * 16 + n1]);
                 }
-            } else {
 #pragma unroll
-                for (int k = 1; k < R2; ++k) {
-                    const W w = tw[k * 16 + n1];
-                    u[k] = mulwc(u[k], w);
-                    v[k] = mulwc(v[k], w);
-                }
-                Dft<R2, +1, T>::run(u);
-                Dft<R2, +1, T>::run(v);
-            }
-#pragma unroll
-            for (int k = 0; k < R2; ++k) {
-                const int o = sidx<N, R2, SW>(n1l + CPR * k, x);
-                Ps[o] = u[k];
-                Ss[o] = v[k];
+                for (int k = 0; k < R2; ++k) F[sidx<N, R2, SW>(n1l + CPR * k, x)] = v[k];
             }
         }
     };
@@ -326,7 +322,7 @@ __global__ void __launch_bounds__(NT, 1) ssfm_plain_kernel(const InstDesc* __res
         for (int j = tid; j < JCB; j += NT) {
             const int xl = j % (N / C), k2 = j / (N / C);
             const int x = crank * (N / C) + xl;
-#pragma unroll
+#pragma unroll 1
             for (int f = 0; f < 2; ++f) {
                 V* const* R = f ? rS : rP;
                 const W px = f ? pxs[x] : pxp[x];
@@ -334,18 +330,26 @@ __global__ void __launch_bounds__(NT, 1) ssfm_plain_kernel(const InstDesc* __res
                 V u[16];
 #pragma unroll
                 for (int n = 0; n < 16; ++n) u[n] = R[n % C][sidx<N, R2, SW>(n / C + CPR * k2, x)];
-                Dft<16, -1, T>::run(u);
+#pragma unroll 1
+                for (int it = 0; it < 2; ++it) {
+                    if (it) {
 #pragma unroll
-                for (int k1 = 0; k1 < 16; ++k1) u[k1] = mulw(mulw(u[k1], py[k2 + R2 * k1]), px);
-                Dft<16, +1, T>::run(u);
+                        for (int n = 0; n < 16; ++n) u[n] = cj(u[n]);
+                    }
+                    Dft<16, -1, T>::run(u);
+                    if (!it) {
+#pragma unroll
+                        for (int k1 = 0; k1 < 16; ++k1) u[k1] = mulw(mulw(u[k1], py[k2 + R2 * k1]), px);
+                    } else {
+#pragma unroll
+                        for (int n = 0; n < 16; ++n) u[n] = cj(u[n]);
+                    }
+                }
 #pragma unroll
                 for (int n = 0; n < 16; ++n) R[n % C][sidx<N, R2, SW>(n / C + CPR * k2, x)] = u[n];
             }
         }
     };
-
-    using Neg = std::integral_constant<int, -1>;
-    using Pos = std::integral_constant<int, +1>;
 
     double acc_s = 0.0, acc_p = 0.0;
     pass_ra(0, coef, coef, acc_s, acc_p);
@@ -355,16 +359,16 @@ __global__ void __launch_bounds__(NT, 1) ssfm_plain_kernel(const InstDesc* __res
     for (int s = 0; s < nsteps; ++s) {
         V* cf_cur = coef + 6 * (s & 1);
         V* cf_nxt = coef + 6 * ((s + 1) & 1);
-        pass_rb(Neg{});
+        pass_rb(false);
         __syncthreads();
-        pass_ca(Neg{});
+        pass_ca(false);
         cluster_sync();
         if (tid < 3 && s + 1 < nsteps) stage_coef<T>(d, z + d.dz, tid, cf_nxt);
         pass_cb();
         cluster_sync();
-        pass_ca(Pos{});
+        pass_ca(true);
         __syncthreads();
-        pass_rb(Pos{});
+        pass_rb(true);
         __syncthreads();
         pass_ra(s + 1 < nsteps ? 1 : 2, cf_cur, cf_nxt, acc_s, acc_p);
         __syncthreads();

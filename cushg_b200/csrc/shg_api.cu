@@ -74,6 +74,7 @@ InstDesc make_plain_desc(const shg_params& p, double Tc, double T_dk) {
     const double np = sellmeier(lp, Tc), ns = sellmeier(ls, Tc);
     d.n = p.nx;
     d.nsteps = shg_steps(&p);
+    d.out_after = p.thermal ? d.nsteps - 1 : d.nsteps;
     d.dz = dz;
     d.dk = delta_k(p, T_dk);
     d.kap_p = 1 * kPi * dQ / (np * lp);
@@ -181,8 +182,9 @@ shg_status shg_check_params(const shg_params* p) {
             return fail(SHG_ERR_INVALID, "unknown conv_rule %d", p->conv_rule);
         if (p->nz < 3 || p->nx < 3) return fail(SHG_ERR_INVALID, "thermal grid needs nx, nz >= 3");
     }
-    if (!find_plain_variant(p->precision, p->nx))
-        return fail(SHG_ERR_UNSUPPORTED, "no kernel built for grid side %d at precision %d", p->nx, p->precision);
+    if (!find_plain_variant(p->precision, p->nx, p->thermal))
+        return fail(SHG_ERR_UNSUPPORTED, "no %s kernel built for grid side %d at precision %d",
+                    p->thermal ? "thermal" : "plain", p->nx, p->precision);
     return SHG_OK;
 }
 

@@ -25,11 +25,24 @@ struct InstDesc {
     // propagator phase θ = -dz (a (dfx^2 sx^2 + dfy^2 sy^2) + b sx) per field,
     // sx, sy the signed FFT frequency indices
     double a_p, b_p, a_s, b_s, dfx, dfy;
-    double pw_s, pw_p;     // power = pw * sum |A|^2  (0.5 eps0 c n dx dy)
+    double pw_s, pw_p;     // power = pw * sum w |A|^2: plain w = 1, pw = 0.5 eps0 c n dx dy;
+                           // thermal w = n(λ, T) of the output slice, pw = 0.5 eps0 c dx dy
     const void* signal_in; // device, n*n complex (natural layout) or null
     void* pump_out;        // device, n*n complex or null
     void* signal_out;      // device, n*n complex or null
     double* power_out;     // device, [2] = {SH power, pump power} or null
+    int32_t out_after;     // the outputs are the fields after this many steps
+    int32_t pad2;
+    // thermal pass only (Solver.h:33-55, Tfield.h:260-276); null / zero in plain runs.
+    // 3D arrays of the working real type, index z*n*n + y*n + x.
+    const void* t_np;      // n(λp, T) per voxel
+    const void* t_ns;      // n(λs, T) per voxel
+    const void* t_dk;      // Δk(T) per voxel
+    void* t_q;             // heat source Q, written slice by slice
+    double kf_p, kf_s;     // 1.0 π dQ / λp, 0.5 π dQ / λs (κ = kf / n)
+    double bf_s;           // βs 0.5 ε0 c (the two-photon term is bf_s n_s |S|^2)
+    double q_p, q_s, q_h;  // αp 0.5 c ε0, αs 0.5 c ε0, 0.5 c ε0: Q = q_p n_p |P|^2 + q_s n_s |S|^2 + βs (q_h n_s |S|^2)^2
+    double beta_s;         // βs
 };
 
 }  // namespace shg

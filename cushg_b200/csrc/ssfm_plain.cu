@@ -8,10 +8,10 @@
 
 namespace shg {
 
-template <typename T, int N, int C, int NT>
+template <typename T, int N, int C, int NT, bool THERM>
 static cudaError_t launch_plain(const InstDesc* descs, int count, cudaStream_t stream) {
-    using Cfg = PlainCfg<T, N, C, NT>;
-    auto kern = ssfm_plain_kernel<T, N, C, NT>;
+    using Cfg = PlainCfg<T, N, C, NT, THERM>;
+    auto kern = ssfm_plain_kernel<T, N, C, NT, THERM>;
     static std::once_flag once;
     static cudaError_t attr_err = cudaSuccess;
     std::call_once(once, [&]() {
@@ -37,7 +37,9 @@ static cudaError_t launch_plain(const InstDesc* descs, int count, cudaStream_t s
 }
 
 #define SHG_PLAIN(T, PREC, N, C, NT) \
-    {PREC, N, C, NT, PlainCfg<T, N, C, NT>::smem_bytes, &launch_plain<T, N, C, NT>}
+    {PREC, N, C, NT, 0, PlainCfg<T, N, C, NT, false>::smem_bytes, &launch_plain<T, N, C, NT, false>}
+#define SHG_THERM(T, PREC, N, C, NT) \
+    {PREC, N, C, NT, 1, PlainCfg<T, N, C, NT, true>::smem_bytes, &launch_plain<T, N, C, NT, true>}
 
 // Threads per CTA of each variant (tuning knobs, overridable at build time).
 #ifndef SHG_NT_F32_SMALL
@@ -73,11 +75,20 @@ static const PlainVariant kPlainVariants[] = {
     SHG_PLAIN(double, 64, 128, 4, SHG_NT_F64),
     SHG_PLAIN(double, 64, 192, 8, 192),
     SHG_PLAIN(double, 64, 256, 16, SHG_NT_F64),
+    // thermal passes (per-voxel n(T), running Δk prefix, Q emission)
+    SHG_THERM(float, 32, 32, 1, 128),
+    SHG_THERM(float, 32, 64, 1, 256),
+    SHG_THERM(float, 32, 128, 2, 256),
+    SHG_THERM(float, 32, 256, 8, 256),
+    SHG_THERM(double, 64, 32, 1, 128),
+    SHG_THERM(double, 64, 64, 1, 256),
+    SHG_THERM(double, 64, 128, 4, 256),
+    SHG_THERM(double, 64, 256, 16, 256),
 };
 
-const PlainVariant* find_plain_variant(int precision, int n) {
+const PlainVariant* find_plain_variant(int precision, int n, int thermal) {
     for (const auto& v : kPlainVariants)
-        if (v.precision == precision && v.n == n) return &v;
+        if (v.precision == precision && v.n == n && v.thermal == (thermal ? 1 : 0)) return &v;
     return nullptr;
 }
 

@@ -38,7 +38,7 @@ namespace shg {
 
 namespace cg = cooperative_groups;
 
-template <typename T, int N, int C, int NT>
+template <typename T, int N, int C, int NT, bool THERM = false>
 struct PlainCfg {
     static constexpr int R1 = 16;
     static constexpr int R2 = N / 16;
@@ -52,8 +52,10 @@ struct PlainCfg {
     static_assert(N % 16 == 0 && 16 % C == 0 && RL * C == N, "bad grid / cluster split");
     // dynamic shared memory: P, S planes, twiddles + 4 propagator vectors (multiplier
     // tables), 2x6 coefficients, reduction scratch
+    // (thermal: plus the running Δk prefix of this CTA's points, FP64)
     static constexpr size_t smem_bytes = sizeof(cx<T>) * (2 * (size_t)PLANE + 12) + sizeof(mult<T>) * 5 * (size_t)N +
-                                         sizeof(double) * (2 * (NT / 32) + 4);
+                                         sizeof(double) * (2 * (NT / 32) + 4) +
+                                         (THERM ? sizeof(double) * (size_t)PLANE : 0);
 };
 
 // physical offset of logical position p of local row lr
@@ -114,9 +116,27 @@ __device__ __forceinline__ void stage_coef(const InstDesc& d, double z, int j, c
     cf[3 + j] = mk<T>((T)(-d.kap_s * sn), (T)(d.kap_s * cs));
 }
 
-template <typename T, int N, int C, int NT>
+// Thermal stage coefficients at one voxel (Solver.h:33-55): κ = kf / n(λ, T(x,y,s)) and the
+// phase DKint (dz inc + s dz) / (s + 1), DKint the running sum of Δk over slices 0..s
+// (PhaseMatching.h:27-44), in FP64.
+template <typename T>
+__device__ __forceinline__ void thermal_coef(const InstDesc& d, double dki, int sl, double np, double ns, cx<T>* cf) {
+    const double kp = d.kf_p / np, ks = d.kf_s / ns;
+    const double sr = (double)sl, b = sr + 1.0;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        const double inc = j == 0 ? 0.0 : (j == 1 ? 0.25 : 0.5);
+        const double phi = dki * (d.dz * inc + sr * d.dz) / b;
+        double sn, cs;
+        sincos(phi, &sn, &cs);
+        cf[j] = mk<T>((T)(kp * sn), (T)(kp * cs));
+        cf[3 + j] = mk<T>((T)(-ks * sn), (T)(ks * cs));
+    }
+}
+
+template <typename T, int N, int C, int NT, bool THERM>
 __global__ void __launch_bounds__(NT, 1) ssfm_plain_kernel(const InstDesc* __restrict__ descs) {
-    using Cfg = PlainCfg<T, N, C, NT>;
+    using Cfg = PlainCfg<T, N, C, NT, THERM>;
     constexpr int R2 = Cfg::R2, RL = Cfg::RL, SW = Cfg::SW;
     constexpr int JA = Cfg::JA, JB = Cfg::JB, JCA = Cfg::JCA, JCB = Cfg::JCB;
     constexpr int CPR = 16 / C;  // column sub-rows per n1 of this CTA
@@ -133,6 +153,7 @@ __global__ void __launch_bounds__(NT, 1) ssfm_plain_kernel(const InstDesc* __res
     W* pyp = pxs + N;            // pump propagator, y factor by frequency, × 1/N^2
     W* pys = pyp + N;            // SH   propagator, y factor
     double* red = reinterpret_cast<double*>(pys + N);  // [2*(NT/32)] + [4]
+    double* dkint = red + 2 * (NT / 32) + 4;           // thermal: [RL*N] running Δk prefix
 
     const int tid = threadIdx.x;
     const int inst = blockIdx.x / C;
@@ -169,7 +190,7 @@ __global__ void __launch_bounds__(NT, 1) ssfm_plain_kernel(const InstDesc* __res
         sincos(thys, &sn, &cs);
         pys[j] = make_mult<T>(cs * inv, sn * inv);
     }
-    if (tid < 3) stage_coef<T>(d, 0.0, tid, coef);
+    if (!THERM && tid < 3) stage_coef<T>(d, 0.0, tid, coef);
 
     // ---- initial fields: setPump (Efields.h:84-119), SH = 0 or given ---------------
     const V* sin_g = reinterpret_cast<const V*>(d.signal_in);
@@ -203,27 +224,62 @@ __global__ void __launch_bounds__(NT, 1) ssfm_plain_kernel(const InstDesc* __res
     // ---- RA: rows, R2-point stage of (row lr, n1) and the pointwise RK4 half-steps -----
     // mode 0: first (natural order in: RK4(z_0), forward), 1: middle (inverse, RK4(z_s),
     // RK4(z_{s+1}), forward), 2: last (inverse, RK4(z_s), outputs)
-    auto pass_ra = [&](int mode, const V* cf_prev, const V* cf_next, double& acc_s, double& acc_p) {
+    using R = T;  // real type of the thermal 3D arrays
+    const R* tnp = reinterpret_cast<const R*>(d.t_np);
+    const R* tns = reinterpret_cast<const R*>(d.t_ns);
+    const R* tdk = reinterpret_cast<const R*>(d.t_dk);
+    R* tq = reinterpret_cast<R*>(d.t_q);
+    constexpr size_t NN = (size_t)N * N;
+
+    // s: index of the step that ends in this pass (-1 in the first pass)
+    auto pass_ra = [&](int mode, int s, const V* cf_prev, const V* cf_next, double& acc_s, double& acc_p) {
         for (int j = tid; j < JA; j += NT) {
             const int n1 = j & 15, lr = j >> 4;
 #pragma unroll 1
             for (int ph = 0; ph < 5; ++ph) {
                 if (ph == 2) {
-                    // pointwise: the two RK4 applications around the step boundary
+                    // pointwise: the two RK4 applications around the step boundary (the second
+                    // half of step s, then the first half of step s+1)
                     const int h0 = mode == 0 ? 1 : 0, h1 = mode == 2 ? 1 : 2;
 #pragma unroll 1
                     for (int k = 0; k < R2; ++k) {
-                        const int o = sidx<N, R2, SW>(lr, n1 + 16 * k);
+                        const int x = n1 + 16 * k;
+                        const int o = sidx<N, R2, SW>(lr, x);
+                        const size_t g = (size_t)(crank + C * lr) * N + x;
                         V p = Ps[o], q = Ss[o];
 #pragma unroll 1
-                        for (int h = h0; h < h1; ++h) rk4_point<T>(p, q, h ? cf_next : cf_prev, hap, has, qs, dz6);
-                        if (mode == 2) {
-                            const size_t g = (size_t)(crank + C * lr) * N + n1 + 16 * k;
-                            if (d.pump_out) reinterpret_cast<V*>(d.pump_out)[g] = p;
-                            if (d.signal_out) reinterpret_cast<V*>(d.signal_out)[g] = q;
-                            acc_s += (double)q.x * (double)q.x + (double)q.y * (double)q.y;
-                            acc_p += (double)p.x * (double)p.x + (double)p.y * (double)p.y;
-                        } else {
+                        for (int h = h0; h < h1; ++h) {
+                            const int sl = s + h;  // slice of this half step
+                            if constexpr (THERM) {
+                                const size_t gz = (size_t)sl * NN + g;
+                                double& dki = dkint[lr * N + x];
+                                if (h == 1) dki = (mode == 0 ? 0.0 : dki) + (double)tdk[gz];
+                                const double np = (double)tnp[gz], ns = (double)tns[gz];
+                                V cf[6];
+                                thermal_coef<T>(d, dki, sl, np, ns, cf);
+                                rk4_point<T>(p, q, cf, hap, has, (T)(0.5 * (d.bf_s * ns)), dz6);
+                                if (h == 0 && tq) {
+                                    // kernelSetQ (Tfield.h:260-276) for slice s, after its step
+                                    const R ap2 = p.x * p.x + p.y * p.y, as2 = q.x * q.x + q.y * q.y;
+                                    const R is = (R)d.q_h * (R)ns * as2;
+                                    tq[gz] = (R)d.q_p * (R)np * ap2 + (R)d.q_s * (R)ns * as2 + (R)d.beta_s * (is * is);
+                                }
+                            } else {
+                                rk4_point<T>(p, q, h ? cf_next : cf_prev, hap, has, qs, dz6);
+                            }
+                            if (h == 0 && s + 1 == d.out_after) {
+                                if (d.pump_out) reinterpret_cast<V*>(d.pump_out)[g] = p;
+                                if (d.signal_out) reinterpret_cast<V*>(d.signal_out)[g] = q;
+                                double ws = 1.0, wp = 1.0;
+                                if constexpr (THERM) {
+                                    ws = (double)tns[(size_t)(s + 1) * NN + g];
+                                    wp = (double)tnp[(size_t)(s + 1) * NN + g];
+                                }
+                                acc_s += ws * ((double)q.x * (double)q.x + (double)q.y * (double)q.y);
+                                acc_p += wp * ((double)p.x * (double)p.x + (double)p.y * (double)p.y);
+                            }
+                        }
+                        if (mode != 2) {
                             Ps[o] = p;
                             Ss[o] = q;
                         }
@@ -352,7 +408,7 @@ __global__ void __launch_bounds__(NT, 1) ssfm_plain_kernel(const InstDesc* __res
     };
 
     double acc_s = 0.0, acc_p = 0.0;
-    pass_ra(0, coef, coef, acc_s, acc_p);
+    pass_ra(0, -1, coef, coef, acc_s, acc_p);
     __syncthreads();
 
     double z = 0.0;
@@ -363,14 +419,14 @@ __global__ void __launch_bounds__(NT, 1) ssfm_plain_kernel(const InstDesc* __res
         __syncthreads();
         pass_ca(false);
         cluster_sync();
-        if (tid < 3 && s + 1 < nsteps) stage_coef<T>(d, z + d.dz, tid, cf_nxt);
+        if (!THERM && tid < 3 && s + 1 < nsteps) stage_coef<T>(d, z + d.dz, tid, cf_nxt);
         pass_cb();
         cluster_sync();
         pass_ca(true);
         __syncthreads();
         pass_rb(true);
         __syncthreads();
-        pass_ra(s + 1 < nsteps ? 1 : 2, cf_cur, cf_nxt, acc_s, acc_p);
+        pass_ra(s + 1 < nsteps ? 1 : 2, s, cf_cur, cf_nxt, acc_s, acc_p);
         __syncthreads();
         z += d.dz;
     }

@@ -14,10 +14,11 @@ struct PlainVariant {
     int n;             // grid side
     int cluster;       // CTAs per instance
     int threads;       // threads per CTA
+    int thermal;       // 1: thermal pass (per-voxel optics, Q emission)
     size_t smem;       // dynamic shared memory per CTA
     cudaError_t (*launch)(const InstDesc* descs, int count, cudaStream_t stream);
 };
 
-const PlainVariant* find_plain_variant(int precision, int n);
+const PlainVariant* find_plain_variant(int precision, int n, int thermal = 0);
 
 }  // namespace shg

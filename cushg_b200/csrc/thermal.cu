@@ -1,0 +1,246 @@
+// thermal.cu — kernels of the 3D heat solve and the temperature-dependent optics.
+//
+// Reference counterparts (src/headers/Tfield.h, PhaseMatching.h):
+//   kernelSetTemperature / kernelSetBottomOvensTemperature / kernelSetOvenSurrounded
+//       -> thermal_init_kernel
+//   kernelHeatEquationTopOpen / kernelHeatEquationOvenSurrounded (one Jacobi sweep)
+//       -> jacobi_kernel (Ti -> Tf; the reference's Tf -> Ti device copy after every
+//          sweep becomes a ping-pong of two buffers)
+//   kernelDifSquareVectors + thrust::reduce (checkConvergence)
+//       -> the RESID form of jacobi_kernel (per-block partials) + reduce_partials_kernel
+//   kernelSetInicialDKThermal and the per-voxel n(λ, T) of dAdz / kernelSetQ
+//       -> optics_kernel (Δk, n_p, n_s per voxel, once per optical pass)
+#include <cuda_runtime.h>
+
+#include "shg_host.h"
+#include "thermal.h"
+
+namespace shg {
+
+template <typename R>
+__global__ void thermal_init_kernel(R* Ta, R* Tb, R* Q, int n, int nz, R temp, R tpelt, int boundary) {
+    const size_t total = (size_t)n * n * nz;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i % n), y = (int)((i / n) % n);
+        bool face;
+        if (boundary == SHG_BOUNDARY_OVEN_SURROUNDED) face = (y == 0 || y == n - 1 || x == 0 || x == n - 1);
+        else face = (y == 0);
+        const R v = face ? tpelt : temp;
+        Ta[i] = v;
+        Tb[i] = v;
+        Q[i] = (R)0;
+    }
+}
+
+// Sellmeier of MgO:sPPLT (Crystal.h:54-70) in FP64 on the device.
+__device__ __forceinline__ double sellmeier_dev(double L, double T) {
+    const double A = 4.502483, B = 0.007294, C = 0.185087, D = -0.02357;
+    const double E = 0.073423, F = 0.199595, G = 0.001, H = 7.99724;
+    const double TK = T + 273.15;
+    const double b = 3.483933e-8 * (TK * TK);
+    const double c = 1.607839e-8 * (TK * TK);
+    const double L2 = L * L;
+    return sqrt(A + (B + b) / (L2 - (C + c) * (C + c)) + E / (L2 - F * F) + G / (L2 - H * H) + D * L2);
+}
+
+// Δk (PhaseMatching.h:47-65), n(λp, T) and n(λs, T) at every voxel, in FP64.
+template <typename R>
+__global__ void optics_kernel(const R* __restrict__ T, R* __restrict__ dk, R* __restrict__ np, R* __restrict__ ns,
+                              size_t total, double lp, double period) {
+    const double ls = 0.5 * lp, pi = 3.14159265358979323846;
+    const double a = 2.2e-6, b = -5.9e-9;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const double t = (double)T[i];
+        const double npv = sellmeier_dev(lp, t), nsv = sellmeier_dev(ls, t);
+        const double d = t - 25.;
+        dk[i] = (R)(2 * pi * (2 * npv / lp - nsv / ls + 1 / (period * (1. + a * d + b * (d * d)))));
+        np[i] = (R)npv;
+        ns[i] = (R)nsv;
+    }
+}
+
+// One Jacobi sweep Ti -> Tf.  Thread block (32, 8) over (x, y), one z plane per grid z.
+// Voxels the reference never writes (the Dirichlet faces) are left untouched, which with
+// two buffers initialised alike keeps them at the oven temperature in both.
+// RESID: each block also writes its partial of sum (Tf - Ti)^2 (rule 0) or max |Tf - Ti|.
+template <typename R, int BOUND, bool RESID>
+__global__ void __launch_bounds__(256) jacobi_kernel(const R* __restrict__ Ti, R* __restrict__ Tf, const R* __restrict__ Q,
+                                                     JacobiCoef<R> k, int rule, double* __restrict__ partial) {
+    const int n = k.n, nz = k.nz;
+    const int x = blockIdx.x * 32 + threadIdx.x;
+    const int y = blockIdx.y * 8 + threadIdx.y;
+    const int z = blockIdx.z;
+    double dres = 0.0;
+    if (x < n && y < n) {
+        const size_t sx = 1, sy = (size_t)n, sz = (size_t)n * n;
+        const size_t i = (size_t)z * sz + (size_t)y * sy + x;
+        const bool xi = x > 0 && x < n - 1, yi = y > 0 && y < n - 1, zi = z > 0 && z < nz - 1;
+        bool wr = true;
+        R v = (R)0;
+        if (BOUND == SHG_BOUNDARY_TOP_OPEN) {
+            if (y == 0) {
+                wr = false;  // Dirichlet face at the oven temperature
+            } else if (xi && yi && zi) {  // inner points (Tfield.h:113-115)
+                v = k.L2 * ((Ti[i + sx] + Ti[i - sx]) * k.idx2 + (Ti[i + sy] + Ti[i - sy]) * k.idy2 +
+                            (Ti[i + sz] + Ti[i - sz]) * k.idz2 + Q[i] * k.iK);
+            } else if (!xi && yi && zi) {  // faces x = 0 / x = Lx (Tfield.h:119-125)
+                const size_t xn = x == 0 ? i + sx : i - sx;
+                v = (Ti[xn] + k.ax * (Ti[i + sy] + Ti[i - sy]) + k.bx * (Ti[i + sz] + Ti[i - sz]) + k.Bix * k.Tinf) * k.fx;
+            } else if (xi && !yi && zi) {  // face y = Ly (Tfield.h:127-129)
+                v = (Ti[i - sy] + k.ay * (Ti[i + sx] + Ti[i - sx]) + k.by * (Ti[i + sz] + Ti[i - sz]) + k.Biy * k.Tinf) * k.fy;
+            } else if (xi && yi && !zi) {  // faces z = 0 / z = Lcr (Tfield.h:131-137)
+                const size_t zn = z == 0 ? i + sz : i - sz;
+                v = (Ti[zn] + k.az * (Ti[i + sx] + Ti[i - sx]) + k.bz * (Ti[i + sy] + Ti[i - sy]) + k.Biz * k.Tinf) * k.fz;
+            } else if (!xi && yi && !zi) {  // vertical edges (Tfield.h:143-157)
+                const size_t xn = x == 0 ? i + sx : i - sx, zn = z == 0 ? i + sz : i - sz;
+                v = (k.av * Ti[xn] + k.bv * Ti[zn] + k.cv * (Ti[i + sy] + Ti[i - sy]) + k.tv) * k.V;
+            } else if (xi && !yi && !zi) {  // horizontal edges (Tfield.h:161-167)
+                const size_t zn = z == 0 ? i + sz : i - sz;
+                v = (k.ah * Ti[i - sy] + k.bh * Ti[zn] + k.ch * (Ti[i - sx] + Ti[i + sx]) + k.th) * k.H;
+            } else if (!xi && !yi && zi) {  // depth edges (Tfield.h:171-177)
+                const size_t xn = x == 0 ? i + sx : i - sx;
+                v = (k.ad * Ti[i - sy] + k.bd * Ti[xn] + k.cd * (Ti[i + sz] + Ti[i - sz]) + k.td) * k.D;
+            } else {  // vertices (Tfield.h:181-196)
+                const size_t xn = x == 0 ? i + sx : i - sx, zn = z == 0 ? i + sz : i - sz;
+                v = (k.AV * Ti[xn] + k.BV * Ti[i - sy] + k.CV * Ti[zn] + k.Tinf * k.BiD) * k.GV;
+            }
+        } else {
+            if (!(xi && yi)) {
+                wr = false;  // lateral faces held at the oven temperature
+            } else if (zi) {
+                v = k.L2 * ((Ti[i + sx] + Ti[i - sx]) * k.idx2 + (Ti[i + sy] + Ti[i - sy]) * k.idy2 +
+                            (Ti[i + sz] + Ti[i - sz]) * k.idz2 + Q[i] * k.iK);
+            } else {  // z faces (Tfield.h:229-236)
+                const size_t zn = z == 0 ? i + sz : i - sz;
+                v = (Ti[zn] + k.az * (Ti[i + sx] + Ti[i - sx]) + k.bz * (Ti[i + sy] + Ti[i - sy]) + k.Biz * k.Tinf) * k.fz;
+            }
+        }
+        if (wr) {
+            Tf[i] = v;
+            if (RESID) {
+                const double dd = (double)(R)(v - Ti[i]);
+                dres = rule == SHG_CONV_MAXABS ? fabs(dd) : dd * dd;
+            }
+        }
+    }
+    if (RESID) {
+        const bool mx = rule == SHG_CONV_MAXABS;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double other = __shfl_down_sync(0xffffffffu, dres, o);
+            dres = mx ? fmax(dres, other) : dres + other;
+        }
+        __shared__ double wsum[8];
+        const int w = threadIdx.y;
+        if (threadIdx.x == 0) wsum[w] = dres;
+        __syncthreads();
+        if (threadIdx.x == 0 && threadIdx.y == 0) {
+            double a = 0.0;
+            for (int q = 0; q < 8; ++q) a = mx ? fmax(a, wsum[q]) : a + wsum[q];
+            partial[((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = a;
+        }
+    }
+}
+
+// Deterministic second stage: one block sums (or maxes) the partials in a fixed order.
+__global__ void reduce_partials_kernel(const double* __restrict__ partial, size_t count, int rule, double* out) {
+    __shared__ double s[256];
+    const bool mx = rule == SHG_CONV_MAXABS;
+    double a = 0.0;
+    for (size_t i = threadIdx.x; i < count; i += blockDim.x) a = mx ? fmax(a, partial[i]) : a + partial[i];
+    s[threadIdx.x] = a;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) s[threadIdx.x] = mx ? fmax(s[threadIdx.x], s[threadIdx.x + o]) : s[threadIdx.x] + s[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = s[0];
+}
+
+template <typename R>
+JacobiCoef<R> make_jacobi_coef(const shg_params& p) {
+    JacobiCoef<R> k;
+    const double dx = p.lx / (p.nx - 1), dy = p.ly / (p.ny - 1), dz = p.lz / (p.nz - 1);
+    const double K = p.kappa, h = p.h_conv, Tinf = p.t_inf;
+    const double Bix = h * dx / K, Biy = h * dy / K, Biz = h * dz / K;
+    const double ax = dx * dx / (2 * dy * dy), ay = dy * dy / (2 * dx * dx), az = dz * dz / (2 * dx * dx);
+    const double bx = dx * dx / (2 * dz * dz), by = dy * dy / (2 * dz * dz), bz = dz * dz / (2 * dy * dy);
+    const double av = dz / (2 * dx), bv = dx / (2 * dz), cv = dx * dz / (4 * dy * dy);
+    const double ah = dz / (2 * dy), bh = dy / (2 * dz), ch = dy * dz / (4 * dx * dx);
+    const double ad = dx / (2 * dy), bd = dy / (2 * dx), cd = dx * dy / (4 * dz * dz);
+    const double AV = dy * dz / dx, BV = dx * dz / dy, CV = dx * dy / dz, BiD = Bix * dy + Biy * dz + Biz * dx;
+    k.n = p.nx;
+    k.nz = p.nz;
+    k.L2 = (R)(1 / (2 / (dx * dx) + 2 / (dy * dy) + 2 / (dz * dz)));
+    k.idx2 = (R)(1 / (dx * dx));
+    k.idy2 = (R)(1 / (dy * dy));
+    k.idz2 = (R)(1 / (dz * dz));
+    k.iK = (R)(1 / K);
+    k.Tinf = (R)Tinf;
+    k.Bix = (R)Bix; k.Biy = (R)Biy; k.Biz = (R)Biz;
+    k.ax = (R)ax; k.ay = (R)ay; k.az = (R)az; k.bx = (R)bx; k.by = (R)by; k.bz = (R)bz;
+    k.fx = (R)(1 / (1 + 2 * ax + 2 * bx + Bix));
+    k.fy = (R)(1 / (1 + 2 * ay + 2 * by + Biy));
+    k.fz = (R)(1 / (1 + 2 * az + 2 * bz + Biz));
+    k.av = (R)av; k.bv = (R)bv; k.cv = (R)cv;
+    k.V = (R)(1 / (av + bv + 2 * cv + 0.5 * (Bix + Biz)));
+    k.tv = (R)(0.5 * Tinf * (Bix + Biz));
+    k.ah = (R)ah; k.bh = (R)bh; k.ch = (R)ch;
+    k.H = (R)(1 / (ah + bh + 2 * ch + 0.5 * (Biy + Biz)));
+    k.th = (R)(0.5 * Tinf * (Biy + Biz));
+    k.ad = (R)ad; k.bd = (R)bd; k.cd = (R)cd;
+    k.D = (R)(1 / (ad + bd + 2 * cd + 0.5 * (Bix + Biy)));
+    k.td = (R)(0.5 * Tinf * (Bix + Biy));
+    k.AV = (R)AV; k.BV = (R)BV; k.CV = (R)CV; k.BiD = (R)BiD;
+    k.GV = (R)(1 / (AV + BV + CV + BiD));
+    return k;
+}
+
+template <typename R>
+cudaError_t launch_thermal_init(R* Ta, R* Tb, R* Q, const shg_params& p, cudaStream_t s) {
+    const size_t total = (size_t)p.nx * p.nx * p.nz;
+    const int blocks = (int)std::min<size_t>((total + 255) / 256, 148 * 16);
+    thermal_init_kernel<R><<<blocks, 256, 0, s>>>(Ta, Tb, Q, p.nx, p.nz, (R)p.temp, (R)p.t_peltier, p.boundary);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_optics(const R* T, R* dk, R* np, R* ns, const shg_params& p, cudaStream_t s) {
+    const size_t total = (size_t)p.nx * p.nx * p.nz;
+    const int blocks = (int)std::min<size_t>((total + 255) / 256, 148 * 16);
+    optics_kernel<R><<<blocks, 256, 0, s>>>(T, dk, np, ns, total, p.lambda_p, p.period);
+    return cudaGetLastError();
+}
+
+size_t jacobi_partials(const shg_params& p) {
+    return (size_t)((p.nx + 31) / 32) * ((p.nx + 7) / 8) * p.nz;
+}
+
+template <typename R>
+cudaError_t launch_jacobi(const R* Ti, R* Tf, const R* Q, const JacobiCoef<R>& k, int boundary, bool resid, int rule,
+                          double* partial, double* out, cudaStream_t s) {
+    dim3 block(32, 8, 1);
+    dim3 grid((k.n + 31) / 32, (k.n + 7) / 8, k.nz);
+    if (boundary == SHG_BOUNDARY_OVEN_SURROUNDED) {
+        if (resid) jacobi_kernel<R, SHG_BOUNDARY_OVEN_SURROUNDED, true><<<grid, block, 0, s>>>(Ti, Tf, Q, k, rule, partial);
+        else jacobi_kernel<R, SHG_BOUNDARY_OVEN_SURROUNDED, false><<<grid, block, 0, s>>>(Ti, Tf, Q, k, rule, partial);
+    } else {
+        if (resid) jacobi_kernel<R, SHG_BOUNDARY_TOP_OPEN, true><<<grid, block, 0, s>>>(Ti, Tf, Q, k, rule, partial);
+        else jacobi_kernel<R, SHG_BOUNDARY_TOP_OPEN, false><<<grid, block, 0, s>>>(Ti, Tf, Q, k, rule, partial);
+    }
+    if (resid) reduce_partials_kernel<<<1, 256, 0, s>>>(partial, (size_t)grid.x * grid.y * grid.z, rule, out);
+    return cudaGetLastError();
+}
+
+template JacobiCoef<float> make_jacobi_coef<float>(const shg_params&);
+template JacobiCoef<double> make_jacobi_coef<double>(const shg_params&);
+template cudaError_t launch_thermal_init<float>(float*, float*, float*, const shg_params&, cudaStream_t);
+template cudaError_t launch_thermal_init<double>(double*, double*, double*, const shg_params&, cudaStream_t);
+template cudaError_t launch_optics<float>(const float*, float*, float*, float*, const shg_params&, cudaStream_t);
+template cudaError_t launch_optics<double>(const double*, double*, double*, double*, const shg_params&, cudaStream_t);
+template cudaError_t launch_jacobi<float>(const float*, float*, const float*, const JacobiCoef<float>&, int, bool, int,
+                                          double*, double*, cudaStream_t);
+template cudaError_t launch_jacobi<double>(const double*, double*, const double*, const JacobiCoef<double>&, int, bool,
+                                           int, double*, double*, cudaStream_t);
+
+}  // namespace shg

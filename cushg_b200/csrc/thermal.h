@@ -1,0 +1,34 @@
+// thermal.h — launchers of the heat-solve and temperature-optics kernels (thermal.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "../../include/shg.h"
+
+namespace shg {
+
+// Coefficients of one Jacobi sweep of kernelHeatEquationTopOpen / OvenSurrounded
+// (src/headers/Tfield.h:99-106, 211-215), computed in FP64 and rounded to R; divisions
+// of the reference become multiplications by these reciprocals.
+template <typename R>
+struct JacobiCoef {
+    int n, nz;
+    R L2, idx2, idy2, idz2, iK, Tinf;
+    R Bix, Biy, Biz;
+    R ax, ay, az, bx, by, bz, fx, fy, fz;
+    R av, bv, cv, V, tv;
+    R ah, bh, ch, H, th;
+    R ad, bd, cd, D, td;
+    R AV, BV, CV, BiD, GV;
+};
+
+template <typename R> JacobiCoef<R> make_jacobi_coef(const shg_params& p);
+template <typename R> cudaError_t launch_thermal_init(R* Ta, R* Tb, R* Q, const shg_params& p, cudaStream_t s);
+template <typename R> cudaError_t launch_optics(const R* T, R* dk, R* np, R* ns, const shg_params& p, cudaStream_t s);
+// one sweep Ti -> Tf; with resid, also the convergence value of that sweep into *out
+template <typename R>
+cudaError_t launch_jacobi(const R* Ti, R* Tf, const R* Q, const JacobiCoef<R>& k, int boundary, bool resid, int rule,
+                          double* partial, double* out, cudaStream_t s);
+size_t jacobi_partials(const shg_params& p);
+
+}  // namespace shg

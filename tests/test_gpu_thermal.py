@@ -1,0 +1,88 @@
+"""Parity of the thermal run (Jacobi heat solve + temperature-dependent optics + Q
+emission, the reference's -DTHERMAL outer loop) through the C ABI, against the reference's
+own FP64 outputs (tests/golden/thermal64_n32*.npz) and the CPU oracle.
+
+Tolerances: fields relative L2 <= 1e-10, temperatures max |ΔT| <= 1e-9 K, SH power 1e-10,
+identical Jacobi sweep counts and outer-iteration counts."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from cushg_b200 import params as P
+from cushg_b200 import shg
+from oracle import golden_cases as G
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+THERMAL_GOLDEN = ["thermal64_n32", "thermal64_n32_oven"]
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.complex128) - b) / np.linalg.norm(b))
+
+
+@pytest.mark.parametrize("name", THERMAL_GOLDEN)
+def test_thermal_fp64_matches_reference(name):
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    meta = json.loads(str(z["meta"]))
+    p = G.params_of(name)
+    r = shg.solve(p, want_temperature=True)
+    assert r.stats.jacobi_sweeps == sum(meta["jacobi_sweeps"])
+    assert r.stats.outer_iterations == len(meta["jacobi_sweeps"])
+    assert np.abs(r.temperature - z["T"]).max() <= 1e-9
+    assert rel_l2(r.pump, z["pump"]) <= 1e-10
+    assert rel_l2(r.signal, z["signal"]) <= 1e-10
+
+
+@pytest.mark.parametrize("name", THERMAL_GOLDEN)
+def test_thermal_fp64_matches_oracle(name):
+    p = G.params_of(name)
+    r = shg.solve(p, want_temperature=True)
+    rc, pump, sig, st, T = O.solve(p, want_temperature=True)
+    assert rc == 0
+    assert r.stats.jacobi_sweeps == st.jacobi_sweeps
+    assert np.abs(r.temperature - T).max() <= 1e-9
+    assert rel_l2(r.signal, sig) <= 1e-10
+    # the thermal fields inherit the rounding of tens of thousands of Jacobi sweeps through
+    # n(T) and Δk(T), so the power is held to 1e-10 rather than the plain path's 1e-12
+    assert abs(r.sh_power - st.sh_power) / st.sh_power <= 1e-10
+
+
+@pytest.mark.parametrize("n", [64, 128])
+def test_thermal_fp64_larger_grids_match_oracle(n):
+    p = P.workload(n, 12, 6000.0, 20.0, 30.0, 3000.0, 33.0, precision=64, thermal=1)
+    p.alpha_p, p.alpha_s, p.beta_s = 2e-5, 1e-4, 1e-3
+    p.max_outer = 2
+    p.check_every = 200
+    p.conv_rule = P.SHG_CONV_MAXABS
+    p.jacobi_tol = 1e-3
+    r = shg.solve(p, want_temperature=True)
+    rc, pump, sig, st, T = O.solve(p, want_temperature=True)
+    assert rc == 0
+    assert r.stats.jacobi_sweeps == st.jacobi_sweeps
+    assert np.abs(r.temperature - T).max() <= 1e-9
+    assert rel_l2(r.signal, sig) <= 1e-10
+    assert rel_l2(r.pump, pump) <= 1e-10
+
+
+def test_thermal_sweep_cap_reports_not_converged():
+    p = G.params_of("thermal64_n32").replace(max_sweeps=100)
+    with pytest.raises(shg.ShgError) as e:
+        shg.solve(p)
+    assert e.value.status == P.SHG_ERR_NOT_CONVERGED
+
+
+def test_thermal_fp32_against_fp64_oracle():
+    """FP32 fields and temperatures against the FP64 oracle with the same stopping rule
+    (max |ΔT| < 1e-3 K checked every 1000 sweeps, so both stop after the same sweeps)."""
+    p = G.params_of("thermal64_n32").replace(conv_rule=P.SHG_CONV_MAXABS, jacobi_tol=1e-3, check_every=1000)
+    rc, pump, sig, st, T = O.solve(p, want_temperature=True)
+    r = shg.solve(p.replace(precision=32), want_temperature=True)
+    assert r.stats.jacobi_sweeps == st.jacobi_sweeps
+    assert np.abs(r.temperature - T).max() <= 1e-2
+    assert rel_l2(r.signal, sig) <= 1e-3
+    assert abs(r.sh_power - st.sh_power) / st.sh_power <= 1e-3

@@ -315,6 +315,41 @@ def run_reference(args, rank: int, world: int) -> dict | None:
     }
 
 
+def run_thermal(args) -> dict:
+    """Thermal workload (outside the default sweep line): one full thermal solve of the
+    128x128 / nz = 200 FP64 configuration (20 mm, 20 W, w0 = 40 µm, oven 40 °C, Jacobi to
+    max|ΔT| < 1e-6 K inside <= 5 outer iterations), timed with CUDA events."""
+    import torch
+    from cushg_b200 import shg
+
+    p = P.config_thermal_128()
+    if args.thermal_side:
+        p = p.replace(nx=args.thermal_side, ny=args.thermal_side)
+    if args.thermal_max_sweeps:
+        p = p.replace(max_sweeps=args.thermal_max_sweeps)
+    cdt = torch.complex128 if p.precision == 64 else torch.complex64
+    pump = torch.empty((p.ny, p.nx), dtype=cdt, device="cuda")
+    sig = torch.empty_like(pump)
+    with ClockSampler(0) as clk:
+        t0 = time.perf_counter()
+        try:
+            st = shg.solve_device(p, pump, sig)
+            status = "ok"
+        except shg.ShgError as e:  # e.g. the sweep cap
+            st, status = None, str(e)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+    vox = p.nx * p.ny * p.nz
+    out = {"metric": "thermal solve (Jacobi voxel-sweeps/s)", "workload": "thermal 128x128x200 FP64", "status": status,
+           "wall_s": wall, "clocks": clk.summary()}
+    if st is not None:
+        out.update({"device_ms": st.device_ms, "jacobi_sweeps": st.jacobi_sweeps, "outer_iterations": st.outer_iterations,
+                    "sh_power_w": st.sh_power, "value": vox * st.jacobi_sweeps / (st.device_ms * 1e-3),
+                    "unit": "voxel-sweeps/s",
+                    "jacobi_gbs_algorithmic": 24 * vox * st.jacobi_sweeps / (st.device_ms * 1e-3) / 1e9})
+    return out
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -326,12 +361,17 @@ def main() -> int:
     ap.add_argument("--class-side", type=int, default=0, help="profile case: one grid-size class only")
     ap.add_argument("--class-count", type=int, default=18)
     ap.add_argument("--class-nz", type=int, default=24)
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "thermal"])
+    ap.add_argument("--thermal-side", type=int, default=0)
+    ap.add_argument("--thermal-max-sweeps", type=int, default=0)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.impl == "reference":
+    if args.workload == "thermal":
+        out = run_thermal(args) if rank == 0 else None
+    elif args.impl == "reference":
         out = run_reference(args, rank, world)
     else:
         out = run_ours(args, rank, world, local_rank)

@@ -3,7 +3,8 @@
     python -m cushg_b200.build [--force]
 
 Every .cu under cushg_b200/csrc is compiled by nvcc for `arch=compute_100a,code=sm_100a`
-into an object under cushg_b200/_objs/ and linked into cushg_b200/libshg_b200.so.
+into an object under cushg_b200/_objs/ and linked into cushg_b200/libshg_b200.so; the
+command-line drop-in csrc/cli/cushg_main.cpp links against it as cushg_b200/cushg.
 Objects are rebuilt only when their sources or headers changed; independent objects
 compile in parallel.
 """
@@ -21,6 +22,8 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 OBJ = os.path.join(PKG, "_objs")
 LIB = os.path.join(PKG, "libshg_b200.so")
+CLI = os.path.join(PKG, "cushg")
+CLI_SRC = os.path.join(CSRC, "cli", "cushg_main.cpp")
 
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -60,8 +63,15 @@ def build(force: bool = False, verbose: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    if force or _stale(CLI, [CLI_SRC, LIB, os.path.join(ROOT, "include", "shg.h")]):
+        cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
+        cmd = [cxx, "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), CLI_SRC, "-o", CLI, "-L", PKG,
+               "-lshg_b200", "-Wl,-rpath,$ORIGIN"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"CLI build failed:\n{r.stdout}\n{r.stderr}")
     if verbose:
-        print("built", LIB)
+        print("built", LIB, "and", CLI)
     return LIB
 
 

@@ -52,7 +52,7 @@ cudaError_t fork_streams(int dev, ForkStreams** out) {
 }  // namespace
 
 shg_status plain_solve_device(const shg_params& p, const void* signal_in, void* pump_out, void* signal_out,
-                              shg_stats* stats, cudaStream_t stream) {
+                              shg_stats* stats, cudaStream_t stream, void* slices_p, void* slices_s) {
     const PlainVariant* v = find_plain_variant(p.precision, p.nx);
     if (!v) return fail(SHG_ERR_UNSUPPORTED, "no kernel for grid side %d", p.nx);
     InstDesc d = make_plain_desc(p, p.temp, p.temp);
@@ -60,6 +60,9 @@ shg_status plain_solve_device(const shg_params& p, const void* signal_in, void* 
     d.has_signal_in = signal_in ? 1 : 0;
     d.pump_out = pump_out;
     d.signal_out = signal_out;
+    d.slices_p = slices_p;
+    d.slices_s = slices_s;
+    d.nslices = (slices_p || slices_s) ? p.nz : 0;
     cudaError_t e;
     void* buf = nullptr;
     const size_t bytes = sizeof(InstDesc) + 2 * sizeof(double);

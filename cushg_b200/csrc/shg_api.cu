@@ -219,8 +219,9 @@ shg_status shg_solve_device(const shg_params* p, const void* signal_in_dev, void
     return plain_solve_device(*p, signal_in_dev, pump_out_dev, signal_out_dev, stats, stream);
 }
 
-shg_status shg_solve(const shg_params* p, const void* signal_in, void* pump_out, void* signal_out,
-                     void* temperature_out, shg_stats* stats) {
+// Host-buffer solve shared by shg_solve (last slice) and shg_solve_slices (every slice).
+static shg_status solve_host(const shg_params* p, const void* signal_in, void* pump_out, void* signal_out,
+                             void* temperature_out, shg_stats* stats, bool slices) {
     shg_status st = shg_check_params(p);
     if (st != SHG_OK) return st;
     int ndev = 0;
@@ -229,6 +230,7 @@ shg_status shg_solve(const shg_params* p, const void* signal_in, void* pump_out,
         return fail(SHG_ERR_NO_DEVICE, "no CUDA device visible");
     }
     const size_t plane = (size_t)p->nx * p->ny * complex_bytes(*p);
+    const size_t outb = slices ? plane * (size_t)p->nz : plane;
     const size_t tbytes = (size_t)p->nx * p->ny * p->nz * (p->precision == 32 ? 4 : 8);
     cudaStream_t s = nullptr;
     cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
@@ -237,8 +239,8 @@ shg_status shg_solve(const shg_params* p, const void* signal_in, void* pump_out,
     shg_status rc = SHG_OK;
     do {
         if (signal_in && (e = cudaMallocAsync(&din, plane, s)) != cudaSuccess) { rc = cuda_fail(e, "cudaMallocAsync"); break; }
-        if ((e = cudaMallocAsync(&dp, plane, s)) != cudaSuccess) { rc = cuda_fail(e, "cudaMallocAsync"); break; }
-        if ((e = cudaMallocAsync(&ds, plane, s)) != cudaSuccess) { rc = cuda_fail(e, "cudaMallocAsync"); break; }
+        if (pump_out && (e = cudaMallocAsync(&dp, outb, s)) != cudaSuccess) { rc = cuda_fail(e, "cudaMallocAsync"); break; }
+        if (signal_out && (e = cudaMallocAsync(&ds, outb, s)) != cudaSuccess) { rc = cuda_fail(e, "cudaMallocAsync"); break; }
         if (temperature_out && p->thermal && (e = cudaMallocAsync(&dT, tbytes, s)) != cudaSuccess) {
             rc = cuda_fail(e, "cudaMallocAsync");
             break;
@@ -247,13 +249,18 @@ shg_status shg_solve(const shg_params* p, const void* signal_in, void* pump_out,
             rc = cuda_fail(e, "cudaMemcpyAsync H2D");
             break;
         }
-        rc = shg_solve_device(p, din, dp, ds, dT, stats, s);
+        if (slices) {
+            rc = p->thermal ? thermal_solve_device(*p, din, nullptr, nullptr, dT, stats, s, dp, ds)
+                            : plain_solve_device(*p, din, nullptr, nullptr, stats, s, dp, ds);
+        } else {
+            rc = shg_solve_device(p, din, dp, ds, dT, stats, s);
+        }
         if (rc != SHG_OK) break;
-        if (pump_out && (e = cudaMemcpyAsync(pump_out, dp, plane, cudaMemcpyDeviceToHost, s)) != cudaSuccess) {
+        if (dp && (e = cudaMemcpyAsync(pump_out, dp, outb, cudaMemcpyDeviceToHost, s)) != cudaSuccess) {
             rc = cuda_fail(e, "cudaMemcpyAsync D2H");
             break;
         }
-        if (signal_out && (e = cudaMemcpyAsync(signal_out, ds, plane, cudaMemcpyDeviceToHost, s)) != cudaSuccess) {
+        if (ds && (e = cudaMemcpyAsync(signal_out, ds, outb, cudaMemcpyDeviceToHost, s)) != cudaSuccess) {
             rc = cuda_fail(e, "cudaMemcpyAsync D2H");
             break;
         }
@@ -270,6 +277,16 @@ shg_status shg_solve(const shg_params* p, const void* signal_in, void* pump_out,
     cudaStreamSynchronize(s);
     cudaStreamDestroy(s);
     return rc;
+}
+
+shg_status shg_solve(const shg_params* p, const void* signal_in, void* pump_out, void* signal_out,
+                     void* temperature_out, shg_stats* stats) {
+    return solve_host(p, signal_in, pump_out, signal_out, temperature_out, stats, false);
+}
+
+shg_status shg_solve_slices(const shg_params* p, const void* signal_in, void* pump_slices, void* signal_slices,
+                            void* temperature_out, shg_stats* stats) {
+    return solve_host(p, signal_in, pump_slices, signal_slices, temperature_out, stats, true);
 }
 
 shg_status shg_solve_batch_device(const shg_params* params, int32_t count, void* const* pump_out_dev,

@@ -32,7 +32,9 @@ struct InstDesc {
     void* signal_out;      // device, n*n complex or null
     double* power_out;     // device, [2] = {SH power, pump power} or null
     int32_t out_after;     // the outputs are the fields after this many steps
-    int32_t pad2;
+    int32_t nslices;       // number of planes in slices_p / slices_s (nz), 0 if none
+    void* slices_p;        // device, nslices*n*n complex: the fields before each step s
+    void* slices_s;        //   (the reference's save_only_last = false dump), or null
     // thermal pass only (Solver.h:33-55, Tfield.h:260-276); null / zero in plain runs.
     // 3D arrays of the working real type, index z*n*n + y*n + x.
     const void* t_np;      // n(λp, T) per voxel

@@ -207,6 +207,8 @@ __global__ void __launch_bounds__(NT, 1) ssfm_plain_kernel(const InstDesc* __res
         const double er = ex * cs, ei = ex * sn;
         Ps[sidx<N, R2, SW>(lr, x)] = mk<T>((T)(d.amp_re * er - d.amp_im * ei), (T)(d.amp_re * ei + d.amp_im * er));
         Ss[sidx<N, R2, SW>(lr, x)] = d.has_signal_in ? sin_g[(size_t)y * N + x] : mk<T>((T)0, (T)0);
+        if (d.slices_p) reinterpret_cast<V*>(d.slices_p)[(size_t)y * N + x] = Ps[sidx<N, R2, SW>(lr, x)];
+        if (d.slices_s) reinterpret_cast<V*>(d.slices_s)[(size_t)y * N + x] = Ss[sidx<N, R2, SW>(lr, x)];
     }
     __syncthreads();
 
@@ -266,6 +268,12 @@ __global__ void __launch_bounds__(NT, 1) ssfm_plain_kernel(const InstDesc* __res
                                 }
                             } else {
                                 rk4_point<T>(p, q, h ? cf_next : cf_prev, hap, has, qs, dz6);
+                            }
+                            if (h == 0 && s + 1 < d.nslices) {
+                                // per-slice record: the fields before step s+1 (Solver.h:289-295)
+                                const size_t gs = (size_t)(s + 1) * NN + g;
+                                if (d.slices_p) reinterpret_cast<V*>(d.slices_p)[gs] = p;
+                                if (d.slices_s) reinterpret_cast<V*>(d.slices_s)[gs] = q;
                             }
                             if (h == 0 && s + 1 == d.out_after) {
                                 if (d.pump_out) reinterpret_cast<V*>(d.pump_out)[g] = p;

@@ -27,7 +27,7 @@ namespace {
 
 template <typename R>
 shg_status thermal_run(const shg_params& p, const void* signal_in, void* pump_out, void* signal_out,
-                       void* temperature_out, shg_stats* stats, cudaStream_t s) {
+                       void* temperature_out, shg_stats* stats, cudaStream_t s, void* slices_p, void* slices_s) {
     const PlainVariant* v = find_plain_variant(p.precision, p.nx, 1);
     if (!v) return fail(SHG_ERR_UNSUPPORTED, "no thermal kernel for grid side %d", p.nx);
     const int n = p.nx, nz = p.nz;
@@ -137,6 +137,9 @@ shg_status thermal_run(const shg_params& p, const void* signal_in, void* pump_ou
             d.pump_out = pump_out;
             d.signal_out = signal_out;
             d.power_out = power;
+            d.slices_p = slices_p;
+            d.slices_s = slices_s;
+            d.nslices = (slices_p || slices_s) ? nz : 0;
             if ((e = cudaMemcpyAsync(ddesc, &d, sizeof(d), cudaMemcpyHostToDevice, s)) != cudaSuccess) {
                 rc = cuda_fail(e, "descriptor");
                 break;
@@ -182,9 +185,11 @@ shg_status thermal_run(const shg_params& p, const void* signal_in, void* pump_ou
 }  // namespace
 
 shg_status thermal_solve_device(const shg_params& p, const void* signal_in, void* pump_out, void* signal_out,
-                                void* temperature_out, shg_stats* stats, cudaStream_t stream) {
-    if (p.precision == 32) return thermal_run<float>(p, signal_in, pump_out, signal_out, temperature_out, stats, stream);
-    return thermal_run<double>(p, signal_in, pump_out, signal_out, temperature_out, stats, stream);
+                                void* temperature_out, shg_stats* stats, cudaStream_t stream, void* slices_p,
+                                void* slices_s) {
+    if (p.precision == 32)
+        return thermal_run<float>(p, signal_in, pump_out, signal_out, temperature_out, stats, stream, slices_p, slices_s);
+    return thermal_run<double>(p, signal_in, pump_out, signal_out, temperature_out, stats, stream, slices_p, slices_s);
 }
 
 }  // namespace shg

@@ -23,7 +23,7 @@ LIB_PATH = os.path.join(PKG, "libshg_b200.so")
 
 # every entry point declared in include/shg.h
 EXPORTS = (
-    "shg_default_params", "shg_check_params", "shg_steps", "shg_solve", "shg_solve_device",
+    "shg_default_params", "shg_check_params", "shg_steps", "shg_solve", "shg_solve_slices", "shg_solve_device",
     "shg_solve_batch_device", "shg_solve_batch_device_noalloc", "shg_last_error", "shg_status_string",
     "shg_version",
 )
@@ -57,6 +57,8 @@ def lib() -> ctypes.CDLL:
         L.shg_steps.restype = ctypes.c_int32
         L.shg_solve.argtypes = [P, vp, vp, vp, vp, ctypes.POINTER(ShgStats)]
         L.shg_solve.restype = ctypes.c_int
+        L.shg_solve_slices.argtypes = [P, vp, vp, vp, vp, ctypes.POINTER(ShgStats)]
+        L.shg_solve_slices.restype = ctypes.c_int
         L.shg_solve_device.argtypes = [P, vp, vp, vp, vp, ctypes.POINTER(ShgStats), vp]
         L.shg_solve_device.restype = ctypes.c_int
         L.shg_solve_batch_device.argtypes = [P, ctypes.c_int32, ctypes.POINTER(vp), ctypes.POINTER(vp),
@@ -109,6 +111,19 @@ def solve(p: ShgParams, signal_in: np.ndarray | None = None, want_temperature: b
     st = ShgStats()
     _check(lib().shg_solve(ctypes.byref(p), _ptr(sin), _ptr(pump), _ptr(sig), _ptr(T), ctypes.byref(st)))
     return Result(pump=pump, signal=sig, stats=st, temperature=T)
+
+
+def solve_slices(p: ShgParams, signal_in: np.ndarray | None = None, want_temperature: bool = False):
+    """One instance keeping every slice (shg_solve_slices): returns (pump[nz, ny, nx],
+    signal[nz, ny, nx], stats, T or None), plane s = the fields before step s."""
+    cdt = p.complex_dtype
+    pump = np.empty((p.nz, p.ny, p.nx), dtype=cdt)
+    sig = np.empty((p.nz, p.ny, p.nx), dtype=cdt)
+    T = np.empty((p.nz, p.ny, p.nx), dtype=p.real_dtype) if (want_temperature and p.thermal) else None
+    sin = None if signal_in is None else np.ascontiguousarray(np.asarray(signal_in, dtype=cdt).reshape(p.ny, p.nx))
+    st = ShgStats()
+    _check(lib().shg_solve_slices(ctypes.byref(p), _ptr(sin), _ptr(pump), _ptr(sig), _ptr(T), ctypes.byref(st)))
+    return pump, sig, st, T
 
 
 def run(power: float, waist: float, focalpoint: float, temp: float, t_inf: float, t_peltier: float,

@@ -139,6 +139,15 @@ SHG_API int32_t shg_steps(const shg_params* p);
 SHG_API shg_status shg_solve(const shg_params* p, const void* signal_in, void* pump_out,
                      void* signal_out, void* temperature_out, shg_stats* stats);
 
+/*
+ * Solve one instance and keep the fields of every slice: the save_only_last = false mode of
+ * Solver::run, which writes Pump_<s> / Signal_<s> before each step s (Solver.h:289-295).
+ * pump_slices, signal_slices: host buffers of nz planes of nx*ny complex each (plane s holds
+ * the fields before step s; plane nz-1 equals shg_solve's outputs), may be NULL.
+ */
+SHG_API shg_status shg_solve_slices(const shg_params* p, const void* signal_in, void* pump_slices,
+                                    void* signal_slices, void* temperature_out, shg_stats* stats);
+
 /* The same with device buffers on a caller stream (a cudaStream_t, NULL = legacy
  * default stream).  Plain runs are asynchronous; thermal runs synchronise at each
  * Jacobi convergence check.  stats, if given, is filled after a synchronise. */

@@ -89,8 +89,26 @@ CASES = {
 }
 
 
+def _timing_256(precision: int) -> P.ShgParams:
+    # 256 x 256, nz = 400, 20 mm, 30 W, w0 = 35 µm, focus at 0.4 L, 30 °C
+    return P.config_adjoint().replace(precision=precision)
+
+
+# Reference builds used only to time the reference program against this library
+# (oracle/time_reference.py); their outputs are not stored.
+TIMING_CASES = {
+    "time_f32_n256_nz400": {"precision": 32, "params": _d(_timing_256(32))},
+    "time_f64_n256_nz400": {"precision": 64, "params": _d(_timing_256(64))},
+    "time_thermal_c2": {"precision": 64, "params": _d(P.config_thermal_128().replace(
+        conv_rule=P.SHG_CONV_REFERENCE, jacobi_tol=0.0, check_every=5000, max_outer=5))},
+    "time_f32_n128_nz200": {"precision": 32, "params": _d(P.workload(128, 200, 20000.0, 20.0, 40.0, 10000.0, 40.0,
+                                                                       precision=32))},
+}
+
+
 def params_of(name: str) -> P.ShgParams:
     p = P.ShgParams()
-    for k, v in CASES[name]["params"].items():
+    src = CASES[name] if name in CASES else TIMING_CASES[name]
+    for k, v in src["params"].items():
         setattr(p, k, v)
     return p

@@ -36,7 +36,7 @@ REF_SRC = "/root/reference/src"
 OUT = os.path.join(HERE, "_ref")
 
 sys.path.insert(0, os.path.dirname(HERE))
-from oracle.golden_cases import CASES  # noqa: E402
+from oracle.golden_cases import CASES, TIMING_CASES  # noqa: E402
 
 
 def _sub(text: str, pattern: str, repl: str, count_expected: int | None = None, flags=0) -> str:
@@ -153,9 +153,10 @@ def main(argv: list[str]) -> int:
     if not os.path.isdir(REF_SRC):
         print("reference sources not present; nothing to build")
         return 0
-    names = argv[1:] or list(CASES)
+    allc = {**CASES, **TIMING_CASES}
+    names = argv[1:] or list(allc)
     for n in names:
-        exe = build_case(n, CASES[n])
+        exe = build_case(n, allc[n])
         print("built", exe)
     return 0
 

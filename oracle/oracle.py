@@ -38,6 +38,8 @@ def lib():
         vp = ctypes.c_void_p
         L.shgo_solve.argtypes = [P, vp, vp, vp, vp, ctypes.POINTER(ShgStats)]
         L.shgo_solve.restype = ctypes.c_int
+        L.shgo_solve_poling.argtypes = [P, vp, vp, vp, vp, vp, ctypes.POINTER(ShgStats)]
+        L.shgo_solve_poling.restype = ctypes.c_int
         L.shgo_march_plain_f64.argtypes = [P, ctypes.c_int, vp, vp]
         L.shgo_march_plain_f32.argtypes = [P, ctypes.c_int, vp, vp]
         L.shgo_batch_plain.argtypes = [P, ctypes.c_int, vp, vp, ctypes.c_int]
@@ -72,8 +74,10 @@ def max_threads() -> int:
     return int(lib().shgo_max_threads())
 
 
-def solve(p: ShgParams, signal_in: np.ndarray | None = None, want_temperature: bool = False):
-    """Whole run (plain or thermal).  Returns (pump, signal, stats, T or None)."""
+def solve(p: ShgParams, signal_in: np.ndarray | None = None, want_temperature: bool = False,
+          poling: np.ndarray | None = None):
+    """Whole run (plain or thermal).  Returns (pump, signal, stats, T or None).  poling: per-step
+    phase [rad] added to the mismatch phase (plain runs)."""
     cdt = p.complex_dtype
     n = p.points
     pump = np.zeros((p.ny, p.nx), dtype=cdt)
@@ -83,7 +87,9 @@ def solve(p: ShgParams, signal_in: np.ndarray | None = None, want_temperature: b
     if signal_in is not None:
         sin = np.ascontiguousarray(signal_in.astype(cdt).reshape(n))
     st = ShgStats()
-    rc = lib().shgo_solve(ctypes.byref(p), _ptr(sin), _ptr(pump), _ptr(sig), _ptr(T), ctypes.byref(st))
+    pol = None if poling is None else np.ascontiguousarray(np.asarray(poling, dtype=np.float64))
+    rc = lib().shgo_solve_poling(ctypes.byref(p), _ptr(sin), _ptr(pol), _ptr(pump), _ptr(sig), _ptr(T),
+                                 ctypes.byref(st))
     return rc, pump, sig, st, T
 
 

@@ -106,15 +106,22 @@ int shgo_max_threads(void) {
 #endif
 }
 
-/* Whole run, like shg_solve: precision selects the buffer element type. */
-int shgo_solve(const shg_params* p, const void* signal_in, void* pump_out, void* signal_out, void* T_out, shg_stats* st) {
+/* Whole run, like shg_solve: precision selects the buffer element type.  poling (plain
+ * runs only, may be NULL): a phase in rad added to the mismatch phase of every RK4 stage of
+ * step s, one value per step. */
+int shgo_solve_poling(const shg_params* p, const void* signal_in, const double* poling, void* pump_out, void* signal_out,
+                      void* T_out, shg_stats* st) {
     if (!p || p->nx != p->ny || p->nx < 4 || (p->nx & 1) || p->nz < 2 || p->nx > 1024) return SHG_ERR_INVALID;
     if (p->precision == 32) {
         return p->thermal ? solve_thermal_f32(p, (const float*)signal_in, (float*)pump_out, (float*)signal_out, (float*)T_out, st)
-                          : solve_plain_f32(p, (const float*)signal_in, (float*)pump_out, (float*)signal_out, st);
+                          : solve_plain_f32(p, (const float*)signal_in, poling, (float*)pump_out, (float*)signal_out, st);
     }
     return p->thermal ? solve_thermal_f64(p, (const double*)signal_in, (double*)pump_out, (double*)signal_out, (double*)T_out, st)
-                      : solve_plain_f64(p, (const double*)signal_in, (double*)pump_out, (double*)signal_out, st);
+                      : solve_plain_f64(p, (const double*)signal_in, poling, (double*)pump_out, (double*)signal_out, st);
+}
+
+int shgo_solve(const shg_params* p, const void* signal_in, void* pump_out, void* signal_out, void* T_out, shg_stats* st) {
+    return shgo_solve_poling(p, signal_in, NULL, pump_out, signal_out, T_out, st);
 }
 
 /* Plain march of `steps` SSFM steps from the given fields (in place), FP64.
@@ -124,7 +131,7 @@ int shgo_march_plain_f64(const shg_params* p, int steps, double* pump, double* s
     make_cfg_f64(p, &c);
     optics_f64 o;
     optics_init_f64(&o, &c, c.temp);
-    cwes_plain_f64(&c, &o, steps, (cpx_f64*)pump, (cpx_f64*)signal);
+    cwes_plain_f64(&c, &o, steps, NULL, (cpx_f64*)pump, (cpx_f64*)signal);
     optics_free_f64(&o);
     return SHG_OK;
 }
@@ -134,7 +141,7 @@ int shgo_march_plain_f32(const shg_params* p, int steps, float* pump, float* sig
     make_cfg_f32(p, &c);
     optics_f32 o;
     optics_init_f32(&o, &c, c.temp);
-    cwes_plain_f32(&c, &o, steps, (cpx_f32*)pump, (cpx_f32*)signal);
+    cwes_plain_f32(&c, &o, steps, NULL, (cpx_f32*)pump, (cpx_f32*)signal);
     optics_free_f32(&o);
     return SHG_OK;
 }
@@ -158,7 +165,7 @@ int shgo_batch_plain(const shg_params* ps, int count, const int* steps, double* 
             cpx_f32* S = (cpx_f32*)calloc(n, sizeof(cpx_f32));
             optics_f32 o; optics_init_f32(&o, &c, c.temp);
             set_pump_f32(&c, c.temp, P);
-            cwes_plain_f32(&c, &o, st, P, S);
+            cwes_plain_f32(&c, &o, st, NULL, P, S);
             if (sh_power) sh_power[i] = power_of_f32(&c, S, NULL, sellmeier_f32(c.ls, c.temp));
             optics_free_f32(&o); free(P); free(S);
         } else {
@@ -167,7 +174,7 @@ int shgo_batch_plain(const shg_params* ps, int count, const int* steps, double* 
             cpx_f64* S = (cpx_f64*)calloc(n, sizeof(cpx_f64));
             optics_f64 o; optics_init_f64(&o, &c, c.temp);
             set_pump_f64(&c, c.temp, P);
-            cwes_plain_f64(&c, &o, st, P, S);
+            cwes_plain_f64(&c, &o, st, NULL, P, S);
             if (sh_power) sh_power[i] = power_of_f64(&c, S, NULL, sellmeier_f64(c.ls, c.temp));
             optics_free_f64(&o); free(P); free(S);
         }

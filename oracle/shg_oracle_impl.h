@@ -274,12 +274,13 @@ static inline void SFX(rk4_point)(const SFX(cfg)* c, const SFX(pointc)* k, R phi
 }
 
 /* solverRK4 of a plain run (uniform T, Δk; Solver.h:231-259): the stage phase
- * is (z + dz*inc) * Δk with inc in {0, 0.25, 0.5}. */
-static void SFX(rk4_plain)(const SFX(cfg)* c, const SFX(pointc)* k, R dk, R z, CPX* P, CPX* S) {
+ * is (z + dz*inc) * Δk with inc in {0, 0.25, 0.5}, plus the step's poling phase (a
+ * per-slice phase of the QPM grating; zero in the reference, which has a uniform grating). */
+static void SFX(rk4_plain)(const SFX(cfg)* c, const SFX(pointc)* k, R dk, R z, R poling, CPX* P, CPX* S) {
     int n = c->nx * c->ny;
-    R phi0 = (z + c->dz * (R)0.0) * dk;
-    R phi1 = (z + c->dz * (R)0.25) * dk;
-    R phi2 = (z + c->dz * (R)0.5) * dk;
+    R phi0 = (z + c->dz * (R)0.0) * dk + poling;
+    R phi1 = (z + c->dz * (R)0.25) * dk + poling;
+    R phi2 = (z + c->dz * (R)0.5) * dk + poling;
 #pragma omp parallel for schedule(static) if (shgo_threads > 1) num_threads(shgo_threads)
     for (int i = 0; i < n; ++i) SFX(rk4_point)(c, k, phi0, phi1, phi2, &P[i], &S[i]);
 }
@@ -466,20 +467,20 @@ static void SFX(optics_init)(SFX(optics)* o, const SFX(cfg)* c, R Tc) {
 static void SFX(optics_free)(SFX(optics)* o) { SFX(fft_plan_free)(&o->pl); free(o->prop_p); free(o->prop_s); }
 
 /* One SSFM step of a plain run at position z. */
-static void SFX(ssfm_plain)(const SFX(optics)* o, const SFX(pointc)* k, R dk, R z, CPX* P, CPX* S) {
-    SFX(rk4_plain)(o->c, k, dk, z, P, S);
+static void SFX(ssfm_plain)(const SFX(optics)* o, const SFX(pointc)* k, R dk, R z, R poling, CPX* P, CPX* S) {
+    SFX(rk4_plain)(o->c, k, dk, z, poling, P, S);
     SFX(diffraction)(o->c, &o->pl, o->prop_p, P);
     SFX(diffraction)(o->c, &o->pl, o->prop_s, S);
-    SFX(rk4_plain)(o->c, k, dk, z, P, S);
+    SFX(rk4_plain)(o->c, k, dk, z, poling, P, S);
 }
 
 /* Plain CWES: nsteps steps from z = 0, z accumulated as z += dz (Solver.h:303). */
-static void SFX(cwes_plain)(const SFX(cfg)* c, const SFX(optics)* o, int nsteps, CPX* P, CPX* S) {
+static void SFX(cwes_plain)(const SFX(cfg)* c, const SFX(optics)* o, int nsteps, const double* poling, CPX* P, CPX* S) {
     SFX(pointc) k = SFX(point_consts)(c, SFX(sellmeier)(c->lp, c->temp), SFX(sellmeier)(c->ls, c->temp), 0);
     R dk = SFX(delta_k)(c, c->temp);
     R z = (R)0.0;
     for (int s = 0; s < nsteps; ++s) {
-        SFX(ssfm_plain)(o, &k, dk, z, P, S);
+        SFX(ssfm_plain)(o, &k, dk, z, poling ? (R)poling[s] : (R)0, P, S);
         z += c->dz;
     }
 }
@@ -493,7 +494,8 @@ static void SFX(init_signal)(CPX* S, const R* signal_in, size_t n) {
 }
 
 /* Plain run, Solver.h:376-383. */
-static int SFX(solve_plain)(const shg_params* p, const R* signal_in, R* pump_out, R* signal_out, shg_stats* st) {
+static int SFX(solve_plain)(const shg_params* p, const R* signal_in, const double* poling, R* pump_out, R* signal_out,
+                            shg_stats* st) {
     SFX(cfg) c;
     SFX(make_cfg)(p, &c);
     size_t n = (size_t)c.nx * c.ny;
@@ -505,7 +507,7 @@ static int SFX(solve_plain)(const shg_params* p, const R* signal_in, R* pump_out
     SFX(set_pump)(&c, c.temp, P);
     SFX(init_signal)(S, signal_in, n);
     int steps = c.nz - 1;
-    SFX(cwes_plain)(&c, &o, steps, P, S);
+    SFX(cwes_plain)(&c, &o, steps, poling, P, S);
     if (pump_out) memcpy(pump_out, P, sizeof(CPX) * n);
     if (signal_out) memcpy(signal_out, S, sizeof(CPX) * n);
     if (st) {

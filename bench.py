@@ -350,6 +350,35 @@ def run_thermal(args) -> dict:
     return out
 
 
+def run_adjoint(args) -> dict:
+    """Adjoint workload (outside the default sweep line): gradients of the SH power of the
+    256x256 / nz = 400 FP32 run (20 mm, 30 W, w0 = 35 µm, focus 0.4 L, 30 °C) with respect to
+    waist, focus, oven temperature and a 399-entry poling-phase vector drawn from N(0, 0.1 rad),
+    checkpoints every 20 steps; against the forward march alone."""
+    import torch
+    from cushg_b200 import shg
+
+    p = P.config_adjoint().replace(precision=args.precision)
+    pol = np.random.default_rng(0).normal(0.0, 0.1, size=p.nz - 1)
+    for _ in range(args.warmup):
+        shg.grad(p, pol, checkpoint_every=20)
+    g_ms = []
+    for _ in range(args.steps):
+        g = shg.grad(p, pol, checkpoint_every=20)
+        g_ms.append(g["device_ms"])
+    pump = torch.empty((p.ny, p.nx), dtype=torch.complex64 if p.precision == 32 else torch.complex128, device="cuda")
+    sig = torch.empty_like(pump)
+    f_ms = []
+    for _ in range(args.steps):
+        st = shg.solve_device(p, pump, sig)
+        f_ms.append(st.device_ms)
+    gm, fm = statistics.median(g_ms), statistics.median(f_ms)
+    return {"metric": "adjoint grads/s", "value": 1e3 / gm, "unit": "gradients/s", "workload":
+            "256x256 nz=400, 3 scalars + 399-vector, checkpoints every 20", "precision": p.precision,
+            "grad_ms": gm, "forward_ms": fm, "grad_over_forward": gm / fm, "sh_power_w": g["sh_power"],
+            "d_waist": g["d_waist"], "d_focus": g["d_focus"], "d_temp": g["d_temp"]}
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -361,7 +390,7 @@ def main() -> int:
     ap.add_argument("--class-side", type=int, default=0, help="profile case: one grid-size class only")
     ap.add_argument("--class-count", type=int, default=18)
     ap.add_argument("--class-nz", type=int, default=24)
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "thermal"])
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "thermal", "adjoint"])
     ap.add_argument("--thermal-side", type=int, default=0)
     ap.add_argument("--thermal-max-sweeps", type=int, default=0)
     args = ap.parse_args()
@@ -371,6 +400,8 @@ def main() -> int:
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.workload == "thermal":
         out = run_thermal(args) if rank == 0 else None
+    elif args.workload == "adjoint":
+        out = run_adjoint(args) if rank == 0 else None
     elif args.impl == "reference":
         out = run_reference(args, rank, world)
     else:

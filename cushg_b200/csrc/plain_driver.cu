@@ -52,7 +52,8 @@ cudaError_t fork_streams(int dev, ForkStreams** out) {
 }  // namespace
 
 shg_status plain_solve_device(const shg_params& p, const void* signal_in, void* pump_out, void* signal_out,
-                              shg_stats* stats, cudaStream_t stream, void* slices_p, void* slices_s) {
+                              shg_stats* stats, cudaStream_t stream, void* slices_p, void* slices_s,
+                              const double* poling_dev) {
     const PlainVariant* v = find_plain_variant(p.precision, p.nx);
     if (!v) return fail(SHG_ERR_UNSUPPORTED, "no kernel for grid side %d", p.nx);
     InstDesc d = make_plain_desc(p, p.temp, p.temp);
@@ -63,6 +64,7 @@ shg_status plain_solve_device(const shg_params& p, const void* signal_in, void* 
     d.slices_p = slices_p;
     d.slices_s = slices_s;
     d.nslices = (slices_p || slices_s) ? p.nz : 0;
+    d.poling = poling_dev;
     cudaError_t e;
     void* buf = nullptr;
     const size_t bytes = sizeof(InstDesc) + 2 * sizeof(double);

@@ -289,6 +289,40 @@ shg_status shg_solve_slices(const shg_params* p, const void* signal_in, void* pu
     return solve_host(p, signal_in, pump_slices, signal_slices, temperature_out, stats, true);
 }
 
+shg_status shg_sh_power(const shg_params* p, const double* poling, double* sh_power) {
+    shg_status st = shg_check_params(p);
+    if (st != SHG_OK) return st;
+    if (!sh_power) return fail(SHG_ERR_INVALID, "sh_power is NULL");
+    if (p->thermal) return fail(SHG_ERR_UNSUPPORTED, "shg_sh_power is for plain runs");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(SHG_ERR_NO_DEVICE, "no CUDA device visible");
+    }
+    const int nsteps = shg_steps(p);
+    cudaStream_t s = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
+    double* dpol = nullptr;
+    shg_status rc = SHG_OK;
+    do {
+        if (poling) {
+            if ((e = cudaMallocAsync((void**)&dpol, sizeof(double) * nsteps, s)) != cudaSuccess ||
+                (e = cudaMemcpyAsync(dpol, poling, sizeof(double) * nsteps, cudaMemcpyHostToDevice, s)) != cudaSuccess) {
+                rc = cuda_fail(e, "poling upload");
+                break;
+            }
+        }
+        shg_stats stats;
+        rc = plain_solve_device(*p, nullptr, nullptr, nullptr, &stats, s, nullptr, nullptr, dpol);
+        if (rc == SHG_OK) *sh_power = stats.sh_power;
+    } while (0);
+    if (dpol) cudaFreeAsync(dpol, s);
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+    return rc;
+}
+
 shg_status shg_solve_batch_device(const shg_params* params, int32_t count, void* const* pump_out_dev,
                                   void* const* signal_out_dev, double* sh_power_out, void* stream_) {
     clear_error();

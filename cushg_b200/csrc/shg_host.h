@@ -22,7 +22,7 @@ size_t complex_bytes(const shg_params& p);
 // plain runs (plain_driver.cu)
 shg_status plain_solve_device(const shg_params& p, const void* signal_in, void* pump_out, void* signal_out,
                               shg_stats* stats, cudaStream_t stream, void* slices_p = nullptr,
-                              void* slices_s = nullptr);
+                              void* slices_s = nullptr, const double* poling_dev = nullptr);
 shg_status plain_solve_batch(const shg_params* params, int count, void* const* pump_out, void* const* signal_out,
                              double* sh_power_out, cudaStream_t stream);
 

@@ -31,6 +31,7 @@ struct InstDesc {
     void* pump_out;        // device, n*n complex or null
     void* signal_out;      // device, n*n complex or null
     double* power_out;     // device, [2] = {SH power, pump power} or null
+    const double* poling;  // device, per-step poling phase [rad] added to the mismatch phase, or null
     int32_t out_after;     // the outputs are the fields after this many steps
     int32_t nslices;       // number of planes in slices_p / slices_s (nz), 0 if none
     void* slices_p;        // device, nslices*n*n complex: the fields before each step s

@@ -1,0 +1,579 @@
+// ssfm_adjoint.cuh — hand-written adjoint of the plain SSFM march: gradients of the SH output
+// power J = pw_s sum |S|^2 with respect to the beam waist, the focal position, the oven
+// temperature and a per-step poling-phase vector.  No counterpart in the reference, which
+// has no gradients; the forward model is the reference's scheme (Solver.h:189-308).
+//
+// Forward step s:  x_s --N_s--> a1 --L--> a2_s --N_s--> x_{s+1}   (N_s: the RK4 application
+// at z_s, L: diffraction).  Backward, with adjoints g = dJ/dRe + i dJ/dIm of the fields:
+//     mu2 = N_s^T(a2_s) lambda_{s+1},   mu1 = L^H mu2,   lambda_s = N_s^T(x_s) mu1
+// where N_s^T is the vector-Jacobian product of the RK4 scheme (stage values recomputed from
+// the input point) and L^H the diffraction with the conjugate propagator.
+//
+// One cluster owns the instance for the whole computation, with the same shared-memory
+// layout and transform passes as the forward march (ssfm_plain.cuh):
+//   1. forward march, keeping x_{mK} (checkpoints every K steps) in global memory;
+//   2. for each segment m from the last: re-march from x_{mK}, keeping a2_s and the
+//      propagated spectra of each step of the segment; then march the adjoint back through
+//      the segment; the adjoint fields are parked in global memory between segments.
+// Parameter sensitivities are accumulated on the way: the stage coefficients' dependence
+// on κ, Δk, the two-photon term and the poling phase (RK4 adjoint), the propagator phases'
+// dependence on n(T) (adjoint diffraction, with the stored spectra), and the initial pump's
+// dependence on waist, focus and T (central differences of the closed-form Gaussian).
+#pragma once
+
+#include "ssfm_plain.cuh"
+
+namespace shg {
+
+// accumulators (per CTA) of the adjoint
+enum {
+    kAccKp = 0,     // sum Re(conj(g_dP) t)          = κp dJ/dκp
+    kAccKs = 1,     // sum Re(conj(g_dS) u)          = κs dJ/dκs
+    kAccDk = 2,     // sum phase sensitivity (z + dz inc)   = dJ/dΔk
+    kAccQs = 3,     // sum Re(conj(g_dS) (-|S|^2 S)) = dJ/dqs
+    kAccPropP = 4,  // sum over steps, frequencies of Re(conj(Λ) i Y) q   (pump)
+    kAccPropS = 5,  //                                                 (SH)
+    kAccG0w = 6,    // Re <λ0_P, dP0/dwaist>
+    kAccG0f = 7,    // Re <λ0_P, dP0/dfocus>
+    kAccG0T = 8,    // Re <λ0_P, dP0/dT>
+    kAccJ = 9,      // sum |S_out|^2
+    kAdjAcc = 10
+};
+
+struct AdjDesc {
+    int32_t K;          // checkpoint interval (steps)
+    int32_t M;          // number of checkpoints (x_{mK}, m = 0..M-1)
+    void* ckpt;         // M x 2 x n*n complex (pump, SH) before step mK, natural layout
+    void* seg_a2;       // K x 2 x n*n: fields after the diffraction of each step of a segment
+    void* seg_y;        // K x 2 x n*n: propagated spectra of each step (CB order: fy*n + column)
+    void* lam;          // 2 x n*n: adjoint fields between segments
+    const double* zs;   // nsteps: z at the start of each step (the forward's accumulation)
+    double* part;       // [C][kAdjAcc] per-CTA accumulators
+    double* phi;        // [nsteps][C] per-CTA dJ/dφ_s
+    double pert[6][4];  // pump (amp_re, amp_im, den_re, den_im) at waist±hw, focus±hf, T±hT
+    double inv2h[3];    // 1 / (2 h) of those differences
+};
+
+// Vector-Jacobian product of dA/dz at (p, s) (see dadz): adds to (gp, gs) the adjoints of
+// the inputs given the adjoints (gdp, gds) of (dp, ds), and to sens[] the parameter terms
+// (sens[0] κp, [1] κs, [2] Δk (weight wz = z + dz inc), [3] qs, [4] poling phase).
+template <typename T>
+__device__ __forceinline__ void dadz_vjp(cx<T> p, cx<T> s, cx<T> cP, cx<T> cS, T hap, T has, T qs, cx<T> gdp,
+                                         cx<T> gds, cx<T>& gp, cx<T>& gs, double wz, double* sens) {
+    const cx<T> t = mul<T>(cP, mulc<T>(s, p));                   // cP s conj(p)
+    const cx<T> pp = mk<T>(p.x * p.x - p.y * p.y, (T)2 * p.x * p.y);
+    const cx<T> u = mul<T>(cS, pp);                               // cS p^2
+    const T a2 = s.x * s.x + s.y * s.y;
+    // g_p: -hap g_dP + cP s conj(g_dP) + conj(2 cS p) g_dS
+    const cx<T> a = mulc<T>(mul<T>(cP, s), gdp);
+    const cx<T> b = mulc<T>(gds, mul<T>(cS, p));
+    gp = mk<T>(gp.x - hap * gdp.x + a.x + (T)2 * b.x, gp.y - hap * gdp.y + a.y + (T)2 * b.y);
+    // g_s: conj(cP) p g_dP + (-has - 2 qs |s|^2) g_dS - qs s^2 conj(g_dS)
+    const cx<T> c = mul<T>(mulc<T>(p, cP), gdp);
+    const cx<T> ss = mk<T>(s.x * s.x - s.y * s.y, (T)2 * s.x * s.y);
+    const cx<T> e = mulc<T>(ss, gds);
+    const T h = -has - (T)2 * qs * a2;
+    gs = mk<T>(gs.x + c.x + h * gds.x - qs * e.x, gs.y + c.y + h * gds.y - qs * e.y);
+    const double ekp = (double)gdp.x * t.x + (double)gdp.y * t.y;
+    const double eks = (double)gds.x * u.x + (double)gds.y * u.y;
+    const double eph = ((double)gdp.x * t.y - (double)gdp.y * t.x) - ((double)gds.x * u.y - (double)gds.y * u.x);
+    const double eqs = -(double)a2 * ((double)gds.x * s.x + (double)gds.y * s.y);
+    sens[0] += ekp;
+    sens[1] += eks;
+    sens[2] += eph * wz;
+    sens[3] += eqs;
+    sens[4] += eph;
+}
+
+// Vector-Jacobian product of one RK4 application (rk4_point) at input (p, s) with stage
+// coefficients cf (phases at z, z + dz/4, z + dz/2): (gp, gs) holds the adjoint of the
+// output on entry and of the input on return.
+template <typename T>
+__device__ __forceinline__ void rk4_vjp(cx<T> p, cx<T> s, const cx<T>* cf, T hap, T has, T qs, T dz6, double z,
+                                        double dz, cx<T>& gp, cx<T>& gs, double* sens) {
+    using V = cx<T>;
+    V k1p, k1s, k2p, k2s, k3p, k3s, k4p, k4s;
+    dadz<T>(p, s, cf[0], cf[3], hap, has, qs, k1p, k1s);
+    const V u2p = mk<T>(p.x + (T)0.5 * k1p.x, p.y + (T)0.5 * k1p.y), u2s = mk<T>(s.x + (T)0.5 * k1s.x, s.y + (T)0.5 * k1s.y);
+    dadz<T>(u2p, u2s, cf[1], cf[4], hap, has, qs, k2p, k2s);
+    const V u3p = mk<T>(p.x + (T)0.5 * k2p.x, p.y + (T)0.5 * k2p.y), u3s = mk<T>(s.x + (T)0.5 * k2s.x, s.y + (T)0.5 * k2s.y);
+    dadz<T>(u3p, u3s, cf[1], cf[4], hap, has, qs, k3p, k3s);
+    const V u4p = add<T>(p, k3p), u4s = add<T>(s, k3s);
+    (void)k4p;
+    (void)k4s;
+    const V gop = gp, gos = gs;
+    V g3p = scale<T>(gop, (T)2 * dz6), g3s = scale<T>(gos, (T)2 * dz6);
+    V g2p = g3p, g2s = g3s;
+    V g1p = scale<T>(gop, dz6), g1s = scale<T>(gos, dz6);
+    V hp = mk<T>(0, 0), hs = mk<T>(0, 0);
+    dadz_vjp<T>(u4p, u4s, cf[2], cf[5], hap, has, qs, g1p, g1s, hp, hs, z + 0.5 * dz, sens);  // g_k4 = dz6 g
+    gp = add<T>(gop, hp);
+    gs = add<T>(gos, hs);
+    g3p = add<T>(g3p, hp);
+    g3s = add<T>(g3s, hs);
+    hp = mk<T>(0, 0);
+    hs = mk<T>(0, 0);
+    dadz_vjp<T>(u3p, u3s, cf[1], cf[4], hap, has, qs, g3p, g3s, hp, hs, z + 0.25 * dz, sens);
+    gp = add<T>(gp, hp);
+    gs = add<T>(gs, hs);
+    g2p = add<T>(g2p, scale<T>(hp, (T)0.5));
+    g2s = add<T>(g2s, scale<T>(hs, (T)0.5));
+    hp = mk<T>(0, 0);
+    hs = mk<T>(0, 0);
+    dadz_vjp<T>(u2p, u2s, cf[1], cf[4], hap, has, qs, g2p, g2s, hp, hs, z + 0.25 * dz, sens);
+    gp = add<T>(gp, hp);
+    gs = add<T>(gs, hs);
+    g1p = add<T>(g1p, scale<T>(hp, (T)0.5));
+    g1s = add<T>(g1s, scale<T>(hs, (T)0.5));
+    hp = mk<T>(0, 0);
+    hs = mk<T>(0, 0);
+    dadz_vjp<T>(p, s, cf[0], cf[3], hap, has, qs, g1p, g1s, hp, hs, z, sens);
+    gp = add<T>(gp, hp);
+    gs = add<T>(gs, hs);
+}
+
+template <typename T, int N, int C, int NT>
+__global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __restrict__ descs,
+                                                             const AdjDesc* __restrict__ adescs) {
+    using Cfg = PlainCfg<T, N, C, NT, false>;
+    constexpr int R2 = Cfg::R2, SW = Cfg::SW;
+    constexpr int JA = Cfg::JA, JB = Cfg::JB, JCA = Cfg::JCA, JCB = Cfg::JCB;
+    constexpr int CPR = 16 / C;
+    constexpr size_t NN = (size_t)N * N;
+    using V = cx<T>;
+    using W = mult<T>;
+
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* Ps = reinterpret_cast<V*>(smem_raw);
+    V* Ss = Ps + Cfg::PLANE;
+    V* coef = Ss + Cfg::PLANE;  // [2][6], by step parity
+    W* tw = reinterpret_cast<W*>(coef + 12);
+    W* pxp = tw + N;
+    W* pxs = pxp + N;
+    W* pyp = pxs + N;
+    W* pys = pyp + N;
+    double* red = reinterpret_cast<double*>(pys + N);  // [2*(NT/32)] + [4]
+
+    const int tid = threadIdx.x;
+    const int crank = (C > 1) ? (int)cg::this_cluster().block_rank() : 0;
+    const InstDesc d = descs[0];
+    const AdjDesc& a = *adescs;
+    const int nsteps = d.nsteps;
+    const int K = a.K;
+    const T hap = (T)d.hap, has = (T)d.has, qs = (T)d.qs, dz6 = (T)(d.dz / 6.0);
+    V* ckpt = reinterpret_cast<V*>(a.ckpt);
+    V* seg_a2 = reinterpret_cast<V*>(a.seg_a2);
+    V* seg_y = reinterpret_cast<V*>(a.seg_y);
+    V* lam = reinterpret_cast<V*>(a.lam);
+
+    auto cluster_sync = [&]() {
+        if constexpr (C > 1) cg::this_cluster().sync();
+        else __syncthreads();
+    };
+    auto cj = [](V v) { return mk<T>(v.x, -v.y); };
+
+    init_tables<T, N>(d, tw, pxp, pxs, pyp, pys, tid, NT);
+
+    double acc[kAdjAcc];
+#pragma unroll
+    for (int i = 0; i < kAdjAcc; ++i) acc[i] = 0.0;
+
+    // ---- plane transfers between shared memory and global (natural layout) ------------
+    auto load_planes = [&](const V* gp, const V* gs) {
+        for (int e = tid; e < Cfg::PLANE; e += NT) {
+            const int lr = e / N, x = e % N;
+            const size_t g = (size_t)(crank + C * lr) * N + x;
+            Ps[sidx<N, R2, SW>(lr, x)] = gp[g];
+            Ss[sidx<N, R2, SW>(lr, x)] = gs[g];
+        }
+    };
+    auto store_planes = [&](V* gp, V* gs) {
+        for (int e = tid; e < Cfg::PLANE; e += NT) {
+            const int lr = e / N, x = e % N;
+            const size_t g = (size_t)(crank + C * lr) * N + x;
+            gp[g] = Ps[sidx<N, R2, SW>(lr, x)];
+            gs[g] = Ss[sidx<N, R2, SW>(lr, x)];
+        }
+    };
+
+    // ---- transform passes (as in the forward march) -----------------------------------
+    // R2-point row stage of job (lr, n1): forward = DFT then twiddle; inverse =
+    // conj(DFT(conj(x) W)).
+    auto row_a = [&](V* F, int lr, int n1, bool inv) {
+        V v[R2];
+#pragma unroll
+        for (int k = 0; k < R2; ++k) v[k] = F[sidx<N, R2, SW>(lr, n1 + 16 * k)];
+        if (inv) {
+            v[0] = cj(v[0]);
+#pragma unroll
+            for (int k = 1; k < R2; ++k) v[k] = mulw(cj(v[k]), tw[k * 16 + n1]);
+        }
+        Dft<R2, -1, T>::run(v);
+        if (inv) {
+#pragma unroll
+            for (int k = 0; k < R2; ++k) v[k] = cj(v[k]);
+        } else {
+#pragma unroll
+            for (int k = 1; k < R2; ++k) v[k] = mulw(v[k], tw[k * 16 + n1]);
+        }
+#pragma unroll
+        for (int k = 0; k < R2; ++k) F[sidx<N, R2, SW>(lr, n1 + 16 * k)] = v[k];
+    };
+    auto pass_rb = [&](bool inv) {
+        for (int j = tid; j < JB; j += NT) {
+            const int k2 = j % R2, lr = j / R2;
+#pragma unroll 1
+            for (int f = 0; f < 2; ++f) {
+                V* F = f ? Ss : Ps;
+                V u[16];
+#pragma unroll
+                for (int n = 0; n < 16; ++n) {
+                    u[n] = F[sidx<N, R2, SW>(lr, n + 16 * k2)];
+                    if (inv) u[n] = cj(u[n]);
+                }
+                Dft<16, -1, T>::run(u);
+#pragma unroll
+                for (int n = 0; n < 16; ++n) F[sidx<N, R2, SW>(lr, n + 16 * k2)] = inv ? cj(u[n]) : u[n];
+            }
+        }
+    };
+    auto pass_ca = [&](bool inv) {
+        for (int j = tid; j < JCA; j += NT) {
+            const int x = j % N, n1l = j / N;
+            const int n1 = crank + C * n1l;
+#pragma unroll 1
+            for (int f = 0; f < 2; ++f) {
+                V* F = f ? Ss : Ps;
+                V v[R2];
+#pragma unroll
+                for (int k = 0; k < R2; ++k) v[k] = F[sidx<N, R2, SW>(n1l + CPR * k, x)];
+                if (inv) {
+                    v[0] = cj(v[0]);
+#pragma unroll
+                    for (int k = 1; k < R2; ++k) v[k] = mulw(cj(v[k]), tw[k * 16 + n1]);
+                }
+                Dft<R2, -1, T>::run(v);
+                if (inv) {
+#pragma unroll
+                    for (int k = 0; k < R2; ++k) v[k] = cj(v[k]);
+                } else {
+#pragma unroll
+                    for (int k = 1; k < R2; ++k) v[k] = mulw(v[k], tw[k * 16 + n1]);
+                }
+#pragma unroll
+                for (int k = 0; k < R2; ++k) F[sidx<N, R2, SW>(n1l + CPR * k, x)] = v[k];
+            }
+        }
+    };
+    // CB: forward (store the propagated spectrum of step slot `ys` when ys >= 0) or
+    // adjoint (conjugate propagator; accumulate the n(T) sensitivity with the stored spectrum)
+    auto pass_cb = [&](bool adjoint, int ys) {
+        V* rP[C];
+        V* rS[C];
+#pragma unroll
+        for (int r = 0; r < C; ++r) {
+            if constexpr (C > 1) {
+                rP[r] = cg::this_cluster().map_shared_rank(Ps, r);
+                rS[r] = cg::this_cluster().map_shared_rank(Ss, r);
+            } else {
+                rP[r] = Ps;
+                rS[r] = Ss;
+            }
+        }
+        for (int j = tid; j < JCB; j += NT) {
+            const int xl = j % (N / C), k2 = j / (N / C);
+            const int x = crank * (N / C) + xl;
+            const int fx = (x >> 4) + R2 * (x & 15);
+            const double sx = (double)(fx < N / 2 ? fx : fx - N);
+#pragma unroll 1
+            for (int f = 0; f < 2; ++f) {
+                V* const* R = f ? rS : rP;
+                const W px = f ? pxs[x] : pxp[x];
+                const W* py = f ? pys : pyp;
+                V* ybuf = (ys >= 0) ? seg_y + ((size_t)ys * 2 + f) * NN : nullptr;
+                V u[16];
+#pragma unroll
+                for (int n = 0; n < 16; ++n) u[n] = R[n % C][sidx<N, R2, SW>(n / C + CPR * k2, x)];
+#pragma unroll 1
+                for (int it = 0; it < 2; ++it) {
+                    if (it) {
+#pragma unroll
+                        for (int n = 0; n < 16; ++n) u[n] = cj(u[n]);
+                    }
+                    Dft<16, -1, T>::run(u);
+                    if (!it) {
+#pragma unroll
+                        for (int k1 = 0; k1 < 16; ++k1) {
+                            const int fy = k2 + R2 * k1;
+                            const size_t yo = (size_t)fy * N + x;
+                            if (!adjoint) {
+                                u[k1] = mulw(mulw(u[k1], py[fy]), px);
+                                if (ybuf) ybuf[yo] = u[k1];
+                            } else {
+                                // dJ/dθ_f = Re(conj(Λ) i Y): Λ = this spectrum / N^2, Y = stored D X,
+                                // stored as D X / N^2 -> Re(conj(u) i Ystored)
+                                const V yv = ybuf[yo];
+                                const double c = (double)u[k1].x * (-(double)yv.y) + (double)u[k1].y * (double)yv.x;
+                                const double sy = (double)(fy < N / 2 ? fy : fy - N);
+                                acc[f ? kAccPropS : kAccPropP] += c * (d.dfx * d.dfx * (sx * sx) + d.dfy * d.dfy * (sy * sy));
+                                // conjugate propagator: conj(py) conj(px), via conj(conj(u) py px)
+                                u[k1] = cj(mulw(mulw(cj(u[k1]), py[fy]), px));
+                            }
+                        }
+                    } else {
+#pragma unroll
+                        for (int n = 0; n < 16; ++n) u[n] = cj(u[n]);
+                    }
+                }
+#pragma unroll
+                for (int n = 0; n < 16; ++n) R[n % C][sidx<N, R2, SW>(n / C + CPR * k2, x)] = u[n];
+            }
+        }
+    };
+
+    auto coefs = [&](int s) {  // stage coefficients of step s into its parity slot
+        if (tid < 3) stage_coef<T>(d, s, a.zs[s], tid, coef + 6 * (s & 1));
+    };
+
+    // ---- forward march over steps [sb, se) from the fields in shared memory ------------
+    // ckpt_mode: keep x_{mK} (and x_sb) as checkpoints; seg_mode: keep a2_s and spectra of
+    // the segment and stop after a2_{se-1}.  With neither (the full march's end), the SH
+    // output becomes the adjoint seed lambda = (0, 2 pw_s S) and J is accumulated.
+    auto march = [&](int sb, int se, bool ckpt_mode, bool seg_mode) {
+        coefs(sb);
+        if (ckpt_mode && sb % K == 0) store_planes(ckpt + (size_t)(sb / K) * 2 * NN, ckpt + ((size_t)(sb / K) * 2 + 1) * NN);
+        __syncthreads();
+        // first half of step sb, forward row stage
+        for (int j = tid; j < JA; j += NT) {
+            const int n1 = j & 15, lr = j >> 4;
+#pragma unroll 1
+            for (int k = 0; k < R2; ++k) {
+                const int o = sidx<N, R2, SW>(lr, n1 + 16 * k);
+                V p = Ps[o], q = Ss[o];
+                rk4_point<T>(p, q, coef + 6 * (sb & 1), hap, has, qs, dz6);
+                Ps[o] = p;
+                Ss[o] = q;
+            }
+#pragma unroll 1
+            for (int f = 0; f < 2; ++f) row_a(f ? Ss : Ps, lr, n1, false);
+        }
+        __syncthreads();
+        for (int s = sb; s < se; ++s) {
+            pass_rb(false);
+            __syncthreads();
+            pass_ca(false);
+            cluster_sync();
+            if (s + 1 < nsteps) coefs(s + 1);
+            pass_cb(false, seg_mode ? s - sb : -1);
+            cluster_sync();
+            pass_ca(true);
+            __syncthreads();
+            pass_rb(true);
+            __syncthreads();
+            const bool last = (s + 1 == se);
+            for (int j = tid; j < JA; j += NT) {
+                const int n1 = j & 15, lr = j >> 4;
+#pragma unroll 1
+                for (int f = 0; f < 2; ++f) row_a(f ? Ss : Ps, lr, n1, true);
+#pragma unroll 1
+                for (int k = 0; k < R2; ++k) {
+                    const int x = n1 + 16 * k;
+                    const int o = sidx<N, R2, SW>(lr, x);
+                    const size_t g = (size_t)(crank + C * lr) * N + x;
+                    V p = Ps[o], q = Ss[o];
+                    if (seg_mode) {
+                        seg_a2[((size_t)(s - sb) * 2) * NN + g] = p;
+                        seg_a2[((size_t)(s - sb) * 2 + 1) * NN + g] = q;
+                        if (last) continue;
+                    }
+                    rk4_point<T>(p, q, coef + 6 * (s & 1), hap, has, qs, dz6);  // x_{s+1}
+                    if (s + 1 == nsteps) {
+                        // adjoint seed: J = pw_s sum |S|^2 -> g_S = 2 pw_s S, g_P = 0
+                        acc[kAccJ] += (double)q.x * q.x + (double)q.y * q.y;
+                        Ps[o] = mk<T>(0, 0);
+                        Ss[o] = mk<T>((T)(2.0 * d.pw_s * q.x), (T)(2.0 * d.pw_s * q.y));
+                        continue;
+                    }
+                    if (ckpt_mode && (s + 1) % K == 0) {
+                        ckpt[((size_t)((s + 1) / K) * 2) * NN + g] = p;
+                        ckpt[((size_t)((s + 1) / K) * 2 + 1) * NN + g] = q;
+                    }
+                    if (!last) rk4_point<T>(p, q, coef + 6 * ((s + 1) & 1), hap, has, qs, dz6);
+                    Ps[o] = p;
+                    Ss[o] = q;
+                }
+                if (!last && s + 1 < nsteps) {
+#pragma unroll 1
+                    for (int f = 0; f < 2; ++f) row_a(f ? Ss : Ps, lr, n1, false);
+                }
+            }
+            __syncthreads();
+        }
+    };
+
+    // ---- per-step poling sensitivity: block sum of each thread's part of Φ_s -------------
+    double* wred = red;  // [NT/32]
+    auto flush_phi = [&](int s, double v) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if ((tid & 31) == 0) wred[tid >> 5] = v;
+        __syncthreads();
+        if (tid == 0) {
+            double t = 0.0;
+            for (int w = 0; w < NT / 32; ++w) t += wred[w];
+            a.phi[(size_t)s * C + crank] = t;
+        }
+        __syncthreads();
+    };
+    auto add_sens = [&](const double* sn) {
+        acc[kAccKp] += sn[0];
+        acc[kAccKs] += sn[1];
+        acc[kAccDk] += sn[2];
+        acc[kAccQs] += sn[3];
+    };
+
+    // ---- adjoint march back over [sb, se) from lambda_se in shared memory ---------------
+    auto backward = [&](int sb, int se) {
+        coefs(se - 1);
+        __syncthreads();
+        double phi_cur = 0.0;  // this thread's part of Φ_s for the step being finished
+        // mu2_{se-1} = N^T(a2_{se-1}) lambda_se, then the forward row stage
+        for (int j = tid; j < JA; j += NT) {
+            const int n1 = j & 15, lr = j >> 4;
+#pragma unroll 1
+            for (int k = 0; k < R2; ++k) {
+                const int x = n1 + 16 * k;
+                const int o = sidx<N, R2, SW>(lr, x);
+                const size_t g = (size_t)(crank + C * lr) * N + x;
+                const size_t sl = (size_t)(se - 1 - sb) * 2;
+                V gp = Ps[o], gs = Ss[o];
+                double sn[5] = {0, 0, 0, 0, 0};
+                rk4_vjp<T>(seg_a2[sl * NN + g], seg_a2[(sl + 1) * NN + g], coef + 6 * ((se - 1) & 1), hap, has, qs, dz6,
+                           a.zs[se - 1], d.dz, gp, gs, sn);
+                add_sens(sn);
+                phi_cur += sn[4];
+                Ps[o] = gp;
+                Ss[o] = gs;
+            }
+#pragma unroll 1
+            for (int f = 0; f < 2; ++f) row_a(f ? Ss : Ps, lr, n1, false);
+        }
+        __syncthreads();
+        for (int s = se - 1; s >= sb; --s) {
+            pass_rb(false);
+            __syncthreads();
+            pass_ca(false);
+            cluster_sync();
+            if (s > sb) coefs(s - 1);
+            pass_cb(true, s - sb);
+            cluster_sync();
+            pass_ca(true);
+            __syncthreads();
+            pass_rb(true);
+            __syncthreads();
+            double phi_prev = 0.0;  // this thread's part of Φ_{s-1} (from a2_{s-1})
+            for (int j = tid; j < JA; j += NT) {
+                const int n1 = j & 15, lr = j >> 4;
+#pragma unroll 1
+                for (int f = 0; f < 2; ++f) row_a(f ? Ss : Ps, lr, n1, true);
+#pragma unroll 1
+                for (int k = 0; k < R2; ++k) {
+                    const int x = n1 + 16 * k;
+                    const int o = sidx<N, R2, SW>(lr, x);
+                    const size_t g = (size_t)(crank + C * lr) * N + x;
+                    V gp = Ps[o], gs = Ss[o];
+                    // x_s: the checkpoint at the segment start, else N_{s-1}(a2_{s-1})
+                    V xp, xs, bp = mk<T>(0, 0), bs = mk<T>(0, 0);
+                    if (s == sb) {
+                        xp = ckpt[((size_t)(sb / K) * 2) * NN + g];
+                        xs = ckpt[((size_t)(sb / K) * 2 + 1) * NN + g];
+                    } else {
+                        const size_t sl = (size_t)(s - 1 - sb) * 2;
+                        bp = seg_a2[sl * NN + g];
+                        bs = seg_a2[(sl + 1) * NN + g];
+                        xp = bp;
+                        xs = bs;
+                        rk4_point<T>(xp, xs, coef + 6 * ((s - 1) & 1), hap, has, qs, dz6);
+                    }
+                    double sn[5] = {0, 0, 0, 0, 0};
+                    rk4_vjp<T>(xp, xs, coef + 6 * (s & 1), hap, has, qs, dz6, a.zs[s], d.dz, gp, gs, sn);
+                    add_sens(sn);
+                    phi_cur += sn[4];
+                    if (s > sb) {
+                        // step s-1's second application: mu2_{s-1} = N^T(a2_{s-1}) lambda_s
+                        double sn2[5] = {0, 0, 0, 0, 0};
+                        rk4_vjp<T>(bp, bs, coef + 6 * ((s - 1) & 1), hap, has, qs, dz6, a.zs[s - 1], d.dz, gp, gs, sn2);
+                        add_sens(sn2);
+                        phi_prev += sn2[4];
+                    }
+                    Ps[o] = gp;
+                    Ss[o] = gs;
+                }
+                if (s > sb) {
+#pragma unroll 1
+                    for (int f = 0; f < 2; ++f) row_a(f ? Ss : Ps, lr, n1, false);
+                }
+            }
+            __syncthreads();
+            flush_phi(s, phi_cur);
+            phi_cur = phi_prev;
+        }
+    };
+
+    // ============================ the computation ======================================
+    // x_0: the pump of setPump, SH = 0
+    for (int e = tid; e < Cfg::PLANE; e += NT) {
+        const int lr = e / N, x = e % N;
+        const double2 pv = pump_value(d, x, crank + C * lr, d.amp_re, d.amp_im, d.den_re, d.den_im);
+        Ps[sidx<N, R2, SW>(lr, x)] = mk<T>((T)pv.x, (T)pv.y);
+        Ss[sidx<N, R2, SW>(lr, x)] = mk<T>((T)0, (T)0);
+    }
+    __syncthreads();
+    march(0, nsteps, true, false);  // smem: lambda_nsteps
+    store_planes(lam, lam + NN);
+    for (int m = a.M - 1; m >= 0; --m) {
+        const int sb = m * K, se = min(sb + K, nsteps);
+        __syncthreads();
+        load_planes(ckpt + (size_t)m * 2 * NN, ckpt + ((size_t)m * 2 + 1) * NN);
+        __syncthreads();
+        march(sb, se, false, true);
+        cluster_sync();
+        load_planes(lam, lam + NN);
+        __syncthreads();
+        backward(sb, se);
+        store_planes(lam, lam + NN);
+    }
+    __syncthreads();
+    // dJ/dθ of the initial pump: Re <λ0_P, dP0/dθ>, dP0/dθ by central differences of the
+    // closed form (waist, focus, T)
+    for (int e = tid; e < Cfg::PLANE; e += NT) {
+        const int lr = e / N, x = e % N, y = crank + C * lr;
+        const V l0 = Ps[sidx<N, R2, SW>(lr, x)];
+#pragma unroll 1
+        for (int q = 0; q < 3; ++q) {
+            const double2 pp = pump_value(d, x, y, a.pert[2 * q][0], a.pert[2 * q][1], a.pert[2 * q][2], a.pert[2 * q][3]);
+            const double2 pm =
+                pump_value(d, x, y, a.pert[2 * q + 1][0], a.pert[2 * q + 1][1], a.pert[2 * q + 1][2], a.pert[2 * q + 1][3]);
+            const double dre = (pp.x - pm.x) * a.inv2h[q], dim = (pp.y - pm.y) * a.inv2h[q];
+            acc[kAccG0w + q] += (double)l0.x * dre + (double)l0.y * dim;
+        }
+    }
+    // per-CTA accumulators, block-reduced in a fixed order
+#pragma unroll 1
+    for (int i = 0; i < kAdjAcc; ++i) {
+        double v = acc[i];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if ((tid & 31) == 0) wred[tid >> 5] = v;
+        __syncthreads();
+        if (tid == 0) {
+            double t = 0.0;
+            for (int w = 0; w < NT / 32; ++w) t += wred[w];
+            a.part[(size_t)crank * kAdjAcc + i] = t;
+        }
+        __syncthreads();
+    }
+    cluster_sync();
+}
+
+}  // namespace shg

@@ -103,17 +103,65 @@ __device__ __forceinline__ void rk4_point(cx<T>& P, cx<T>& S, const cx<T>* cf, T
     S = mk<T>(s.x + as.x * dz6, s.y + as.y * dz6);
 }
 
-// stage coefficients of the plain dAdz at position z: phases (z + dz*{0, 1/4, 1/2}) Δk,
-// computed in FP64 (Solver.h:68-74 with increment 0.5*{0, 0.5, 1})
+// stage coefficients of the plain dAdz of step s at position z: phases (z + dz*{0, 1/4,
+// 1/2}) Δk (Solver.h:68-74 with increment 0.5*{0, 0.5, 1}) plus the step's poling phase,
+// computed in FP64
 template <typename T>
-__device__ __forceinline__ void stage_coef(const InstDesc& d, double z, int j, cx<T>* cf) {
+__device__ __forceinline__ void stage_coef(const InstDesc& d, int s, double z, int j, cx<T>* cf) {
     const double inc = j == 0 ? 0.0 : (j == 1 ? 0.25 : 0.5);
-    const double phi = (z + d.dz * inc) * d.dk;
+    const double phi = (z + d.dz * inc) * d.dk + (d.poling ? d.poling[s] : 0.0);
     double sn, cs;
     sincos(phi, &sn, &cs);
     // i κ e^{-iφ} = κ (sin φ, cos φ);  i κ e^{+iφ} = κ (-sin φ, cos φ)
     cf[j] = mk<T>((T)(d.kap_p * sn), (T)(d.kap_p * cs));
     cf[3 + j] = mk<T>((T)(-d.kap_s * sn), (T)(d.kap_s * cs));
+}
+
+// Multiplier tables of one instance: twiddles tw[k*16 + n1] = W_N^{n1 k}; the x factors of
+// the pump / SH propagators by physical column position (frequency perm(j) = (j>>4) +
+// R2*(j&15)); the y factors by frequency with the 1/(NX*NY) of the inverse FFT folded in.
+// Propagator phase θ = -dz (a (dfx^2 sx^2 + dfy^2 sy^2) + b sx) (Efields.h:122-141) with the
+// fftshift of Efields.h:32-81 expressed through signed frequency indices.
+template <typename T, int N>
+__device__ __forceinline__ void init_tables(const InstDesc& d, mult<T>* tw, mult<T>* pxp, mult<T>* pxs, mult<T>* pyp,
+                                            mult<T>* pys, int tid, int nt) {
+    constexpr int R2 = N / 16;
+    for (int j = tid; j < N; j += nt) {
+        double sn, cs;
+        sincospi(-2.0 * (double)((j & 15) * (j >> 4)) / (double)N, &sn, &cs);
+        tw[j] = make_mult<T>(cs, sn);
+        const int fx = (j >> 4) + R2 * (j & 15);
+        const double sx = (double)(fx < N / 2 ? fx : fx - N);
+        const double thxp = -d.dz * (d.a_p * (d.dfx * d.dfx * (sx * sx)) + d.b_p * sx);
+        const double thxs = -d.dz * (d.a_s * (d.dfx * d.dfx * (sx * sx)) + d.b_s * sx);
+        sincos(thxp, &sn, &cs);
+        pxp[j] = make_mult<T>(cs, sn);
+        sincos(thxs, &sn, &cs);
+        pxs[j] = make_mult<T>(cs, sn);
+        const double sy = (double)(j < N / 2 ? j : j - N);
+        const double inv = 1.0 / ((double)N * (double)N);
+        const double thyp = -d.dz * (d.a_p * (d.dfy * d.dfy * (sy * sy)));
+        const double thys = -d.dz * (d.a_s * (d.dfy * d.dfy * (sy * sy)));
+        sincos(thyp, &sn, &cs);
+        pyp[j] = make_mult<T>(cs * inv, sn * inv);
+        sincos(thys, &sn, &cs);
+        pys[j] = make_mult<T>(cs * inv, sn * inv);
+    }
+}
+
+// Focused Gaussian pump at grid point (x, y), setPump (Efields.h:84-119):
+// (Ap0 / MX) exp(-(((x - uX) dx)^2 + ((y - uY) dy)^2) / (wX2 MX)), in FP64.
+__device__ __forceinline__ double2 pump_value(const InstDesc& d, int x, int y, double amp_re, double amp_im,
+                                              double den_re, double den_im) {
+    const double ax = ((double)x - d.ux) * d.dx, ay = ((double)y - d.uy) * d.dy;
+    const double num = -(ax * ax) - (ay * ay);
+    const double dd = den_re * den_re + den_im * den_im;
+    const double are = (num * den_re) / dd, aim = (-num * den_im) / dd;
+    const double ex = exp(are);
+    double sn, cs;
+    sincos(aim, &sn, &cs);
+    const double er = ex * cs, ei = ex * sn;
+    return make_double2(amp_re * er - amp_im * ei, amp_re * ei + amp_im * er);
 }
 
 // Thermal stage coefficients at one voxel (Solver.h:33-55): κ = kf / n(λ, T(x,y,s)) and the
@@ -167,45 +215,16 @@ __global__ void __launch_bounds__(NT, 1) ssfm_plain_kernel(const InstDesc* __res
     };
 
     // ---- tables -----------------------------------------------------------------
-    for (int j = tid; j < N; j += NT) {
-        double sn, cs;
-        sincospi(-2.0 * (double)((j & 15) * (j >> 4)) / (double)N, &sn, &cs);
-        tw[j] = make_mult<T>(cs, sn);
-        // x factor at physical column position j: frequency perm(j) = (j>>4) + R2*(j&15)
-        const int fx = (j >> 4) + R2 * (j & 15);
-        const double sx = (double)(fx < N / 2 ? fx : fx - N);
-        const double thxp = -d.dz * (d.a_p * (d.dfx * d.dfx * (sx * sx)) + d.b_p * sx);
-        const double thxs = -d.dz * (d.a_s * (d.dfx * d.dfx * (sx * sx)) + d.b_s * sx);
-        sincos(thxp, &sn, &cs);
-        pxp[j] = make_mult<T>(cs, sn);
-        sincos(thxs, &sn, &cs);
-        pxs[j] = make_mult<T>(cs, sn);
-        // y factor at frequency j, with the 1/(NX*NY) of the inverse FFT folded in
-        const double sy = (double)(j < N / 2 ? j : j - N);
-        const double inv = 1.0 / ((double)N * (double)N);
-        const double thyp = -d.dz * (d.a_p * (d.dfy * d.dfy * (sy * sy)));
-        const double thys = -d.dz * (d.a_s * (d.dfy * d.dfy * (sy * sy)));
-        sincos(thyp, &sn, &cs);
-        pyp[j] = make_mult<T>(cs * inv, sn * inv);
-        sincos(thys, &sn, &cs);
-        pys[j] = make_mult<T>(cs * inv, sn * inv);
-    }
-    if (!THERM && tid < 3) stage_coef<T>(d, 0.0, tid, coef);
+    init_tables<T, N>(d, tw, pxp, pxs, pyp, pys, tid, NT);
+    if (!THERM && tid < 3) stage_coef<T>(d, 0, 0.0, tid, coef);
 
     // ---- initial fields: setPump (Efields.h:84-119), SH = 0 or given ---------------
     const V* sin_g = reinterpret_cast<const V*>(d.signal_in);
     for (int e = tid; e < Cfg::PLANE; e += NT) {
         const int lr = e / N, x = e % N;
         const int y = crank + C * lr;
-        const double ax = ((double)x - d.ux) * d.dx, ay = ((double)y - d.uy) * d.dy;
-        const double num = -(ax * ax) - (ay * ay);
-        const double dd = d.den_re * d.den_re + d.den_im * d.den_im;
-        const double are = (num * d.den_re) / dd, aim = (-num * d.den_im) / dd;
-        const double ex = exp(are);
-        double sn, cs;
-        sincos(aim, &sn, &cs);
-        const double er = ex * cs, ei = ex * sn;
-        Ps[sidx<N, R2, SW>(lr, x)] = mk<T>((T)(d.amp_re * er - d.amp_im * ei), (T)(d.amp_re * ei + d.amp_im * er));
+        const double2 pv = pump_value(d, x, y, d.amp_re, d.amp_im, d.den_re, d.den_im);
+        Ps[sidx<N, R2, SW>(lr, x)] = mk<T>((T)pv.x, (T)pv.y);
         Ss[sidx<N, R2, SW>(lr, x)] = d.has_signal_in ? sin_g[(size_t)y * N + x] : mk<T>((T)0, (T)0);
         if (d.slices_p) reinterpret_cast<V*>(d.slices_p)[(size_t)y * N + x] = Ps[sidx<N, R2, SW>(lr, x)];
         if (d.slices_s) reinterpret_cast<V*>(d.slices_s)[(size_t)y * N + x] = Ss[sidx<N, R2, SW>(lr, x)];
@@ -427,7 +446,7 @@ __global__ void __launch_bounds__(NT, 1) ssfm_plain_kernel(const InstDesc* __res
         __syncthreads();
         pass_ca(false);
         cluster_sync();
-        if (!THERM && tid < 3 && s + 1 < nsteps) stage_coef<T>(d, z + d.dz, tid, cf_nxt);
+        if (!THERM && tid < 3 && s + 1 < nsteps) stage_coef<T>(d, s + 1, z + d.dz, tid, cf_nxt);
         pass_cb();
         cluster_sync();
         pass_ca(true);

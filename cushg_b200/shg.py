@@ -24,9 +24,19 @@ LIB_PATH = os.path.join(PKG, "libshg_b200.so")
 # every entry point declared in include/shg.h
 EXPORTS = (
     "shg_default_params", "shg_check_params", "shg_steps", "shg_solve", "shg_solve_slices", "shg_solve_device",
-    "shg_solve_batch_device", "shg_solve_batch_device_noalloc", "shg_last_error", "shg_status_string",
-    "shg_version",
+    "shg_solve_batch_device", "shg_solve_batch_device_noalloc", "shg_grad", "shg_sh_power", "shg_last_error",
+    "shg_status_string", "shg_version",
 )
+
+
+class ShgGradResult(ctypes.Structure):
+    """``shg_grad_result`` of include/shg.h."""
+
+    _fields_ = [
+        ("sh_power", ctypes.c_double), ("d_waist", ctypes.c_double), ("d_focus", ctypes.c_double),
+        ("d_temp", ctypes.c_double), ("d_poling", ctypes.POINTER(ctypes.c_double)), ("device_ms", ctypes.c_double),
+        ("checkpoint_every", ctypes.c_int32), ("steps", ctypes.c_int32), ("reserved", ctypes.c_double * 4),
+    ]
 
 
 class ShgError(RuntimeError):
@@ -66,6 +76,10 @@ def lib() -> ctypes.CDLL:
         L.shg_solve_batch_device.restype = ctypes.c_int
         L.shg_solve_batch_device_noalloc.argtypes = L.shg_solve_batch_device.argtypes
         L.shg_solve_batch_device_noalloc.restype = ctypes.c_int
+        L.shg_grad.argtypes = [P, ctypes.POINTER(ctypes.c_double), ctypes.c_int32, ctypes.POINTER(ShgGradResult)]
+        L.shg_grad.restype = ctypes.c_int
+        L.shg_sh_power.argtypes = [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+        L.shg_sh_power.restype = ctypes.c_int
         L.shg_last_error.restype = ctypes.c_char_p
         L.shg_status_string.argtypes = [ctypes.c_int32]
         L.shg_status_string.restype = ctypes.c_char_p
@@ -167,6 +181,33 @@ def solve_batch_device(ps: list[ShgParams], pump_outs=None, signal_outs=None, st
     s = None if stream is None else vp(stream)
     _check(lib().shg_solve_batch_device(arr, n, ptrs(pump_outs), ptrs(signal_outs), pp, s))
     return power
+
+
+def _dptr(a):
+    return None if a is None else a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def grad(p: ShgParams, poling: np.ndarray | None = None, checkpoint_every: int = 0) -> dict:
+    """Gradients of the SH output power by the adjoint march (shg_grad): returns a dict with
+    sh_power, d_waist, d_focus, d_temp, d_poling (array of shg_steps values), device_ms."""
+    n = steps(p)
+    pol = None if poling is None else np.ascontiguousarray(np.asarray(poling, dtype=np.float64))
+    if pol is not None and pol.shape != (n,):
+        raise ValueError(f"poling must have {n} values")
+    dpol = np.zeros(n, dtype=np.float64)
+    r = ShgGradResult()
+    r.d_poling = _dptr(dpol)
+    _check(lib().shg_grad(ctypes.byref(p), _dptr(pol), int(checkpoint_every), ctypes.byref(r)))
+    return {"sh_power": r.sh_power, "d_waist": r.d_waist, "d_focus": r.d_focus, "d_temp": r.d_temp,
+            "d_poling": dpol, "device_ms": r.device_ms, "checkpoint_every": r.checkpoint_every, "steps": r.steps}
+
+
+def sh_power(p: ShgParams, poling: np.ndarray | None = None) -> float:
+    """SH output power of a plain run with an optional per-step poling phase (shg_sh_power)."""
+    pol = None if poling is None else np.ascontiguousarray(np.asarray(poling, dtype=np.float64))
+    out = ctypes.c_double(0.0)
+    _check(lib().shg_sh_power(ctypes.byref(p), _dptr(pol), ctypes.byref(out)))
+    return float(out.value)
 
 
 NOALLOC_MAX_INSTANCES = 64

@@ -183,6 +183,34 @@ SHG_API shg_status shg_solve_batch_device_noalloc(const shg_params* params, int3
                                                   void* const* pump_out_dev, void* const* signal_out_dev,
                                                   double* sh_power_out, void* stream);
 
+/* Gradients of the SH output power (plain runs), from shg_grad. */
+typedef struct shg_grad_result {
+    double sh_power;          /* J = SH output power [W] */
+    double d_waist;           /* dJ/dwaist [W/µm] */
+    double d_focus;           /* dJ/dfocus [W/µm] */
+    double d_temp;            /* dJ/dtemp [W/K]: the oven temperature of a plain run (n, Δk, pump, propagators) */
+    double* d_poling;         /* caller array of shg_steps(p) values dJ/dφ_s [W/rad], or NULL */
+    double device_ms;         /* device time of the forward + adjoint march */
+    int32_t checkpoint_every; /* checkpoint interval used (steps) */
+    int32_t steps;            /* steps marched */
+    double reserved[4];
+} shg_grad_result;
+
+/*
+ * Gradient of the SH output power of a plain run by the adjoint of the SSFM march.  No
+ * counterpart in the reference (which computes no power and no gradients); the forward
+ * model is the reference's scheme.  poling: NULL or shg_steps(p) phases [rad], a per-step
+ * phase of the QPM grating added to the mismatch phase of that step's RK4 stages (zero for
+ * the reference's uniform grating).  checkpoint_every: fields are kept every that many steps
+ * and re-marched in between (<= 0: about sqrt(steps)).  Host buffers, synchronous.
+ */
+SHG_API shg_status shg_grad(const shg_params* p, const double* poling, int32_t checkpoint_every,
+                            shg_grad_result* out);
+
+/* SH output power of a plain run with an optional per-step poling phase (as shg_grad),
+ * forward only.  Host, synchronous. */
+SHG_API shg_status shg_sh_power(const shg_params* p, const double* poling, double* sh_power);
+
 /* Message of the last failing call on this thread ("" if none). */
 SHG_API const char* shg_last_error(void);
 SHG_API const char* shg_status_string(int32_t status);

@@ -1,0 +1,82 @@
+"""Adjoint gradients of the SH output power (shg_grad) against central finite differences of
+the forward march, in FP64, and FP32 against FP64.
+
+The forward model with a per-step poling phase is first checked against the oracle; the
+gradients must match central differences to 1e-5 relative (FP64) and the FP32 adjoint the
+FP64 adjoint to 1e-3 (relative to each gradient's scale)."""
+import numpy as np
+import pytest
+
+from cushg_b200 import params as P
+from cushg_b200 import shg
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def case(n=64, nz=31, precision=64):
+    p = P.workload(n, nz, 10000.0, 20.0, 28.0, 4000.0, 27.5, precision=precision)
+    p.lx = p.ly = 12 * 28.0
+    return p
+
+
+def poling_vector(p, seed=3, sigma=0.1):
+    return np.random.default_rng(seed).normal(0.0, sigma, size=p.nz - 1)
+
+
+def test_forward_with_poling_matches_oracle():
+    p = case()
+    pol = poling_vector(p)
+    j = shg.sh_power(p, pol)
+    rc, pump, sig, st, _ = O.solve(p, poling=pol)
+    assert rc == 0
+    assert abs(j - st.sh_power) / st.sh_power <= 1e-12
+    # and the poling phase matters
+    assert abs(j - shg.sh_power(p)) / j > 1e-4
+
+
+def fd(f, x, h):
+    return (f(x + h) - f(x - h)) / (2 * h)
+
+
+@pytest.mark.parametrize("n", [64, 128])
+def test_fp64_adjoint_matches_finite_differences(n):
+    p = case(n)
+    pol = poling_vector(p)
+    g = shg.grad(p, pol, checkpoint_every=5)
+    assert abs(g["sh_power"] - shg.sh_power(p, pol)) / g["sh_power"] <= 1e-12
+    dw = fd(lambda w: shg.sh_power(p.replace(waist=w), pol), p.waist, 1e-5 * p.waist)
+    df = fd(lambda f: shg.sh_power(p.replace(focus=f), pol), p.focus, 1e-5 * p.lz)
+    dT = fd(lambda t: shg.sh_power(p.replace(temp=t, t_peltier=t), pol), p.temp, 1e-4)
+    assert abs(g["d_waist"] - dw) <= 1e-5 * abs(dw)
+    assert abs(g["d_focus"] - df) <= 1e-5 * abs(df) + 1e-9 * abs(dw)
+    assert abs(g["d_temp"] - dT) <= 1e-5 * abs(dT)
+    scale = np.abs(g["d_poling"]).max()
+    for s in (0, 7, p.nz // 2, p.nz - 2):
+        def f(v, s=s):
+            q = pol.copy()
+            q[s] = v
+            return shg.sh_power(p, q)
+        assert abs(g["d_poling"][s] - fd(f, pol[s], 1e-6)) <= 1e-5 * scale
+
+
+def test_checkpoint_interval_does_not_change_gradients():
+    p = case()
+    pol = poling_vector(p)
+    ref = shg.grad(p, pol, checkpoint_every=1)
+    for k in (4, 7, p.nz - 1):
+        g = shg.grad(p, pol, checkpoint_every=k)
+        for key in ("sh_power", "d_waist", "d_focus", "d_temp"):
+            assert abs(g[key] - ref[key]) <= 1e-12 * abs(ref[key]) + 1e-300, key
+        assert np.allclose(g["d_poling"], ref["d_poling"], rtol=0, atol=1e-12 * np.abs(ref["d_poling"]).max())
+
+
+def test_fp32_adjoint_close_to_fp64():
+    p = case(128)
+    pol = poling_vector(p)
+    g64 = shg.grad(p, pol)
+    g32 = shg.grad(p.replace(precision=32), pol)
+    for key in ("sh_power", "d_waist", "d_focus", "d_temp"):
+        assert abs(g32[key] - g64[key]) <= 1e-3 * abs(g64[key]), key
+    scale = np.abs(g64["d_poling"]).max()
+    assert np.abs(g32["d_poling"] - g64["d_poling"]).max() <= 1e-3 * scale

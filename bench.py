@@ -360,11 +360,12 @@ def run_adjoint(args) -> dict:
 
     p = P.config_adjoint().replace(precision=args.precision)
     pol = np.random.default_rng(0).normal(0.0, 0.1, size=p.nz - 1)
+    kk = args.checkpoint_every
     for _ in range(args.warmup):
-        shg.grad(p, pol, checkpoint_every=20)
+        shg.grad(p, pol, checkpoint_every=kk)
     g_ms = []
     for _ in range(args.steps):
-        g = shg.grad(p, pol, checkpoint_every=20)
+        g = shg.grad(p, pol, checkpoint_every=kk)
         g_ms.append(g["device_ms"])
     pump = torch.empty((p.ny, p.nx), dtype=torch.complex64 if p.precision == 32 else torch.complex128, device="cuda")
     sig = torch.empty_like(pump)
@@ -374,7 +375,7 @@ def run_adjoint(args) -> dict:
         f_ms.append(st.device_ms)
     gm, fm = statistics.median(g_ms), statistics.median(f_ms)
     return {"metric": "adjoint grads/s", "value": 1e3 / gm, "unit": "gradients/s", "workload":
-            "256x256 nz=400, 3 scalars + 399-vector, checkpoints every 20", "precision": p.precision,
+            f"256x256 nz=400, 3 scalars + 399-vector, checkpoints every {g['checkpoint_every']}", "precision": p.precision,
             "grad_ms": gm, "forward_ms": fm, "grad_over_forward": gm / fm, "sh_power_w": g["sh_power"],
             "d_waist": g["d_waist"], "d_focus": g["d_focus"], "d_temp": g["d_temp"]}
 
@@ -392,6 +393,7 @@ def main() -> int:
     ap.add_argument("--class-nz", type=int, default=24)
     ap.add_argument("--workload", default="sweep", choices=["sweep", "thermal", "adjoint"])
     ap.add_argument("--thermal-side", type=int, default=0)
+    ap.add_argument("--checkpoint-every", type=int, default=20)
     ap.add_argument("--thermal-max-sweeps", type=int, default=0)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)

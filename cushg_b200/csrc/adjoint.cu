@@ -129,7 +129,7 @@ extern "C" shg_status shg_grad(const shg_params* p, const double* poling, int32_
     const size_t b_z = sizeof(double) * nsteps, b_part = sizeof(double) * C * kAdjAcc, b_phi = sizeof(double) * nsteps * C;
     const size_t b_pol = sizeof(double) * nsteps;
     auto up = [](size_t x) { return (x + 255) & ~(size_t)255; };
-    const size_t total = up(b_ckpt) + 2 * up(b_seg) + up(b_lam) + up(b_z) + up(b_part) + up(b_phi) + up(b_pol) +
+    const size_t total = up(b_ckpt) + 3 * up(b_seg) + up(b_lam) + up(b_z) + up(b_part) + up(b_phi) + up(b_pol) +
                          up(sizeof(InstDesc)) + up(sizeof(AdjDesc));
     cudaStream_t s = nullptr;
     cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
@@ -143,6 +143,7 @@ extern "C" shg_status shg_grad(const shg_params* p, const double* poling, int32_
         auto take = [&](size_t b) { char* r = q; q += up(b); return r; };
         a.ckpt = take(b_ckpt);
         a.seg_a2 = take(b_seg);
+        a.seg_x = take(b_seg);
         a.seg_y = take(b_seg);
         a.lam = take(b_lam);
         double* dz_ = reinterpret_cast<double*>(take(b_z));

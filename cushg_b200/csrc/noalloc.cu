@@ -10,7 +10,7 @@
 // but kernel launches and copies into memory that exists since the library was loaded.
 //
 // The scratch (instance descriptors and per-instance power slots) lives in g_noalloc_scratch,
-// a file-scope __device__ array of kNoAllocScratchBytes (~16 KB) that every GPU which loads
+// a file-scope __device__ array of kNoAllocScratchBytes (about 23 KB) that every GPU which loads
 // the library holds until the process exits.  Its limit: at most kNoAllocMaxInstances
 // instances per call.
 //

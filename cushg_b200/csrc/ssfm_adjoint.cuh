@@ -12,9 +12,10 @@
 // One cluster owns the instance for the whole computation, with the same shared-memory
 // layout and transform passes as the forward march (ssfm_plain.cuh):
 //   1. forward march, keeping x_{mK} (checkpoints every K steps) in global memory;
-//   2. for each segment m from the last: re-march from x_{mK}, keeping a2_s and the
-//      propagated spectra of each step of the segment; then march the adjoint back through
-//      the segment; the adjoint fields are parked in global memory between segments.
+//   2. for each segment m from the last: re-march from x_{mK}, keeping x_s, a2_s and the
+//      propagated spectra of each step of the segment (the last segment's come from step 1
+//      directly); then march the adjoint back through the segment; the adjoint fields are
+//      parked in global memory between segments.
 // Parameter sensitivities are accumulated on the way: the stage coefficients' dependence
 // on κ, Δk, the two-photon term and the poling phase (RK4 adjoint), the propagator phases'
 // dependence on n(T) (adjoint diffraction, with the stored spectra), and the initial pump's
@@ -45,6 +46,7 @@ struct AdjDesc {
     int32_t M;          // number of checkpoints (x_{mK}, m = 0..M-1)
     void* ckpt;         // M x 2 x n*n complex (pump, SH) before step mK, natural layout
     void* seg_a2;       // K x 2 x n*n: fields after the diffraction of each step of a segment
+    void* seg_x;        // K x 2 x n*n: fields before each step of a segment
     void* seg_y;        // K x 2 x n*n: propagated spectra of each step (CB order: fy*n + column)
     void* lam;          // 2 x n*n: adjoint fields between segments
     const double* zs;   // nsteps: z at the start of each step (the forward's accumulation)
@@ -174,9 +176,10 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
 
     init_tables<T, N>(d, tw, pxp, pxs, pyp, pys, tid, NT);
 
-    double acc[kAdjAcc];
-#pragma unroll
-    for (int i = 0; i < kAdjAcc; ++i) acc[i] = 0.0;
+    // accumulators (kAcc*), kept as scalars so that nothing is indexed at run time
+    double acc_kp = 0.0, acc_ks = 0.0, acc_dk = 0.0, acc_qs = 0.0, acc_pp = 0.0, acc_ps = 0.0;
+    double acc_g0w = 0.0, acc_g0f = 0.0, acc_g0T = 0.0, acc_j = 0.0;
+    V* seg_x = reinterpret_cast<V*>(a.seg_x);
 
     // ---- plane transfers between shared memory and global (natural layout) ------------
     auto load_planes = [&](const V* gp, const V* gs) {
@@ -315,7 +318,9 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
                                 const V yv = ybuf[yo];
                                 const double c = (double)u[k1].x * (-(double)yv.y) + (double)u[k1].y * (double)yv.x;
                                 const double sy = (double)(fy < N / 2 ? fy : fy - N);
-                                acc[f ? kAccPropS : kAccPropP] += c * (d.dfx * d.dfx * (sx * sx) + d.dfy * d.dfy * (sy * sy));
+                                const double w = c * (d.dfx * d.dfx * (sx * sx) + d.dfy * d.dfy * (sy * sy));
+                                if (f) acc_ps += w;
+                                else acc_pp += w;
                                 // conjugate propagator: conj(py) conj(px), via conj(conj(u) py px)
                                 u[k1] = cj(mulw(mulw(cj(u[k1]), py[fy]), px));
                             }
@@ -336,12 +341,15 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
     };
 
     // ---- forward march over steps [sb, se) from the fields in shared memory ------------
-    // ckpt_mode: keep x_{mK} (and x_sb) as checkpoints; seg_mode: keep a2_s and spectra of
-    // the segment and stop after a2_{se-1}.  With neither (the full march's end), the SH
-    // output becomes the adjoint seed lambda = (0, 2 pw_s S) and J is accumulated.
-    auto march = [&](int sb, int se, bool ckpt_mode, bool seg_mode) {
+    // ckpt_mode: keep x_{mK} as checkpoints.  Steps s >= seg_from keep x_s, a2_s and their
+    // propagated spectra in the segment buffers (slot s - seg_from).  seed: the march runs to
+    // the end and turns the SH output into the adjoint seed lambda = (0, 2 pw_s S)
+    // (accumulating J); otherwise it stops after a2_{se-1}.
+    auto march = [&](int sb, int se, bool ckpt_mode, int seg_from, bool seed) {
         coefs(sb);
         if (ckpt_mode && sb % K == 0) store_planes(ckpt + (size_t)(sb / K) * 2 * NN, ckpt + ((size_t)(sb / K) * 2 + 1) * NN);
+        if (sb >= seg_from)
+            store_planes(seg_x + (size_t)(sb - seg_from) * 2 * NN, seg_x + ((size_t)(sb - seg_from) * 2 + 1) * NN);
         __syncthreads();
         // first half of step sb, forward row stage
         for (int j = tid; j < JA; j += NT) {
@@ -359,12 +367,13 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
         }
         __syncthreads();
         for (int s = sb; s < se; ++s) {
+            const bool keep = s >= seg_from;
             pass_rb(false);
             __syncthreads();
             pass_ca(false);
             cluster_sync();
             if (s + 1 < nsteps) coefs(s + 1);
-            pass_cb(false, seg_mode ? s - sb : -1);
+            pass_cb(false, keep ? s - seg_from : -1);
             cluster_sync();
             pass_ca(true);
             __syncthreads();
@@ -381,15 +390,15 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
                     const int o = sidx<N, R2, SW>(lr, x);
                     const size_t g = (size_t)(crank + C * lr) * N + x;
                     V p = Ps[o], q = Ss[o];
-                    if (seg_mode) {
-                        seg_a2[((size_t)(s - sb) * 2) * NN + g] = p;
-                        seg_a2[((size_t)(s - sb) * 2 + 1) * NN + g] = q;
-                        if (last) continue;
+                    if (keep) {
+                        seg_a2[((size_t)(s - seg_from) * 2) * NN + g] = p;
+                        seg_a2[((size_t)(s - seg_from) * 2 + 1) * NN + g] = q;
                     }
+                    if (last && !seed) continue;
                     rk4_point<T>(p, q, coef + 6 * (s & 1), hap, has, qs, dz6);  // x_{s+1}
                     if (s + 1 == nsteps) {
                         // adjoint seed: J = pw_s sum |S|^2 -> g_S = 2 pw_s S, g_P = 0
-                        acc[kAccJ] += (double)q.x * q.x + (double)q.y * q.y;
+                        acc_j += (double)q.x * q.x + (double)q.y * q.y;
                         Ps[o] = mk<T>(0, 0);
                         Ss[o] = mk<T>((T)(2.0 * d.pw_s * q.x), (T)(2.0 * d.pw_s * q.y));
                         continue;
@@ -398,11 +407,15 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
                         ckpt[((size_t)((s + 1) / K) * 2) * NN + g] = p;
                         ckpt[((size_t)((s + 1) / K) * 2 + 1) * NN + g] = q;
                     }
-                    if (!last) rk4_point<T>(p, q, coef + 6 * ((s + 1) & 1), hap, has, qs, dz6);
+                    if (s + 1 >= seg_from) {
+                        seg_x[((size_t)(s + 1 - seg_from) * 2) * NN + g] = p;
+                        seg_x[((size_t)(s + 1 - seg_from) * 2 + 1) * NN + g] = q;
+                    }
+                    rk4_point<T>(p, q, coef + 6 * ((s + 1) & 1), hap, has, qs, dz6);
                     Ps[o] = p;
                     Ss[o] = q;
                 }
-                if (!last && s + 1 < nsteps) {
+                if (!last) {
 #pragma unroll 1
                     for (int f = 0; f < 2; ++f) row_a(f ? Ss : Ps, lr, n1, false);
                 }
@@ -426,10 +439,10 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
         __syncthreads();
     };
     auto add_sens = [&](const double* sn) {
-        acc[kAccKp] += sn[0];
-        acc[kAccKs] += sn[1];
-        acc[kAccDk] += sn[2];
-        acc[kAccQs] += sn[3];
+        acc_kp += sn[0];
+        acc_ks += sn[1];
+        acc_dk += sn[2];
+        acc_qs += sn[3];
     };
 
     // ---- adjoint march back over [sb, se) from lambda_se in shared memory ---------------
@@ -482,18 +495,14 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
                     const int o = sidx<N, R2, SW>(lr, x);
                     const size_t g = (size_t)(crank + C * lr) * N + x;
                     V gp = Ps[o], gs = Ss[o];
-                    // x_s: the checkpoint at the segment start, else N_{s-1}(a2_{s-1})
-                    V xp, xs, bp = mk<T>(0, 0), bs = mk<T>(0, 0);
-                    if (s == sb) {
-                        xp = ckpt[((size_t)(sb / K) * 2) * NN + g];
-                        xs = ckpt[((size_t)(sb / K) * 2 + 1) * NN + g];
-                    } else {
+                    // x_s and (inside the segment) a2_{s-1} from the segment buffers
+                    const size_t sx_ = (size_t)(s - sb) * 2;
+                    const V xp = seg_x[sx_ * NN + g], xs = seg_x[(sx_ + 1) * NN + g];
+                    V bp = mk<T>(0, 0), bs = mk<T>(0, 0);
+                    if (s > sb) {
                         const size_t sl = (size_t)(s - 1 - sb) * 2;
                         bp = seg_a2[sl * NN + g];
                         bs = seg_a2[(sl + 1) * NN + g];
-                        xp = bp;
-                        xs = bs;
-                        rk4_point<T>(xp, xs, coef + 6 * ((s - 1) & 1), hap, has, qs, dz6);
                     }
                     double sn[5] = {0, 0, 0, 0, 0};
                     rk4_vjp<T>(xp, xs, coef + 6 * (s & 1), hap, has, qs, dz6, a.zs[s], d.dz, gp, gs, sn);
@@ -521,27 +530,35 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
     };
 
     // ============================ the computation ======================================
-    // x_0: the pump of setPump, SH = 0
-    for (int e = tid; e < Cfg::PLANE; e += NT) {
-        const int lr = e / N, x = e % N;
-        const double2 pv = pump_value(d, x, crank + C * lr, d.amp_re, d.amp_im, d.den_re, d.den_im);
-        Ps[sidx<N, R2, SW>(lr, x)] = mk<T>((T)pv.x, (T)pv.y);
-        Ss[sidx<N, R2, SW>(lr, x)] = mk<T>((T)0, (T)0);
-    }
-    __syncthreads();
-    march(0, nsteps, true, false);  // smem: lambda_nsteps
-    store_planes(lam, lam + NN);
+    // One call site each for march and backward (keeps them inlined, with the accumulators
+    // in registers): the last segment's iteration runs the full forward march first.
+    const int last_sb = (a.M - 1) * K;
     for (int m = a.M - 1; m >= 0; --m) {
         const int sb = m * K, se = min(sb + K, nsteps);
+        const bool first = (m == a.M - 1);
+        if (first) {
+            // x_0: the pump of setPump, SH = 0
+            for (int e = tid; e < Cfg::PLANE; e += NT) {
+                const int lr = e / N, x = e % N;
+                const double2 pv = pump_value(d, x, crank + C * lr, d.amp_re, d.amp_im, d.den_re, d.den_im);
+                Ps[sidx<N, R2, SW>(lr, x)] = mk<T>((T)pv.x, (T)pv.y);
+                Ss[sidx<N, R2, SW>(lr, x)] = mk<T>((T)0, (T)0);
+            }
+        } else {
+            store_planes(lam, lam + NN);
+            __syncthreads();
+            load_planes(ckpt + (size_t)m * 2 * NN, ckpt + ((size_t)m * 2 + 1) * NN);
+        }
         __syncthreads();
-        load_planes(ckpt + (size_t)m * 2 * NN, ckpt + ((size_t)m * 2 + 1) * NN);
-        __syncthreads();
-        march(sb, se, false, true);
+        // full march (keeping checkpoints and the last segment, ending in the adjoint seed),
+        // or the re-march of segment m
+        march(first ? 0 : sb, se, first, first ? last_sb : sb, first);
         cluster_sync();
-        load_planes(lam, lam + NN);
-        __syncthreads();
+        if (!first) {
+            load_planes(lam, lam + NN);
+            __syncthreads();
+        }
         backward(sb, se);
-        store_planes(lam, lam + NN);
     }
     __syncthreads();
     // dJ/dθ of the initial pump: Re <λ0_P, dP0/dθ>, dP0/dθ by central differences of the
@@ -555,13 +572,17 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
             const double2 pm =
                 pump_value(d, x, y, a.pert[2 * q + 1][0], a.pert[2 * q + 1][1], a.pert[2 * q + 1][2], a.pert[2 * q + 1][3]);
             const double dre = (pp.x - pm.x) * a.inv2h[q], dim = (pp.y - pm.y) * a.inv2h[q];
-            acc[kAccG0w + q] += (double)l0.x * dre + (double)l0.y * dim;
+            const double v = (double)l0.x * dre + (double)l0.y * dim;
+            if (q == 0) acc_g0w += v;
+            else if (q == 1) acc_g0f += v;
+            else acc_g0T += v;
         }
     }
     // per-CTA accumulators, block-reduced in a fixed order
-#pragma unroll 1
+    const double av[kAdjAcc] = {acc_kp, acc_ks, acc_dk, acc_qs, acc_pp, acc_ps, acc_g0w, acc_g0f, acc_g0T, acc_j};
+#pragma unroll
     for (int i = 0; i < kAdjAcc; ++i) {
-        double v = acc[i];
+        double v = av[i];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
         if ((tid & 31) == 0) wred[tid >> 5] = v;

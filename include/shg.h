@@ -172,7 +172,7 @@ SHG_API shg_status shg_solve_batch_device(const shg_params* params, int32_t coun
  * entry point has no counterpart in the reference.  It is for callers that cannot allocate
  * device memory while they run (hosts that give all free memory to their own allocator,
  * latency-bound loops where an allocation may block or synchronise, plugin hosts that forbid
- * it): its scratch (instance descriptors, power slots) is a fixed ~16 KB __device__ array of
+ * it): its scratch (instance descriptors, power slots) is a fixed ~23 KB __device__ array of
  * the library, held by every GPU that loads it until exit.  Limit: count <= 64 instances
  * (larger counts return SHG_ERR_INVALID).  The first call on a device looks up that array's
  * address and should come before any stream capture.  Calls share the array: calls that

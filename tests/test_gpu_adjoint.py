@@ -80,3 +80,21 @@ def test_fp32_adjoint_close_to_fp64():
         assert abs(g32[key] - g64[key]) <= 1e-3 * abs(g64[key]), key
     scale = np.abs(g64["d_poling"]).max()
     assert np.abs(g32["d_poling"] - g64["d_poling"]).max() <= 1e-3 * scale
+
+
+def test_torch_autograd_binding_gradcheck():
+    import torch
+    from cushg_b200.autograd import SHGPower
+
+    p = case(64, nz=11)
+    w = torch.tensor(p.waist, dtype=torch.float64, requires_grad=True)
+    f = torch.tensor(p.focus, dtype=torch.float64, requires_grad=True)
+    t = torch.tensor(p.temp, dtype=torch.float64, requires_grad=True)
+    pol = torch.tensor(poling_vector(p), dtype=torch.float64, requires_grad=True)
+    j = SHGPower.apply(w, f, t, pol, p)
+    j.backward()
+    g = shg.grad(p, pol.detach().numpy())
+    assert w.grad.item() == g["d_waist"] and t.grad.item() == g["d_temp"]
+    # torch's own finite-difference check of the binding (poling entries and temperature)
+    fn = lambda tt, pp: SHGPower.apply(w.detach(), f.detach(), tt, pp, p)  # noqa: E731
+    assert torch.autograd.gradcheck(fn, (t, pol), eps=1e-6, atol=1e-12, rtol=1e-4)

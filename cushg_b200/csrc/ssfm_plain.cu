@@ -8,10 +8,10 @@
 
 namespace shg {
 
-template <typename T, int N, int C, int NT, bool THERM>
+template <typename T, int N, int C, int NT, bool THERM, int MINB = 1>
 static cudaError_t launch_plain(const InstDesc* descs, int count, cudaStream_t stream) {
     using Cfg = PlainCfg<T, N, C, NT, THERM>;
-    auto kern = ssfm_plain_kernel<T, N, C, NT, THERM>;
+    auto kern = ssfm_plain_kernel<T, N, C, NT, THERM, MINB>;
     static std::once_flag once;
     static cudaError_t attr_err = cudaSuccess;
     std::call_once(once, [&]() {
@@ -38,6 +38,8 @@ static cudaError_t launch_plain(const InstDesc* descs, int count, cudaStream_t s
 
 #define SHG_PLAIN(T, PREC, N, C, NT) \
     {PREC, N, C, NT, 0, PlainCfg<T, N, C, NT, false>::smem_bytes, &launch_plain<T, N, C, NT, false>}
+#define SHG_PLAIN_B(T, PREC, N, C, NT, MINB) \
+    {PREC, N, C, NT, 0, PlainCfg<T, N, C, NT, false>::smem_bytes, &launch_plain<T, N, C, NT, false, MINB>}
 #define SHG_THERM(T, PREC, N, C, NT) \
     {PREC, N, C, NT, 1, PlainCfg<T, N, C, NT, true>::smem_bytes, &launch_plain<T, N, C, NT, true>}
 
@@ -57,17 +59,38 @@ static cudaError_t launch_plain(const InstDesc* descs, int count, cudaStream_t s
 #ifndef SHG_NT_F64
 #define SHG_NT_F64 256
 #endif
+#ifndef SHG_C_F32_128
+#define SHG_C_F32_128 2
+#endif
+#ifndef SHG_C_F32_192
+#define SHG_C_F32_192 4
+#endif
+#ifndef SHG_C_F32_256
+#define SHG_C_F32_256 16
+#endif
+#ifndef SHG_MINB_F32_128
+#define SHG_MINB_F32_128 1
+#endif
+#ifndef SHG_MINB_F32_192
+#define SHG_MINB_F32_192 1
+#endif
+#ifndef SHG_MINB_F32_256
+#define SHG_MINB_F32_256 2
+#endif
+#ifndef SHG_MINB_F32_SMALL
+#define SHG_MINB_F32_SMALL 1
+#endif
 
 // (precision, grid side) -> cluster size and threads per CTA.  The cluster size keeps
 // both planes of one instance in at most ~150 KB of shared memory per CTA.
 static const PlainVariant kPlainVariants[] = {
     SHG_PLAIN(float, 32, 32, 1, 128),
     SHG_PLAIN(float, 32, 48, 1, 192),
-    SHG_PLAIN(float, 32, 64, 1, SHG_NT_F32_SMALL),
+    SHG_PLAIN_B(float, 32, 64, 1, SHG_NT_F32_SMALL, SHG_MINB_F32_SMALL),
     SHG_PLAIN(float, 32, 96, 1, 192),
-    SHG_PLAIN(float, 32, 128, 2, SHG_NT_F32_128),
-    SHG_PLAIN(float, 32, 192, 4, SHG_NT_F32_192),
-    SHG_PLAIN(float, 32, 256, 8, SHG_NT_F32_256),
+    SHG_PLAIN_B(float, 32, 128, SHG_C_F32_128, SHG_NT_F32_128, SHG_MINB_F32_128),
+    SHG_PLAIN_B(float, 32, 192, SHG_C_F32_192, SHG_NT_F32_192, SHG_MINB_F32_192),
+    SHG_PLAIN_B(float, 32, 256, SHG_C_F32_256, SHG_NT_F32_256, SHG_MINB_F32_256),
     SHG_PLAIN(double, 64, 32, 1, 128),
     SHG_PLAIN(double, 64, 48, 1, 192),
     SHG_PLAIN(double, 64, 64, 1, SHG_NT_F64),

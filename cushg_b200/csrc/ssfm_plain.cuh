@@ -182,8 +182,8 @@ __device__ __forceinline__ void thermal_coef(const InstDesc& d, double dki, int 
     }
 }
 
-template <typename T, int N, int C, int NT, bool THERM>
-__global__ void __launch_bounds__(NT, 1) ssfm_plain_kernel(const InstDesc* __restrict__ descs) {
+template <typename T, int N, int C, int NT, bool THERM, int MINB = 1>
+__global__ void __launch_bounds__(NT, MINB) ssfm_plain_kernel(const InstDesc* __restrict__ descs) {
     using Cfg = PlainCfg<T, N, C, NT, THERM>;
     constexpr int R2 = Cfg::R2, RL = Cfg::RL, SW = Cfg::SW;
     constexpr int JA = Cfg::JA, JB = Cfg::JB, JCA = Cfg::JCA, JCB = Cfg::JCB;

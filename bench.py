@@ -327,6 +327,7 @@ def run_thermal(args) -> dict:
         p = p.replace(nx=args.thermal_side, ny=args.thermal_side)
     if args.thermal_max_sweeps:
         p = p.replace(max_sweeps=args.thermal_max_sweeps)
+    p = p.replace(jacobi_block=args.jacobi_block, precision=args.thermal_precision)
     cdt = torch.complex128 if p.precision == 64 else torch.complex64
     pump = torch.empty((p.ny, p.nx), dtype=cdt, device="cuda")
     sig = torch.empty_like(pump)
@@ -340,13 +341,14 @@ def run_thermal(args) -> dict:
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
     vox = p.nx * p.ny * p.nz
-    out = {"metric": "thermal solve (Jacobi voxel-sweeps/s)", "workload": "thermal 128x128x200 FP64", "status": status,
-           "wall_s": wall, "clocks": clk.summary()}
+    out = {"metric": "thermal solve (Jacobi voxel-sweeps/s)",
+           "workload": f"thermal {p.nx}x{p.ny}x{p.nz} FP{p.precision}", "status": status,
+           "jacobi_block": p.jacobi_block or 4, "wall_s": wall, "clocks": clk.summary()}
     if st is not None:
         out.update({"device_ms": st.device_ms, "jacobi_sweeps": st.jacobi_sweeps, "outer_iterations": st.outer_iterations,
                     "sh_power_w": st.sh_power, "value": vox * st.jacobi_sweeps / (st.device_ms * 1e-3),
                     "unit": "voxel-sweeps/s",
-                    "jacobi_gbs_algorithmic": 24 * vox * st.jacobi_sweeps / (st.device_ms * 1e-3) / 1e9})
+                    "jacobi_gbs_algorithmic": 3 * (p.precision // 8) * vox * st.jacobi_sweeps / (st.device_ms * 1e-3) / 1e9})
     return out
 
 
@@ -395,6 +397,8 @@ def main() -> int:
     ap.add_argument("--thermal-side", type=int, default=0)
     ap.add_argument("--checkpoint-every", type=int, default=20)
     ap.add_argument("--thermal-max-sweeps", type=int, default=0)
+    ap.add_argument("--thermal-precision", type=int, default=64, choices=[32, 64])
+    ap.add_argument("--jacobi-block", type=int, default=0, help="sweeps per launch (0 = automatic)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank = int(os.environ.get("RANK", "0"))

@@ -150,6 +150,8 @@ void shg_default_params(shg_params* p) {
     p->crystal = SHG_CRYSTAL_MGO_SPPLT;
     p->jacobi_tol = 0.0;
     p->max_sweeps = 0;
+    p->jacobi_block = 0;
+    p->reserved0 = 0;
 }
 
 static bool finite_all(const shg_params* p) {
@@ -181,6 +183,8 @@ shg_status shg_check_params(const shg_params* p) {
         if (p->conv_rule != SHG_CONV_REFERENCE && p->conv_rule != SHG_CONV_MAXABS)
             return fail(SHG_ERR_INVALID, "unknown conv_rule %d", p->conv_rule);
         if (p->nz < 3 || p->nx < 3) return fail(SHG_ERR_INVALID, "thermal grid needs nx, nz >= 3");
+        if (p->jacobi_block < 0 || p->jacobi_block > 4)
+            return fail(SHG_ERR_INVALID, "jacobi_block %d must be in 0..4", p->jacobi_block);
     }
     if (!find_plain_variant(p->precision, p->nx, p->thermal))
         return fail(SHG_ERR_UNSUPPORTED, "no %s kernel built for grid side %d at precision %d",

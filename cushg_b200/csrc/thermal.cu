@@ -12,6 +12,7 @@
 //       -> optics_kernel (Δk, n_p, n_s per voxel, once per optical pass)
 #include <cuda_runtime.h>
 
+#include "jacobi_point.cuh"
 #include "shg_host.h"
 #include "thermal.h"
 
@@ -66,56 +67,17 @@ __global__ void optics_kernel(const R* __restrict__ T, R* __restrict__ dk, R* __
 template <typename R, int BOUND, bool RESID>
 __global__ void __launch_bounds__(256) jacobi_kernel(const R* __restrict__ Ti, R* __restrict__ Tf, const R* __restrict__ Q,
                                                      JacobiCoef<R> k, int rule, double* __restrict__ partial) {
-    const int n = k.n, nz = k.nz;
+    const int n = k.n;
     const int x = blockIdx.x * 32 + threadIdx.x;
     const int y = blockIdx.y * 8 + threadIdx.y;
     const int z = blockIdx.z;
     double dres = 0.0;
     if (x < n && y < n) {
-        const size_t sx = 1, sy = (size_t)n, sz = (size_t)n * n;
+        const size_t sy = (size_t)n, sz = (size_t)n * n;
         const size_t i = (size_t)z * sz + (size_t)y * sy + x;
-        const bool xi = x > 0 && x < n - 1, yi = y > 0 && y < n - 1, zi = z > 0 && z < nz - 1;
-        bool wr = true;
-        R v = (R)0;
-        if (BOUND == SHG_BOUNDARY_TOP_OPEN) {
-            if (y == 0) {
-                wr = false;  // Dirichlet face at the oven temperature
-            } else if (xi && yi && zi) {  // inner points (Tfield.h:113-115)
-                v = k.L2 * ((Ti[i + sx] + Ti[i - sx]) * k.idx2 + (Ti[i + sy] + Ti[i - sy]) * k.idy2 +
-                            (Ti[i + sz] + Ti[i - sz]) * k.idz2 + Q[i] * k.iK);
-            } else if (!xi && yi && zi) {  // faces x = 0 / x = Lx (Tfield.h:119-125)
-                const size_t xn = x == 0 ? i + sx : i - sx;
-                v = (Ti[xn] + k.ax * (Ti[i + sy] + Ti[i - sy]) + k.bx * (Ti[i + sz] + Ti[i - sz]) + k.Bix * k.Tinf) * k.fx;
-            } else if (xi && !yi && zi) {  // face y = Ly (Tfield.h:127-129)
-                v = (Ti[i - sy] + k.ay * (Ti[i + sx] + Ti[i - sx]) + k.by * (Ti[i + sz] + Ti[i - sz]) + k.Biy * k.Tinf) * k.fy;
-            } else if (xi && yi && !zi) {  // faces z = 0 / z = Lcr (Tfield.h:131-137)
-                const size_t zn = z == 0 ? i + sz : i - sz;
-                v = (Ti[zn] + k.az * (Ti[i + sx] + Ti[i - sx]) + k.bz * (Ti[i + sy] + Ti[i - sy]) + k.Biz * k.Tinf) * k.fz;
-            } else if (!xi && yi && !zi) {  // vertical edges (Tfield.h:143-157)
-                const size_t xn = x == 0 ? i + sx : i - sx, zn = z == 0 ? i + sz : i - sz;
-                v = (k.av * Ti[xn] + k.bv * Ti[zn] + k.cv * (Ti[i + sy] + Ti[i - sy]) + k.tv) * k.V;
-            } else if (xi && !yi && !zi) {  // horizontal edges (Tfield.h:161-167)
-                const size_t zn = z == 0 ? i + sz : i - sz;
-                v = (k.ah * Ti[i - sy] + k.bh * Ti[zn] + k.ch * (Ti[i - sx] + Ti[i + sx]) + k.th) * k.H;
-            } else if (!xi && !yi && zi) {  // depth edges (Tfield.h:171-177)
-                const size_t xn = x == 0 ? i + sx : i - sx;
-                v = (k.ad * Ti[i - sy] + k.bd * Ti[xn] + k.cd * (Ti[i + sz] + Ti[i - sz]) + k.td) * k.D;
-            } else {  // vertices (Tfield.h:181-196)
-                const size_t xn = x == 0 ? i + sx : i - sx, zn = z == 0 ? i + sz : i - sz;
-                v = (k.AV * Ti[xn] + k.BV * Ti[i - sy] + k.CV * Ti[zn] + k.Tinf * k.BiD) * k.GV;
-            }
-        } else {
-            if (!(xi && yi)) {
-                wr = false;  // lateral faces held at the oven temperature
-            } else if (zi) {
-                v = k.L2 * ((Ti[i + sx] + Ti[i - sx]) * k.idx2 + (Ti[i + sy] + Ti[i - sy]) * k.idy2 +
-                            (Ti[i + sz] + Ti[i - sz]) * k.idz2 + Q[i] * k.iK);
-            } else {  // z faces (Tfield.h:229-236)
-                const size_t zn = z == 0 ? i + sz : i - sz;
-                v = (Ti[zn] + k.az * (Ti[i + sx] + Ti[i - sx]) + k.bz * (Ti[i + sy] + Ti[i - sy]) + k.Biz * k.Tinf) * k.fz;
-            }
-        }
-        if (wr) {
+        auto get = [&](int dx, int dy, int dz) -> R { return Ti[i + (ptrdiff_t)dz * sz + (ptrdiff_t)dy * sy + dx]; };
+        R v;
+        if (jacobi_point<R, BOUND>(x, y, z, k, Q[i], get, &v)) {
             Tf[i] = v;
             if (RESID) {
                 const double dd = (double)(R)(v - Ti[i]);

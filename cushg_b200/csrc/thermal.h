@@ -1,6 +1,7 @@
 // thermal.h — launchers of the heat-solve and temperature-optics kernels (thermal.cu).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "../../include/shg.h"
@@ -30,5 +31,14 @@ template <typename R>
 cudaError_t launch_jacobi(const R* Ti, R* Tf, const R* Q, const JacobiCoef<R>& k, int boundary, bool resid, int rule,
                           double* partial, double* out, cudaStream_t s);
 size_t jacobi_partials(const shg_params& p);
+
+// Temporally blocked sweeps (jacobi_tb.cu): `depth` (2..4) sweeps Ti -> Tf in one launch,
+// with Ti and Q read through 3D TMA maps made by make_tb_map.  *err is set to 1 if a
+// staged plane never arrived.
+int jacobi_tb_chunk(int tiles, int nz, int depth, int sms);
+template <typename R> shg_status make_tb_map(const R* base, int n, int nz, CUtensorMap* map);
+template <typename R>
+cudaError_t launch_jacobi_tb(const CUtensorMap& tmT, const CUtensorMap& tmQ, R* Tf, const JacobiCoef<R>& k,
+                             int boundary, int depth, unsigned* err, cudaStream_t s);
 
 }  // namespace shg

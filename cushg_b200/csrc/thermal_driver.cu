@@ -6,6 +6,8 @@
 //     Jacobi sweeps until the convergence value, taken on the first sweep of every
 //     window of check_every sweeps, falls below tol; a value equal to the previous
 //     check counts as converged                              (Solver.h:335-355)
+//     (the checked sweep runs alone; the rest of the window runs jacobi_block sweeps
+//     per launch through the temporally blocked kernel of jacobi_tb.cu)
 //     Δk, n_p, n_s from T; pump, SH and propagators at T(NX/2, NY/2, 0)   (Solver.h:359-362)
 //     one optical pass of nz steps that emits Q slice by slice (Solver.h:365, 300)
 //     stop after a pass whose Jacobi loop converged at its first sweep (Solver.h:367)
@@ -45,9 +47,10 @@ shg_status thermal_run(const shg_params& p, const void* signal_in, void* pump_ou
     R* NP = DK + nt;
     R* NS = NP + nt;
     double* partial = reinterpret_cast<double*>(NS + nt);
-    double* resid = partial + npart;   // [1]
+    double* resid = partial + npart;   // [0] convergence value, [1] staging-error word
     double* power = resid + 2;         // [2]
     InstDesc* ddesc = reinterpret_cast<InstDesc*>(((uintptr_t)(power + 2) + 255) & ~(uintptr_t)255);
+    unsigned* tb_err = reinterpret_cast<unsigned*>(resid + 1);  // set by a blocked sweep whose staging timed out
 
     shg_status rc = SHG_OK;
     cudaEvent_t t0 = nullptr, t1 = nullptr;
@@ -60,12 +63,19 @@ shg_status thermal_run(const shg_params& p, const void* signal_in, void* pump_ou
     const int check_every = p.check_every > 0 ? p.check_every : 5000;
     const int64_t max_sweeps = p.max_sweeps > 0 ? p.max_sweeps : ((int64_t)1 << 40);
     const int max_outer = p.max_outer > 0 ? p.max_outer : 20;
+    const int depth = p.jacobi_block > 0 ? p.jacobi_block : 4;
     int64_t total = 0;
     int outer = 0;
     double last = 0.0;
     R* cur = Ta;  // holds the latest temperature (the reference's Tinic == Tfinal after its copy)
     R* nxt = Tb;
+    CUtensorMap map_a, map_b, map_q;
     do {
+        if (depth > 1 && ((rc = make_tb_map<R>(Ta, n, nz, &map_a)) != SHG_OK ||
+                          (rc = make_tb_map<R>(Tb, n, nz, &map_b)) != SHG_OK ||
+                          (rc = make_tb_map<R>(Q, n, nz, &map_q)) != SHG_OK))
+            break;
+        if ((e = cudaMemsetAsync(resid, 0, 2 * sizeof(double), s)) != cudaSuccess) { rc = cuda_fail(e, "memset"); break; }
         if ((e = launch_thermal_init<R>(Ta, Tb, Q, p, s)) != cudaSuccess) { rc = cuda_fail(e, "thermal init"); break; }
         for (int g = 0; g < max_outer && rc == SHG_OK; ++g) {
             double red = 1.0, aux = -1.0;
@@ -82,26 +92,38 @@ shg_status thermal_run(const shg_params& p, const void* signal_in, void* pump_ou
                     break;
                 }
                 std::swap(cur, nxt);
-                double h = 0.0;
-                if ((e = cudaMemcpyAsync(&h, resid, sizeof(double), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+                double h[2] = {0.0, 0.0};
+                if ((e = cudaMemcpyAsync(h, resid, sizeof(h), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
                     (e = cudaStreamSynchronize(s)) != cudaSuccess) {
                     rc = cuda_fail(e, "jacobi residual");
                     break;
                 }
+                unsigned staged_err = 0;
+                std::memcpy(&staged_err, &h[1], sizeof(staged_err));
+                if (staged_err) {
+                    rc = fail(SHG_ERR_CUDA, "blocked Jacobi sweep: a staged plane did not arrive");
+                    break;
+                }
                 if (counter > 0) aux = red;
-                red = p.conv_rule == SHG_CONV_MAXABS ? h : (double)(R)(std::sqrt((R)h) / (R)(double)nt);
+                red = p.conv_rule == SHG_CONV_MAXABS ? h[0] : (double)(R)(std::sqrt((R)h[0]) / (R)(double)nt);
                 if (red == aux) red = 0.5 * tol;
                 ++counter;
                 if (red < tol) break;
-                // the rest of the window, unchecked
-                for (int w = 1; w < check_every && counter < max_sweeps; ++w) {
-                    if ((e = launch_jacobi<R>(cur, nxt, Q, k, p.boundary, false, p.conv_rule, nullptr, nullptr, s)) !=
-                        cudaSuccess) {
+                // the rest of the window, unchecked: `depth` sweeps per launch
+                int64_t left = std::min<int64_t>(check_every - 1, max_sweeps - counter);
+                while (left > 0) {
+                    const int t = (int)std::min<int64_t>(depth, left);
+                    if (t >= 2)
+                        e = launch_jacobi_tb<R>(cur == Ta ? map_a : map_b, map_q, nxt, k, p.boundary, t, tb_err, s);
+                    else
+                        e = launch_jacobi<R>(cur, nxt, Q, k, p.boundary, false, p.conv_rule, nullptr, nullptr, s);
+                    if (e != cudaSuccess) {
                         rc = cuda_fail(e, "jacobi sweep");
                         break;
                     }
                     std::swap(cur, nxt);
-                    ++counter;
+                    counter += t;
+                    left -= t;
                 }
                 if (rc != SHG_OK) break;
             }

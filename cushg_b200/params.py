@@ -49,6 +49,7 @@ class ShgParams(ctypes.Structure):
         ("max_outer", ctypes.c_int32), ("check_every", ctypes.c_int32),
         ("conv_rule", ctypes.c_int32), ("crystal", ctypes.c_int32),
         ("jacobi_tol", ctypes.c_double), ("max_sweeps", ctypes.c_int64),
+        ("jacobi_block", ctypes.c_int32), ("reserved0", ctypes.c_int32),
     ]
 
     def copy(self) -> "ShgParams":

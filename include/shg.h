@@ -102,6 +102,11 @@ typedef struct shg_params {
     int32_t crystal;        /* SHG_CRYSTAL_* */
     double jacobi_tol;      /* <= 0 selects the reference tolerance 5e-4/TSIZE (Solver.h:332) */
     int64_t max_sweeps;     /* Jacobi sweep cap per outer iteration (<= 0: 2^40) */
+    /* Sweeps fused per launch between convergence checks (temporal blocking): 0 = automatic
+     * (4), 1 = one sweep per launch, 2..4 = that many.  Every setting gives the same
+     * temperatures bit for bit; the checked sweep of each window always runs alone. */
+    int32_t jacobi_block;
+    int32_t reserved0;
 } shg_params;
 
 /* Per-call report. */

@@ -88,3 +88,28 @@ def test_thermal_fp32_against_fp64_oracle():
     assert np.abs(r.temperature - T).max() <= 2e-2
     assert rel_l2(r.signal, sig) <= 2e-2
     assert abs(r.sh_power - st.sh_power) / st.sh_power <= 2e-2
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+@pytest.mark.parametrize("boundary", [P.SHG_BOUNDARY_TOP_OPEN, P.SHG_BOUNDARY_OVEN_SURROUNDED])
+@pytest.mark.parametrize("n,nz,check_every", [(64, 50, 8), (32, 23, 7), (128, 40, 30)])
+def test_blocked_sweeps_are_bit_identical(precision, boundary, n, nz, check_every):
+    """Fusing 2, 3 or 4 sweeps per launch (TMA-staged temporal blocking) gives the same
+    temperatures, fields and sweep counts, bit for bit, as one sweep per launch.  The grids
+    leave partial tiles at the +x / +y edges and split z into chunks; check windows of
+    check_every - 1 unchecked sweeps leave remainders of 1, 2 and 3 sweeps."""
+    p = P.workload(n, nz, 6000.0, 3.0, 30.0, 3000.0, 33.0, precision=precision, thermal=1)
+    p.alpha_p, p.alpha_s, p.beta_s = 2e-5, 1e-4, 1e-3
+    p.boundary = boundary
+    p.max_outer = 2
+    p.check_every = check_every
+    p.conv_rule = P.SHG_CONV_MAXABS
+    p.jacobi_tol = 2e-3
+    p.max_sweeps = 4000
+    ref = shg.solve(p.replace(jacobi_block=1), want_temperature=True)
+    for blk in (0, 2, 3):
+        r = shg.solve(p.replace(jacobi_block=blk), want_temperature=True)
+        assert r.stats.jacobi_sweeps == ref.stats.jacobi_sweeps
+        assert r.stats.outer_iterations == ref.stats.outer_iterations
+        assert np.array_equal(r.temperature, ref.temperature), blk
+        assert np.array_equal(r.signal, ref.signal) and np.array_equal(r.pump, ref.pump)

@@ -32,8 +32,11 @@ def rel_l2(a, b):
 def test_oracle_matches_reference_fp64(name):
     z, meta = load(name)
     p = G.params_of(name)
-    # the fixture was made from exactly these parameters
-    assert meta["params"] == p.as_dict()
+    # the fixture was made from exactly these parameters (fields added to shg_params after
+    # the fixture was written are execution settings at their defaults)
+    d = p.as_dict()
+    assert {k: v for k, v in d.items() if k in meta["params"]} == meta["params"]
+    assert all(d[k] == 0 for k in d if k not in meta["params"])
     rc, pump, sig, st, T = O.solve(p, want_temperature=True)
     assert rc == 0
     # output-field relative L2 <= 1e-10 for the plain FP64 path

@@ -325,6 +325,8 @@ def run_thermal(args) -> dict:
     p = P.config_thermal_128()
     if args.thermal_side:
         p = p.replace(nx=args.thermal_side, ny=args.thermal_side)
+    if args.thermal_nz:
+        p = p.replace(nz=args.thermal_nz)
     if args.thermal_max_sweeps:
         p = p.replace(max_sweeps=args.thermal_max_sweeps)
     p = p.replace(jacobi_block=args.jacobi_block, precision=args.thermal_precision)
@@ -352,6 +354,54 @@ def run_thermal(args) -> dict:
     return out
 
 
+def run_jacobi(args) -> dict:
+    """Heat-solve workload (outside the default sweep line): `--jacobi-sweeps` Jacobi sweeps
+    of the heat equation per step through shg_heat_sweeps_device on the thermal grid (default
+    128 x 128 x 200, FP64, top-open boundary), from a uniform 40 °C start with a random heat
+    source; timed with CUDA events on the launching stream."""
+    import torch
+    from cushg_b200 import shg
+
+    p = P.config_thermal_128()
+    if args.thermal_side:
+        p = p.replace(nx=args.thermal_side, ny=args.thermal_side)
+    if args.thermal_nz:
+        p = p.replace(nz=args.thermal_nz)
+    p = p.replace(jacobi_block=args.jacobi_block, precision=args.thermal_precision)
+    tdt = torch.float64 if p.precision == 64 else torch.float32
+    vox = p.nx * p.ny * p.nz
+    T = torch.full((p.nz, p.ny, p.nx), 40.0, dtype=tdt, device="cuda")
+    g = torch.Generator(device="cuda").manual_seed(0)
+    Q = torch.rand((p.nz, p.ny, p.nx), dtype=tdt, device="cuda", generator=g) * 1e-6
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+    k = args.jacobi_sweeps
+    for _ in range(args.warmup):
+        shg.heat_sweeps_device(p, T, Q, k, stream=sptr)
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(0) as clk:
+        for a, b in evs:
+            a.record(stream)
+            shg.heat_sweeps_device(p, T, Q, k, stream=sptr)
+            b.record(stream)
+        torch.cuda.synchronize()
+    ms = statistics.median(x.elapsed_time(y) for x, y in evs)
+    per_sweep_s = ms * 1e-3 / k
+    bpv = 3 * (p.precision // 8)
+    hbm_peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs", 6650.0) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else 6650.0
+    gbs = bpv * vox / per_sweep_s / 1e9
+    return {"metric": "Jacobi voxel-sweeps/s", "value": vox / per_sweep_s, "unit": "voxel-sweeps/s",
+            "workload": f"heat sweeps {p.nx}x{p.ny}x{p.nz} FP{p.precision}, {k} sweeps per call",
+            "jacobi_block": args.jacobi_block, "ms_per_call": ms, "us_per_sweep": per_sweep_s * 1e6,
+            "working_set_mb": 3 * vox * (p.precision // 8) / 1e6,
+            "roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm_peak, "unit": "GB/s", "frac": gbs / hbm_peak,
+                         "note": f"{bpv} B per voxel-sweep algorithmic (read T, read Q, write T); above 1.0 means "
+                                 f"the sweep runs from L2 or fuses sweeps"},
+            "clocks": clk.summary()}
+
+
 def run_adjoint(args) -> dict:
     """Adjoint workload (outside the default sweep line): gradients of the SH power of the
     256x256 / nz = 400 FP32 run (20 mm, 30 W, w0 = 35 µm, focus 0.4 L, 30 °C) with respect to
@@ -361,6 +411,8 @@ def run_adjoint(args) -> dict:
     from cushg_b200 import shg
 
     p = P.config_adjoint().replace(precision=args.precision)
+    if args.adjoint_nz:
+        p = p.replace(nz=args.adjoint_nz)
     pol = np.random.default_rng(0).normal(0.0, 0.1, size=p.nz - 1)
     kk = args.checkpoint_every
     for _ in range(args.warmup):
@@ -377,7 +429,8 @@ def run_adjoint(args) -> dict:
         f_ms.append(st.device_ms)
     gm, fm = statistics.median(g_ms), statistics.median(f_ms)
     return {"metric": "adjoint grads/s", "value": 1e3 / gm, "unit": "gradients/s", "workload":
-            f"256x256 nz=400, 3 scalars + 399-vector, checkpoints every {g['checkpoint_every']}", "precision": p.precision,
+            f"256x256 nz={p.nz}, 3 scalars + {p.nz - 1}-vector, checkpoints every {g['checkpoint_every']}",
+            "precision": p.precision,
             "grad_ms": gm, "forward_ms": fm, "grad_over_forward": gm / fm, "sh_power_w": g["sh_power"],
             "d_waist": g["d_waist"], "d_focus": g["d_focus"], "d_temp": g["d_temp"]}
 
@@ -393,9 +446,12 @@ def main() -> int:
     ap.add_argument("--class-side", type=int, default=0, help="profile case: one grid-size class only")
     ap.add_argument("--class-count", type=int, default=18)
     ap.add_argument("--class-nz", type=int, default=24)
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "thermal", "adjoint"])
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "thermal", "adjoint", "jacobi"])
+    ap.add_argument("--jacobi-sweeps", type=int, default=400)
     ap.add_argument("--thermal-side", type=int, default=0)
+    ap.add_argument("--thermal-nz", type=int, default=0)
     ap.add_argument("--checkpoint-every", type=int, default=20)
+    ap.add_argument("--adjoint-nz", type=int, default=0, help="adjoint workload with this nz (profiling case)")
     ap.add_argument("--thermal-max-sweeps", type=int, default=0)
     ap.add_argument("--thermal-precision", type=int, default=64, choices=[32, 64])
     ap.add_argument("--jacobi-block", type=int, default=0, help="sweeps per launch (0 = automatic)")
@@ -408,6 +464,8 @@ def main() -> int:
         out = run_thermal(args) if rank == 0 else None
     elif args.workload == "adjoint":
         out = run_adjoint(args) if rank == 0 else None
+    elif args.workload == "jacobi":
+        out = run_jacobi(args) if rank == 0 else None
     elif args.impl == "reference":
         out = run_reference(args, rank, world)
     else:

@@ -163,7 +163,7 @@ static bool finite_all(const shg_params* p) {
     return true;
 }
 
-shg_status shg_check_params(const shg_params* p) {
+static shg_status check_params_impl(const shg_params* p, bool need_kernel) {
     clear_error();
     if (!p) return fail(SHG_ERR_INVALID, "params is NULL");
     if (!finite_all(p)) return fail(SHG_ERR_INVALID, "a parameter is NaN or infinite");
@@ -186,11 +186,13 @@ shg_status shg_check_params(const shg_params* p) {
         if (p->jacobi_block < 0 || p->jacobi_block > 4)
             return fail(SHG_ERR_INVALID, "jacobi_block %d must be in 0..4", p->jacobi_block);
     }
-    if (!find_plain_variant(p->precision, p->nx, p->thermal))
+    if (need_kernel && !find_plain_variant(p->precision, p->nx, p->thermal))
         return fail(SHG_ERR_UNSUPPORTED, "no %s kernel built for grid side %d at precision %d",
                     p->thermal ? "thermal" : "plain", p->nx, p->precision);
     return SHG_OK;
 }
+
+shg_status shg_check_params(const shg_params* p) { return check_params_impl(p, true); }
 
 int32_t shg_steps(const shg_params* p) {
     if (!p) return 0;
@@ -325,6 +327,20 @@ shg_status shg_sh_power(const shg_params* p, const double* poling, double* sh_po
     cudaStreamSynchronize(s);
     cudaStreamDestroy(s);
     return rc;
+}
+
+shg_status shg_heat_sweeps_device(const shg_params* p, void* temperature_dev, const void* q_dev, int64_t sweeps,
+                                  void* stream) {
+    clear_error();
+    if (!p) return fail(SHG_ERR_INVALID, "params is NULL");
+    shg_params q = *p;
+    q.thermal = 1;
+    shg_status st = check_params_impl(&q, false);  // the heat solve needs no optical kernel
+    if (st != SHG_OK) return st;
+    if (!temperature_dev || !q_dev) return fail(SHG_ERR_INVALID, "temperature or Q is NULL");
+    if (sweeps < 0) return fail(SHG_ERR_INVALID, "sweeps must be >= 0");
+    if (sweeps == 0) return SHG_OK;
+    return heat_sweeps_device(q, temperature_dev, q_dev, sweeps, (cudaStream_t)stream);
 }
 
 shg_status shg_solve_batch_device(const shg_params* params, int32_t count, void* const* pump_out_dev,

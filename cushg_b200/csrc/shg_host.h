@@ -30,5 +30,7 @@ shg_status plain_solve_batch(const shg_params* params, int count, void* const* p
 shg_status thermal_solve_device(const shg_params& p, const void* signal_in, void* pump_out, void* signal_out,
                                 void* temperature_out, shg_stats* stats, cudaStream_t stream,
                                 void* slices_p = nullptr, void* slices_s = nullptr);
+shg_status heat_sweeps_device(const shg_params& p, void* temperature, const void* q, int64_t sweeps,
+                              cudaStream_t stream);
 
 }  // namespace shg

@@ -15,6 +15,7 @@
 // The host reads one scalar per check window; everything else stays on the device.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <utility>
@@ -26,6 +27,50 @@
 namespace shg {
 
 namespace {
+
+// Sweeps per launch: the caller's jacobi_block, else one.  On B200 the one-sweep kernel
+// (one voxel per thread, neighbours through L1 / L2) measured faster than the blocked kernel
+// at every depth and size tried, from L2-resident grids (128x128x200) to grids 20x the L2
+// (512x512x250 FP64): 16.6 vs 28.9 us per sweep at 128x128x200 FP64, 325 vs 357 us at
+// 512x512x250 FP64.  The blocked kernel is issue-bound (halo recomputation, one barrier per
+// plane), not memory-bound.
+int sweep_depth(const shg_params& p) {
+    if (p.jacobi_block > 0) return p.jacobi_block;
+    return 1;
+}
+
+// TMA maps of the two temperature buffers and Q for the blocked sweeps.
+template <typename R>
+struct SweepMaps {
+    CUtensorMap a, b, q;
+};
+
+template <typename R>
+shg_status make_sweep_maps(const R* Ta, const R* Tb, const R* Q, int n, int nz, SweepMaps<R>* m) {
+    shg_status rc;
+    if ((rc = make_tb_map<R>(Ta, n, nz, &m->a)) != SHG_OK) return rc;
+    if ((rc = make_tb_map<R>(Tb, n, nz, &m->b)) != SHG_OK) return rc;
+    return make_tb_map<R>(Q, n, nz, &m->q);
+}
+
+// `count` unchecked sweeps, `depth` per launch, ping-ponging cur / nxt (Ta and Tb of the
+// maps); on return cur holds the latest temperature.
+template <typename R>
+cudaError_t run_sweeps(R*& cur, R*& nxt, const R* Ta, const SweepMaps<R>& m, const R* Q, const JacobiCoef<R>& k,
+                       int boundary, int depth, int64_t count, unsigned* tb_err, cudaStream_t s) {
+    while (count > 0) {
+        const int t = (int)std::min<int64_t>(depth, count);
+        cudaError_t e;
+        if (t >= 2)
+            e = launch_jacobi_tb<R>(cur == Ta ? m.a : m.b, m.q, nxt, k, boundary, t, tb_err, s);
+        else
+            e = launch_jacobi<R>(cur, nxt, Q, k, boundary, false, 0, nullptr, nullptr, s);
+        if (e != cudaSuccess) return e;
+        std::swap(cur, nxt);
+        count -= t;
+    }
+    return cudaSuccess;
+}
 
 template <typename R>
 shg_status thermal_run(const shg_params& p, const void* signal_in, void* pump_out, void* signal_out,
@@ -63,18 +108,15 @@ shg_status thermal_run(const shg_params& p, const void* signal_in, void* pump_ou
     const int check_every = p.check_every > 0 ? p.check_every : 5000;
     const int64_t max_sweeps = p.max_sweeps > 0 ? p.max_sweeps : ((int64_t)1 << 40);
     const int max_outer = p.max_outer > 0 ? p.max_outer : 20;
-    const int depth = p.jacobi_block > 0 ? p.jacobi_block : 4;
+    const int depth = sweep_depth(p);
     int64_t total = 0;
     int outer = 0;
     double last = 0.0;
     R* cur = Ta;  // holds the latest temperature (the reference's Tinic == Tfinal after its copy)
     R* nxt = Tb;
-    CUtensorMap map_a, map_b, map_q;
+    SweepMaps<R> maps;
     do {
-        if (depth > 1 && ((rc = make_tb_map<R>(Ta, n, nz, &map_a)) != SHG_OK ||
-                          (rc = make_tb_map<R>(Tb, n, nz, &map_b)) != SHG_OK ||
-                          (rc = make_tb_map<R>(Q, n, nz, &map_q)) != SHG_OK))
-            break;
+        if (depth > 1 && (rc = make_sweep_maps<R>(Ta, Tb, Q, n, nz, &maps)) != SHG_OK) break;
         if ((e = cudaMemsetAsync(resid, 0, 2 * sizeof(double), s)) != cudaSuccess) { rc = cuda_fail(e, "memset"); break; }
         if ((e = launch_thermal_init<R>(Ta, Tb, Q, p, s)) != cudaSuccess) { rc = cuda_fail(e, "thermal init"); break; }
         for (int g = 0; g < max_outer && rc == SHG_OK; ++g) {
@@ -110,22 +152,12 @@ shg_status thermal_run(const shg_params& p, const void* signal_in, void* pump_ou
                 ++counter;
                 if (red < tol) break;
                 // the rest of the window, unchecked: `depth` sweeps per launch
-                int64_t left = std::min<int64_t>(check_every - 1, max_sweeps - counter);
-                while (left > 0) {
-                    const int t = (int)std::min<int64_t>(depth, left);
-                    if (t >= 2)
-                        e = launch_jacobi_tb<R>(cur == Ta ? map_a : map_b, map_q, nxt, k, p.boundary, t, tb_err, s);
-                    else
-                        e = launch_jacobi<R>(cur, nxt, Q, k, p.boundary, false, p.conv_rule, nullptr, nullptr, s);
-                    if (e != cudaSuccess) {
-                        rc = cuda_fail(e, "jacobi sweep");
-                        break;
-                    }
-                    std::swap(cur, nxt);
-                    counter += t;
-                    left -= t;
+                const int64_t left = std::min<int64_t>(check_every - 1, max_sweeps - counter);
+                if ((e = run_sweeps<R>(cur, nxt, Ta, maps, Q, k, p.boundary, depth, left, tb_err, s)) != cudaSuccess) {
+                    rc = cuda_fail(e, "jacobi sweep");
+                    break;
                 }
-                if (rc != SHG_OK) break;
+                counter += std::max<int64_t>(left, 0);
             }
             total += counter;
             last = red;
@@ -204,7 +236,59 @@ shg_status thermal_run(const shg_params& p, const void* signal_in, void* pump_ou
     return rc;
 }
 
+template <typename R>
+shg_status heat_run(const shg_params& p, R* T, const R* Q, int64_t sweeps, cudaStream_t s) {
+    const int n = p.nx, nz = p.nz;
+    const size_t nt = (size_t)n * n * nz, arr = sizeof(R) * nt;
+    const int depth = sweep_depth(p);
+    cudaError_t e;
+    char* buf = nullptr;
+    if ((e = cudaMallocAsync((void**)&buf, arr + 256, s)) != cudaSuccess) return cuda_fail(e, "cudaMallocAsync");
+    R* other = reinterpret_cast<R*>(buf);
+    unsigned* tb_err = reinterpret_cast<unsigned*>(buf + arr);
+    shg_status rc = SHG_OK;
+    do {
+        SweepMaps<R> maps;
+        if (depth > 1 && (rc = make_sweep_maps<R>(T, other, Q, n, nz, &maps)) != SHG_OK) break;
+        // both buffers start alike, so the voxels no sweep writes (Dirichlet faces) agree
+        if ((e = cudaMemcpyAsync(other, T, arr, cudaMemcpyDeviceToDevice, s)) != cudaSuccess ||
+            (e = cudaMemsetAsync(tb_err, 0, sizeof(unsigned), s)) != cudaSuccess) {
+            rc = cuda_fail(e, "heat sweeps set-up");
+            break;
+        }
+        const JacobiCoef<R> k = make_jacobi_coef<R>(p);
+        R* cur = T;
+        R* nxt = other;
+        if ((e = run_sweeps<R>(cur, nxt, T, maps, Q, k, p.boundary, depth, sweeps, tb_err, s)) != cudaSuccess) {
+            rc = cuda_fail(e, "jacobi sweep");
+            break;
+        }
+        if (cur != T && (e = cudaMemcpyAsync(T, cur, arr, cudaMemcpyDeviceToDevice, s)) != cudaSuccess) {
+            rc = cuda_fail(e, "heat sweeps result");
+            break;
+        }
+        unsigned h = 0;
+        if ((e = cudaMemcpyAsync(&h, tb_err, sizeof(h), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(s)) != cudaSuccess) {
+            rc = cuda_fail(e, "heat sweeps");
+            break;
+        }
+        if (h) rc = fail(SHG_ERR_CUDA, "blocked Jacobi sweep: a staged plane did not arrive");
+    } while (0);
+    cudaFreeAsync(buf, s);
+    e = cudaGetLastError();
+    if (rc == SHG_OK && e != cudaSuccess) rc = cuda_fail(e, "heat sweeps");
+    return rc;
+}
+
 }  // namespace
+
+shg_status heat_sweeps_device(const shg_params& p, void* temperature, const void* q, int64_t sweeps,
+                              cudaStream_t stream) {
+    if (p.precision == 32)
+        return heat_run<float>(p, reinterpret_cast<float*>(temperature), reinterpret_cast<const float*>(q), sweeps, stream);
+    return heat_run<double>(p, reinterpret_cast<double*>(temperature), reinterpret_cast<const double*>(q), sweeps, stream);
+}
 
 shg_status thermal_solve_device(const shg_params& p, const void* signal_in, void* pump_out, void* signal_out,
                                 void* temperature_out, shg_stats* stats, cudaStream_t stream, void* slices_p,

@@ -25,7 +25,7 @@ LIB_PATH = os.path.join(PKG, "libshg_b200.so")
 EXPORTS = (
     "shg_default_params", "shg_check_params", "shg_steps", "shg_solve", "shg_solve_slices", "shg_solve_device",
     "shg_solve_batch_device", "shg_solve_batch_device_noalloc", "shg_grad", "shg_sh_power", "shg_last_error",
-    "shg_status_string", "shg_version",
+    "shg_status_string", "shg_version", "shg_heat_sweeps_device",
 )
 
 
@@ -80,6 +80,8 @@ def lib() -> ctypes.CDLL:
         L.shg_grad.restype = ctypes.c_int
         L.shg_sh_power.argtypes = [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
         L.shg_sh_power.restype = ctypes.c_int
+        L.shg_heat_sweeps_device.argtypes = [P, vp, vp, ctypes.c_int64, vp]
+        L.shg_heat_sweeps_device.restype = ctypes.c_int
         L.shg_last_error.restype = ctypes.c_char_p
         L.shg_status_string.argtypes = [ctypes.c_int32]
         L.shg_status_string.restype = ctypes.c_char_p
@@ -181,6 +183,15 @@ def solve_batch_device(ps: list[ShgParams], pump_outs=None, signal_outs=None, st
     s = None if stream is None else vp(stream)
     _check(lib().shg_solve_batch_device(arr, n, ptrs(pump_outs), ptrs(signal_outs), pp, s))
     return power
+
+
+def heat_sweeps_device(p: ShgParams, temperature, q, sweeps: int, stream=None) -> None:
+    """`sweeps` Jacobi sweeps of the heat equation in place on a device tensor
+    (shg_heat_sweeps_device); temperature and q are contiguous real tensors of shape
+    (nz, ny, nx) in the precision of p."""
+    s = None if stream is None else ctypes.c_void_p(stream)
+    _check(lib().shg_heat_sweeps_device(ctypes.byref(p), ctypes.c_void_p(temperature.data_ptr()),
+                                        ctypes.c_void_p(q.data_ptr()), int(sweeps), s))
 
 
 def _dptr(a):

@@ -103,7 +103,8 @@ typedef struct shg_params {
     double jacobi_tol;      /* <= 0 selects the reference tolerance 5e-4/TSIZE (Solver.h:332) */
     int64_t max_sweeps;     /* Jacobi sweep cap per outer iteration (<= 0: 2^40) */
     /* Sweeps fused per launch between convergence checks (temporal blocking): 0 = automatic
-     * (4), 1 = one sweep per launch, 2..4 = that many.  Every setting gives the same
+     * (one sweep per launch, the fastest on B200 at every grid size measured), 1 = one
+     * sweep per launch, 2..4 = that many through the TMA-staged blocked kernel.  Every setting gives the same
      * temperatures bit for bit; the checked sweep of each window always runs alone. */
     int32_t jacobi_block;
     int32_t reserved0;
@@ -187,6 +188,19 @@ SHG_API shg_status shg_solve_batch_device(const shg_params* params, int32_t coun
 SHG_API shg_status shg_solve_batch_device_noalloc(const shg_params* params, int32_t count,
                                                   void* const* pump_out_dev, void* const* signal_out_dev,
                                                   double* sh_power_out, void* stream);
+
+/*
+ * `sweeps` Jacobi sweeps of the heat equation on caller device buffers, without
+ * convergence checks: the Tfield::upDate loop of the thermal run (Tfield.h:350-364,
+ * Solver.h:339-355; kernelHeatEquationTopOpen / OvenSurrounded, Tfield.h:93-240).
+ *   temperature_dev  nx*ny*nz reals: the starting temperature on entry, the result on
+ *                    return; voxels the model holds fixed (Dirichlet faces) keep their value.
+ *   q_dev            nx*ny*nz reals: the heat source Q.
+ * Uses the grid, precision, kappa, h_conv, t_inf, boundary and jacobi_block of *p (p->thermal
+ * is ignored).  Stream-ordered on `stream`; synchronises once at the end.
+ */
+SHG_API shg_status shg_heat_sweeps_device(const shg_params* p, void* temperature_dev, const void* q_dev,
+                                          int64_t sweeps, void* stream);
 
 /* Gradients of the SH output power (plain runs), from shg_grad. */
 typedef struct shg_grad_result {

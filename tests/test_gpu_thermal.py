@@ -107,9 +107,44 @@ def test_blocked_sweeps_are_bit_identical(precision, boundary, n, nz, check_ever
     p.jacobi_tol = 2e-3
     p.max_sweeps = 4000
     ref = shg.solve(p.replace(jacobi_block=1), want_temperature=True)
-    for blk in (0, 2, 3):
+    for blk in (0, 2, 3, 4):
         r = shg.solve(p.replace(jacobi_block=blk), want_temperature=True)
         assert r.stats.jacobi_sweeps == ref.stats.jacobi_sweeps
         assert r.stats.outer_iterations == ref.stats.outer_iterations
         assert np.array_equal(r.temperature, ref.temperature), blk
         assert np.array_equal(r.signal, ref.signal) and np.array_equal(r.pump, ref.pump)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [64, 32])
+@pytest.mark.parametrize("boundary", [P.SHG_BOUNDARY_TOP_OPEN, P.SHG_BOUNDARY_OVEN_SURROUNDED])
+def test_heat_sweeps_match_oracle(precision, boundary):
+    """shg_heat_sweeps_device (the Tfield::upDate loop) against the oracle's sweep repeated,
+    from a random temperature and heat source, for every sweep depth; depths agree bit for
+    bit with one sweep per launch."""
+    import torch
+
+    n, nz, sweeps = 48, 21, 11
+    p = P.workload(n, nz, 6000.0, 3.0, 30.0, 3000.0, 33.0, precision=precision, thermal=1)
+    p.boundary = boundary
+    rng = np.random.default_rng(7)
+    rdt = np.float64 if precision == 64 else np.float32
+    T0 = (30.0 + 5.0 * rng.random((nz, n, n))).astype(rdt)
+    Q = (1e-6 * rng.random((nz, n, n))).astype(rdt)
+    Ti, Tf = T0.copy(), T0.copy()
+    for _ in range(sweeps):
+        O.jacobi_sweep(p, Ti, Q, Tf)
+        Ti, Tf = Tf, Ti
+    tdt = torch.float64 if precision == 64 else torch.float32
+    q_d = torch.from_numpy(Q).to("cuda")
+    outs = {}
+    for blk in (1, 2, 3, 4, 0):
+        t_d = torch.from_numpy(T0).to("cuda")
+        shg.heat_sweeps_device(p.replace(jacobi_block=blk), t_d, q_d, sweeps)
+        torch.cuda.synchronize()
+        outs[blk] = t_d.cpu().numpy()
+        assert outs[blk].dtype == np.dtype(rdt) and t_d.dtype == tdt
+    for blk in (2, 3, 4, 0):
+        assert np.array_equal(outs[blk], outs[1]), blk
+    tol = 1e-12 if precision == 64 else 2e-6
+    assert np.max(np.abs(outs[1] - Ti)) / np.max(np.abs(Ti)) < tol

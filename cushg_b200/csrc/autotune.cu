@@ -1,0 +1,113 @@
+// autotune.cu — shg_autotune: picks, per (precision, grid side) class, the compiled variant of
+// the fused march (cluster split, threads per CTA) with the highest throughput on this
+// device.  The reference fixes its launch shapes at compile time (src/cuSHG.cu:22-23) and
+// has nothing to tune.
+//
+// The tuning batch: enough instances of the class to fill the device three times over for
+// the variant with the most resident clusters, nz = 33 (32 steps), parameters spread like a
+// sweep (waist, focus, power), so the timing sees the steady state of a persistent launch.
+// Each variant runs once untimed, then three times between CUDA events; the median counts.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "shg_host.h"
+#include "ssfm_variants.h"
+
+using namespace shg;
+
+extern "C" shg_status shg_autotune(int32_t precision, int32_t n, shg_tune_result* out) {
+    clear_error();
+    if (!out) return fail(SHG_ERR_INVALID, "out is NULL");
+    if (precision != 32 && precision != 64) return fail(SHG_ERR_INVALID, "precision must be 32 or 64");
+    const PlainVariant* cand[16];
+    const int nc = plain_candidates(precision, n, cand, 16);
+    if (nc == 0) return fail(SHG_ERR_UNSUPPORTED, "no kernel built for grid side %d at precision %d", n, precision);
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(SHG_ERR_NO_DEVICE, "no CUDA device visible");
+    }
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    // instances: three device fills for the variant with the smallest cluster
+    int cmin = 16;
+    for (int i = 0; i < nc; ++i) cmin = std::min(cmin, cand[i]->cluster);
+    const int count = std::max(8, 3 * 2 * sms / cmin);
+    shg_params base;
+    shg_default_params(&base);
+    base.nx = base.ny = n;
+    base.nz = 33;
+    base.precision = precision;
+    base.lz = 10000.0;
+    std::vector<InstDesc> descs(count);
+    for (int i = 0; i < count; ++i) {
+        shg_params q = base;
+        const double u = (i + 0.5) / count;
+        q.waist = 15.0 + 45.0 * u;
+        q.lx = q.ly = 12.0 * q.waist;
+        q.focus = q.lz * u;
+        q.power = 1.0 + 49.0 * (1.0 - u);
+        descs[i] = make_plain_desc(q, q.temp, q.temp);
+        descs[i].slot = i;
+    }
+    cudaStream_t s = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
+    void* buf = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    shg_status rc = SHG_OK;
+    double rate[16] = {0};
+    do {
+        if ((e = cudaMallocAsync(&buf, sizeof(InstDesc) * (size_t)count + 256, s)) != cudaSuccess) {
+            rc = cuda_fail(e, "cudaMallocAsync");
+            break;
+        }
+        InstDesc* dd = reinterpret_cast<InstDesc*>(buf);
+        int* queue = reinterpret_cast<int*>(dd + count);
+        if ((e = cudaMemcpyAsync(dd, descs.data(), sizeof(InstDesc) * (size_t)count, cudaMemcpyHostToDevice, s)) !=
+                cudaSuccess ||
+            (e = cudaEventCreate(&ev[0])) != cudaSuccess || (e = cudaEventCreate(&ev[1])) != cudaSuccess) {
+            rc = cuda_fail(e, "tuning set-up");
+            break;
+        }
+        const double work = (double)count * n * n * (base.nz - 1);
+        for (int c = 0; c < nc && rc == SHG_OK; ++c) {
+            float ms[4] = {0, 0, 0, 0};
+            for (int r = 0; r < 4; ++r) {
+                if ((e = cudaMemsetAsync(queue, 0, sizeof(int), s)) != cudaSuccess ||
+                    (e = cudaEventRecord(ev[0], s)) != cudaSuccess ||
+                    (e = cand[c]->launch(dd, count, queue, s)) != cudaSuccess ||
+                    (e = cudaEventRecord(ev[1], s)) != cudaSuccess || (e = cudaEventSynchronize(ev[1])) != cudaSuccess ||
+                    (e = cudaEventElapsedTime(&ms[r], ev[0], ev[1])) != cudaSuccess) {
+                    rc = cuda_fail(e, "tuning launch");
+                    break;
+                }
+            }
+            std::sort(ms + 1, ms + 4);  // ms[0] is the untimed first run
+            rate[c] = work / (ms[2] * 1e-3);
+        }
+    } while (0);
+    for (cudaEvent_t x : ev)
+        if (x) cudaEventDestroy(x);
+    if (buf) cudaFreeAsync(buf, s);
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+    if (rc != SHG_OK) return rc;
+    int best = 0;
+    for (int c = 1; c < nc; ++c)
+        if (rate[c] > rate[best]) best = c;
+    set_plain_choice(cand[best]);
+    std::memset(out, 0, sizeof(*out));
+    out->precision = precision;
+    out->n = n;
+    out->cluster = cand[best]->cluster;
+    out->threads = cand[best]->threads;
+    out->candidates = nc;
+    out->pt_steps_per_s = rate[best];
+    out->default_pt_steps_per_s = rate[0];
+    return SHG_OK;
+}

@@ -122,7 +122,7 @@ extern "C" shg_status shg_solve_batch_device_noalloc(const shg_params* params, i
     for (int k = 0; k < count;) {
         int j = k;
         while (j < count && var[order[j]] == var[order[k]]) ++j;
-        if ((e = var[order[k]]->launch(ddesc + k, j - k, stream)) != cudaSuccess)
+        if ((e = var[order[k]]->launch(ddesc + k, j - k, nullptr, stream)) != cudaSuccess)
             return cuda_fail(e, "launch ssfm_plain_kernel");
         k = j;
     }

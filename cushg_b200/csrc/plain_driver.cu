@@ -1,11 +1,14 @@
 // plain_driver.cu — host driver of plain (non-thermal) runs: one instance, or a batch of
 // instances with uneven grid sizes and step counts.
 //
-// The batch replaces the one-process-per-point sweep of src/cuSHG.sh:58-94: instances are
-// grouped by compiled variant (precision, grid side), each group is one launch of the
-// fused march with one cluster per instance, groups run concurrently on forked streams,
-// and inside a group instances are ordered longest-first so the block scheduler packs
-// the SMs like a longest-processing-time queue.
+// The batch replaces the one-process-per-point sweep of src/cuSHG.sh:58-94.  Instances are
+// grouped by compiled variant (precision, grid side); each group is ONE persistent launch
+// of the fused march, as many clusters as fit on the device, fed by a device work queue
+// (an atomic counter over the group's descriptors, ordered longest march first, so the
+// clusters drain it like a longest-processing-time schedule).  Groups run concurrently on
+// forked streams, the largest total work first, so the smaller classes fill the SMs the
+// largest one frees at its tail.  A batch plan (shg_batch_plan_*) captures the same
+// sequence once into a CUDA graph and replays it.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -84,7 +87,7 @@ shg_status plain_solve_device(const shg_params& p, const void* signal_in, void* 
             cudaEventCreate(&t1);
             cudaEventRecord(t0, stream);
         }
-        if ((e = v->launch(dd, 1, stream)) != cudaSuccess) { rc = cuda_fail(e, "launch ssfm_plain_kernel"); break; }
+        if ((e = v->launch(dd, 1, nullptr, stream)) != cudaSuccess) { rc = cuda_fail(e, "launch ssfm_plain_kernel"); break; }
         if (stats) {
             cudaEventRecord(t1, stream);
             double h[2] = {0, 0};
@@ -111,10 +114,20 @@ shg_status plain_solve_device(const shg_params& p, const void* signal_in, void* 
     return rc;
 }
 
-shg_status plain_solve_batch(const shg_params* params, int count, void* const* pump_out, void* const* signal_out,
-                             double* sh_power_out, cudaStream_t stream) {
-    if (count == 0) return SHG_OK;
-    // group by variant, longest march first inside a group
+// Batch layout: instances grouped by variant (longest march first inside a group), groups
+// ordered by total work, descriptors in that order.
+struct BatchLayout {
+    struct Group {
+        const PlainVariant* v;
+        int begin, end;
+        double work;
+    };
+    std::vector<InstDesc> descs;  // execution order
+    std::vector<Group> groups;
+};
+
+static BatchLayout batch_layout(const shg_params* params, int count, void* const* pump_out, void* const* signal_out,
+                                double* power_slots) {
     struct Item { const PlainVariant* v; int idx; double cost; };
     std::vector<Item> items(count);
     for (int i = 0; i < count; ++i) {
@@ -125,65 +138,82 @@ shg_status plain_solve_batch(const shg_params* params, int count, void* const* p
         if (a.v != b.v) return a.v < b.v;
         return a.cost > b.cost;
     });
-    std::vector<InstDesc> descs(count);
-    cudaError_t e;
-    void* buf = nullptr;
-    const size_t bytes = sizeof(InstDesc) * (size_t)count + 2 * sizeof(double) * (size_t)count;
-    if ((e = cudaMallocAsync(&buf, bytes, stream)) != cudaSuccess) return cuda_fail(e, "cudaMallocAsync");
-    InstDesc* dd = reinterpret_cast<InstDesc*>(buf);
-    double* pw = reinterpret_cast<double*>(reinterpret_cast<char*>(buf) + sizeof(InstDesc) * (size_t)count);
+    BatchLayout L;
+    L.descs.resize(count);
     for (int k = 0; k < count; ++k) {
         const int i = items[k].idx;
         InstDesc d = make_plain_desc(params[i], params[i].temp, params[i].temp);
         d.slot = i;
         d.pump_out = pump_out ? pump_out[i] : nullptr;
         d.signal_out = signal_out ? signal_out[i] : nullptr;
-        d.power_out = pw + 2 * (size_t)i;
-        descs[k] = d;
+        d.power_out = power_slots + 2 * (size_t)i;
+        L.descs[k] = d;
     }
+    for (int k = 0; k < count;) {
+        int j = k;
+        double w = 0;
+        while (j < count && items[j].v == items[k].v) w += items[j++].cost;
+        L.groups.push_back({items[k].v, k, j, w});
+        k = j;
+    }
+    std::sort(L.groups.begin(), L.groups.end(),
+              [](const BatchLayout::Group& a, const BatchLayout::Group& b) { return a.work > b.work; });
+    return L;
+}
+
+// Enqueue the batched march on `stream`: zero the groups' work-queue counters, then one
+// persistent launch per group, the groups on the fork streams `fs` (joined back into
+// `stream`) when there are several.  Capturable into a CUDA graph.
+static cudaError_t enqueue_batch(const BatchLayout& L, const InstDesc* dd, int* queues, cudaStream_t stream,
+                                 cudaStream_t* fs, cudaEvent_t* ev, int nfork) {
+    cudaError_t e;
+    const int ng = (int)L.groups.size();
+    if ((e = cudaMemsetAsync(queues, 0, sizeof(int) * (size_t)ng, stream)) != cudaSuccess) return e;
+    if (ng == 1) return L.groups[0].v->launch(dd + L.groups[0].begin, L.groups[0].end - L.groups[0].begin, queues, stream);
+    const int nf = std::min(ng, nfork);
+    if ((e = cudaEventRecord(ev[nfork], stream)) != cudaSuccess) return e;
+    for (int g = 0; g < nf; ++g)
+        if ((e = cudaStreamWaitEvent(fs[g], ev[nfork], 0)) != cudaSuccess) return e;
+    for (int g = 0; g < ng; ++g) {
+        const BatchLayout::Group& G = L.groups[g];
+        if ((e = G.v->launch(dd + G.begin, G.end - G.begin, queues + g, fs[g % nf])) != cudaSuccess) return e;
+    }
+    for (int g = 0; g < nf; ++g) {
+        if ((e = cudaEventRecord(ev[g], fs[g])) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(stream, ev[g], 0)) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+static size_t batch_bytes(int count) {
+    return sizeof(InstDesc) * (size_t)count + 2 * sizeof(double) * (size_t)count + sizeof(int) * 64;
+}
+
+shg_status plain_solve_batch(const shg_params* params, int count, void* const* pump_out, void* const* signal_out,
+                             double* sh_power_out, cudaStream_t stream) {
+    if (count == 0) return SHG_OK;
+    cudaError_t e;
+    void* buf = nullptr;
+    if ((e = cudaMallocAsync(&buf, batch_bytes(count), stream)) != cudaSuccess) return cuda_fail(e, "cudaMallocAsync");
+    InstDesc* dd = reinterpret_cast<InstDesc*>(buf);
+    double* pw = reinterpret_cast<double*>(dd + count);
+    int* queues = reinterpret_cast<int*>(pw + 2 * (size_t)count);
+    const BatchLayout L = batch_layout(params, count, pump_out, signal_out, pw);
     shg_status rc = SHG_OK;
     do {
-        if ((e = cudaMemcpyAsync(dd, descs.data(), sizeof(InstDesc) * (size_t)count, cudaMemcpyHostToDevice,
+        if (L.groups.size() > 64) { rc = fail(SHG_ERR_UNSUPPORTED, "more than 64 kernel variants in one batch"); break; }
+        if ((e = cudaMemcpyAsync(dd, L.descs.data(), sizeof(InstDesc) * (size_t)count, cudaMemcpyHostToDevice,
                                  stream)) != cudaSuccess) {
             rc = cuda_fail(e, "cudaMemcpyAsync descs");
             break;
         }
-        // groups: [begin, end) runs of the same variant, biggest total work first
-        struct Group { const PlainVariant* v; int begin, end; double work; };
-        std::vector<Group> groups;
-        for (int k = 0; k < count;) {
-            int j = k;
-            double w = 0;
-            while (j < count && items[j].v == items[k].v) w += items[j++].cost;
-            groups.push_back({items[k].v, k, j, w});
-            k = j;
-        }
-        std::sort(groups.begin(), groups.end(), [](const Group& a, const Group& b) { return a.work > b.work; });
-        if (groups.size() == 1) {
-            if ((e = groups[0].v->launch(dd + groups[0].begin, groups[0].end - groups[0].begin, stream)) != cudaSuccess) {
-                rc = cuda_fail(e, "launch ssfm_plain_kernel");
-                break;
-            }
-        } else {
-            int dev = 0;
-            cudaGetDevice(&dev);
-            ForkStreams* f = nullptr;
-            if ((e = fork_streams(dev, &f)) != cudaSuccess) { rc = cuda_fail(e, "stream pool"); break; }
-            const int ng = (int)std::min<size_t>(groups.size(), ForkStreams::kMax);
-            cudaEventRecord(f->ev[ForkStreams::kMax], stream);
-            for (int g = 0; g < (int)groups.size(); ++g) {
-                cudaStream_t s = f->s[g % ng];
-                if (g < ng) cudaStreamWaitEvent(s, f->ev[ForkStreams::kMax], 0);
-                if ((e = groups[g].v->launch(dd + groups[g].begin, groups[g].end - groups[g].begin, s)) != cudaSuccess) {
-                    rc = cuda_fail(e, "launch ssfm_plain_kernel");
-                    break;
-                }
-            }
-            for (int g = 0; g < ng; ++g) {
-                cudaEventRecord(f->ev[g], f->s[g]);
-                cudaStreamWaitEvent(stream, f->ev[g], 0);
-            }
-            if (rc != SHG_OK) break;
+        int dev = 0;
+        cudaGetDevice(&dev);
+        ForkStreams* f = nullptr;
+        if ((e = fork_streams(dev, &f)) != cudaSuccess) { rc = cuda_fail(e, "stream pool"); break; }
+        if ((e = enqueue_batch(L, dd, queues, stream, f->s, f->ev, ForkStreams::kMax)) != cudaSuccess) {
+            rc = cuda_fail(e, "launch ssfm_plain_kernel");
+            break;
         }
         if (sh_power_out) {
             std::vector<double> h(2 * (size_t)count);
@@ -203,3 +233,118 @@ shg_status plain_solve_batch(const shg_params* params, int count, void* const* p
 }
 
 }  // namespace shg
+
+// ------------------------------------------------------------------ batch plans (graphs)
+struct shg_batch_plan {
+    int count = 0;
+    int device = 0;
+    void* buf = nullptr;          // descriptors, power slots, queue counters (cudaMalloc)
+    double* powers = nullptr;     // device, [2 * count]
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t fork[shg::ForkStreams::kMax] = {};
+    cudaEvent_t ev[shg::ForkStreams::kMax + 1] = {};
+};
+
+using namespace shg;
+
+static void plan_release(shg_batch_plan* P) {
+    if (!P) return;
+    if (P->exec) cudaGraphExecDestroy(P->exec);
+    if (P->graph) cudaGraphDestroy(P->graph);
+    for (cudaStream_t s : P->fork)
+        if (s) cudaStreamDestroy(s);
+    for (cudaEvent_t e : P->ev)
+        if (e) cudaEventDestroy(e);
+    if (P->buf) cudaFree(P->buf);
+    delete P;
+}
+
+extern "C" shg_status shg_batch_plan_create(const shg_params* params, int32_t count, void* const* pump_out_dev,
+                                            void* const* signal_out_dev, shg_batch_plan** plan) {
+    clear_error();
+    if (!plan) return fail(SHG_ERR_INVALID, "plan is NULL");
+    *plan = nullptr;
+    if (!params || count <= 0) return fail(SHG_ERR_INVALID, "params is NULL or count <= 0");
+    for (int i = 0; i < count; ++i) {
+        shg_status st = shg_check_params(&params[i]);
+        if (st != SHG_OK) return fail(st, "instance %d: %s", i, shg_last_error());
+        if (params[i].thermal) return fail(SHG_ERR_UNSUPPORTED, "instance %d: batched runs are plain (thermal == 0)", i);
+        if (params[i].precision != params[0].precision)
+            return fail(SHG_ERR_INVALID, "instance %d: all instances must share one precision", i);
+    }
+    shg_batch_plan* P = new shg_batch_plan;
+    P->count = count;
+    cudaError_t e;
+    shg_status rc = SHG_OK;
+    cudaStream_t cap = nullptr;
+    do {
+        if ((e = cudaGetDevice(&P->device)) != cudaSuccess) { rc = cuda_fail(e, "cudaGetDevice"); break; }
+        if ((e = cudaMalloc(&P->buf, batch_bytes(count))) != cudaSuccess) { rc = cuda_fail(e, "cudaMalloc"); break; }
+        InstDesc* dd = reinterpret_cast<InstDesc*>(P->buf);
+        P->powers = reinterpret_cast<double*>(dd + count);
+        int* queues = reinterpret_cast<int*>(P->powers + 2 * (size_t)count);
+        const BatchLayout L = batch_layout(params, count, pump_out_dev, signal_out_dev, P->powers);
+        if (L.groups.size() > 64) { rc = fail(SHG_ERR_UNSUPPORTED, "more than 64 kernel variants in one batch"); break; }
+        if ((e = cudaMemcpy(dd, L.descs.data(), sizeof(InstDesc) * (size_t)count, cudaMemcpyHostToDevice)) != cudaSuccess) {
+            rc = cuda_fail(e, "cudaMemcpy descriptors");
+            break;
+        }
+        for (auto& s : P->fork)
+            if ((e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)) != cudaSuccess) break;
+        if (e == cudaSuccess)
+            for (auto& ev : P->ev)
+                if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) break;
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
+        if (e != cudaSuccess) { rc = cuda_fail(e, "plan streams"); break; }
+        // a first launch outside the capture sets the kernels' attributes and sizes
+        for (const auto& G : L.groups)
+            if ((e = G.v->launch(dd + G.begin, 0, queues, cap)) != cudaSuccess) break;
+        if (e != cudaSuccess) { rc = cuda_fail(e, "kernel set-up"); break; }
+        if ((e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) {
+            rc = cuda_fail(e, "cudaStreamBeginCapture");
+            break;
+        }
+        const cudaError_t ee = enqueue_batch(L, dd, queues, cap, P->fork, P->ev, ForkStreams::kMax);
+        e = cudaStreamEndCapture(cap, &P->graph);
+        if (ee != cudaSuccess) { rc = cuda_fail(ee, "capture of the batched march"); break; }
+        if (e != cudaSuccess) { rc = cuda_fail(e, "cudaStreamEndCapture"); break; }
+        if ((e = cudaGraphInstantiate(&P->exec, P->graph, 0)) != cudaSuccess) {
+            rc = cuda_fail(e, "cudaGraphInstantiate");
+            break;
+        }
+    } while (0);
+    if (cap) cudaStreamDestroy(cap);
+    if (rc != SHG_OK) {
+        plan_release(P);
+        return rc;
+    }
+    *plan = P;
+    return SHG_OK;
+}
+
+extern "C" shg_status shg_batch_plan_launch(shg_batch_plan* plan, void* stream) {
+    clear_error();
+    if (!plan || !plan->exec) return fail(SHG_ERR_INVALID, "plan is NULL");
+    const cudaError_t e = cudaGraphLaunch(plan->exec, (cudaStream_t)stream);
+    return e == cudaSuccess ? SHG_OK : cuda_fail(e, "cudaGraphLaunch");
+}
+
+extern "C" shg_status shg_batch_plan_powers(shg_batch_plan* plan, double* sh_power_out, void* stream) {
+    clear_error();
+    if (!plan || !sh_power_out) return fail(SHG_ERR_INVALID, "plan or sh_power_out is NULL");
+    std::vector<double> h(2 * (size_t)plan->count);
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(h.data(), plan->powers, sizeof(double) * h.size(), cudaMemcpyDeviceToHost,
+                             (cudaStream_t)stream)) != cudaSuccess ||
+        (e = cudaStreamSynchronize((cudaStream_t)stream)) != cudaSuccess)
+        return cuda_fail(e, "plan powers");
+    for (int i = 0; i < plan->count; ++i) sh_power_out[i] = h[2 * (size_t)i];
+    return SHG_OK;
+}
+
+extern "C" void shg_batch_plan_destroy(shg_batch_plan* plan) {
+    if (!plan) return;
+    cudaDeviceSynchronize();
+    plan_release(plan);
+}

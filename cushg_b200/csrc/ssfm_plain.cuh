@@ -182,8 +182,13 @@ __device__ __forceinline__ void thermal_coef(const InstDesc& d, double dki, int 
     }
 }
 
+// Persistent march: each cluster takes instances from the device work queue *queue (an
+// atomic counter the host zeroes before the launch, instances in the descriptor order the
+// host chose: longest march first) until the queue is empty.  queue == nullptr: one
+// instance per cluster, instance = cluster index.
 template <typename T, int N, int C, int NT, bool THERM, int MINB = 1>
-__global__ void __launch_bounds__(NT, MINB) ssfm_plain_kernel(const InstDesc* __restrict__ descs) {
+__global__ void __launch_bounds__(NT, MINB)
+    ssfm_plain_kernel(const InstDesc* __restrict__ descs, int count, int* __restrict__ queue) {
     using Cfg = PlainCfg<T, N, C, NT, THERM>;
     constexpr int R2 = Cfg::R2, RL = Cfg::RL, SW = Cfg::SW;
     constexpr int JA = Cfg::JA, JB = Cfg::JB, JCA = Cfg::JCA, JCB = Cfg::JCB;
@@ -204,292 +209,310 @@ __global__ void __launch_bounds__(NT, MINB) ssfm_plain_kernel(const InstDesc* __
     double* dkint = red + 2 * (NT / 32) + 4;           // thermal: [RL*N] running Δk prefix
 
     const int tid = threadIdx.x;
-    const int inst = blockIdx.x / C;
     const int crank = (C > 1) ? (int)cg::this_cluster().block_rank() : 0;
-    const InstDesc d = descs[inst];
-    const int nsteps = d.nsteps;
 
     auto cluster_sync = [&]() {
         if constexpr (C > 1) cg::this_cluster().sync();
         else __syncthreads();
     };
 
-    // ---- tables -----------------------------------------------------------------
-    init_tables<T, N>(d, tw, pxp, pxs, pyp, pys, tid, NT);
-    if (!THERM && tid < 3) stage_coef<T>(d, 0, 0.0, tid, coef);
-
-    // ---- initial fields: setPump (Efields.h:84-119), SH = 0 or given ---------------
-    const V* sin_g = reinterpret_cast<const V*>(d.signal_in);
-    for (int e = tid; e < Cfg::PLANE; e += NT) {
-        const int lr = e / N, x = e % N;
-        const int y = crank + C * lr;
-        const double2 pv = pump_value(d, x, y, d.amp_re, d.amp_im, d.den_re, d.den_im);
-        Ps[sidx<N, R2, SW>(lr, x)] = mk<T>((T)pv.x, (T)pv.y);
-        Ss[sidx<N, R2, SW>(lr, x)] = d.has_signal_in ? sin_g[(size_t)y * N + x] : mk<T>((T)0, (T)0);
-        if (d.slices_p) reinterpret_cast<V*>(d.slices_p)[(size_t)y * N + x] = Ps[sidx<N, R2, SW>(lr, x)];
-        if (d.slices_s) reinterpret_cast<V*>(d.slices_s)[(size_t)y * N + x] = Ss[sidx<N, R2, SW>(lr, x)];
-    }
-    __syncthreads();
-
-    const T hap = (T)d.hap, has = (T)d.has, qs = (T)d.qs, dz6 = (T)(d.dz / 6.0);
-
-    // nsteps >= 1 (the host rejects nz < 2)
-    //
-    // Code size matters more than instruction count here: the step loop cycles through
-    // every pass, so each pass keeps a single copy of its transform (the inverse is computed
-    // as conj(DFT(conj(x))) with the forward body) and the two fields go through it in a
-    // rolled loop.  Forward R2 stage: DFT then twiddle W_N^{n1 k}; inverse: conj twiddle then
-    // IDFT, i.e. conj(DFT(conj(x) W)).
-    auto cj = [](V a) { return mk<T>(a.x, -a.y); };
-
-    // ---- RA: rows, R2-point stage of (row lr, n1) and the pointwise RK4 half-steps -----
-    // mode 0: first (natural order in: RK4(z_0), forward), 1: middle (inverse, RK4(z_s),
-    // RK4(z_{s+1}), forward), 2: last (inverse, RK4(z_s), outputs)
-    using R = T;  // real type of the thermal 3D arrays
-    const R* tnp = reinterpret_cast<const R*>(d.t_np);
-    const R* tns = reinterpret_cast<const R*>(d.t_ns);
-    const R* tdk = reinterpret_cast<const R*>(d.t_dk);
-    R* tq = reinterpret_cast<R*>(d.t_q);
-    constexpr size_t NN = (size_t)N * N;
-
-    // s: index of the step that ends in this pass (-1 in the first pass)
-    auto pass_ra = [&](int mode, int s, const V* cf_prev, const V* cf_next, double& acc_s, double& acc_p) {
-        for (int j = tid; j < JA; j += NT) {
-            const int n1 = j & 15, lr = j >> 4;
+    // next instance of this cluster: rank 0 takes it from the queue and the others read it
+    // from rank 0's shared memory; the second barrier keeps rank 0 (and its shared memory)
+    // alive until every CTA has read it
+    __shared__ int s_next;
+    auto take = [&]() -> int {
+        if (crank == 0 && tid == 0) s_next = atomicAdd(queue, 1);
+        cluster_sync();
+        int v = s_next;
+        if constexpr (C > 1) v = *cg::this_cluster().map_shared_rank(&s_next, 0);
+        cluster_sync();
+        return v;
+    };
+    int inst = queue ? take() : (int)(blockIdx.x / C);
 #pragma unroll 1
-            for (int ph = 0; ph < 5; ++ph) {
-                if (ph == 2) {
-                    // pointwise: the two RK4 applications around the step boundary (the second
-                    // half of step s, then the first half of step s+1)
-                    const int h0 = mode == 0 ? 1 : 0, h1 = mode == 2 ? 1 : 2;
+    while (inst < count) {
+        const InstDesc d = descs[inst];
+        const int nsteps = d.nsteps;
+
+        // ---- tables -----------------------------------------------------------------
+        init_tables<T, N>(d, tw, pxp, pxs, pyp, pys, tid, NT);
+        if (!THERM && tid < 3) stage_coef<T>(d, 0, 0.0, tid, coef);
+
+        // ---- initial fields: setPump (Efields.h:84-119), SH = 0 or given ---------------
+        const V* sin_g = reinterpret_cast<const V*>(d.signal_in);
+        for (int e = tid; e < Cfg::PLANE; e += NT) {
+            const int lr = e / N, x = e % N;
+            const int y = crank + C * lr;
+            const double2 pv = pump_value(d, x, y, d.amp_re, d.amp_im, d.den_re, d.den_im);
+            Ps[sidx<N, R2, SW>(lr, x)] = mk<T>((T)pv.x, (T)pv.y);
+            Ss[sidx<N, R2, SW>(lr, x)] = d.has_signal_in ? sin_g[(size_t)y * N + x] : mk<T>((T)0, (T)0);
+            if (d.slices_p) reinterpret_cast<V*>(d.slices_p)[(size_t)y * N + x] = Ps[sidx<N, R2, SW>(lr, x)];
+            if (d.slices_s) reinterpret_cast<V*>(d.slices_s)[(size_t)y * N + x] = Ss[sidx<N, R2, SW>(lr, x)];
+        }
+        __syncthreads();
+
+        const T hap = (T)d.hap, has = (T)d.has, qs = (T)d.qs, dz6 = (T)(d.dz / 6.0);
+
+        // nsteps >= 1 (the host rejects nz < 2)
+        //
+        // Code size matters more than instruction count here: the step loop cycles through
+        // every pass, so each pass keeps a single copy of its transform (the inverse is computed
+        // as conj(DFT(conj(x))) with the forward body) and the two fields go through it in a
+        // rolled loop.  Forward R2 stage: DFT then twiddle W_N^{n1 k}; inverse: conj twiddle then
+        // IDFT, i.e. conj(DFT(conj(x) W)).
+        auto cj = [](V a) { return mk<T>(a.x, -a.y); };
+
+        // ---- RA: rows, R2-point stage of (row lr, n1) and the pointwise RK4 half-steps -----
+        // mode 0: first (natural order in: RK4(z_0), forward), 1: middle (inverse, RK4(z_s),
+        // RK4(z_{s+1}), forward), 2: last (inverse, RK4(z_s), outputs)
+        using R = T;  // real type of the thermal 3D arrays
+        const R* tnp = reinterpret_cast<const R*>(d.t_np);
+        const R* tns = reinterpret_cast<const R*>(d.t_ns);
+        const R* tdk = reinterpret_cast<const R*>(d.t_dk);
+        R* tq = reinterpret_cast<R*>(d.t_q);
+        constexpr size_t NN = (size_t)N * N;
+
+        // s: index of the step that ends in this pass (-1 in the first pass)
+        auto pass_ra = [&](int mode, int s, const V* cf_prev, const V* cf_next, double& acc_s, double& acc_p) {
+            for (int j = tid; j < JA; j += NT) {
+                const int n1 = j & 15, lr = j >> 4;
 #pragma unroll 1
-                    for (int k = 0; k < R2; ++k) {
-                        const int x = n1 + 16 * k;
-                        const int o = sidx<N, R2, SW>(lr, x);
-                        const size_t g = (size_t)(crank + C * lr) * N + x;
-                        V p = Ps[o], q = Ss[o];
+                for (int ph = 0; ph < 5; ++ph) {
+                    if (ph == 2) {
+                        // pointwise: the two RK4 applications around the step boundary (the second
+                        // half of step s, then the first half of step s+1)
+                        const int h0 = mode == 0 ? 1 : 0, h1 = mode == 2 ? 1 : 2;
 #pragma unroll 1
-                        for (int h = h0; h < h1; ++h) {
-                            const int sl = s + h;  // slice of this half step
-                            if constexpr (THERM) {
-                                const size_t gz = (size_t)sl * NN + g;
-                                double& dki = dkint[lr * N + x];
-                                if (h == 1) dki = (mode == 0 ? 0.0 : dki) + (double)tdk[gz];
-                                const double np = (double)tnp[gz], ns = (double)tns[gz];
-                                V cf[6];
-                                thermal_coef<T>(d, dki, sl, np, ns, cf);
-                                rk4_point<T>(p, q, cf, hap, has, (T)(0.5 * (d.bf_s * ns)), dz6);
-                                if (h == 0 && tq) {
-                                    // kernelSetQ (Tfield.h:260-276) for slice s, after its step
-                                    const R ap2 = p.x * p.x + p.y * p.y, as2 = q.x * q.x + q.y * q.y;
-                                    const R is = (R)d.q_h * (R)ns * as2;
-                                    tq[gz] = (R)d.q_p * (R)np * ap2 + (R)d.q_s * (R)ns * as2 + (R)d.beta_s * (is * is);
-                                }
-                            } else {
-                                rk4_point<T>(p, q, h ? cf_next : cf_prev, hap, has, qs, dz6);
-                            }
-                            if (h == 0 && s + 1 < d.nslices) {
-                                // per-slice record: the fields before step s+1 (Solver.h:289-295)
-                                const size_t gs = (size_t)(s + 1) * NN + g;
-                                if (d.slices_p) reinterpret_cast<V*>(d.slices_p)[gs] = p;
-                                if (d.slices_s) reinterpret_cast<V*>(d.slices_s)[gs] = q;
-                            }
-                            if (h == 0 && s + 1 == d.out_after) {
-                                if (d.pump_out) reinterpret_cast<V*>(d.pump_out)[g] = p;
-                                if (d.signal_out) reinterpret_cast<V*>(d.signal_out)[g] = q;
-                                double ws = 1.0, wp = 1.0;
+                        for (int k = 0; k < R2; ++k) {
+                            const int x = n1 + 16 * k;
+                            const int o = sidx<N, R2, SW>(lr, x);
+                            const size_t g = (size_t)(crank + C * lr) * N + x;
+                            V p = Ps[o], q = Ss[o];
+#pragma unroll 1
+                            for (int h = h0; h < h1; ++h) {
+                                const int sl = s + h;  // slice of this half step
                                 if constexpr (THERM) {
-                                    ws = (double)tns[(size_t)(s + 1) * NN + g];
-                                    wp = (double)tnp[(size_t)(s + 1) * NN + g];
+                                    const size_t gz = (size_t)sl * NN + g;
+                                    double& dki = dkint[lr * N + x];
+                                    if (h == 1) dki = (mode == 0 ? 0.0 : dki) + (double)tdk[gz];
+                                    const double np = (double)tnp[gz], ns = (double)tns[gz];
+                                    V cf[6];
+                                    thermal_coef<T>(d, dki, sl, np, ns, cf);
+                                    rk4_point<T>(p, q, cf, hap, has, (T)(0.5 * (d.bf_s * ns)), dz6);
+                                    if (h == 0 && tq) {
+                                        // kernelSetQ (Tfield.h:260-276) for slice s, after its step
+                                        const R ap2 = p.x * p.x + p.y * p.y, as2 = q.x * q.x + q.y * q.y;
+                                        const R is = (R)d.q_h * (R)ns * as2;
+                                        tq[gz] = (R)d.q_p * (R)np * ap2 + (R)d.q_s * (R)ns * as2 + (R)d.beta_s * (is * is);
+                                    }
+                                } else {
+                                    rk4_point<T>(p, q, h ? cf_next : cf_prev, hap, has, qs, dz6);
                                 }
-                                acc_s += ws * ((double)q.x * (double)q.x + (double)q.y * (double)q.y);
-                                acc_p += wp * ((double)p.x * (double)p.x + (double)p.y * (double)p.y);
+                                if (h == 0 && s + 1 < d.nslices) {
+                                    // per-slice record: the fields before step s+1 (Solver.h:289-295)
+                                    const size_t gs = (size_t)(s + 1) * NN + g;
+                                    if (d.slices_p) reinterpret_cast<V*>(d.slices_p)[gs] = p;
+                                    if (d.slices_s) reinterpret_cast<V*>(d.slices_s)[gs] = q;
+                                }
+                                if (h == 0 && s + 1 == d.out_after) {
+                                    if (d.pump_out) reinterpret_cast<V*>(d.pump_out)[g] = p;
+                                    if (d.signal_out) reinterpret_cast<V*>(d.signal_out)[g] = q;
+                                    double ws = 1.0, wp = 1.0;
+                                    if constexpr (THERM) {
+                                        ws = (double)tns[(size_t)(s + 1) * NN + g];
+                                        wp = (double)tnp[(size_t)(s + 1) * NN + g];
+                                    }
+                                    acc_s += ws * ((double)q.x * (double)q.x + (double)q.y * (double)q.y);
+                                    acc_p += wp * ((double)p.x * (double)p.x + (double)p.y * (double)p.y);
+                                }
+                            }
+                            if (mode != 2) {
+                                Ps[o] = p;
+                                Ss[o] = q;
                             }
                         }
-                        if (mode != 2) {
-                            Ps[o] = p;
-                            Ss[o] = q;
-                        }
+                        continue;
                     }
-                    continue;
-                }
-                const bool inv = ph < 2;
-                if ((inv && mode == 0) || (!inv && mode == 2)) continue;
-                V* F = (ph == 1 || ph == 3) ? Ss : Ps;
-                V v[R2];
+                    const bool inv = ph < 2;
+                    if ((inv && mode == 0) || (!inv && mode == 2)) continue;
+                    V* F = (ph == 1 || ph == 3) ? Ss : Ps;
+                    V v[R2];
 #pragma unroll
-                for (int k = 0; k < R2; ++k) v[k] = F[sidx<N, R2, SW>(lr, n1 + 16 * k)];
-                if (inv) {
-                    v[0] = cj(v[0]);
+                    for (int k = 0; k < R2; ++k) v[k] = F[sidx<N, R2, SW>(lr, n1 + 16 * k)];
+                    if (inv) {
+                        v[0] = cj(v[0]);
 #pragma unroll
-                    for (int k = 1; k < R2; ++k) v[k] = mulw(cj(v[k]), tw[k * 16 + n1]);
-                }
-                Dft<R2, -1, T>::run(v);
-                if (inv) {
-#pragma unroll
-                    for (int k = 0; k < R2; ++k) v[k] = cj(v[k]);
-                } else {
-#pragma unroll
-                    for (int k = 1; k < R2; ++k) v[k] = mulw(v[k], tw[k * 16 + n1]);
-                }
-#pragma unroll
-                for (int k = 0; k < R2; ++k) F[sidx<N, R2, SW>(lr, n1 + 16 * k)] = v[k];
-            }
-        }
-    };
-
-    // ---- RB: rows, 16-point DFT over n1 (in place, digit-reversed output) ----------
-    auto pass_rb = [&](bool inv) {
-        for (int j = tid; j < JB; j += NT) {
-            const int k2 = j % R2, lr = j / R2;
-#pragma unroll 1
-            for (int f = 0; f < 2; ++f) {
-                V* F = f ? Ss : Ps;
-                V u[16];
-#pragma unroll
-                for (int n = 0; n < 16; ++n) {
-                    u[n] = F[sidx<N, R2, SW>(lr, n + 16 * k2)];
-                    if (inv) u[n] = cj(u[n]);
-                }
-                Dft<16, -1, T>::run(u);
-#pragma unroll
-                for (int n = 0; n < 16; ++n) F[sidx<N, R2, SW>(lr, n + 16 * k2)] = inv ? cj(u[n]) : u[n];
-            }
-        }
-    };
-
-    // ---- CA: columns, R2-point stage over n2 on this CTA's rows ----------------------
-    auto pass_ca = [&](bool inv) {
-        for (int j = tid; j < JCA; j += NT) {
-            const int x = j % N, n1l = j / N;
-            const int n1 = crank + C * n1l;
-#pragma unroll 1
-            for (int f = 0; f < 2; ++f) {
-                V* F = f ? Ss : Ps;
-                V v[R2];
-#pragma unroll
-                for (int k = 0; k < R2; ++k) v[k] = F[sidx<N, R2, SW>(n1l + CPR * k, x)];
-                if (inv) {
-                    v[0] = cj(v[0]);
-#pragma unroll
-                    for (int k = 1; k < R2; ++k) v[k] = mulw(cj(v[k]), tw[k * 16 + n1]);
-                }
-                Dft<R2, -1, T>::run(v);
-                if (inv) {
-#pragma unroll
-                    for (int k = 0; k < R2; ++k) v[k] = cj(v[k]);
-                } else {
-#pragma unroll
-                    for (int k = 1; k < R2; ++k) v[k] = mulw(v[k], tw[k * 16 + n1]);
-                }
-#pragma unroll
-                for (int k = 0; k < R2; ++k) F[sidx<N, R2, SW>(n1l + CPR * k, x)] = v[k];
-            }
-        }
-    };
-
-    // ---- CB: columns, DFT over n1 across the cluster, propagator, IDFT ----------------
-    auto pass_cb = [&]() {
-        V* rP[C];
-        V* rS[C];
-#pragma unroll
-        for (int r = 0; r < C; ++r) {
-            if constexpr (C > 1) {
-                rP[r] = cg::this_cluster().map_shared_rank(Ps, r);
-                rS[r] = cg::this_cluster().map_shared_rank(Ss, r);
-            } else {
-                rP[r] = Ps;
-                rS[r] = Ss;
-            }
-        }
-        for (int j = tid; j < JCB; j += NT) {
-            const int xl = j % (N / C), k2 = j / (N / C);
-            const int x = crank * (N / C) + xl;
-#pragma unroll 1
-            for (int f = 0; f < 2; ++f) {
-                V* const* R = f ? rS : rP;
-                const W px = f ? pxs[x] : pxp[x];
-                const W* py = f ? pys : pyp;
-                V u[16];
-#pragma unroll
-                for (int n = 0; n < 16; ++n) u[n] = R[n % C][sidx<N, R2, SW>(n / C + CPR * k2, x)];
-#pragma unroll 1
-                for (int it = 0; it < 2; ++it) {
-                    if (it) {
-#pragma unroll
-                        for (int n = 0; n < 16; ++n) u[n] = cj(u[n]);
+                        for (int k = 1; k < R2; ++k) v[k] = mulw(cj(v[k]), tw[k * 16 + n1]);
                     }
-                    Dft<16, -1, T>::run(u);
-                    if (!it) {
+                    Dft<R2, -1, T>::run(v);
+                    if (inv) {
 #pragma unroll
-                        for (int k1 = 0; k1 < 16; ++k1) u[k1] = mulw(mulw(u[k1], py[k2 + R2 * k1]), px);
+                        for (int k = 0; k < R2; ++k) v[k] = cj(v[k]);
                     } else {
 #pragma unroll
-                        for (int n = 0; n < 16; ++n) u[n] = cj(u[n]);
+                        for (int k = 1; k < R2; ++k) v[k] = mulw(v[k], tw[k * 16 + n1]);
                     }
+#pragma unroll
+                    for (int k = 0; k < R2; ++k) F[sidx<N, R2, SW>(lr, n1 + 16 * k)] = v[k];
                 }
-#pragma unroll
-                for (int n = 0; n < 16; ++n) R[n % C][sidx<N, R2, SW>(n / C + CPR * k2, x)] = u[n];
             }
-        }
-    };
+        };
 
-    double acc_s = 0.0, acc_p = 0.0;
-    pass_ra(0, -1, coef, coef, acc_s, acc_p);
-    __syncthreads();
-
-    double z = 0.0;
-    for (int s = 0; s < nsteps; ++s) {
-        V* cf_cur = coef + 6 * (s & 1);
-        V* cf_nxt = coef + 6 * ((s + 1) & 1);
-        pass_rb(false);
-        __syncthreads();
-        pass_ca(false);
-        cluster_sync();
-        if (!THERM && tid < 3 && s + 1 < nsteps) stage_coef<T>(d, s + 1, z + d.dz, tid, cf_nxt);
-        pass_cb();
-        cluster_sync();
-        pass_ca(true);
-        __syncthreads();
-        pass_rb(true);
-        __syncthreads();
-        pass_ra(s + 1 < nsteps ? 1 : 2, s, cf_cur, cf_nxt, acc_s, acc_p);
-        __syncthreads();
-        z += d.dz;
-    }
-
-    // ---- SH and pump power: deterministic block + cluster reduction --------------------
+        // ---- RB: rows, 16-point DFT over n1 (in place, digit-reversed output) ----------
+        auto pass_rb = [&](bool inv) {
+            for (int j = tid; j < JB; j += NT) {
+                const int k2 = j % R2, lr = j / R2;
+#pragma unroll 1
+                for (int f = 0; f < 2; ++f) {
+                    V* F = f ? Ss : Ps;
+                    V u[16];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        acc_s += __shfl_down_sync(0xffffffffu, acc_s, o);
-        acc_p += __shfl_down_sync(0xffffffffu, acc_p, o);
-    }
-    const int warp = tid >> 5, lane = tid & 31;
-    if (lane == 0) {
-        red[2 * warp] = acc_s;
-        red[2 * warp + 1] = acc_p;
-    }
-    __syncthreads();
-    double* part = red + 2 * (NT / 32);
-    if (tid == 0) {
-        double a = 0.0, b = 0.0;
-        for (int w = 0; w < NT / 32; ++w) { a += red[2 * w]; b += red[2 * w + 1]; }
-        part[0] = a;
-        part[1] = b;
-    }
-    cluster_sync();
-    if (crank == 0 && tid == 0 && d.power_out) {
-        double a = 0.0, b = 0.0;
-        for (int r = 0; r < C; ++r) {
-            const double* pr = part;
-            if constexpr (C > 1) pr = cg::this_cluster().map_shared_rank(part, r);
-            a += pr[0];
-            b += pr[1];
+                    for (int n = 0; n < 16; ++n) {
+                        u[n] = F[sidx<N, R2, SW>(lr, n + 16 * k2)];
+                        if (inv) u[n] = cj(u[n]);
+                    }
+                    Dft<16, -1, T>::run(u);
+#pragma unroll
+                    for (int n = 0; n < 16; ++n) F[sidx<N, R2, SW>(lr, n + 16 * k2)] = inv ? cj(u[n]) : u[n];
+                }
+            }
+        };
+
+        // ---- CA: columns, R2-point stage over n2 on this CTA's rows ----------------------
+        auto pass_ca = [&](bool inv) {
+            for (int j = tid; j < JCA; j += NT) {
+                const int x = j % N, n1l = j / N;
+                const int n1 = crank + C * n1l;
+#pragma unroll 1
+                for (int f = 0; f < 2; ++f) {
+                    V* F = f ? Ss : Ps;
+                    V v[R2];
+#pragma unroll
+                    for (int k = 0; k < R2; ++k) v[k] = F[sidx<N, R2, SW>(n1l + CPR * k, x)];
+                    if (inv) {
+                        v[0] = cj(v[0]);
+#pragma unroll
+                        for (int k = 1; k < R2; ++k) v[k] = mulw(cj(v[k]), tw[k * 16 + n1]);
+                    }
+                    Dft<R2, -1, T>::run(v);
+                    if (inv) {
+#pragma unroll
+                        for (int k = 0; k < R2; ++k) v[k] = cj(v[k]);
+                    } else {
+#pragma unroll
+                        for (int k = 1; k < R2; ++k) v[k] = mulw(v[k], tw[k * 16 + n1]);
+                    }
+#pragma unroll
+                    for (int k = 0; k < R2; ++k) F[sidx<N, R2, SW>(n1l + CPR * k, x)] = v[k];
+                }
+            }
+        };
+
+        // ---- CB: columns, DFT over n1 across the cluster, propagator, IDFT ----------------
+        auto pass_cb = [&]() {
+            V* rP[C];
+            V* rS[C];
+#pragma unroll
+            for (int r = 0; r < C; ++r) {
+                if constexpr (C > 1) {
+                    rP[r] = cg::this_cluster().map_shared_rank(Ps, r);
+                    rS[r] = cg::this_cluster().map_shared_rank(Ss, r);
+                } else {
+                    rP[r] = Ps;
+                    rS[r] = Ss;
+                }
+            }
+            for (int j = tid; j < JCB; j += NT) {
+                const int xl = j % (N / C), k2 = j / (N / C);
+                const int x = crank * (N / C) + xl;
+#pragma unroll 1
+                for (int f = 0; f < 2; ++f) {
+                    V* const* R = f ? rS : rP;
+                    const W px = f ? pxs[x] : pxp[x];
+                    const W* py = f ? pys : pyp;
+                    V u[16];
+#pragma unroll
+                    for (int n = 0; n < 16; ++n) u[n] = R[n % C][sidx<N, R2, SW>(n / C + CPR * k2, x)];
+#pragma unroll 1
+                    for (int it = 0; it < 2; ++it) {
+                        if (it) {
+#pragma unroll
+                            for (int n = 0; n < 16; ++n) u[n] = cj(u[n]);
+                        }
+                        Dft<16, -1, T>::run(u);
+                        if (!it) {
+#pragma unroll
+                            for (int k1 = 0; k1 < 16; ++k1) u[k1] = mulw(mulw(u[k1], py[k2 + R2 * k1]), px);
+                        } else {
+#pragma unroll
+                            for (int n = 0; n < 16; ++n) u[n] = cj(u[n]);
+                        }
+                    }
+#pragma unroll
+                    for (int n = 0; n < 16; ++n) R[n % C][sidx<N, R2, SW>(n / C + CPR * k2, x)] = u[n];
+                }
+            }
+        };
+
+        double acc_s = 0.0, acc_p = 0.0;
+        pass_ra(0, -1, coef, coef, acc_s, acc_p);
+        __syncthreads();
+
+        double z = 0.0;
+        for (int s = 0; s < nsteps; ++s) {
+            V* cf_cur = coef + 6 * (s & 1);
+            V* cf_nxt = coef + 6 * ((s + 1) & 1);
+            pass_rb(false);
+            __syncthreads();
+            pass_ca(false);
+            cluster_sync();
+            if (!THERM && tid < 3 && s + 1 < nsteps) stage_coef<T>(d, s + 1, z + d.dz, tid, cf_nxt);
+            pass_cb();
+            cluster_sync();
+            pass_ca(true);
+            __syncthreads();
+            pass_rb(true);
+            __syncthreads();
+            pass_ra(s + 1 < nsteps ? 1 : 2, s, cf_cur, cf_nxt, acc_s, acc_p);
+            __syncthreads();
+            z += d.dz;
         }
-        d.power_out[0] = a * d.pw_s;
-        d.power_out[1] = b * d.pw_p;
-    }
-    cluster_sync();
+
+        // ---- SH and pump power: deterministic block + cluster reduction --------------------
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            acc_s += __shfl_down_sync(0xffffffffu, acc_s, o);
+            acc_p += __shfl_down_sync(0xffffffffu, acc_p, o);
+        }
+        const int warp = tid >> 5, lane = tid & 31;
+        if (lane == 0) {
+            red[2 * warp] = acc_s;
+            red[2 * warp + 1] = acc_p;
+        }
+        __syncthreads();
+        double* part = red + 2 * (NT / 32);
+        if (tid == 0) {
+            double a = 0.0, b = 0.0;
+            for (int w = 0; w < NT / 32; ++w) { a += red[2 * w]; b += red[2 * w + 1]; }
+            part[0] = a;
+            part[1] = b;
+        }
+        cluster_sync();
+        if (crank == 0 && tid == 0 && d.power_out) {
+            double a = 0.0, b = 0.0;
+            for (int r = 0; r < C; ++r) {
+                const double* pr = part;
+                if constexpr (C > 1) pr = cg::this_cluster().map_shared_rank(part, r);
+                a += pr[0];
+                b += pr[1];
+            }
+            d.power_out[0] = a * d.pw_s;
+            d.power_out[1] = b * d.pw_p;
+        }
+        cluster_sync();
+        if (!queue) break;
+        inst = take();
+    }  // instances
 }
 
 }  // namespace shg

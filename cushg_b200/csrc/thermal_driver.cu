@@ -198,7 +198,7 @@ shg_status thermal_run(const shg_params& p, const void* signal_in, void* pump_ou
                 rc = cuda_fail(e, "descriptor");
                 break;
             }
-            if ((e = v->launch(ddesc, 1, s)) != cudaSuccess) { rc = cuda_fail(e, "thermal optical pass"); break; }
+            if ((e = v->launch(ddesc, 1, nullptr, s)) != cudaSuccess) { rc = cuda_fail(e, "thermal optical pass"); break; }
             ++outer;
             if (counter == 1 && g != 0) break;  // Solver.h:367
         }

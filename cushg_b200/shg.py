@@ -25,8 +25,16 @@ LIB_PATH = os.path.join(PKG, "libshg_b200.so")
 EXPORTS = (
     "shg_default_params", "shg_check_params", "shg_steps", "shg_solve", "shg_solve_slices", "shg_solve_device",
     "shg_solve_batch_device", "shg_solve_batch_device_noalloc", "shg_grad", "shg_sh_power", "shg_last_error",
-    "shg_status_string", "shg_version", "shg_heat_sweeps_device",
+    "shg_status_string", "shg_version", "shg_heat_sweeps_device", "shg_batch_plan_create", "shg_batch_plan_launch",
+    "shg_batch_plan_powers", "shg_batch_plan_destroy", "shg_autotune",
 )
+
+
+class ShgTuneResult(ctypes.Structure):
+    """``shg_tune_result`` of include/shg.h."""
+    _fields_ = [("precision", ctypes.c_int32), ("n", ctypes.c_int32), ("cluster", ctypes.c_int32),
+                ("threads", ctypes.c_int32), ("candidates", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("pt_steps_per_s", ctypes.c_double), ("default_pt_steps_per_s", ctypes.c_double)]
 
 
 class ShgGradResult(ctypes.Structure):
@@ -82,6 +90,17 @@ def lib() -> ctypes.CDLL:
         L.shg_sh_power.restype = ctypes.c_int
         L.shg_heat_sweeps_device.argtypes = [P, vp, vp, ctypes.c_int64, vp]
         L.shg_heat_sweeps_device.restype = ctypes.c_int
+        L.shg_batch_plan_create.argtypes = [P, ctypes.c_int32, ctypes.POINTER(vp), ctypes.POINTER(vp),
+                                            ctypes.POINTER(vp)]
+        L.shg_batch_plan_create.restype = ctypes.c_int
+        L.shg_batch_plan_launch.argtypes = [vp, vp]
+        L.shg_batch_plan_launch.restype = ctypes.c_int
+        L.shg_batch_plan_powers.argtypes = [vp, ctypes.POINTER(ctypes.c_double), vp]
+        L.shg_batch_plan_powers.restype = ctypes.c_int
+        L.shg_batch_plan_destroy.argtypes = [vp]
+        L.shg_batch_plan_destroy.restype = None
+        L.shg_autotune.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ShgTuneResult)]
+        L.shg_autotune.restype = ctypes.c_int
         L.shg_last_error.restype = ctypes.c_char_p
         L.shg_status_string.argtypes = [ctypes.c_int32]
         L.shg_status_string.restype = ctypes.c_char_p
@@ -244,3 +263,54 @@ def solve_batch_device_noalloc(ps: list[ShgParams], pump_outs=None, signal_outs=
     s = None if stream is None else vp(stream)
     _check(lib().shg_solve_batch_device_noalloc(arr, n, ptrs(pump_outs), ptrs(signal_outs), pp, s))
     return power
+
+
+class BatchPlan:
+    """A batched march captured into a CUDA graph (shg_batch_plan_*): create once for a list
+    of parameter sets and device output tensors, then ``launch`` replays it on a stream and
+    ``powers`` reads the SH powers of the last finished replay."""
+
+    def __init__(self, ps: list[ShgParams], pump_outs=None, signal_outs=None):
+        n = len(ps)
+        self.count = n
+        arr = (ShgParams * n)(*ps)
+        vp = ctypes.c_void_p
+
+        def ptrs(ts):
+            if ts is None:
+                return None
+            return (vp * n)(*[vp(t.data_ptr()) if t is not None else None for t in ts])
+
+        self._keep = (pump_outs, signal_outs)
+        self._h = vp()
+        _check(lib().shg_batch_plan_create(arr, n, ptrs(pump_outs), ptrs(signal_outs), ctypes.byref(self._h)))
+
+    def launch(self, stream=None) -> None:
+        _check(lib().shg_batch_plan_launch(self._h, None if stream is None else ctypes.c_void_p(stream)))
+
+    def powers(self, stream=None) -> np.ndarray:
+        out = np.zeros(self.count, dtype=np.float64)
+        _check(lib().shg_batch_plan_powers(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                           None if stream is None else ctypes.c_void_p(stream)))
+        return out
+
+    def close(self) -> None:
+        if self._h:
+            lib().shg_batch_plan_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def autotune(precision: int, n: int) -> dict:
+    """shg_autotune: time every compiled variant of the (precision, n) class and use the
+    fastest from now on; returns the choice and the rates."""
+    r = ShgTuneResult()
+    _check(lib().shg_autotune(int(precision), int(n), ctypes.byref(r)))
+    return {"precision": r.precision, "n": r.n, "cluster": r.cluster, "threads": r.threads,
+            "candidates": r.candidates, "pt_steps_per_s": r.pt_steps_per_s,
+            "default_pt_steps_per_s": r.default_pt_steps_per_s}

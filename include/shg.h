@@ -174,6 +174,50 @@ SHG_API shg_status shg_solve_batch_device(const shg_params* params, int32_t coun
                                   double* sh_power_out, void* stream);
 
 /*
+ * Batch plans: the batched march of shg_solve_batch_device captured once into a CUDA graph,
+ * with its descriptors, work-queue counters and power slots allocated at creation, then
+ * replayed by shg_batch_plan_launch with one graph launch (no host work per replay).  For
+ * sweeps run repeatedly over the same parameter sets and output buffers (optimisation
+ * loops, repeated measurements).  No counterpart in the reference, whose sweep is one
+ * process per point (src/cuSHG.sh:58-94).
+ *   shg_batch_plan_create   validates like shg_solve_batch_device, uploads the descriptors
+ *                           and captures the launches (current device); synchronous.
+ *   shg_batch_plan_launch   replays the graph on `stream`; launches of one plan that overlap
+ *                           on the GPU race on its work queues and power slots.
+ *   shg_batch_plan_powers   copies the SH powers of the last finished replay to the host
+ *                           array sh_power_out[count] (stream-ordered, then synchronises).
+ *   shg_batch_plan_destroy  synchronises the device and frees the plan.
+ */
+typedef struct shg_batch_plan shg_batch_plan;
+SHG_API shg_status shg_batch_plan_create(const shg_params* params, int32_t count, void* const* pump_out_dev,
+                                         void* const* signal_out_dev, shg_batch_plan** plan);
+SHG_API shg_status shg_batch_plan_launch(shg_batch_plan* plan, void* stream);
+SHG_API shg_status shg_batch_plan_powers(shg_batch_plan* plan, double* sh_power_out, void* stream);
+SHG_API void shg_batch_plan_destroy(shg_batch_plan* plan);
+
+/* Result of shg_autotune. */
+typedef struct shg_tune_result {
+    int32_t precision, n;       /* the grid-size class tuned */
+    int32_t cluster, threads;   /* the chosen split: CTAs per instance, threads per CTA */
+    int32_t candidates;         /* compiled variants timed */
+    int32_t reserved;
+    double pt_steps_per_s;      /* the chosen variant's rate on the tuning batch */
+    double default_pt_steps_per_s; /* the default variant's rate on the same batch */
+} shg_tune_result;
+
+/*
+ * Autotuner of the fused march's schedule for one (precision, grid side) class: times every
+ * compiled variant of the class (cluster split and threads per CTA of the row / column FFT
+ * passes) on a synthetic batch that fills the device several times over, and makes the
+ * fastest the variant every later plain run and batch of that class uses in this process
+ * (results are the same to the last bit of the fields; SH powers may differ in the last
+ * bits, the cluster reduction order being the split's).  Synchronous; call it before any
+ * stream capture.  No counterpart in the reference (compile-time launch shapes,
+ * src/cuSHG.cu:22-23).
+ */
+SHG_API shg_status shg_autotune(int32_t precision, int32_t n, shg_tune_result* out);
+
+/*
  * The batched plain march of shg_solve_batch_device without any device allocation.  This
  * entry point has no counterpart in the reference.  It is for callers that cannot allocate
  * device memory while they run (hosts that give all free memory to their own allocator,

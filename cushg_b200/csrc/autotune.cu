@@ -34,9 +34,10 @@ extern "C" shg_status shg_autotune(int32_t precision, int32_t n, shg_tune_result
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     // instances: three device fills for the variant with the smallest cluster
-    int cmin = 16;
-    for (int i = 0; i < nc; ++i) cmin = std::min(cmin, cand[i]->cluster);
-    const int count = std::max(8, 3 * 2 * sms / cmin);
+    int cmin = 0;  // smallest cluster of the fused candidates (0: multi-pass only)
+    for (int i = 0; i < nc; ++i)
+        if (cand[i]->cluster > 0) cmin = cmin ? std::min(cmin, cand[i]->cluster) : cand[i]->cluster;
+    const int count = cmin ? std::max(8, 3 * 2 * sms / cmin) : 8;
     shg_params base;
     shg_default_params(&base);
     base.nx = base.ny = n;
@@ -80,7 +81,7 @@ extern "C" shg_status shg_autotune(int32_t precision, int32_t n, shg_tune_result
             for (int r = 0; r < 4; ++r) {
                 if ((e = cudaMemsetAsync(queue, 0, sizeof(int), s)) != cudaSuccess ||
                     (e = cudaEventRecord(ev[0], s)) != cudaSuccess ||
-                    (e = cand[c]->launch(dd, count, queue, s)) != cudaSuccess ||
+                    (e = run_variant(cand[c], dd, descs.data(), count, queue, s)) != cudaSuccess ||
                     (e = cudaEventRecord(ev[1], s)) != cudaSuccess || (e = cudaEventSynchronize(ev[1])) != cudaSuccess ||
                     (e = cudaEventElapsedTime(&ms[r], ev[0], ev[1])) != cudaSuccess) {
                     rc = cuda_fail(e, "tuning launch");

@@ -1,4 +1,4 @@
-// dft.cuh — register-resident small DFTs (2, 3, 4, 8, 12, 16 points) used as the
+// dft.cuh — register-resident small DFTs (2, 3, 4, 8, 12, 16, 32 points) used as the
 // butterflies of the transverse 2D FFT of the SSFM step.
 //
 // All indices are compile-time constants after unrolling, so the arrays live in
@@ -45,6 +45,16 @@ __host__ __device__ constexpr double cos12(int m) {
          : 0.866025403784438646764;
 }
 __host__ __device__ constexpr double sin12(int m) { return cos12((m + 9) % 12); }
+// cos / sin of 2π m / 32 from the first octant (m in [0, 32))
+__host__ __device__ constexpr double cos32q(int m) {  // m in [0, 8]
+    return m == 0 ? 1.0 : m == 1 ? 0.980785280403230449126 : m == 2 ? 0.923879532511286756128
+         : m == 3 ? 0.831469612302545237079 : m == 4 ? 0.707106781186547524401 : m == 5 ? 0.555570233019602224743
+         : m == 6 ? 0.382683432365089771728 : m == 7 ? 0.195090322016128267848 : 0.0;
+}
+__host__ __device__ constexpr double cos32(int m) {
+    return m <= 8 ? cos32q(m) : m <= 16 ? -cos32q(16 - m) : m <= 24 ? -cos32q(m - 16) : cos32q(32 - m);
+}
+__host__ __device__ constexpr double sin32(int m) { return cos32((m + 24) & 31); }  // sin x = cos(x - π/2)
 
 // v * (c + i s) for a constant (c, s) known in double.  In float the constant is split
 // into hi + lo parts and applied with fused multiply-adds, so its rounding does not
@@ -61,7 +71,7 @@ __device__ __forceinline__ cx<T> rot_const(cx<T> v, double c, double s) {
     }
 }
 
-// v * e^{SIGN 2πi m / M} for M dividing 16 or 12; m is a compile-time constant
+// v * e^{SIGN 2πi m / M} for M dividing 16, 12 or 32; m is a compile-time constant
 // after unrolling, so the branches fold.
 template <int M, int SIGN, typename T>
 __device__ __forceinline__ cx<T> rot(cx<T> v, int m) {
@@ -73,6 +83,9 @@ __device__ __forceinline__ cx<T> rot(cx<T> v, int m) {
     if (16 % M == 0) {
         const int q = m * (16 / M);
         return rot_const<T>(v, cos16(q), SIGN * sin16(q));
+    } else if (32 % M == 0) {
+        const int q = m * (32 / M);
+        return rot_const<T>(v, cos32(q), SIGN * sin32(q));
     } else {
         const int q = m * (12 / M);
         return rot_const<T>(v, cos12(q), SIGN * sin12(q));
@@ -188,6 +201,9 @@ template <int SIGN, typename T> struct Dft<12, SIGN, T> {
 };
 template <int SIGN, typename T> struct Dft<16, SIGN, T> {
     static __device__ __forceinline__ void run(cx<T> (&v)[16]) { dft_two_factor<4, 4, SIGN, T>(v); }
+};
+template <int SIGN, typename T> struct Dft<32, SIGN, T> {
+    static __device__ __forceinline__ void run(cx<T> (&v)[32]) { dft_two_factor<2, 16, SIGN, T>(v); }
 };
 
 }  // namespace shg

@@ -95,7 +95,10 @@ extern "C" shg_status shg_solve_batch_device_noalloc(const shg_params* params, i
     int order[kNoAllocMaxInstances];
     for (int i = 0; i < count; ++i) {
         order[i] = i;
-        var[i] = find_plain_variant(params[i].precision, params[i].nx);
+        var[i] = find_plain_variant(params[i].precision, params[i].nx, 0, params[i].march);
+        if (var[i]->mp)
+            return fail(SHG_ERR_UNSUPPORTED, "instance %d: the multi-pass march (side %d) needs device workspace", i,
+                        params[i].nx);
     }
     std::sort(order, order + count, [&](int a, int b) {
         if (var[a] != var[b]) return var[a] < var[b];

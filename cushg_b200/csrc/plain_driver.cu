@@ -57,7 +57,7 @@ cudaError_t fork_streams(int dev, ForkStreams** out) {
 shg_status plain_solve_device(const shg_params& p, const void* signal_in, void* pump_out, void* signal_out,
                               shg_stats* stats, cudaStream_t stream, void* slices_p, void* slices_s,
                               const double* poling_dev) {
-    const PlainVariant* v = find_plain_variant(p.precision, p.nx);
+    const PlainVariant* v = find_plain_variant(p.precision, p.nx, 0, p.march);
     if (!v) return fail(SHG_ERR_UNSUPPORTED, "no kernel for grid side %d", p.nx);
     InstDesc d = make_plain_desc(p, p.temp, p.temp);
     d.signal_in = signal_in;
@@ -87,7 +87,7 @@ shg_status plain_solve_device(const shg_params& p, const void* signal_in, void* 
             cudaEventCreate(&t1);
             cudaEventRecord(t0, stream);
         }
-        if ((e = v->launch(dd, 1, nullptr, stream)) != cudaSuccess) { rc = cuda_fail(e, "launch ssfm_plain_kernel"); break; }
+        if ((e = run_variant(v, dd, &d, 1, nullptr, stream)) != cudaSuccess) { rc = cuda_fail(e, "launch ssfm_plain_kernel"); break; }
         if (stats) {
             cudaEventRecord(t1, stream);
             double h[2] = {0, 0};
@@ -131,7 +131,7 @@ static BatchLayout batch_layout(const shg_params* params, int count, void* const
     struct Item { const PlainVariant* v; int idx; double cost; };
     std::vector<Item> items(count);
     for (int i = 0; i < count; ++i) {
-        const PlainVariant* v = find_plain_variant(params[i].precision, params[i].nx);
+        const PlainVariant* v = find_plain_variant(params[i].precision, params[i].nx, 0, params[i].march);
         items[i] = {v, i, (double)params[i].nx * params[i].nx * shg_steps(&params[i])};
     }
     std::stable_sort(items.begin(), items.end(), [](const Item& a, const Item& b) {
@@ -169,14 +169,18 @@ static cudaError_t enqueue_batch(const BatchLayout& L, const InstDesc* dd, int* 
     cudaError_t e;
     const int ng = (int)L.groups.size();
     if ((e = cudaMemsetAsync(queues, 0, sizeof(int) * (size_t)ng, stream)) != cudaSuccess) return e;
-    if (ng == 1) return L.groups[0].v->launch(dd + L.groups[0].begin, L.groups[0].end - L.groups[0].begin, queues, stream);
+    if (ng == 1)
+        return run_variant(L.groups[0].v, dd + L.groups[0].begin, L.descs.data() + L.groups[0].begin,
+                           L.groups[0].end - L.groups[0].begin, queues, stream);
     const int nf = std::min(ng, nfork);
     if ((e = cudaEventRecord(ev[nfork], stream)) != cudaSuccess) return e;
     for (int g = 0; g < nf; ++g)
         if ((e = cudaStreamWaitEvent(fs[g], ev[nfork], 0)) != cudaSuccess) return e;
     for (int g = 0; g < ng; ++g) {
         const BatchLayout::Group& G = L.groups[g];
-        if ((e = G.v->launch(dd + G.begin, G.end - G.begin, queues + g, fs[g % nf])) != cudaSuccess) return e;
+        if ((e = run_variant(G.v, dd + G.begin, L.descs.data() + G.begin, G.end - G.begin, queues + g, fs[g % nf])) !=
+            cudaSuccess)
+            return e;
     }
     for (int g = 0; g < nf; ++g) {
         if ((e = cudaEventRecord(ev[g], fs[g])) != cudaSuccess) return e;
@@ -299,7 +303,7 @@ extern "C" shg_status shg_batch_plan_create(const shg_params* params, int32_t co
         if (e != cudaSuccess) { rc = cuda_fail(e, "plan streams"); break; }
         // a first launch outside the capture sets the kernels' attributes and sizes
         for (const auto& G : L.groups)
-            if ((e = G.v->launch(dd + G.begin, 0, queues, cap)) != cudaSuccess) break;
+            if ((e = run_variant(G.v, dd + G.begin, L.descs.data() + G.begin, 0, queues, cap)) != cudaSuccess) break;
         if (e != cudaSuccess) { rc = cuda_fail(e, "kernel set-up"); break; }
         if ((e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) {
             rc = cuda_fail(e, "cudaStreamBeginCapture");

@@ -151,7 +151,7 @@ void shg_default_params(shg_params* p) {
     p->jacobi_tol = 0.0;
     p->max_sweeps = 0;
     p->jacobi_block = 0;
-    p->reserved0 = 0;
+    p->march = SHG_MARCH_AUTO;
 }
 
 static bool finite_all(const shg_params* p) {
@@ -186,8 +186,11 @@ static shg_status check_params_impl(const shg_params* p, bool need_kernel) {
         if (p->jacobi_block < 0 || p->jacobi_block > 4)
             return fail(SHG_ERR_INVALID, "jacobi_block %d must be in 0..4", p->jacobi_block);
     }
-    if (need_kernel && !find_plain_variant(p->precision, p->nx, p->thermal))
-        return fail(SHG_ERR_UNSUPPORTED, "no %s kernel built for grid side %d at precision %d",
+    if (p->march < SHG_MARCH_AUTO || p->march > SHG_MARCH_MULTIPASS)
+        return fail(SHG_ERR_INVALID, "unknown march %d", p->march);
+    if (need_kernel && !find_plain_variant(p->precision, p->nx, p->thermal, p->march))
+        return fail(SHG_ERR_UNSUPPORTED, "no %s%s kernel built for grid side %d at precision %d",
+                    p->march == SHG_MARCH_FUSED ? "fused " : p->march == SHG_MARCH_MULTIPASS ? "multi-pass " : "",
                     p->thermal ? "thermal" : "plain", p->nx, p->precision);
     return SHG_OK;
 }

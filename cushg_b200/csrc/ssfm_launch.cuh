@@ -59,6 +59,6 @@ cudaError_t launch_plain(const InstDesc* descs, int count, int* queue, cudaStrea
 
 #define SHG_VARIANT(T, PREC, N, C, NT, MINB, THERM)                                                  \
     {PREC, N, C, NT, MINB, THERM ? 1 : 0, PlainCfg<T, N, C, NT, THERM>::smem_bytes,                   \
-     &launch_plain<T, N, C, NT, THERM, MINB>}
+     &launch_plain<T, N, C, NT, THERM, MINB>, nullptr}
 
 }  // namespace shg

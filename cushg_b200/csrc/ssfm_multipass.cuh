@@ -1,0 +1,356 @@
+// ssfm_multipass.cuh — the SSFM march for grids whose two field planes do not fit in the
+// shared memory of one thread-block cluster: 512 x 512 is 4 MB in FP32 and 8 MB in FP64,
+// against 16 CTAs x 227 KB.  The planes stay in global memory (a few instances at a time
+// stay resident in the 126 MB L2) and every SSFM step is two launches:
+//
+//   row pass     RB rows of both fields per CTA: inverse row transform, RK4 at the end of
+//                step s, RK4 at the start of step s+1 (with the heat source, slice records and
+//                outputs of boundary_point), forward row transform
+//   column pass  CW columns of one field per CTA: forward column transform, propagator,
+//                inverse column transform
+//
+// The transforms are the four-step FFT of the fused march (ssfm_plain.cuh) with N = 16 R2
+// (R2 = 32 at N = 512): the same digit-reversed frequency order between the passes, the same
+// twiddle and propagator tables, the same per-point arithmetic in the same order.  On a grid
+// side both kernels are built for, the two agree up to where the compiler contracts a
+// multiply and an add into one fused multiply-add differently (a last-bit effect).
+//
+// Reference counterparts as for the fused march: Solver::SSFM / CWES (src/headers/Solver.h:
+// 267-308) with solverRK4 (:189-264) and diffraction (:153-186, cuFFT, kernelComplexProduct,
+// cuFFTscale Efields.h:15-29).
+#pragma once
+
+#include "ssfm_plain.cuh"
+
+namespace shg {
+
+template <typename T, int N>
+struct MpCfg {
+    static constexpr int R2 = N / 16;
+    static constexpr int SW = sizeof(T) == 4 ? 16 : 8;  // complex slots per 128 B
+    static constexpr int RB = sizeof(T) == 4 ? 8 : 4;   // rows per row-pass CTA
+    static constexpr int RNT = RB * 16;                  // row-pass threads: one (row, n1) job each
+    static constexpr int CW = SW;                        // columns per column-pass CTA: one 128 B row segment
+    static constexpr int CNT = 16 * CW;                  // column-pass threads: one (column, n1) job each
+    static constexpr int RPART = N / RB;                 // row-pass CTAs per instance (power partials)
+    static constexpr size_t row_smem = sizeof(cx<T>) * (2 * (size_t)RB * N + 12) + sizeof(mult<T>) * N +
+                                       sizeof(double) * 2 * (RNT / 32);
+    static constexpr size_t col_smem = sizeof(cx<T>) * (size_t)N * CW + sizeof(mult<T>) * (2 * (size_t)N + CW);
+    static_assert(N % 16 == 0 && RB * RPART == N && N % CW == 0, "bad multi-pass split");
+};
+
+// Per-instance workspace in global memory, at base + inst * stride: the two field planes,
+// the multiplier tables (twiddles tw, propagator factors pxp, pxs, pyp, pys: N each), the
+// row-pass power partials, the running Δk prefix (thermal) and the step positions z_s.
+struct MpLayout {
+    char* base;
+    size_t stride;
+    size_t off_s, off_tab, off_part, off_dk, off_zs;
+};
+
+template <typename T, int N>
+__host__ __device__ inline MpLayout mp_layout(char* base, int max_steps, bool thermal) {
+    using Cfg = MpCfg<T, N>;
+    auto up = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    MpLayout L;
+    L.base = base;
+    const size_t plane = sizeof(cx<T>) * (size_t)N * N;
+    L.off_s = up(plane);
+    L.off_tab = L.off_s + up(plane);
+    L.off_part = L.off_tab + up(sizeof(mult<T>) * 5 * (size_t)N);
+    L.off_dk = L.off_part + up(sizeof(double) * 2 * Cfg::RPART);
+    L.off_zs = L.off_dk + (thermal ? up(sizeof(double) * (size_t)N * N) : 0);
+    L.stride = L.off_zs + up(sizeof(double) * ((size_t)max_steps + 1));
+    return L;
+}
+
+// Tables and step positions of each instance (one block per instance).  z_s is accumulated
+// like the fused march's z (+= dz per step), so both see the same stage phases.
+template <typename T, int N>
+__global__ void __launch_bounds__(256) mp_setup_kernel(const InstDesc* __restrict__ descs, MpLayout L) {
+    const InstDesc d = descs[blockIdx.x];
+    char* w = L.base + (size_t)blockIdx.x * L.stride;
+    mult<T>* tab = reinterpret_cast<mult<T>*>(w + L.off_tab);
+    init_tables<T, N>(d, tab, tab + N, tab + 2 * N, tab + 3 * N, tab + 4 * N, threadIdx.x, blockDim.x);
+    if (threadIdx.x == 0) {
+        double* zs = reinterpret_cast<double*>(w + L.off_zs);
+        double z = 0.0;
+        zs[0] = z;
+        for (int k = 0; k < d.nsteps; ++k) {
+            z += d.dz;
+            zs[k + 1] = z;
+        }
+    }
+}
+
+// The R2-point stage of the four-step transform on the elements n2 = 0..R2-1 of one n1:
+// forward = DFT, then twiddle W_N^{n1 k}; inverse = conj(DFT(conj(x) W)).
+template <typename T, int R2>
+__device__ __forceinline__ void r2_stage(cx<T> (&v)[R2], const mult<T>* tw, int n1, bool inv) {
+    auto cj = [](cx<T> a) { return mk<T>(a.x, -a.y); };
+    if (inv) {
+        v[0] = cj(v[0]);
+#pragma unroll
+        for (int k = 1; k < R2; ++k) v[k] = mulw(cj(v[k]), tw[k * 16 + n1]);
+    }
+    Dft<R2, -1, T>::run(v);
+    if (inv) {
+#pragma unroll
+        for (int k = 0; k < R2; ++k) v[k] = cj(v[k]);
+    } else {
+#pragma unroll
+        for (int k = 1; k < R2; ++k) v[k] = mulw(v[k], tw[k * 16 + n1]);
+    }
+}
+
+// Row pass of step s (s = -1: the first pass, which builds the initial fields; s = nsteps-1:
+// the last, which writes the outputs and this CTA's power partials).  Grid (N / RB, count).
+template <typename T, int N, bool THERM>
+__global__ void __launch_bounds__(MpCfg<T, N>::RNT)
+    mp_row_kernel(const InstDesc* __restrict__ descs, MpLayout L, int s) {
+    using Cfg = MpCfg<T, N>;
+    constexpr int R2 = Cfg::R2, RB = Cfg::RB, SW = Cfg::SW, NT = Cfg::RNT;
+    using V = cx<T>;
+    using W = mult<T>;
+    const InstDesc d = descs[blockIdx.y];
+    if (s >= d.nsteps) return;  // this instance has finished its march
+    const int mode = s < 0 ? 0 : (s + 1 < d.nsteps ? 1 : 2);
+    char* wbase = L.base + (size_t)blockIdx.y * L.stride;
+    V* gP = reinterpret_cast<V*>(wbase);
+    V* gS = reinterpret_cast<V*>(wbase + L.off_s);
+    const W* gtab = reinterpret_cast<const W*>(wbase + L.off_tab);
+    const double* zs = reinterpret_cast<const double*>(wbase + L.off_zs);
+
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* Ps = reinterpret_cast<V*>(smem_raw);
+    V* Ss = Ps + RB * N;
+    V* coef = Ss + RB * N;  // [0..5] step s, [6..11] step s+1
+    W* tw = reinterpret_cast<W*>(coef + 12);
+    double* red = reinterpret_cast<double*>(tw + N);
+    const int tid = threadIdx.x, y0 = blockIdx.x * RB;
+    auto cj = [](V a) { return mk<T>(a.x, -a.y); };
+
+    for (int j = tid; j < N; j += NT) tw[j] = gtab[j];
+    if (!THERM && tid < 3) {
+        if (mode == 0) {
+            stage_coef<T>(d, 0, 0.0, tid, coef + 6);
+        } else {
+            stage_coef<T>(d, s, zs[s], tid, coef);
+            if (mode == 1) stage_coef<T>(d, s + 1, zs[s + 1], tid, coef + 6);
+        }
+    }
+    if (mode == 0) {
+        // setPump (Efields.h:84-119); SH = 0 or the given field
+        const V* sin_g = reinterpret_cast<const V*>(d.signal_in);
+        for (int e = tid; e < RB * N; e += NT) {
+            const int lr = e / N, x = e % N;
+            const int y = y0 + lr;
+            const double2 pv = pump_value(d, x, y, d.amp_re, d.amp_im, d.den_re, d.den_im);
+            const V p0 = mk<T>((T)pv.x, (T)pv.y);
+            const V s0 = d.has_signal_in ? sin_g[(size_t)y * N + x] : mk<T>((T)0, (T)0);
+            Ps[sidx<N, R2, SW>(lr, x)] = p0;
+            Ss[sidx<N, R2, SW>(lr, x)] = s0;
+            if (d.slices_p) reinterpret_cast<V*>(d.slices_p)[(size_t)y * N + x] = p0;
+            if (d.slices_s) reinterpret_cast<V*>(d.slices_s)[(size_t)y * N + x] = s0;
+        }
+    } else {
+        for (int e = tid; e < RB * N; e += NT) {
+            const int lr = e / N, x = e % N;
+            const size_t g = (size_t)(y0 + lr) * N + x;
+            Ps[sidx<N, R2, SW>(lr, x)] = gP[g];
+            Ss[sidx<N, R2, SW>(lr, x)] = gS[g];
+        }
+    }
+    __syncthreads();
+
+    // 16-point stage over n1 of every (row, k2), both fields
+    auto n1_pass = [&](bool inv) {
+        for (int j = tid; j < RB * R2; j += NT) {
+            const int k2 = j % R2, lr = j / R2;
+#pragma unroll 1
+            for (int f = 0; f < 2; ++f) {
+                V* F = f ? Ss : Ps;
+                V u[16];
+#pragma unroll
+                for (int n = 0; n < 16; ++n) {
+                    u[n] = F[sidx<N, R2, SW>(lr, n + 16 * k2)];
+                    if (inv) u[n] = cj(u[n]);
+                }
+                Dft<16, -1, T>::run(u);
+#pragma unroll
+                for (int n = 0; n < 16; ++n) F[sidx<N, R2, SW>(lr, n + 16 * k2)] = inv ? cj(u[n]) : u[n];
+            }
+        }
+    };
+    if (mode != 0) {
+        n1_pass(true);
+        __syncthreads();
+    }
+
+    const T hap = (T)d.hap, has = (T)d.has, qs = (T)d.qs, dz6 = (T)(d.dz / 6.0);
+    double acc_s = 0.0, acc_p = 0.0;
+    {
+        const int n1 = tid & 15, lr = tid >> 4;  // one (row, n1) job per thread
+        double* dkint = THERM ? reinterpret_cast<double*>(wbase + L.off_dk) : nullptr;
+#pragma unroll 1
+        for (int f = 0; f < 2 && mode != 0; ++f) {
+            V* F = f ? Ss : Ps;
+            V v[R2];
+#pragma unroll
+            for (int k = 0; k < R2; ++k) v[k] = F[sidx<N, R2, SW>(lr, n1 + 16 * k)];
+            r2_stage<T, R2>(v, tw, n1, true);
+#pragma unroll
+            for (int k = 0; k < R2; ++k) F[sidx<N, R2, SW>(lr, n1 + 16 * k)] = v[k];
+        }
+#pragma unroll 1
+        for (int k = 0; k < R2; ++k) {
+            const int x = n1 + 16 * k;
+            const int o = sidx<N, R2, SW>(lr, x);
+            const size_t g = (size_t)(y0 + lr) * N + x;
+            V p = Ps[o], q = Ss[o];
+            boundary_point<T, THERM>(d, mode, s, g, (size_t)N * N, p, q, coef, coef + 6, hap, has, qs, dz6,
+                                     THERM ? dkint + g : nullptr, acc_s, acc_p);
+            if (mode != 2) {
+                Ps[o] = p;
+                Ss[o] = q;
+            }
+        }
+#pragma unroll 1
+        for (int f = 0; f < 2 && mode != 2; ++f) {
+            V* F = f ? Ss : Ps;
+            V v[R2];
+#pragma unroll
+            for (int k = 0; k < R2; ++k) v[k] = F[sidx<N, R2, SW>(lr, n1 + 16 * k)];
+            r2_stage<T, R2>(v, tw, n1, false);
+#pragma unroll
+            for (int k = 0; k < R2; ++k) F[sidx<N, R2, SW>(lr, n1 + 16 * k)] = v[k];
+        }
+    }
+    __syncthreads();
+    if (mode != 2) {
+        n1_pass(false);
+        __syncthreads();
+        for (int e = tid; e < RB * N; e += NT) {
+            const int lr = e / N, x = e % N;
+            const size_t g = (size_t)(y0 + lr) * N + x;
+            gP[g] = Ps[sidx<N, R2, SW>(lr, x)];
+            gS[g] = Ss[sidx<N, R2, SW>(lr, x)];
+        }
+        return;
+    }
+    // last step: this CTA's share of the SH and pump power sums, block-reduced in a fixed order
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        acc_s += __shfl_down_sync(0xffffffffu, acc_s, o);
+        acc_p += __shfl_down_sync(0xffffffffu, acc_p, o);
+    }
+    if ((tid & 31) == 0) {
+        red[2 * (tid >> 5)] = acc_s;
+        red[2 * (tid >> 5) + 1] = acc_p;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double a = 0.0, b = 0.0;
+        for (int w = 0; w < NT / 32; ++w) {
+            a += red[2 * w];
+            b += red[2 * w + 1];
+        }
+        double* part = reinterpret_cast<double*>(wbase + L.off_part);
+        part[2 * blockIdx.x] = a;
+        part[2 * blockIdx.x + 1] = b;
+    }
+}
+
+// Column pass of step s: the diffraction of one field over CW columns.  Grid (N / CW, 2
+// fields, count).
+template <typename T, int N>
+__global__ void __launch_bounds__(MpCfg<T, N>::CNT)
+    mp_col_kernel(const InstDesc* __restrict__ descs, MpLayout L, int s) {
+    using Cfg = MpCfg<T, N>;
+    constexpr int R2 = Cfg::R2, CW = Cfg::CW, NT = Cfg::CNT;
+    using V = cx<T>;
+    using W = mult<T>;
+    if (s >= descs[blockIdx.z].nsteps) return;
+    const int f = blockIdx.y;  // 0 pump, 1 SH
+    char* wbase = L.base + (size_t)blockIdx.z * L.stride;
+    V* F = reinterpret_cast<V*>(wbase + (f ? L.off_s : 0));
+    const W* gtab = reinterpret_cast<const W*>(wbase + L.off_tab);
+
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* tile = reinterpret_cast<V*>(smem_raw);  // element (y, c) at y * CW + c
+    W* tw = reinterpret_cast<W*>(tile + N * CW);
+    W* py = tw + N;  // y factor of this field's propagator, by frequency, × 1/N^2
+    W* px = py + N;  // x factor of this field's propagator for the CTA's columns
+    const int tid = threadIdx.x, x0 = blockIdx.x * CW;
+    auto cj = [](V a) { return mk<T>(a.x, -a.y); };
+
+    for (int j = tid; j < N; j += NT) {
+        tw[j] = gtab[j];
+        py[j] = gtab[(f ? 4 : 3) * N + j];
+    }
+    if (tid < CW) px[tid] = gtab[(f ? 2 : 1) * N + x0 + tid];
+    for (int e = tid; e < N * CW; e += NT) {
+        const int y = e / CW, c = e % CW;
+        tile[e] = F[(size_t)y * N + x0 + c];
+    }
+    __syncthreads();
+    auto col_stage = [&](bool inv) {  // R2-point stage over n2 of every (column, n1)
+        const int c = tid % CW, n1 = tid / CW;
+        V v[R2];
+#pragma unroll
+        for (int k = 0; k < R2; ++k) v[k] = tile[(n1 + 16 * k) * CW + c];
+        r2_stage<T, R2>(v, tw, n1, inv);
+#pragma unroll
+        for (int k = 0; k < R2; ++k) tile[(n1 + 16 * k) * CW + c] = v[k];
+    };
+    col_stage(false);
+    __syncthreads();
+    // 16-point DFT over n1 of every (column, k2), propagator by frequency, inverse DFT
+    for (int j = tid; j < R2 * CW; j += NT) {
+        const int c = j % CW, k2 = j / CW;
+        V u[16];
+#pragma unroll
+        for (int n = 0; n < 16; ++n) u[n] = tile[(n + 16 * k2) * CW + c];
+#pragma unroll 1
+        for (int it = 0; it < 2; ++it) {
+            if (it) {
+#pragma unroll
+                for (int n = 0; n < 16; ++n) u[n] = cj(u[n]);
+            }
+            Dft<16, -1, T>::run(u);
+            if (!it) {
+#pragma unroll
+                for (int k1 = 0; k1 < 16; ++k1) u[k1] = mulw(mulw(u[k1], py[k2 + R2 * k1]), px[c]);
+            } else {
+#pragma unroll
+                for (int n = 0; n < 16; ++n) u[n] = cj(u[n]);
+            }
+        }
+#pragma unroll
+        for (int n = 0; n < 16; ++n) tile[(n + 16 * k2) * CW + c] = u[n];
+    }
+    __syncthreads();
+    col_stage(true);
+    __syncthreads();
+    for (int e = tid; e < N * CW; e += NT) {
+        const int y = e / CW, c = e % CW;
+        F[(size_t)y * N + x0 + c] = tile[e];
+    }
+}
+
+// SH and pump power of each instance from its row-pass partials, summed in a fixed order.
+template <typename T, int N>
+__global__ void mp_power_kernel(const InstDesc* __restrict__ descs, MpLayout L) {
+    const InstDesc& d = descs[blockIdx.x];
+    if (threadIdx.x != 0 || !d.power_out) return;
+    const double* part = reinterpret_cast<const double*>(L.base + (size_t)blockIdx.x * L.stride + L.off_part);
+    double a = 0.0, b = 0.0;
+    for (int r = 0; r < MpCfg<T, N>::RPART; ++r) {
+        a += part[2 * r];
+        b += part[2 * r + 1];
+    }
+    d.power_out[0] = a * d.pw_s;
+    d.power_out[1] = b * d.pw_p;
+}
+
+}  // namespace shg

@@ -182,6 +182,63 @@ __device__ __forceinline__ void thermal_coef(const InstDesc& d, double dki, int 
     }
 }
 
+// The pointwise work of a row pass at grid point g (index y*n + x in the plane): the RK4
+// applications around a step boundary, h = 0 the second half of step s and h = 1 the first
+// half of step s+1 (Solver.h:267-273); mode 0 (s = -1, the first pass) runs h = 1 only, mode
+// 2 (the last step) h = 0 only.  With them: the heat source of slice s (thermal), the
+// per-slice record of the fields before step s+1 and the outputs after step out_after with
+// their power sums.  dki: this point's running Δk prefix (thermal), else unused.
+template <typename T, bool THERM>
+__device__ __forceinline__ void boundary_point(const InstDesc& d, int mode, int s, size_t g, size_t nn, cx<T>& p,
+                                               cx<T>& q, const cx<T>* cf_prev, const cx<T>* cf_next, T hap, T has,
+                                               T qs, T dz6, double* dki, double& acc_s, double& acc_p) {
+    using V = cx<T>;
+    using R = T;  // real type of the thermal 3D arrays
+    const R* tnp = reinterpret_cast<const R*>(d.t_np);
+    const R* tns = reinterpret_cast<const R*>(d.t_ns);
+    const R* tdk = reinterpret_cast<const R*>(d.t_dk);
+    R* tq = reinterpret_cast<R*>(d.t_q);
+    const int h0 = mode == 0 ? 1 : 0, h1 = mode == 2 ? 1 : 2;
+#pragma unroll 1
+    for (int h = h0; h < h1; ++h) {
+        const int sl = s + h;  // slice of this half step
+        if constexpr (THERM) {
+            const size_t gz = (size_t)sl * nn + g;
+            if (h == 1) *dki = (mode == 0 ? 0.0 : *dki) + (double)tdk[gz];
+            const double np = (double)tnp[gz], ns = (double)tns[gz];
+            V cf[6];
+            thermal_coef<T>(d, *dki, sl, np, ns, cf);
+            rk4_point<T>(p, q, cf, hap, has, (T)(0.5 * (d.bf_s * ns)), dz6);
+            if (h == 0 && tq) {
+                // kernelSetQ (Tfield.h:260-276) for slice s, after its step
+                const R ap2 = p.x * p.x + p.y * p.y, as2 = q.x * q.x + q.y * q.y;
+                const R is = (R)d.q_h * (R)ns * as2;
+                tq[gz] = (R)d.q_p * (R)np * ap2 + (R)d.q_s * (R)ns * as2 + (R)d.beta_s * (is * is);
+            }
+        } else {
+            (void)dki;
+            rk4_point<T>(p, q, h ? cf_next : cf_prev, hap, has, qs, dz6);
+        }
+        if (h == 0 && s + 1 < d.nslices) {
+            // per-slice record: the fields before step s+1 (Solver.h:289-295)
+            const size_t gs = (size_t)(s + 1) * nn + g;
+            if (d.slices_p) reinterpret_cast<V*>(d.slices_p)[gs] = p;
+            if (d.slices_s) reinterpret_cast<V*>(d.slices_s)[gs] = q;
+        }
+        if (h == 0 && s + 1 == d.out_after) {
+            if (d.pump_out) reinterpret_cast<V*>(d.pump_out)[g] = p;
+            if (d.signal_out) reinterpret_cast<V*>(d.signal_out)[g] = q;
+            double ws = 1.0, wp = 1.0;
+            if constexpr (THERM) {
+                ws = (double)tns[(size_t)(s + 1) * nn + g];
+                wp = (double)tnp[(size_t)(s + 1) * nn + g];
+            }
+            acc_s += ws * ((double)q.x * (double)q.x + (double)q.y * (double)q.y);
+            acc_p += wp * ((double)p.x * (double)p.x + (double)p.y * (double)p.y);
+        }
+    }
+}
+
 // Persistent march: each cluster takes instances from the device work queue *queue (an
 // atomic counter the host zeroes before the launch, instances in the descriptor order the
 // host chose: longest march first) until the queue is empty.  queue == nullptr: one
@@ -265,12 +322,6 @@ __global__ void __launch_bounds__(NT, MINB)
         // ---- RA: rows, R2-point stage of (row lr, n1) and the pointwise RK4 half-steps -----
         // mode 0: first (natural order in: RK4(z_0), forward), 1: middle (inverse, RK4(z_s),
         // RK4(z_{s+1}), forward), 2: last (inverse, RK4(z_s), outputs)
-        using R = T;  // real type of the thermal 3D arrays
-        const R* tnp = reinterpret_cast<const R*>(d.t_np);
-        const R* tns = reinterpret_cast<const R*>(d.t_ns);
-        const R* tdk = reinterpret_cast<const R*>(d.t_dk);
-        R* tq = reinterpret_cast<R*>(d.t_q);
-        constexpr size_t NN = (size_t)N * N;
 
         // s: index of the step that ends in this pass (-1 in the first pass)
         auto pass_ra = [&](int mode, int s, const V* cf_prev, const V* cf_next, double& acc_s, double& acc_p) {
@@ -281,51 +332,14 @@ __global__ void __launch_bounds__(NT, MINB)
                     if (ph == 2) {
                         // pointwise: the two RK4 applications around the step boundary (the second
                         // half of step s, then the first half of step s+1)
-                        const int h0 = mode == 0 ? 1 : 0, h1 = mode == 2 ? 1 : 2;
 #pragma unroll 1
                         for (int k = 0; k < R2; ++k) {
                             const int x = n1 + 16 * k;
                             const int o = sidx<N, R2, SW>(lr, x);
                             const size_t g = (size_t)(crank + C * lr) * N + x;
                             V p = Ps[o], q = Ss[o];
-#pragma unroll 1
-                            for (int h = h0; h < h1; ++h) {
-                                const int sl = s + h;  // slice of this half step
-                                if constexpr (THERM) {
-                                    const size_t gz = (size_t)sl * NN + g;
-                                    double& dki = dkint[lr * N + x];
-                                    if (h == 1) dki = (mode == 0 ? 0.0 : dki) + (double)tdk[gz];
-                                    const double np = (double)tnp[gz], ns = (double)tns[gz];
-                                    V cf[6];
-                                    thermal_coef<T>(d, dki, sl, np, ns, cf);
-                                    rk4_point<T>(p, q, cf, hap, has, (T)(0.5 * (d.bf_s * ns)), dz6);
-                                    if (h == 0 && tq) {
-                                        // kernelSetQ (Tfield.h:260-276) for slice s, after its step
-                                        const R ap2 = p.x * p.x + p.y * p.y, as2 = q.x * q.x + q.y * q.y;
-                                        const R is = (R)d.q_h * (R)ns * as2;
-                                        tq[gz] = (R)d.q_p * (R)np * ap2 + (R)d.q_s * (R)ns * as2 + (R)d.beta_s * (is * is);
-                                    }
-                                } else {
-                                    rk4_point<T>(p, q, h ? cf_next : cf_prev, hap, has, qs, dz6);
-                                }
-                                if (h == 0 && s + 1 < d.nslices) {
-                                    // per-slice record: the fields before step s+1 (Solver.h:289-295)
-                                    const size_t gs = (size_t)(s + 1) * NN + g;
-                                    if (d.slices_p) reinterpret_cast<V*>(d.slices_p)[gs] = p;
-                                    if (d.slices_s) reinterpret_cast<V*>(d.slices_s)[gs] = q;
-                                }
-                                if (h == 0 && s + 1 == d.out_after) {
-                                    if (d.pump_out) reinterpret_cast<V*>(d.pump_out)[g] = p;
-                                    if (d.signal_out) reinterpret_cast<V*>(d.signal_out)[g] = q;
-                                    double ws = 1.0, wp = 1.0;
-                                    if constexpr (THERM) {
-                                        ws = (double)tns[(size_t)(s + 1) * NN + g];
-                                        wp = (double)tnp[(size_t)(s + 1) * NN + g];
-                                    }
-                                    acc_s += ws * ((double)q.x * (double)q.x + (double)q.y * (double)q.y);
-                                    acc_p += wp * ((double)p.x * (double)p.x + (double)p.y * (double)p.y);
-                                }
-                            }
+                            boundary_point<T, THERM>(d, mode, s, g, (size_t)N * N, p, q, cf_prev, cf_next, hap, has,
+                                                     qs, dz6, THERM ? &dkint[lr * N + x] : nullptr, acc_s, acc_p);
                             if (mode != 2) {
                                 Ps[o] = p;
                                 Ss[o] = q;

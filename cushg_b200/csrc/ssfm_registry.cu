@@ -3,6 +3,7 @@
 #include <mutex>
 #include <vector>
 
+#include "../../include/shg.h"
 #include "ssfm_variants.h"
 
 namespace shg {
@@ -15,7 +16,8 @@ std::vector<const PlainVariant*> g_chosen;  // tuned variants, one per (precisio
 template <typename F>
 void for_each_variant(F&& f) {
     const VariantTable tables[] = {variants_f32_small(), variants_f32_128(), variants_f32_192(), variants_f32_256(),
-                                   variants_f64_small(), variants_f64_large(), variants_thermal()};
+                                   variants_f64_small(), variants_f64_large(), variants_thermal(),
+                                   variants_multipass()};
     for (const VariantTable& t : tables)
         for (int i = 0; i < t.count; ++i)
             if (f(&t.v[i])) return;
@@ -23,19 +25,24 @@ void for_each_variant(F&& f) {
 
 }  // namespace
 
-const PlainVariant* find_plain_variant(int precision, int n, int thermal) {
+const PlainVariant* find_plain_variant(int precision, int n, int thermal, int march) {
     const int th = thermal ? 1 : 0;
-    {
+    if (march == SHG_MARCH_AUTO) {
         std::lock_guard<std::mutex> lk(g_mu);
         for (const PlainVariant* v : g_chosen)
             if (v->precision == precision && v->n == n && v->thermal == th) return v;
     }
-    const PlainVariant* found = nullptr;
+    const PlainVariant *fused = nullptr, *multi = nullptr;
     for_each_variant([&](const PlainVariant* v) {
-        if (v->precision == precision && v->n == n && v->thermal == th) found = v;
-        return found != nullptr;
+        if (v->precision == precision && v->n == n && v->thermal == th) {
+            if (v->mp && !multi) multi = v;
+            if (!v->mp && !fused) fused = v;
+        }
+        return false;
     });
-    return found;
+    if (march == SHG_MARCH_FUSED) return fused;
+    if (march == SHG_MARCH_MULTIPASS) return multi;
+    return fused ? fused : multi;
 }
 
 int plain_candidates(int precision, int n, const PlainVariant** out, int max) {

@@ -75,7 +75,7 @@ cudaError_t run_sweeps(R*& cur, R*& nxt, const R* Ta, const SweepMaps<R>& m, con
 template <typename R>
 shg_status thermal_run(const shg_params& p, const void* signal_in, void* pump_out, void* signal_out,
                        void* temperature_out, shg_stats* stats, cudaStream_t s, void* slices_p, void* slices_s) {
-    const PlainVariant* v = find_plain_variant(p.precision, p.nx, 1);
+    const PlainVariant* v = find_plain_variant(p.precision, p.nx, 1, p.march);
     if (!v) return fail(SHG_ERR_UNSUPPORTED, "no thermal kernel for grid side %d", p.nx);
     const int n = p.nx, nz = p.nz;
     const size_t nt = (size_t)n * n * nz;
@@ -198,7 +198,7 @@ shg_status thermal_run(const shg_params& p, const void* signal_in, void* pump_ou
                 rc = cuda_fail(e, "descriptor");
                 break;
             }
-            if ((e = v->launch(ddesc, 1, nullptr, s)) != cudaSuccess) { rc = cuda_fail(e, "thermal optical pass"); break; }
+            if ((e = run_variant(v, ddesc, &d, 1, nullptr, s)) != cudaSuccess) { rc = cuda_fail(e, "thermal optical pass"); break; }
             ++outer;
             if (counter == 1 && g != 0) break;  // Solver.h:367
         }

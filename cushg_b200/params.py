@@ -26,6 +26,9 @@ SHG_BOUNDARY_TOP_OPEN = 0
 SHG_BOUNDARY_OVEN_SURROUNDED = 1
 SHG_CONV_REFERENCE = 0
 SHG_CONV_MAXABS = 1
+SHG_MARCH_AUTO = 0
+SHG_MARCH_FUSED = 1
+SHG_MARCH_MULTIPASS = 2
 
 # physical constants of src/headers/Crystal.h:19-21 (µm, ps, W, V)
 C_UM_PS = 299792458 * 1e6 / 1e12
@@ -49,7 +52,7 @@ class ShgParams(ctypes.Structure):
         ("max_outer", ctypes.c_int32), ("check_every", ctypes.c_int32),
         ("conv_rule", ctypes.c_int32), ("crystal", ctypes.c_int32),
         ("jacobi_tol", ctypes.c_double), ("max_sweeps", ctypes.c_int64),
-        ("jacobi_block", ctypes.c_int32), ("reserved0", ctypes.c_int32),
+        ("jacobi_block", ctypes.c_int32), ("march", ctypes.c_int32),
     ]
 
     def copy(self) -> "ShgParams":

@@ -107,8 +107,17 @@ typedef struct shg_params {
      * sweep per launch, 2..4 = that many through the TMA-staged blocked kernel.  Every setting gives the same
      * temperatures bit for bit; the checked sweep of each window always runs alone. */
     int32_t jacobi_block;
-    int32_t reserved0;
+    /* Which SSFM march to run (SHG_MARCH_*): automatic picks the fused cluster march where
+     * one is built for the grid side (planes in shared memory, sides <= 256) and the
+     * multi-pass march otherwise (planes in global memory, side 512). */
+    int32_t march;
 } shg_params;
+
+enum {
+    SHG_MARCH_AUTO = 0,      /* fused where built (the autotuner's choice if it ran), else multi-pass */
+    SHG_MARCH_FUSED = 1,     /* one thread-block cluster per instance, fields in shared memory */
+    SHG_MARCH_MULTIPASS = 2  /* fields in global memory, a row and a column launch per step */
+};
 
 /* Per-call report. */
 typedef struct shg_stats {

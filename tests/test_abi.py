@@ -74,3 +74,15 @@ def test_status_strings():
     L = shg.lib()
     assert L.shg_status_string(0) == b"ok"
     assert L.shg_version().startswith(b"libshg_b200")
+
+
+def test_march_selector_is_validated():
+    """512 x 512 is built as a multi-pass march only, 64 x 64 as a fused march only."""
+    p512 = P.workload(512, 9, 6000.0, 5.0, 30.0, 3000.0, 30.0, precision=32)
+    assert shg.check_params(p512) == P.SHG_OK
+    assert shg.check_params(p512.replace(march=P.SHG_MARCH_MULTIPASS)) == P.SHG_OK
+    assert shg.check_params(p512.replace(march=P.SHG_MARCH_FUSED)) == P.SHG_ERR_UNSUPPORTED
+    assert shg.check_params(p512.replace(march=7)) == P.SHG_ERR_INVALID
+    p64 = P.config_plain_64()
+    assert shg.check_params(p64.replace(march=P.SHG_MARCH_MULTIPASS)) == P.SHG_ERR_UNSUPPORTED
+    assert shg.check_params(p64.replace(march=P.SHG_MARCH_FUSED)) == P.SHG_OK

@@ -415,33 +415,68 @@ def run_adjoint(args) -> dict:
     """Adjoint workload (outside the default sweep line): gradients of the SH power of the
     256x256 / nz = 400 FP32 run (20 mm, 30 W, w0 = 35 µm, focus 0.4 L, 30 °C) with respect to
     waist, focus, oven temperature and a 399-entry poling-phase vector drawn from N(0, 0.1 rad),
-    checkpoints every 20 steps; against the forward march alone."""
+    checkpoints every 20 steps.
+
+    value: gradients/s of a batch of `--adjoint-batch` such instances (poling seeds 0..B-1) in
+    one shg_grad_batch launch; grad_over_forward: that batch's time over the batched forward
+    march of the same instances (both fill the GPU, so this is the cost ratio).  The single
+    instance's latency against its forward march is reported beside it."""
     import torch
     from cushg_b200 import shg
 
     p = P.config_adjoint().replace(precision=args.precision)
     if args.adjoint_nz:
         p = p.replace(nz=args.adjoint_nz)
-    pol = np.random.default_rng(0).normal(0.0, 0.1, size=p.nz - 1)
+    nst = p.nz - 1
     kk = args.checkpoint_every
+    cdt = torch.complex64 if p.precision == 32 else torch.complex128
+
+    def polv(seed):
+        return np.random.default_rng(seed).normal(0.0, 0.1, size=nst)
+
+    # single instance: latency
+    pol = polv(0)
     for _ in range(args.warmup):
         shg.grad(p, pol, checkpoint_every=kk)
     g_ms = []
     for _ in range(args.steps):
         g = shg.grad(p, pol, checkpoint_every=kk)
         g_ms.append(g["device_ms"])
-    pump = torch.empty((p.ny, p.nx), dtype=torch.complex64 if p.precision == 32 else torch.complex128, device="cuda")
+    pump = torch.empty((p.ny, p.nx), dtype=cdt, device="cuda")
     sig = torch.empty_like(pump)
-    f_ms = []
-    for _ in range(args.steps):
-        st = shg.solve_device(p, pump, sig)
-        f_ms.append(st.device_ms)
+    for _ in range(args.warmup):
+        shg.solve_device(p, pump, sig)
+    f_ms = [shg.solve_device(p, pump, sig).device_ms for _ in range(args.steps)]
     gm, fm = statistics.median(g_ms), statistics.median(f_ms)
-    return {"metric": "adjoint grads/s", "value": 1e3 / gm, "unit": "gradients/s", "workload":
-            f"256x256 nz={p.nz}, 3 scalars + {p.nz - 1}-vector, checkpoints every {g['checkpoint_every']}",
-            "precision": p.precision,
-            "grad_ms": gm, "forward_ms": fm, "grad_over_forward": gm / fm, "sh_power_w": g["sh_power"],
-            "d_waist": g["d_waist"], "d_focus": g["d_focus"], "d_temp": g["d_temp"]}
+
+    # batch: throughput and cost ratio
+    B = args.adjoint_batch
+    ps = [p] * B
+    pols = [polv(i) for i in range(B)]
+    for _ in range(max(1, args.warmup - 2)):
+        shg.grad_batch(ps, pols, checkpoint_every=kk)
+    gb = [shg.grad_batch(ps, pols, checkpoint_every=kk)[0]["device_ms"] for _ in range(args.steps)]
+    pumps = [torch.empty((p.ny, p.nx), dtype=cdt, device="cuda") for _ in range(B)]
+    sigs = [torch.empty_like(t) for t in pumps]
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        shg.solve_batch_device(ps, pumps, sigs, stream=stream.cuda_stream, want_power=False)
+    torch.cuda.synchronize()
+    fb = []
+    for _ in range(args.steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        shg.solve_batch_device(ps, pumps, sigs, stream=stream.cuda_stream, want_power=False)
+        b.record(stream)
+        torch.cuda.synchronize()
+        fb.append(a.elapsed_time(b))
+    gbm, fbm = statistics.median(gb), statistics.median(fb)
+    return {"metric": "adjoint grads/s", "value": B * 1e3 / gbm, "unit": "gradients/s",
+            "workload": f"{B} x (256x256 nz={p.nz}, 3 scalars + {nst}-vector), checkpoints every {g['checkpoint_every']}",
+            "precision": p.precision, "batch": B, "batch_grad_ms": gbm, "batch_forward_ms": fbm,
+            "grad_over_forward": gbm / fbm,
+            "single": {"grad_ms": gm, "forward_ms": fm, "grad_over_forward": gm / fm},
+            "sh_power_w": g["sh_power"], "d_waist": g["d_waist"], "d_focus": g["d_focus"], "d_temp": g["d_temp"]}
 
 
 def main() -> int:
@@ -462,6 +497,7 @@ def main() -> int:
     ap.add_argument("--thermal-nz", type=int, default=0)
     ap.add_argument("--checkpoint-every", type=int, default=20)
     ap.add_argument("--adjoint-nz", type=int, default=0, help="adjoint workload with this nz (profiling case)")
+    ap.add_argument("--adjoint-batch", type=int, default=18, help="instances of the batched gradient")
     ap.add_argument("--thermal-max-sweeps", type=int, default=0)
     ap.add_argument("--thermal-precision", type=int, default=64, choices=[32, 64])
     ap.add_argument("--jacobi-block", type=int, default=0, help="sweeps per launch (0 = automatic)")

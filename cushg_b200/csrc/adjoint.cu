@@ -1,5 +1,6 @@
 // adjoint.cu — instantiations and host driver of the adjoint march (ssfm_adjoint.cuh):
-// shg_grad of include/shg.h.
+// shg_grad and shg_grad_batch of include/shg.h.  A batch is one launch with one cluster per
+// instance, each with its own checkpoints, segment buffers and accumulators.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -18,11 +19,11 @@ namespace {
 struct AdjVariant {
     int precision, n, cluster, threads;
     size_t smem;
-    cudaError_t (*launch)(const InstDesc*, const AdjDesc*, cudaStream_t);
+    cudaError_t (*launch)(const InstDesc*, const AdjDesc*, int count, cudaStream_t);
 };
 
 template <typename T, int N, int C, int NT>
-cudaError_t launch_adjoint(const InstDesc* d, const AdjDesc* a, cudaStream_t stream) {
+cudaError_t launch_adjoint(const InstDesc* d, const AdjDesc* a, int count, cudaStream_t stream) {
     using Cfg = PlainCfg<T, N, C, NT, false>;
     auto kern = ssfm_adjoint_kernel<T, N, C, NT>;
     static std::once_flag once;
@@ -34,7 +35,7 @@ cudaError_t launch_adjoint(const InstDesc* d, const AdjDesc* a, cudaStream_t str
     });
     if (attr_err != cudaSuccess) return attr_err;
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(C, 1, 1);
+    cfg.gridDim = dim3((unsigned)(C * count), 1, 1);
     cfg.blockDim = dim3(NT, 1, 1);
     cfg.dynamicSmemBytes = Cfg::smem_bytes;
     cfg.stream = stream;
@@ -52,7 +53,7 @@ cudaError_t launch_adjoint(const InstDesc* d, const AdjDesc* a, cudaStream_t str
 
 const AdjVariant kAdjVariants[] = {
     SHG_ADJ(float, 32, 32, 1, 128),  SHG_ADJ(float, 32, 64, 1, 256),   SHG_ADJ(float, 32, 128, 2, 256),
-    SHG_ADJ(float, 32, 256, 8, 256), SHG_ADJ(double, 64, 32, 1, 128),  SHG_ADJ(double, 64, 64, 1, 256),
+    SHG_ADJ(float, 32, 256, 16, 256), SHG_ADJ(double, 64, 32, 1, 128),  SHG_ADJ(double, 64, 64, 1, 256),
     SHG_ADJ(double, 64, 128, 4, 256), SHG_ADJ(double, 64, 256, 16, 256),
 };
 
@@ -80,57 +81,76 @@ void pump_params(const shg_params& p, double w, double f, double T, double* out4
 
 using namespace shg;
 
-extern "C" shg_status shg_grad(const shg_params* p, const double* poling, int32_t checkpoint_every,
-                               shg_grad_result* out) {
-    shg_status st = shg_check_params(p);
-    if (st != SHG_OK) return st;
+namespace {
+
+// Per-instance host state of a gradient batch.
+struct GradJob {
+    InstDesc d;
+    AdjDesc a;
+    int nsteps, K, M;
+    size_t off_ckpt, off_seg, off_lam, off_z, off_part, off_phi, off_pol;  // in the instance's workspace
+    size_t bytes;
+};
+
+shg_status grad_batch(const shg_params* ps, int count, const double* const* poling, int32_t checkpoint_every,
+                      shg_grad_result* out) {
+    for (int i = 0; i < count; ++i) {
+        shg_status st = shg_check_params(&ps[i]);
+        if (st != SHG_OK) return count > 1 ? fail(st, "instance %d: %s", i, shg_last_error()) : st;
+        if (ps[i].thermal) return fail(SHG_ERR_UNSUPPORTED, "gradients are for plain runs (thermal == 0)");
+        if (ps[i].precision != ps[0].precision || ps[i].nx != ps[0].nx)
+            return fail(SHG_ERR_INVALID, "instance %d: a gradient batch shares one precision and grid side", i);
+    }
     if (!out) return fail(SHG_ERR_INVALID, "out is NULL");
-    if (p->thermal) return fail(SHG_ERR_UNSUPPORTED, "gradients are for plain runs (thermal == 0)");
-    const AdjVariant* v = find_adj(p->precision, p->nx);
-    if (!v) return fail(SHG_ERR_UNSUPPORTED, "no adjoint kernel for grid side %d at precision %d", p->nx, p->precision);
+    const shg_params& p0 = ps[0];
+    const AdjVariant* v = find_adj(p0.precision, p0.nx);
+    if (!v) return fail(SHG_ERR_UNSUPPORTED, "no adjoint kernel for grid side %d at precision %d", p0.nx, p0.precision);
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();
         return fail(SHG_ERR_NO_DEVICE, "no CUDA device visible");
     }
-    const int nsteps = shg_steps(p);
-    const int K = checkpoint_every > 0 ? std::min(checkpoint_every, nsteps)
-                                       : std::max(1, (int)std::lround(std::sqrt((double)nsteps)));
-    const int M = (nsteps + K - 1) / K;
     const int C = v->cluster;
-    const size_t NN = (size_t)p->nx * p->nx;
-    const size_t cb = complex_bytes(*p);
-
-    InstDesc d = make_plain_desc(*p, p->temp, p->temp);
-    AdjDesc a;
-    std::memset(&a, 0, sizeof(a));
-    a.K = K;
-    a.M = M;
-    // central differences of the closed-form pump
-    const double hw = 1e-5 * p->waist, hf = 1e-5 * std::max(std::fabs(p->focus), p->lz), hT = 1e-3;
-    pump_params(*p, p->waist + hw, p->focus, p->temp, a.pert[0]);
-    pump_params(*p, p->waist - hw, p->focus, p->temp, a.pert[1]);
-    pump_params(*p, p->waist, p->focus + hf, p->temp, a.pert[2]);
-    pump_params(*p, p->waist, p->focus - hf, p->temp, a.pert[3]);
-    pump_params(*p, p->waist, p->focus, p->temp + hT, a.pert[4]);
-    pump_params(*p, p->waist, p->focus, p->temp - hT, a.pert[5]);
-    a.inv2h[0] = 1.0 / (2 * hw);
-    a.inv2h[1] = 1.0 / (2 * hf);
-    a.inv2h[2] = 1.0 / (2 * hT);
-    std::vector<double> zs(nsteps);
-    double z = 0.0;
-    for (int s = 0; s < nsteps; ++s) {
-        zs[s] = z;
-        z += d.dz;  // the forward's accumulation (Solver.h:303)
-    }
-
-    // device workspace
-    const size_t b_ckpt = (size_t)M * 2 * NN * cb, b_seg = (size_t)K * 2 * NN * cb, b_lam = 2 * NN * cb;
-    const size_t b_z = sizeof(double) * nsteps, b_part = sizeof(double) * C * kAdjAcc, b_phi = sizeof(double) * nsteps * C;
-    const size_t b_pol = sizeof(double) * nsteps;
+    const size_t NN = (size_t)p0.nx * p0.nx;
+    const size_t cb = complex_bytes(p0);
     auto up = [](size_t x) { return (x + 255) & ~(size_t)255; };
-    const size_t total = up(b_ckpt) + 3 * up(b_seg) + up(b_lam) + up(b_z) + up(b_part) + up(b_phi) + up(b_pol) +
-                         up(sizeof(InstDesc)) + up(sizeof(AdjDesc));
+    std::vector<GradJob> jobs(count);
+    size_t total = 0;
+    for (int i = 0; i < count; ++i) {
+        const shg_params& p = ps[i];
+        GradJob& J = jobs[i];
+        J.nsteps = shg_steps(&p);
+        J.K = checkpoint_every > 0 ? std::min(checkpoint_every, J.nsteps)
+                                   : std::max(1, (int)std::lround(std::sqrt((double)J.nsteps)));
+        J.M = (J.nsteps + J.K - 1) / J.K;
+        J.d = make_plain_desc(p, p.temp, p.temp);
+        std::memset(&J.a, 0, sizeof(J.a));
+        J.a.K = J.K;
+        J.a.M = J.M;
+        // central differences of the closed-form pump
+        const double hw = 1e-5 * p.waist, hf = 1e-5 * std::max(std::fabs(p.focus), p.lz), hT = 1e-3;
+        pump_params(p, p.waist + hw, p.focus, p.temp, J.a.pert[0]);
+        pump_params(p, p.waist - hw, p.focus, p.temp, J.a.pert[1]);
+        pump_params(p, p.waist, p.focus + hf, p.temp, J.a.pert[2]);
+        pump_params(p, p.waist, p.focus - hf, p.temp, J.a.pert[3]);
+        pump_params(p, p.waist, p.focus, p.temp + hT, J.a.pert[4]);
+        pump_params(p, p.waist, p.focus, p.temp - hT, J.a.pert[5]);
+        J.a.inv2h[0] = 1.0 / (2 * hw);
+        J.a.inv2h[1] = 1.0 / (2 * hf);
+        J.a.inv2h[2] = 1.0 / (2 * hT);
+        size_t o = 0;
+        J.off_ckpt = o; o += up((size_t)J.M * 2 * NN * cb);
+        J.off_seg = o;  o += 3 * up((size_t)J.K * 2 * NN * cb);
+        J.off_lam = o;  o += up(2 * NN * cb);
+        J.off_z = o;    o += up(sizeof(double) * J.nsteps);
+        J.off_part = o; o += up(sizeof(double) * C * kAdjAcc);
+        J.off_phi = o;  o += up(sizeof(double) * (size_t)J.nsteps * C);
+        J.off_pol = o;  o += up(sizeof(double) * J.nsteps);
+        J.bytes = o;
+        total += o;
+    }
+    const size_t b_desc = up(sizeof(InstDesc) * (size_t)count), b_adesc = up(sizeof(AdjDesc) * (size_t)count);
+    total += b_desc + b_adesc;
     cudaStream_t s = nullptr;
     cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
     if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
@@ -139,75 +159,97 @@ extern "C" shg_status shg_grad(const shg_params* p, const double* poling, int32_
     cudaEvent_t t0 = nullptr, t1 = nullptr;
     do {
         if ((e = cudaMallocAsync((void**)&buf, total, s)) != cudaSuccess) { rc = cuda_fail(e, "cudaMallocAsync"); break; }
-        char* q = buf;
-        auto take = [&](size_t b) { char* r = q; q += up(b); return r; };
-        a.ckpt = take(b_ckpt);
-        a.seg_a2 = take(b_seg);
-        a.seg_x = take(b_seg);
-        a.seg_y = take(b_seg);
-        a.lam = take(b_lam);
-        double* dz_ = reinterpret_cast<double*>(take(b_z));
-        a.zs = dz_;
-        a.part = reinterpret_cast<double*>(take(b_part));
-        a.phi = reinterpret_cast<double*>(take(b_phi));
-        double* dpol = reinterpret_cast<double*>(take(b_pol));
-        InstDesc* dd = reinterpret_cast<InstDesc*>(take(sizeof(InstDesc)));
-        AdjDesc* da = reinterpret_cast<AdjDesc*>(take(sizeof(AdjDesc)));
-        d.poling = poling ? dpol : nullptr;
-        if ((e = cudaMemcpyAsync(dz_, zs.data(), b_z, cudaMemcpyHostToDevice, s)) != cudaSuccess ||
-            (poling && (e = cudaMemcpyAsync(dpol, poling, b_pol, cudaMemcpyHostToDevice, s)) != cudaSuccess) ||
-            (e = cudaMemcpyAsync(dd, &d, sizeof(d), cudaMemcpyHostToDevice, s)) != cudaSuccess ||
-            (e = cudaMemcpyAsync(da, &a, sizeof(a), cudaMemcpyHostToDevice, s)) != cudaSuccess) {
+        std::vector<InstDesc> hd(count);
+        std::vector<AdjDesc> ha(count);
+        char* q = buf + b_desc + b_adesc;
+        for (int i = 0; i < count && rc == SHG_OK; ++i) {
+            GradJob& J = jobs[i];
+            J.a.ckpt = q + J.off_ckpt;
+            J.a.seg_a2 = q + J.off_seg;
+            J.a.seg_x = q + J.off_seg + up((size_t)J.K * 2 * NN * cb);
+            J.a.seg_y = q + J.off_seg + 2 * up((size_t)J.K * 2 * NN * cb);
+            J.a.lam = q + J.off_lam;
+            J.a.zs = reinterpret_cast<const double*>(q + J.off_z);
+            J.a.part = reinterpret_cast<double*>(q + J.off_part);
+            J.a.phi = reinterpret_cast<double*>(q + J.off_phi);
+            J.d.poling = (poling && poling[i]) ? reinterpret_cast<const double*>(q + J.off_pol) : nullptr;
+            std::vector<double> zs(J.nsteps);
+            double z = 0.0;
+            for (int k = 0; k < J.nsteps; ++k) {
+                zs[k] = z;
+                z += J.d.dz;  // the forward's accumulation (Solver.h:303)
+            }
+            if ((e = cudaMemcpyAsync(q + J.off_z, zs.data(), sizeof(double) * J.nsteps, cudaMemcpyHostToDevice, s)) !=
+                    cudaSuccess ||
+                (J.d.poling && (e = cudaMemcpyAsync(q + J.off_pol, poling[i], sizeof(double) * J.nsteps,
+                                                    cudaMemcpyHostToDevice, s)) != cudaSuccess))
+                rc = cuda_fail(e, "cudaMemcpyAsync");
+            hd[i] = J.d;
+            ha[i] = J.a;
+            q += J.bytes;
+        }
+        if (rc != SHG_OK) break;
+        InstDesc* dd = reinterpret_cast<InstDesc*>(buf);
+        AdjDesc* da = reinterpret_cast<AdjDesc*>(buf + b_desc);
+        if ((e = cudaMemcpyAsync(dd, hd.data(), sizeof(InstDesc) * count, cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(da, ha.data(), sizeof(AdjDesc) * count, cudaMemcpyHostToDevice, s)) != cudaSuccess) {
             rc = cuda_fail(e, "cudaMemcpyAsync");
             break;
         }
         cudaEventCreate(&t0);
         cudaEventCreate(&t1);
         cudaEventRecord(t0, s);
-        if ((e = v->launch(dd, da, s)) != cudaSuccess) { rc = cuda_fail(e, "launch ssfm_adjoint_kernel"); break; }
+        if ((e = v->launch(dd, da, count, s)) != cudaSuccess) { rc = cuda_fail(e, "launch ssfm_adjoint_kernel"); break; }
         cudaEventRecord(t1, s);
-        std::vector<double> part((size_t)C * kAdjAcc), phi((size_t)nsteps * C);
-        if ((e = cudaMemcpyAsync(part.data(), a.part, b_part, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
-            (e = cudaMemcpyAsync(phi.data(), a.phi, b_phi, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
-            (e = cudaStreamSynchronize(s)) != cudaSuccess) {
-            rc = cuda_fail(e, "adjoint march");
-            break;
-        }
+        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) { rc = cuda_fail(e, "adjoint march"); break; }
         float ms = 0.f;
         cudaEventElapsedTime(&ms, t0, t1);
-        double A[kAdjAcc] = {0};
-        for (int c = 0; c < C; ++c)
-            for (int i = 0; i < kAdjAcc; ++i) A[i] += part[(size_t)c * kAdjAcc + i];
-        // temperature derivatives of the scalar constants (central differences in FP64)
-        const double lp = p->lambda_p, ls = 0.5 * lp, T = p->temp, h = 1e-3;
-        const double np = sellmeier(lp, T), ns = sellmeier(ls, T);
-        const double dnp = (sellmeier(lp, T + h) - sellmeier(lp, T - h)) / (2 * h);
-        const double dns = (sellmeier(ls, T + h) - sellmeier(ls, T - h)) / (2 * h);
-        const double ddk = (delta_k(*p, T + h) - delta_k(*p, T - h)) / (2 * h);
-        const double J = d.pw_s * A[kAccJ];
-        double dT = 0.0;
-        dT += A[kAccKp] * (-dnp / np);                     // κp = π dQ / (n_p λp)
-        dT += A[kAccKs] * (-dns / ns);                     // κs = 0.5 π dQ / (n_s λs)
-        dT += A[kAccDk] * ddk;                             // Δk(T)
-        dT += A[kAccQs] * d.qs * (dns / ns);               // two-photon term ∝ n_s
-        dT += d.dz * A[kAccPropP] * d.a_p * (dnp / np);    // propagator phase a = 2π²/k ∝ 1/n
-        dT += d.dz * A[kAccPropS] * d.a_s * (dns / ns);
-        dT += A[kAccG0T];                                  // initial pump
-        dT += J * (dns / ns);                              // power normalisation ∝ n_s
-        std::memset(out->reserved, 0, sizeof(out->reserved));
-        out->sh_power = J;
-        out->d_waist = A[kAccG0w];
-        out->d_focus = A[kAccG0f];
-        out->d_temp = dT;
-        out->device_ms = ms;
-        out->checkpoint_every = K;
-        out->steps = nsteps;
-        if (out->d_poling)
-            for (int k = 0; k < nsteps; ++k) {
-                double t = 0.0;
-                for (int c = 0; c < C; ++c) t += phi[(size_t)k * C + c];
-                out->d_poling[k] = t;
+        for (int i = 0; i < count && rc == SHG_OK; ++i) {
+            const GradJob& J = jobs[i];
+            const shg_params& p = ps[i];
+            std::vector<double> part((size_t)C * kAdjAcc), phi((size_t)J.nsteps * C);
+            if ((e = cudaMemcpy(part.data(), J.a.part, sizeof(double) * part.size(), cudaMemcpyDeviceToHost)) !=
+                    cudaSuccess ||
+                (e = cudaMemcpy(phi.data(), J.a.phi, sizeof(double) * phi.size(), cudaMemcpyDeviceToHost)) != cudaSuccess) {
+                rc = cuda_fail(e, "adjoint results");
+                break;
             }
+            double A[kAdjAcc] = {0};
+            for (int c = 0; c < C; ++c)
+                for (int k = 0; k < kAdjAcc; ++k) A[k] += part[(size_t)c * kAdjAcc + k];
+            // temperature derivatives of the scalar constants (central differences in FP64)
+            const double lp = p.lambda_p, ls = 0.5 * lp, T = p.temp, h = 1e-3;
+            const double np = sellmeier(lp, T), ns = sellmeier(ls, T);
+            const double dnp = (sellmeier(lp, T + h) - sellmeier(lp, T - h)) / (2 * h);
+            const double dns = (sellmeier(ls, T + h) - sellmeier(ls, T - h)) / (2 * h);
+            const double ddk = (delta_k(p, T + h) - delta_k(p, T - h)) / (2 * h);
+            const InstDesc& d = J.d;
+            const double Jp = d.pw_s * A[kAccJ];
+            double dT = 0.0;
+            dT += A[kAccKp] * (-dnp / np);                     // κp = π dQ / (n_p λp)
+            dT += A[kAccKs] * (-dns / ns);                     // κs = 0.5 π dQ / (n_s λs)
+            dT += A[kAccDk] * ddk;                             // Δk(T)
+            dT += A[kAccQs] * d.qs * (dns / ns);               // two-photon term ∝ n_s
+            dT += d.dz * A[kAccPropP] * d.a_p * (dnp / np);    // propagator phase a = 2π²/k ∝ 1/n
+            dT += d.dz * A[kAccPropS] * d.a_s * (dns / ns);
+            dT += A[kAccG0T];                                  // initial pump
+            dT += Jp * (dns / ns);                             // power normalisation ∝ n_s
+            shg_grad_result& r = out[i];
+            std::memset(r.reserved, 0, sizeof(r.reserved));
+            r.sh_power = Jp;
+            r.d_waist = A[kAccG0w];
+            r.d_focus = A[kAccG0f];
+            r.d_temp = dT;
+            r.device_ms = ms;
+            r.checkpoint_every = J.K;
+            r.steps = J.nsteps;
+            if (r.d_poling)
+                for (int k = 0; k < J.nsteps; ++k) {
+                    double t = 0.0;
+                    for (int c = 0; c < C; ++c) t += phi[(size_t)k * C + c];
+                    r.d_poling[k] = t;
+                }
+        }
     } while (0);
     if (t0) cudaEventDestroy(t0);
     if (t1) cudaEventDestroy(t1);
@@ -217,4 +259,20 @@ extern "C" shg_status shg_grad(const shg_params* p, const double* poling, int32_
     e = cudaGetLastError();
     if (rc == SHG_OK && e != cudaSuccess) rc = cuda_fail(e, "adjoint");
     return rc;
+}
+
+}  // namespace
+
+extern "C" shg_status shg_grad(const shg_params* p, const double* poling, int32_t checkpoint_every,
+                               shg_grad_result* out) {
+    clear_error();
+    if (!p) return fail(SHG_ERR_INVALID, "params is NULL");
+    return grad_batch(p, 1, &poling, checkpoint_every, out);
+}
+
+extern "C" shg_status shg_grad_batch(const shg_params* params, int32_t count, const double* const* poling,
+                                     int32_t checkpoint_every, shg_grad_result* out) {
+    clear_error();
+    if (!params || count <= 0) return fail(SHG_ERR_INVALID, "params is NULL or count <= 0");
+    return grad_batch(params, count, poling, checkpoint_every, out);
 }

@@ -9,8 +9,9 @@
 // where N_s^T is the vector-Jacobian product of the RK4 scheme (stage values recomputed from
 // the input point) and L^H the diffraction with the conjugate propagator.
 //
-// One cluster owns the instance for the whole computation, with the same shared-memory
-// layout and transform passes as the forward march (ssfm_plain.cuh):
+// One cluster owns an instance for the whole computation (a launch holds one cluster per
+// instance of a batch), with the same shared-memory layout and transform passes as the
+// forward march (ssfm_plain.cuh):
 //   1. forward march, keeping x_{mK} (checkpoints every K steps) in global memory;
 //   2. for each segment m from the last: re-march from x_{mK}, keeping x_s, a2_s and the
 //      propagated spectra of each step of the segment (the last segment's come from step 1
@@ -57,11 +58,13 @@ struct AdjDesc {
 };
 
 // Vector-Jacobian product of dA/dz at (p, s) (see dadz): adds to (gp, gs) the adjoints of
-// the inputs given the adjoints (gdp, gds) of (dp, ds), and to sens[] the parameter terms
-// (sens[0] κp, [1] κs, [2] Δk (weight wz = z + dz inc), [3] qs, [4] poling phase).
+// the inputs given the adjoints (gdp, gds) of (dp, ds), and to sens[] the parameter terms in
+// the working precision: sens[0] κp, [1] κs, [2] Σ inc·e_φ, [3] qs, [4] Σ e_φ, where e_φ is
+// the mismatch-phase term and inc the stage's offset in units of dz (0, 1/4, 1/2), so that
+// the Δk term of a step at z is z·sens[4] + dz·sens[2] and its poling term sens[4].
 template <typename T>
 __device__ __forceinline__ void dadz_vjp(cx<T> p, cx<T> s, cx<T> cP, cx<T> cS, T hap, T has, T qs, cx<T> gdp,
-                                         cx<T> gds, cx<T>& gp, cx<T>& gs, double wz, double* sens) {
+                                         cx<T> gds, cx<T>& gp, cx<T>& gs, T inc, T* sens) {
     const cx<T> t = mul<T>(cP, mulc<T>(s, p));                   // cP s conj(p)
     const cx<T> pp = mk<T>(p.x * p.x - p.y * p.y, (T)2 * p.x * p.y);
     const cx<T> u = mul<T>(cS, pp);                               // cS p^2
@@ -76,23 +79,20 @@ __device__ __forceinline__ void dadz_vjp(cx<T> p, cx<T> s, cx<T> cP, cx<T> cS, T
     const cx<T> e = mulc<T>(ss, gds);
     const T h = -has - (T)2 * qs * a2;
     gs = mk<T>(gs.x + c.x + h * gds.x - qs * e.x, gs.y + c.y + h * gds.y - qs * e.y);
-    const double ekp = (double)gdp.x * t.x + (double)gdp.y * t.y;
-    const double eks = (double)gds.x * u.x + (double)gds.y * u.y;
-    const double eph = ((double)gdp.x * t.y - (double)gdp.y * t.x) - ((double)gds.x * u.y - (double)gds.y * u.x);
-    const double eqs = -(double)a2 * ((double)gds.x * s.x + (double)gds.y * s.y);
-    sens[0] += ekp;
-    sens[1] += eks;
-    sens[2] += eph * wz;
-    sens[3] += eqs;
+    const T eph = (gdp.x * t.y - gdp.y * t.x) - (gds.x * u.y - gds.y * u.x);
+    sens[0] += gdp.x * t.x + gdp.y * t.y;
+    sens[1] += gds.x * u.x + gds.y * u.y;
+    sens[2] += eph * inc;
+    sens[3] += -a2 * (gds.x * s.x + gds.y * s.y);
     sens[4] += eph;
 }
 
 // Vector-Jacobian product of one RK4 application (rk4_point) at input (p, s) with stage
 // coefficients cf (phases at z, z + dz/4, z + dz/2): (gp, gs) holds the adjoint of the
-// output on entry and of the input on return.
+// output on entry and of the input on return; sens[] as for dadz_vjp.
 template <typename T>
-__device__ __forceinline__ void rk4_vjp(cx<T> p, cx<T> s, const cx<T>* cf, T hap, T has, T qs, T dz6, double z,
-                                        double dz, cx<T>& gp, cx<T>& gs, double* sens) {
+__device__ __forceinline__ void rk4_vjp(cx<T> p, cx<T> s, const cx<T>* cf, T hap, T has, T qs, T dz6, cx<T>& gp,
+                                        cx<T>& gs, T* sens) {
     using V = cx<T>;
     V k1p, k1s, k2p, k2s, k3p, k3s, k4p, k4s;
     dadz<T>(p, s, cf[0], cf[3], hap, has, qs, k1p, k1s);
@@ -108,28 +108,28 @@ __device__ __forceinline__ void rk4_vjp(cx<T> p, cx<T> s, const cx<T>* cf, T hap
     V g2p = g3p, g2s = g3s;
     V g1p = scale<T>(gop, dz6), g1s = scale<T>(gos, dz6);
     V hp = mk<T>(0, 0), hs = mk<T>(0, 0);
-    dadz_vjp<T>(u4p, u4s, cf[2], cf[5], hap, has, qs, g1p, g1s, hp, hs, z + 0.5 * dz, sens);  // g_k4 = dz6 g
+    dadz_vjp<T>(u4p, u4s, cf[2], cf[5], hap, has, qs, g1p, g1s, hp, hs, (T)0.5, sens);  // g_k4 = dz6 g
     gp = add<T>(gop, hp);
     gs = add<T>(gos, hs);
     g3p = add<T>(g3p, hp);
     g3s = add<T>(g3s, hs);
     hp = mk<T>(0, 0);
     hs = mk<T>(0, 0);
-    dadz_vjp<T>(u3p, u3s, cf[1], cf[4], hap, has, qs, g3p, g3s, hp, hs, z + 0.25 * dz, sens);
+    dadz_vjp<T>(u3p, u3s, cf[1], cf[4], hap, has, qs, g3p, g3s, hp, hs, (T)0.25, sens);
     gp = add<T>(gp, hp);
     gs = add<T>(gs, hs);
     g2p = add<T>(g2p, scale<T>(hp, (T)0.5));
     g2s = add<T>(g2s, scale<T>(hs, (T)0.5));
     hp = mk<T>(0, 0);
     hs = mk<T>(0, 0);
-    dadz_vjp<T>(u2p, u2s, cf[1], cf[4], hap, has, qs, g2p, g2s, hp, hs, z + 0.25 * dz, sens);
+    dadz_vjp<T>(u2p, u2s, cf[1], cf[4], hap, has, qs, g2p, g2s, hp, hs, (T)0.25, sens);
     gp = add<T>(gp, hp);
     gs = add<T>(gs, hs);
     g1p = add<T>(g1p, scale<T>(hp, (T)0.5));
     g1s = add<T>(g1s, scale<T>(hs, (T)0.5));
     hp = mk<T>(0, 0);
     hs = mk<T>(0, 0);
-    dadz_vjp<T>(p, s, cf[0], cf[3], hap, has, qs, g1p, g1s, hp, hs, z, sens);
+    dadz_vjp<T>(p, s, cf[0], cf[3], hap, has, qs, g1p, g1s, hp, hs, (T)0, sens);
     gp = add<T>(gp, hp);
     gs = add<T>(gs, hs);
 }
@@ -158,8 +158,9 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
 
     const int tid = threadIdx.x;
     const int crank = (C > 1) ? (int)cg::this_cluster().block_rank() : 0;
-    const InstDesc d = descs[0];
-    const AdjDesc& a = *adescs;
+    const int inst = blockIdx.x / C;  // one cluster per instance
+    const InstDesc d = descs[inst];
+    const AdjDesc& a = adescs[inst];
     const int nsteps = d.nsteps;
     const int K = a.K;
     const T hap = (T)d.hap, has = (T)d.has, qs = (T)d.qs, dz6 = (T)(d.dz / 6.0);
@@ -283,17 +284,20 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
                 rS[r] = Ss;
             }
         }
+        const T dfy2 = (T)(d.dfy * d.dfy);
         for (int j = tid; j < JCB; j += NT) {
             const int xl = j % (N / C), k2 = j / (N / C);
             const int x = crank * (N / C) + xl;
             const int fx = (x >> 4) + R2 * (x & 15);
             const double sx = (double)(fx < N / 2 ? fx : fx - N);
+            const T fxq = (T)(d.dfx * d.dfx * (sx * sx));  // dfx^2 sx^2 of this column
 #pragma unroll 1
             for (int f = 0; f < 2; ++f) {
                 V* const* R = f ? rS : rP;
                 const W px = f ? pxs[x] : pxp[x];
                 const W* py = f ? pys : pyp;
                 V* ybuf = (ys >= 0) ? seg_y + ((size_t)ys * 2 + f) * NN : nullptr;
+                T wsum = 0;  // this job's propagator-phase sensitivity (adjoint)
                 V u[16];
 #pragma unroll
                 for (int n = 0; n < 16; ++n) u[n] = R[n % C][sidx<N, R2, SW>(n / C + CPR * k2, x)];
@@ -316,11 +320,9 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
                                 // dJ/dθ_f = Re(conj(Λ) i Y): Λ = this spectrum / N^2, Y = stored D X,
                                 // stored as D X / N^2 -> Re(conj(u) i Ystored)
                                 const V yv = ybuf[yo];
-                                const double c = (double)u[k1].x * (-(double)yv.y) + (double)u[k1].y * (double)yv.x;
-                                const double sy = (double)(fy < N / 2 ? fy : fy - N);
-                                const double w = c * (d.dfx * d.dfx * (sx * sx) + d.dfy * d.dfy * (sy * sy));
-                                if (f) acc_ps += w;
-                                else acc_pp += w;
+                                const T c = u[k1].y * yv.x - u[k1].x * yv.y;
+                                const T sy = (T)(fy < N / 2 ? fy : fy - N);
+                                wsum += c * (fxq + dfy2 * (sy * sy));
                                 // conjugate propagator: conj(py) conj(px), via conj(conj(u) py px)
                                 u[k1] = cj(mulw(mulw(cj(u[k1]), py[fy]), px));
                             }
@@ -329,6 +331,10 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
 #pragma unroll
                         for (int n = 0; n < 16; ++n) u[n] = cj(u[n]);
                     }
+                }
+                if (adjoint) {
+                    if (f) acc_ps += (double)wsum;
+                    else acc_pp += (double)wsum;
                 }
 #pragma unroll
                 for (int n = 0; n < 16; ++n) R[n % C][sidx<N, R2, SW>(n / C + CPR * k2, x)] = u[n];
@@ -438,11 +444,14 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
         }
         __syncthreads();
     };
-    auto add_sens = [&](const double* sn) {
-        acc_kp += sn[0];
-        acc_ks += sn[1];
-        acc_dk += sn[2];
-        acc_qs += sn[3];
+    // a job's working-precision partials of step s into the FP64 accumulators; returns the
+    // poling term
+    auto add_sens = [&](const T* sn, int s) -> double {
+        acc_kp += (double)sn[0];
+        acc_ks += (double)sn[1];
+        acc_dk += a.zs[s] * (double)sn[4] + d.dz * (double)sn[2];
+        acc_qs += (double)sn[3];
+        return (double)sn[4];
     };
 
     // ---- adjoint march back over [sb, se) from lambda_se in shared memory ---------------
@@ -453,6 +462,7 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
         // mu2_{se-1} = N^T(a2_{se-1}) lambda_se, then the forward row stage
         for (int j = tid; j < JA; j += NT) {
             const int n1 = j & 15, lr = j >> 4;
+            T sn[5] = {0, 0, 0, 0, 0};
 #pragma unroll 1
             for (int k = 0; k < R2; ++k) {
                 const int x = n1 + 16 * k;
@@ -460,14 +470,12 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
                 const size_t g = (size_t)(crank + C * lr) * N + x;
                 const size_t sl = (size_t)(se - 1 - sb) * 2;
                 V gp = Ps[o], gs = Ss[o];
-                double sn[5] = {0, 0, 0, 0, 0};
                 rk4_vjp<T>(seg_a2[sl * NN + g], seg_a2[(sl + 1) * NN + g], coef + 6 * ((se - 1) & 1), hap, has, qs, dz6,
-                           a.zs[se - 1], d.dz, gp, gs, sn);
-                add_sens(sn);
-                phi_cur += sn[4];
+                           gp, gs, sn);
                 Ps[o] = gp;
                 Ss[o] = gs;
             }
+            phi_cur += add_sens(sn, se - 1);
 #pragma unroll 1
             for (int f = 0; f < 2; ++f) row_a(f ? Ss : Ps, lr, n1, false);
         }
@@ -487,6 +495,7 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
             double phi_prev = 0.0;  // this thread's part of Φ_{s-1} (from a2_{s-1})
             for (int j = tid; j < JA; j += NT) {
                 const int n1 = j & 15, lr = j >> 4;
+                T sn[5] = {0, 0, 0, 0, 0}, sn2[5] = {0, 0, 0, 0, 0};  // step s, step s-1
 #pragma unroll 1
                 for (int f = 0; f < 2; ++f) row_a(f ? Ss : Ps, lr, n1, true);
 #pragma unroll 1
@@ -504,20 +513,16 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
                         bp = seg_a2[sl * NN + g];
                         bs = seg_a2[(sl + 1) * NN + g];
                     }
-                    double sn[5] = {0, 0, 0, 0, 0};
-                    rk4_vjp<T>(xp, xs, coef + 6 * (s & 1), hap, has, qs, dz6, a.zs[s], d.dz, gp, gs, sn);
-                    add_sens(sn);
-                    phi_cur += sn[4];
+                    rk4_vjp<T>(xp, xs, coef + 6 * (s & 1), hap, has, qs, dz6, gp, gs, sn);
                     if (s > sb) {
                         // step s-1's second application: mu2_{s-1} = N^T(a2_{s-1}) lambda_s
-                        double sn2[5] = {0, 0, 0, 0, 0};
-                        rk4_vjp<T>(bp, bs, coef + 6 * ((s - 1) & 1), hap, has, qs, dz6, a.zs[s - 1], d.dz, gp, gs, sn2);
-                        add_sens(sn2);
-                        phi_prev += sn2[4];
+                        rk4_vjp<T>(bp, bs, coef + 6 * ((s - 1) & 1), hap, has, qs, dz6, gp, gs, sn2);
                     }
                     Ps[o] = gp;
                     Ss[o] = gs;
                 }
+                phi_cur += add_sens(sn, s);
+                if (s > sb) phi_prev += add_sens(sn2, s - 1);
                 if (s > sb) {
 #pragma unroll 1
                     for (int f = 0; f < 2; ++f) row_a(f ? Ss : Ps, lr, n1, false);

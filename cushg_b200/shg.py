@@ -26,7 +26,7 @@ EXPORTS = (
     "shg_default_params", "shg_check_params", "shg_steps", "shg_solve", "shg_solve_slices", "shg_solve_device",
     "shg_solve_batch_device", "shg_solve_batch_device_noalloc", "shg_grad", "shg_sh_power", "shg_last_error",
     "shg_status_string", "shg_version", "shg_heat_sweeps_device", "shg_batch_plan_create", "shg_batch_plan_launch",
-    "shg_batch_plan_powers", "shg_batch_plan_destroy", "shg_autotune",
+    "shg_batch_plan_powers", "shg_batch_plan_destroy", "shg_autotune", "shg_grad_batch",
 )
 
 
@@ -86,6 +86,9 @@ def lib() -> ctypes.CDLL:
         L.shg_solve_batch_device_noalloc.restype = ctypes.c_int
         L.shg_grad.argtypes = [P, ctypes.POINTER(ctypes.c_double), ctypes.c_int32, ctypes.POINTER(ShgGradResult)]
         L.shg_grad.restype = ctypes.c_int
+        L.shg_grad_batch.argtypes = [P, ctypes.c_int32, ctypes.POINTER(ctypes.POINTER(ctypes.c_double)),
+                                     ctypes.c_int32, ctypes.POINTER(ShgGradResult)]
+        L.shg_grad_batch.restype = ctypes.c_int
         L.shg_sh_power.argtypes = [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
         L.shg_sh_power.restype = ctypes.c_int
         L.shg_heat_sweeps_device.argtypes = [P, vp, vp, ctypes.c_int64, vp]
@@ -230,6 +233,35 @@ def grad(p: ShgParams, poling: np.ndarray | None = None, checkpoint_every: int =
     _check(lib().shg_grad(ctypes.byref(p), _dptr(pol), int(checkpoint_every), ctypes.byref(r)))
     return {"sh_power": r.sh_power, "d_waist": r.d_waist, "d_focus": r.d_focus, "d_temp": r.d_temp,
             "d_poling": dpol, "device_ms": r.device_ms, "checkpoint_every": r.checkpoint_every, "steps": r.steps}
+
+
+def grad_batch(ps: list[ShgParams], polings=None, checkpoint_every: int = 0) -> list[dict]:
+    """Gradients of many plain runs in one launch (shg_grad_batch); polings: None or a list of
+    per-instance poling vectors (entries may be None).  Returns one dict per instance as grad."""
+    n = len(ps)
+    arr = (ShgParams * n)(*ps)
+    DP = ctypes.POINTER(ctypes.c_double)
+    keep = []
+    pol_arr = None
+    if polings is not None:
+        pol_arr = (DP * n)()
+        for i, v in enumerate(polings):
+            if v is not None:
+                a = np.ascontiguousarray(np.asarray(v, dtype=np.float64))
+                if a.shape != (steps(ps[i]),):
+                    raise ValueError(f"poling {i} must have {steps(ps[i])} values")
+                keep.append(a)
+                pol_arr[i] = _dptr(a)
+    res = (ShgGradResult * n)()
+    dpols = []
+    for i in range(n):
+        d = np.zeros(steps(ps[i]), dtype=np.float64)
+        dpols.append(d)
+        res[i].d_poling = _dptr(d)
+    _check(lib().shg_grad_batch(arr, n, pol_arr, int(checkpoint_every), res))
+    return [{"sh_power": r.sh_power, "d_waist": r.d_waist, "d_focus": r.d_focus, "d_temp": r.d_temp,
+             "d_poling": dpols[i], "device_ms": r.device_ms, "checkpoint_every": r.checkpoint_every,
+             "steps": r.steps} for i, r in enumerate(res)]
 
 
 def sh_power(p: ShgParams, poling: np.ndarray | None = None) -> float:

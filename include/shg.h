@@ -279,6 +279,17 @@ typedef struct shg_grad_result {
 SHG_API shg_status shg_grad(const shg_params* p, const double* poling, int32_t checkpoint_every,
                             shg_grad_result* out);
 
+/*
+ * Gradients of `count` plain runs in one launch (one thread-block cluster per instance), for
+ * sweeps and optimisers that need many gradients at once.  All instances share precision and
+ * grid side (nz and every other parameter may differ).  poling: NULL, or an array of `count`
+ * pointers each NULL or to shg_steps(&params[i]) phases.  out[i] as for shg_grad (its
+ * d_poling, if set, receives instance i's vector); device_ms is the whole launch.  No
+ * counterpart in the reference.
+ */
+SHG_API shg_status shg_grad_batch(const shg_params* params, int32_t count, const double* const* poling,
+                                  int32_t checkpoint_every, shg_grad_result* out);
+
 /* SH output power of a plain run with an optional per-step poling phase (as shg_grad),
  * forward only.  Host, synchronous. */
 SHG_API shg_status shg_sh_power(const shg_params* p, const double* poling, double* sh_power);

@@ -4,8 +4,9 @@
 //   kernelSetTemperature / kernelSetBottomOvensTemperature / kernelSetOvenSurrounded
 //       -> thermal_init_kernel
 //   kernelHeatEquationTopOpen / kernelHeatEquationOvenSurrounded (one Jacobi sweep)
-//       -> jacobi_kernel (Ti -> Tf; the reference's Tf -> Ti device copy after every
-//          sweep becomes a ping-pong of two buffers)
+//       -> jacobi_zb_kernel (unchecked sweeps) and jacobi_kernel (the checked sweep of each
+//          window); Ti -> Tf, the reference's Tf -> Ti device copy after every sweep becomes
+//          a ping-pong of two buffers
 //   kernelDifSquareVectors + thrust::reduce (checkConvergence)
 //       -> the RESID form of jacobi_kernel (per-block partials) + reduce_partials_kernel
 //   kernelSetInicialDKThermal and the per-voxel n(λ, T) of dAdz / kernelSetQ
@@ -104,6 +105,46 @@ __global__ void __launch_bounds__(256) jacobi_kernel(const R* __restrict__ Ti, R
     }
 }
 
+// One unchecked Jacobi sweep Ti -> Tf, z-blocked: thread (x, y) updates the column of up to
+// ZB planes z0..z0+ZB-1, keeping T at z-1, z and z+1 in registers as it walks up, so each
+// voxel costs one new load of the centre column and the four lateral neighbours (through
+// L1), and the boundary classification and index arithmetic are paid once per column step
+// instead of per neighbour.  Every voxel is computed by jacobi_point from the same operands
+// as in jacobi_kernel.  Thread block (32, 8), grid (n/32, n/8, nz/ZB).
+//
+// Used for FP32, where the one-voxel kernel is bound by instruction issue (91 thread
+// instructions per voxel, DRAM at 34 % of peak at 256x256x400): 104.5 -> 88.7 us per sweep
+// there, 249 -> 203 us at 512x512x250.  FP64 sweeps are already memory-bound and lose
+// parallelism here (64 -> 78 us at 256x256x200), so they keep jacobi_kernel.
+constexpr int kJacobiZB = 8;
+
+template <typename R, int BOUND>
+__global__ void __launch_bounds__(256) jacobi_zb_kernel(const R* __restrict__ Ti, R* __restrict__ Tf,
+                                                        const R* __restrict__ Q, JacobiCoef<R> k) {
+    const int n = k.n, nz = k.nz;
+    const int x = blockIdx.x * 32 + threadIdx.x;
+    const int y = blockIdx.y * 8 + threadIdx.y;
+    if (x >= n || y >= n) return;
+    const int z0 = blockIdx.z * kJacobiZB, z1 = min(nz, z0 + kJacobiZB);
+    const size_t sy = (size_t)n, sz = (size_t)n * n;
+    size_t i = (size_t)z0 * sz + (size_t)y * sy + x;
+    R below = z0 > 0 ? Ti[i - sz] : (R)0;
+    R cur = Ti[i];
+#pragma unroll 2
+    for (int z = z0; z < z1; ++z, i += sz) {
+        const R above = z + 1 < nz ? Ti[i + sz] : (R)0;
+        auto get = [&](int dx, int dy, int dz) -> R {
+            if (dz > 0) return above;
+            if (dz < 0) return below;
+            return Ti[i + (ptrdiff_t)dy * sy + dx];
+        };
+        R v;
+        if (jacobi_point<R, BOUND>(x, y, z, k, Q[i], get, &v)) Tf[i] = v;
+        below = cur;
+        cur = above;
+    }
+}
+
 // Deterministic second stage: one block sums (or maxes) the partials in a fixed order.
 __global__ void reduce_partials_kernel(const double* __restrict__ partial, size_t count, int rule, double* out) {
     __shared__ double s[256];
@@ -183,6 +224,14 @@ cudaError_t launch_jacobi(const R* Ti, R* Tf, const R* Q, const JacobiCoef<R>& k
                           double* partial, double* out, cudaStream_t s) {
     dim3 block(32, 8, 1);
     dim3 grid((k.n + 31) / 32, (k.n + 7) / 8, k.nz);
+    if (!resid && sizeof(R) == 4) {
+        const dim3 zgrid(grid.x, grid.y, (k.nz + kJacobiZB - 1) / kJacobiZB);
+        if (boundary == SHG_BOUNDARY_OVEN_SURROUNDED)
+            jacobi_zb_kernel<R, SHG_BOUNDARY_OVEN_SURROUNDED><<<zgrid, block, 0, s>>>(Ti, Tf, Q, k);
+        else
+            jacobi_zb_kernel<R, SHG_BOUNDARY_TOP_OPEN><<<zgrid, block, 0, s>>>(Ti, Tf, Q, k);
+        return cudaGetLastError();
+    }
     if (boundary == SHG_BOUNDARY_OVEN_SURROUNDED) {
         if (resid) jacobi_kernel<R, SHG_BOUNDARY_OVEN_SURROUNDED, true><<<grid, block, 0, s>>>(Ti, Tf, Q, k, rule, partial);
         else jacobi_kernel<R, SHG_BOUNDARY_OVEN_SURROUNDED, false><<<grid, block, 0, s>>>(Ti, Tf, Q, k, rule, partial);

@@ -36,6 +36,11 @@ from cushg_b200 import params as P  # noqa: E402
 
 B200_SMS = 148
 FP32_LANES_PER_SM = 128
+# DRAM bytes (read + write) per launch of the dominant kernel of the sweep, the 256 x 256 FP32
+# class (ssfm_plain_kernel<float, 256, 16, 256>), from one ncu launch-list capture of this
+# bench (`--steps 2 --warmup 3 --no-cpu-baseline --no-autotune`, metrics dram__bytes_read.sum
+# and dram__bytes_write.sum); the fields stay on chip, so this is descriptors and outputs
+SWEEP_256_DRAM_BYTES_PER_LAUNCH = 14.30e6
 
 
 def flops_per_point_step(n: int) -> float:
@@ -258,7 +263,9 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
                 "ms_per_step": e2e_ms},
         "gpu_launches": args.steps * len({p.nx for p in ps}),
         "roofline": {"bound": "fp32-issue" if args.precision == 32 else "fp64-issue", "achieved": achieved_tflops,
-                     "peak": peak, "unit": "TFLOP/s", "frac": achieved_tflops / peak, "traffic": None,
+                     "peak": peak, "unit": "TFLOP/s", "frac": achieved_tflops / peak,
+                     "traffic": SWEEP_256_DRAM_BYTES_PER_LAUNCH if (args.precision == 32 and not args.class_side) else None,
+                     "traffic_note": "DRAM bytes per launch of the 256x256 FP32 class, ncu capture of this bench",
                      "peak_source": f"nominal {B200_SMS} SMs x {lanes} lanes x 2 flop x measured median SM clock {sm_mhz:.0f} MHz",
                      "flops_per_launch_group": fl,
                      "hbm": {"achieved": hbm_achieved, "peak": hbm_peak, "unit": "GB/s", "frac": hbm_achieved / hbm_peak,

@@ -401,6 +401,39 @@ def run_thermal(args) -> dict:
     return out
 
 
+def run_thermal_batch(args) -> dict:
+    """Large thermal batch (outside the default sweep line): `--thermal-count` instances of
+    512x512 / nz = 1000 in FP32 (50 W, w0 = 50 µm, 20 mm, ovens evenly spaced 30-65 °C), each a
+    full thermal run through shg_solve_device with a fixed cost per optical-thermal update:
+    `--thermal-fixed-sweeps` Jacobi sweeps (FP64 residual of the last one reported) in each of
+    `--thermal-outer` outer iterations.  Jacobi to max|ΔT| < 1e-6 K at this size needs on the
+    order of 1e6 sweeps per outer iteration, beyond a bench budget."""
+    import torch
+    from cushg_b200 import shg
+
+    ps = P.config_thermal_512(args.thermal_count)
+    runs, jac_vox, opt_pts = [], 0.0, 0.0
+    with ClockSampler(0) as clk:
+        for p in ps:
+            p = p.replace(conv_rule=P.SHG_CONV_FIXED, max_sweeps=args.thermal_fixed_sweeps, max_outer=args.thermal_outer,
+                          precision=32)
+            pump = torch.empty((p.ny, p.nx), dtype=torch.complex64, device="cuda")
+            sig = torch.empty_like(pump)
+            st = shg.solve_device(p, pump, sig)
+            runs.append({"oven_c": round(p.temp, 2), "sh_power_w": st.sh_power, "device_ms": st.device_ms,
+                         "sweeps": st.jacobi_sweeps, "last_max_dT_K": st.last_residual})
+            jac_vox += float(p.nx * p.ny * p.nz) * st.jacobi_sweeps
+            opt_pts += float(p.nx * p.ny * p.nz) * st.outer_iterations
+            del pump, sig
+            torch.cuda.synchronize()
+    total_ms = sum(r["device_ms"] for r in runs)
+    return {"metric": "thermal batch device time", "value": total_ms, "unit": "ms", "higher_is_better": False,
+            "workload": f"{len(ps)} x thermal 512x512x1000 FP32, {args.thermal_outer} outer x "
+                        f"{args.thermal_fixed_sweeps} Jacobi sweeps each",
+            "instances": runs, "voxel_sweeps": jac_vox, "optical_point_steps": opt_pts,
+            "clocks": clk.summary()}
+
+
 def run_jacobi(args) -> dict:
     """Heat-solve workload (outside the default sweep line): `--jacobi-sweeps` Jacobi sweeps
     of the heat equation per step through shg_heat_sweeps_device on the thermal grid (default
@@ -531,7 +564,10 @@ def main() -> int:
     ap.add_argument("--class-side", type=int, default=0, help="profile case: one grid-size class only")
     ap.add_argument("--class-count", type=int, default=18)
     ap.add_argument("--class-nz", type=int, default=24)
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "thermal", "adjoint", "jacobi"])
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "thermal", "adjoint", "jacobi", "thermal-batch"])
+    ap.add_argument("--thermal-count", type=int, default=8)
+    ap.add_argument("--thermal-fixed-sweeps", type=int, default=200)
+    ap.add_argument("--thermal-outer", type=int, default=2)
     ap.add_argument("--jacobi-sweeps", type=int, default=400)
     ap.add_argument("--thermal-side", type=int, default=0)
     ap.add_argument("--thermal-nz", type=int, default=0)
@@ -552,6 +588,8 @@ def main() -> int:
         out = run_adjoint(args) if rank == 0 else None
     elif args.workload == "jacobi":
         out = run_jacobi(args) if rank == 0 else None
+    elif args.workload == "thermal-batch":
+        out = run_thermal_batch(args) if rank == 0 else None
     elif args.impl == "reference":
         out = run_reference(args, rank, world)
     else:

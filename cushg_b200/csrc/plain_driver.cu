@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -104,6 +105,8 @@ shg_status plain_solve_device(const shg_params& p, const void* signal_in, void* 
             stats->steps = d.nsteps;
             stats->outer_iterations = 1;
             stats->device_ms = ms;
+            if (!std::isfinite(h[0]) || !std::isfinite(h[1]))
+                rc = fail(SHG_ERR_NONFINITE, "SH / pump power %g / %g", h[0], h[1]);
         }
     } while (0);
     if (t0) cudaEventDestroy(t0);
@@ -228,6 +231,10 @@ shg_status plain_solve_batch(const shg_params* params, int count, void* const* p
                 break;
             }
             for (int i = 0; i < count; ++i) sh_power_out[i] = h[2 * (size_t)i];
+            for (int i = 0; i < count && rc == SHG_OK; ++i)
+                if (!std::isfinite(h[2 * (size_t)i]) || !std::isfinite(h[2 * (size_t)i + 1]))
+                    rc = fail(SHG_ERR_NONFINITE, "instance %d: SH / pump power %g / %g", i, h[2 * (size_t)i],
+                              h[2 * (size_t)i + 1]);
         }
     } while (0);
     cudaFreeAsync(buf, stream);

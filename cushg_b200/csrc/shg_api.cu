@@ -35,7 +35,8 @@ shg_status fail(shg_status st, const char* fmt, ...) {
 }
 
 shg_status cuda_fail(cudaError_t e, const char* what) {
-    return fail(SHG_ERR_CUDA, "%s: %s (%d)", what, cudaGetErrorString(e), (int)e);
+    const shg_status st = e == cudaErrorMemoryAllocation ? SHG_ERR_NOMEM : SHG_ERR_CUDA;
+    return fail(st, "%s: %s (%d)", what, cudaGetErrorString(e), (int)e);
 }
 
 void clear_error() { g_last_error.clear(); }
@@ -180,8 +181,10 @@ static shg_status check_params_impl(const shg_params* p, bool need_kernel) {
         if (!(p->kappa > 0) || p->h_conv < 0) return fail(SHG_ERR_INVALID, "kappa must be > 0, h_conv >= 0");
         if (p->boundary != SHG_BOUNDARY_TOP_OPEN && p->boundary != SHG_BOUNDARY_OVEN_SURROUNDED)
             return fail(SHG_ERR_INVALID, "unknown boundary %d", p->boundary);
-        if (p->conv_rule != SHG_CONV_REFERENCE && p->conv_rule != SHG_CONV_MAXABS)
+        if (p->conv_rule != SHG_CONV_REFERENCE && p->conv_rule != SHG_CONV_MAXABS && p->conv_rule != SHG_CONV_FIXED)
             return fail(SHG_ERR_INVALID, "unknown conv_rule %d", p->conv_rule);
+        if (p->conv_rule == SHG_CONV_FIXED && (p->max_sweeps <= 0 || p->max_outer <= 0))
+            return fail(SHG_ERR_INVALID, "conv_rule FIXED needs max_sweeps > 0 and max_outer > 0");
         if (p->nz < 3 || p->nx < 3) return fail(SHG_ERR_INVALID, "thermal grid needs nx, nz >= 3");
         if (p->jacobi_block < 0 || p->jacobi_block > 4)
             return fail(SHG_ERR_INVALID, "jacobi_block %d must be in 0..4", p->jacobi_block);
@@ -213,6 +216,7 @@ const char* shg_status_string(int32_t s) {
         case SHG_ERR_NOMEM: return "out of memory";
         case SHG_ERR_NOT_CONVERGED: return "Jacobi did not converge";
         case SHG_ERR_NO_DEVICE: return "no CUDA device";
+        case SHG_ERR_NONFINITE: return "non-finite result";
         default: return "unknown status";
     }
 }

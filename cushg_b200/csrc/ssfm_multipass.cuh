@@ -103,8 +103,9 @@ __device__ __forceinline__ void r2_stage(cx<T> (&v)[R2], const mult<T>* tw, int 
     }
 }
 
-// Row pass of step s (s = -1: the first pass, which builds the initial fields; s = nsteps-1:
-// the last, which writes the outputs and this CTA's power partials).  Grid (N / RB, count).
+// Row pass of step s (s = -1: the first pass, which builds the initial fields; the pass with
+// s + 1 = out_after writes the outputs and this CTA's power partials; s = nsteps-1 is the
+// last).  Grid (N / RB, count).
 template <typename T, int N, bool THERM>
 __global__ void __launch_bounds__(MpCfg<T, N>::RNT)
     mp_row_kernel(const InstDesc* __restrict__ descs, MpLayout L, int s) {
@@ -227,6 +228,31 @@ __global__ void __launch_bounds__(MpCfg<T, N>::RNT)
         }
     }
     __syncthreads();
+    if (s + 1 == d.out_after) {
+        // the pass that wrote the outputs (the last step of a plain run, the one before the
+        // last of a thermal run): this CTA's share of the SH and pump power sums,
+        // block-reduced in a fixed order
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            acc_s += __shfl_down_sync(0xffffffffu, acc_s, o);
+            acc_p += __shfl_down_sync(0xffffffffu, acc_p, o);
+        }
+        if ((tid & 31) == 0) {
+            red[2 * (tid >> 5)] = acc_s;
+            red[2 * (tid >> 5) + 1] = acc_p;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double a = 0.0, b = 0.0;
+            for (int w = 0; w < NT / 32; ++w) {
+                a += red[2 * w];
+                b += red[2 * w + 1];
+            }
+            double* part = reinterpret_cast<double*>(wbase + L.off_part);
+            part[2 * blockIdx.x] = a;
+            part[2 * blockIdx.x + 1] = b;
+        }
+    }
     if (mode != 2) {
         n1_pass(false);
         __syncthreads();
@@ -236,28 +262,6 @@ __global__ void __launch_bounds__(MpCfg<T, N>::RNT)
             gP[g] = Ps[sidx<N, R2, SW>(lr, x)];
             gS[g] = Ss[sidx<N, R2, SW>(lr, x)];
         }
-        return;
-    }
-    // last step: this CTA's share of the SH and pump power sums, block-reduced in a fixed order
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        acc_s += __shfl_down_sync(0xffffffffu, acc_s, o);
-        acc_p += __shfl_down_sync(0xffffffffu, acc_p, o);
-    }
-    if ((tid & 31) == 0) {
-        red[2 * (tid >> 5)] = acc_s;
-        red[2 * (tid >> 5) + 1] = acc_p;
-    }
-    __syncthreads();
-    if (tid == 0) {
-        double a = 0.0, b = 0.0;
-        for (int w = 0; w < NT / 32; ++w) {
-            a += red[2 * w];
-            b += red[2 * w + 1];
-        }
-        double* part = reinterpret_cast<double*>(wbase + L.off_part);
-        part[2 * blockIdx.x] = a;
-        part[2 * blockIdx.x + 1] = b;
     }
 }
 

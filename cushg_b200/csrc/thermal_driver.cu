@@ -122,7 +122,36 @@ shg_status thermal_run(const shg_params& p, const void* signal_in, void* pump_ou
         for (int g = 0; g < max_outer && rc == SHG_OK; ++g) {
             double red = 1.0, aux = -1.0;
             int64_t counter = 0;
-            while (red >= tol) {
+            if (p.conv_rule == SHG_CONV_FIXED) {
+                // exactly max_sweeps sweeps; the last one reports max |Tf - Ti|
+                if ((e = run_sweeps<R>(cur, nxt, Ta, maps, Q, k, p.boundary, depth, max_sweeps - 1, tb_err, s)) !=
+                        cudaSuccess ||
+                    (e = launch_jacobi<R>(cur, nxt, Q, k, p.boundary, true, SHG_CONV_MAXABS, partial, resid, s)) !=
+                        cudaSuccess) {
+                    rc = cuda_fail(e, "jacobi sweep");
+                    break;
+                }
+                std::swap(cur, nxt);
+                double h[2] = {0.0, 0.0};
+                if ((e = cudaMemcpyAsync(h, resid, sizeof(h), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+                    (e = cudaStreamSynchronize(s)) != cudaSuccess) {
+                    rc = cuda_fail(e, "jacobi residual");
+                    break;
+                }
+                unsigned staged_err = 0;
+                std::memcpy(&staged_err, &h[1], sizeof(staged_err));
+                if (staged_err) {
+                    rc = fail(SHG_ERR_CUDA, "blocked Jacobi sweep: a staged plane did not arrive");
+                    break;
+                }
+                red = h[0];
+                counter = max_sweeps;
+                if (!std::isfinite(red)) {
+                    rc = fail(SHG_ERR_NONFINITE, "Jacobi residual is %g after %lld sweeps", red, (long long)counter);
+                    break;
+                }
+            }
+            while (p.conv_rule != SHG_CONV_FIXED && red >= tol) {
                 if (counter >= max_sweeps) {
                     rc = fail(SHG_ERR_NOT_CONVERGED, "Jacobi: %lld sweeps without reaching %g (last %g)",
                               (long long)counter, tol, red);
@@ -148,6 +177,10 @@ shg_status thermal_run(const shg_params& p, const void* signal_in, void* pump_ou
                 }
                 if (counter > 0) aux = red;
                 red = p.conv_rule == SHG_CONV_MAXABS ? h[0] : (double)(R)(std::sqrt((R)h[0]) / (R)(double)nt);
+                if (!std::isfinite(red)) {
+                    rc = fail(SHG_ERR_NONFINITE, "Jacobi residual is %g after %lld sweeps", red, (long long)counter);
+                    break;
+                }
                 if (red == aux) red = 0.5 * tol;
                 ++counter;
                 if (red < tol) break;
@@ -200,7 +233,7 @@ shg_status thermal_run(const shg_params& p, const void* signal_in, void* pump_ou
             }
             if ((e = run_variant(v, ddesc, &d, 1, nullptr, s)) != cudaSuccess) { rc = cuda_fail(e, "thermal optical pass"); break; }
             ++outer;
-            if (counter == 1 && g != 0) break;  // Solver.h:367
+            if (p.conv_rule != SHG_CONV_FIXED && counter == 1 && g != 0) break;  // Solver.h:367
         }
         if (rc != SHG_OK) break;
         if (temperature_out &&
@@ -226,6 +259,8 @@ shg_status thermal_run(const shg_params& p, const void* signal_in, void* pump_ou
             stats->steps = nz;
             stats->last_residual = last;
             stats->device_ms = ms;
+            if (!std::isfinite(h[0]) || !std::isfinite(h[1]))
+                rc = fail(SHG_ERR_NONFINITE, "SH / pump power %g / %g", h[0], h[1]);
         }
     } while (0);
     cudaFreeAsync(buf, s);

@@ -21,11 +21,13 @@ SHG_ERR_CUDA = 3
 SHG_ERR_NOMEM = 4
 SHG_ERR_NOT_CONVERGED = 5
 SHG_ERR_NO_DEVICE = 6
+SHG_ERR_NONFINITE = 7
 
 SHG_BOUNDARY_TOP_OPEN = 0
 SHG_BOUNDARY_OVEN_SURROUNDED = 1
 SHG_CONV_REFERENCE = 0
 SHG_CONV_MAXABS = 1
+SHG_CONV_FIXED = 2
 SHG_MARCH_AUTO = 0
 SHG_MARCH_FUSED = 1
 SHG_MARCH_MULTIPASS = 2

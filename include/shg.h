@@ -49,7 +49,9 @@ typedef enum shg_status {
     SHG_ERR_CUDA = 3,          /* a CUDA runtime call failed; see shg_last_error() */
     SHG_ERR_NOMEM = 4,         /* device or host allocation failed */
     SHG_ERR_NOT_CONVERGED = 5, /* Jacobi hit max_sweeps before its tolerance */
-    SHG_ERR_NO_DEVICE = 6      /* no CUDA device is visible */
+    SHG_ERR_NO_DEVICE = 6,     /* no CUDA device is visible */
+    SHG_ERR_NONFINITE = 7      /* the run produced NaN or Inf (SH power or Jacobi residual):
+                                  parameters outside the range the discretisation resolves */
 } shg_status;
 
 /* Heat-equation boundary models (src/headers/Tfield.h). */
@@ -64,7 +66,11 @@ enum {
 enum {
     SHG_CONV_REFERENCE = 0, /* sqrt(sum (Tf-Ti)^2)/TSIZE < tol, checked every check_every
                                sweeps, stagnation exit (Solver.h:332-351) */
-    SHG_CONV_MAXABS = 1     /* max |Tf-Ti| < tol, checked every check_every sweeps */
+    SHG_CONV_MAXABS = 1,    /* max |Tf-Ti| < tol, checked every check_every sweeps */
+    SHG_CONV_FIXED = 2      /* exactly max_sweeps sweeps per outer iteration and exactly
+                               max_outer iterations, no convergence test (a fixed cost per
+                               optical-thermal update); last_residual = max |Tf-Ti| of the
+                               last sweep */
 };
 
 /* Crystals (Sellmeier equations). */

@@ -86,3 +86,10 @@ def test_march_selector_is_validated():
     p64 = P.config_plain_64()
     assert shg.check_params(p64.replace(march=P.SHG_MARCH_MULTIPASS)) == P.SHG_ERR_UNSUPPORTED
     assert shg.check_params(p64.replace(march=P.SHG_MARCH_FUSED)) == P.SHG_OK
+
+
+def test_fixed_sweep_rule_needs_counts():
+    p = P.config_thermal_128().replace(conv_rule=P.SHG_CONV_FIXED, max_sweeps=0)
+    assert shg.check_params(p) == P.SHG_ERR_INVALID
+    assert shg.check_params(p.replace(max_sweeps=10, max_outer=2)) == P.SHG_OK
+    assert shg.check_params(p.replace(conv_rule=3)) == P.SHG_ERR_INVALID

@@ -58,6 +58,8 @@ def test_multipass_thermal_equals_fused(precision):
     assert np.max(np.abs(a.temperature - b.temperature)) <= tol_t
     tol = 1e-10 if precision == 64 else 1e-4
     assert rel_l2(b.signal, a.signal) <= tol and rel_l2(b.pump, a.pump) <= tol
+    assert a.sh_power > 0 and abs(b.sh_power - a.sh_power) <= tol * a.sh_power
+    assert abs(b.stats.pump_power - a.stats.pump_power) <= tol * a.stats.pump_power
 
 
 def test_multipass_512_fp64_matches_oracle():

@@ -120,3 +120,20 @@ def test_device_entry_point_on_torch_stream():
     assert np.array_equal(sig.cpu().numpy(), r.signal)
     assert st.sh_power == r.sh_power
     assert st.device_ms > 0
+
+
+def test_nonfinite_result_is_reported():
+    """A pump power far outside what FP32 resolves overflows the fields: the call returns
+    SHG_ERR_NONFINITE instead of a NaN power, alone and in a batch (naming the instance)."""
+    import torch
+
+    bad = P.config_plain_64().replace(nz=12, power=1e20, precision=32)
+    with pytest.raises(shg.ShgError) as e:
+        shg.solve(bad)
+    assert e.value.status == P.SHG_ERR_NONFINITE
+    good = P.config_plain_64().replace(nz=12, precision=32)
+    ps = [good, bad]
+    outs = [torch.empty((p.ny, p.nx), dtype=torch.complex64, device="cuda") for p in ps]
+    with pytest.raises(shg.ShgError) as e:
+        shg.solve_batch_device(ps, outs, [torch.empty_like(t) for t in outs])
+    assert e.value.status == P.SHG_ERR_NONFINITE and "instance 1" in str(e.value)

@@ -148,3 +148,30 @@ def test_heat_sweeps_match_oracle(precision, boundary):
         assert np.array_equal(outs[blk], outs[1]), blk
     tol = 1e-12 if precision == 64 else 2e-6
     assert np.max(np.abs(outs[1] - Ti)) / np.max(np.abs(Ti)) < tol
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [64, 32])
+def test_fixed_sweep_rule_runs_exact_counts(precision):
+    """conv_rule FIXED: exactly max_sweeps sweeps per outer iteration and max_outer iterations.
+    With one outer iteration the temperature is the initial field (oven on the y = 0 face,
+    the phase-matching temperature elsewhere) after max_sweeps sweeps with Q = 0, which is what
+    shg_heat_sweeps_device gives from that field."""
+    import torch
+
+    p = P.workload(32, 12, 4000.0, 20.0, 25.0, 2000.0, 30.0, precision=precision, thermal=1)
+    p.t_peltier = 35.0
+    p.conv_rule = P.SHG_CONV_FIXED
+    p.max_sweeps = 37
+    p.max_outer = 1
+    r = shg.solve(p, want_temperature=True)
+    assert r.stats.jacobi_sweeps == 37 and r.stats.outer_iterations == 1
+    rdt = np.float64 if precision == 64 else np.float32
+    T0 = np.full((p.nz, p.ny, p.nx), p.temp, dtype=rdt)
+    T0[:, 0, :] = p.t_peltier
+    t_d = torch.from_numpy(T0).to("cuda")
+    shg.heat_sweeps_device(p, t_d, torch.zeros_like(t_d), 37)
+    torch.cuda.synchronize()
+    assert np.max(np.abs(t_d.cpu().numpy() - r.temperature)) <= (1e-12 if precision == 64 else 1e-5)
+    r2 = shg.solve(p.replace(max_outer=3), want_temperature=True)
+    assert r2.stats.jacobi_sweeps == 3 * 37 and r2.stats.outer_iterations == 3

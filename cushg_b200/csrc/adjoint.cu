@@ -98,6 +98,8 @@ shg_status grad_batch(const shg_params* ps, int count, const double* const* poli
         shg_status st = shg_check_params(&ps[i]);
         if (st != SHG_OK) return count > 1 ? fail(st, "instance %d: %s", i, shg_last_error()) : st;
         if (ps[i].thermal) return fail(SHG_ERR_UNSUPPORTED, "gradients are for plain runs (thermal == 0)");
+        if (ps[i].waist_y > 0 && ps[i].waist_y != ps[i].waist)
+            return fail(SHG_ERR_UNSUPPORTED, "gradients are for round beams (waist_y == 0)");
         if (ps[i].precision != ps[0].precision || ps[i].nx != ps[0].nx)
             return fail(SHG_ERR_INVALID, "instance %d: a gradient batch shares one precision and grid side", i);
     }

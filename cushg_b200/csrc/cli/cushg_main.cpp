@@ -1,7 +1,7 @@
 // cushg_main.cpp — command-line drop-in for the reference program (src/cuSHG.cu:27-113).
 //
 //   cushg <power W> <waist um> <oven temperature C> <save_only_last 0|1> <save_temperature 0|1>
-//         [--nx N] [--nz NZ] [--lx um] [--ly um] [--lz um] [--focus um] [--t-inf C]
+//         [--nx N] [--nz NZ] [--lx um] [--ly um] [--lz um] [--focus um] [--waist-y um] [--t-inf C]
 //         [--deff um/V] [--period um] [--alpha-p 1/um] [--alpha-s 1/um] [--beta-s um/W]
 //         [--rho-p rad] [--rho-s rad] [--kappa W/(um K)] [--h-conv W/(um^2 K)] [--lambda um]
 //         [--thermal] [--precision 32|64] [--boundary top-open|oven-surrounded]
@@ -125,6 +125,7 @@ int main(int argc, char** argv) {
         else if (a == "--ly") val(p.ly);
         else if (a == "--lz") val(p.lz);
         else if (a == "--focus") { val(p.focus); focus_given = true; }
+        else if (a == "--waist-y") val(p.waist_y);
         else if (a == "--t-inf") val(p.t_inf);
         else if (a == "--deff") val(p.deff);
         else if (a == "--period") val(p.period);

@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <complex>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -94,6 +95,23 @@ InstDesc make_plain_desc(const shg_params& p, double Tc, double T_dk) {
     d.amp_im = (-Ap0 * mim) / den;
     d.den_re = wX2 * mre;
     d.den_im = wX2 * mim;
+    if (p.waist_y > 0 && p.waist_y != p.waist) {
+        // elliptical beam (the commented-out variant of setPump, Efields.h:113-115):
+        // (Ap0 / (sqrt(MX) sqrt(MY))) exp(-ax^2 / (wX2 MX) - ay^2 / (wY2 MY)), Ap0 normalised
+        // with wX wY
+        const double wY2 = p.waist_y * p.waist_y;
+        const double zRY = kPi * np * wY2 / lp;
+        const double etaY = p.focus / zRY;
+        const double A = std::sqrt(4 * p.power / (kEps0 * kC * kPi * np * p.waist * p.waist_y));
+        const std::complex<double> m = std::sqrt(std::complex<double>(1.0, -etaX)) *
+                                       std::sqrt(std::complex<double>(1.0, -etaY));
+        const std::complex<double> a = A / m;
+        d.elliptic = 1;
+        d.amp_re = a.real();
+        d.amp_im = a.imag();
+        d.deny_re = wY2;
+        d.deny_im = wY2 * -etaY;
+    }
     d.ux = 0.5 * p.nx;
     d.uy = 0.5 * p.ny;
     d.dx = dx;
@@ -153,12 +171,14 @@ void shg_default_params(shg_params* p) {
     p->max_sweeps = 0;
     p->jacobi_block = 0;
     p->march = SHG_MARCH_AUTO;
+    p->reserved1 = 0;
+    p->waist_y = 0.0;
 }
 
 static bool finite_all(const shg_params* p) {
     const double v[] = {p->lx, p->ly, p->lz, p->lambda_p, p->deff, p->period, p->alpha_p, p->alpha_s, p->beta_s,
                         p->rho_p, p->rho_s, p->kappa, p->h_conv, p->power, p->waist, p->focus, p->temp, p->t_inf,
-                        p->t_peltier, p->jacobi_tol};
+                        p->t_peltier, p->jacobi_tol, p->waist_y};
     for (double x : v)
         if (!std::isfinite(x)) return false;
     return true;
@@ -175,6 +195,7 @@ static shg_status check_params_impl(const shg_params* p, bool need_kernel) {
     if (!(p->lx > 0 && p->ly > 0 && p->lz > 0)) return fail(SHG_ERR_INVALID, "lx, ly, lz must be > 0");
     if (!(p->lambda_p > 0.3 && p->lambda_p < 6.0)) return fail(SHG_ERR_INVALID, "lambda_p out of range");
     if (!(p->waist > 0) || p->power < 0 || !(p->period > 0)) return fail(SHG_ERR_INVALID, "waist/power/period");
+    if (p->waist_y < 0) return fail(SHG_ERR_INVALID, "waist_y must be >= 0 (0: round beam)");
     if (p->alpha_p < 0 || p->alpha_s < 0 || p->beta_s < 0) return fail(SHG_ERR_INVALID, "negative absorption");
     if (p->crystal != SHG_CRYSTAL_MGO_SPPLT) return fail(SHG_ERR_UNSUPPORTED, "unknown crystal %d", p->crystal);
     if (p->thermal) {

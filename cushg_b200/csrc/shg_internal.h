@@ -22,6 +22,9 @@ struct InstDesc {
     // pump at z = 0: P = amp * exp(-(ax^2 + ay^2) / den), ax = (x - ux) dx
     double amp_re, amp_im, den_re, den_im;
     double ux, uy, dx, dy;
+    int32_t elliptic;      // 1: elliptical pump, P = amp * exp(-ax^2 / den - ay^2 / deny)
+    int32_t pad0;
+    double deny_re, deny_im;
     // propagator phase θ = -dz (a (dfx^2 sx^2 + dfy^2 sy^2) + b sx) per field,
     // sx, sy the signed FFT frequency indices
     double a_p, b_p, a_s, b_s, dfx, dfy;

@@ -150,10 +150,22 @@ __device__ __forceinline__ void init_tables(const InstDesc& d, mult<T>* tw, mult
 }
 
 // Focused Gaussian pump at grid point (x, y), setPump (Efields.h:84-119):
-// (Ap0 / MX) exp(-(((x - uX) dx)^2 + ((y - uY) dy)^2) / (wX2 MX)), in FP64.
+// (Ap0 / MX) exp(-(((x - uX) dx)^2 + ((y - uY) dy)^2) / (wX2 MX)), in FP64; with d.elliptic
+// the separable variant amp * exp(-ax^2 / (wX2 MX) - ay^2 / (wY2 MY)) (Efields.h:113-115).
 __device__ __forceinline__ double2 pump_value(const InstDesc& d, int x, int y, double amp_re, double amp_im,
                                               double den_re, double den_im) {
     const double ax = ((double)x - d.ux) * d.dx, ay = ((double)y - d.uy) * d.dy;
+    if (d.elliptic) {
+        const double dx2 = den_re * den_re + den_im * den_im;
+        const double dy2 = d.deny_re * d.deny_re + d.deny_im * d.deny_im;
+        const double are = -(ax * ax) * den_re / dx2 - (ay * ay) * d.deny_re / dy2;
+        const double aim = (ax * ax) * den_im / dx2 + (ay * ay) * d.deny_im / dy2;
+        const double ex = exp(are);
+        double sn, cs;
+        sincos(aim, &sn, &cs);
+        const double er = ex * cs, ei = ex * sn;
+        return make_double2(amp_re * er - amp_im * ei, amp_re * ei + amp_im * er);
+    }
     const double num = -(ax * ax) - (ay * ay);
     const double dd = den_re * den_re + den_im * den_im;
     const double are = (num * den_re) / dd, aim = (-num * den_im) / dd;

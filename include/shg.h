@@ -117,6 +117,13 @@ typedef struct shg_params {
      * one is built for the grid side (planes in shared memory, sides <= 256) and the
      * multi-pass march otherwise (planes in global memory, side 512). */
     int32_t march;
+    int32_t reserved1;      /* zero */
+    /* Beam waist radius in y [µm].  <= 0 (default): a round beam of radius `waist`, setPump
+     * as the reference runs it (Efields.h:94, waistY = waistX).  Otherwise the elliptical beam
+     * of the reference's commented-out variant (Efields.h:113-115), with its own Rayleigh
+     * length and focusing term in y, and Ap0 normalised with waist * waist_y so that the beam
+     * carries `power` (the commented code keeps waist^2, which would not). */
+    double waist_y;
 } shg_params;
 
 enum {

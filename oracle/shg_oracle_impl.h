@@ -30,6 +30,12 @@ static inline CPX SFX(rdivc)(R a, CPX b) {
 }
 /* e^{i a}: Operators.h:146-151 */
 static inline CPX SFX(cexpi)(R a) { return SFX(cmk)(COS(a), SIN(a)); }
+/* principal square root: sqrt((|z| + re) / 2) + i sign(im) sqrt((|z| - re) / 2) */
+static inline CPX SFX(csqrt)(CPX a) {
+    R m = SQRT(a.re * a.re + a.im * a.im);
+    R r = SQRT((m + a.re) / (R)2), i = SQRT((m - a.re) / (R)2);
+    return SFX(cmk)(r, a.im < 0 ? -i : i);
+}
 /* e^{a.re + i a.im}: Operators.h:155-161 */
 static inline CPX SFX(cexpc)(CPX a) {
     R e = EXP(a.re);
@@ -55,6 +61,7 @@ typedef struct {
     R deff, dQ, Lambda, alpha_p, alpha_s, beta_s, rho_p, rho_s;
     R kappa, hconv;
     R power, waist, focus, temp, t_inf, t_peltier;
+    R waist_y; /* <= 0 or == waist: round beam */
 } SFX(cfg);
 
 /* Grid steps dx = LX/(NX-1) etc., Crystal.h:34-36; dQ = 2 deff/π, Crystal.h:41. */
@@ -73,6 +80,7 @@ static void SFX(make_cfg)(const shg_params* p, SFX(cfg)* c) {
     c->rho_p = (R)p->rho_p; c->rho_s = (R)p->rho_s;
     c->kappa = (R)p->kappa; c->hconv = (R)p->h_conv;
     c->power = (R)p->power; c->waist = (R)p->waist; c->focus = (R)p->focus;
+    c->waist_y = (R)p->waist_y;
     c->temp = (R)p->temp; c->t_inf = (R)p->t_inf; c->t_peltier = (R)p->t_peltier;
 }
 
@@ -175,6 +183,24 @@ static void SFX(set_pump)(const SFX(cfg)* c, R Tc, CPX* pump) {
     CPX MX = SFX(cmk)((R)1, -etaX);
     CPX amp = SFX(rdivc)(Ap0, MX);
     CPX den = SFX(cscale)(MX, wX2);
+    if (c->waist_y > 0 && c->waist_y != c->waist) {
+        /* the elliptical variant (Efields.h:113-115, commented out in the reference):
+         * (A / (sqrt(MX) sqrt(MY))) exp(-ax^2 / (wX2 MX) - ay^2 / (wY2 MY)), A normalised with
+         * waist * waist_y so that the beam carries the pump power */
+        R wY2 = c->waist_y * c->waist_y;
+        R etaY = c->focus / (PI * np * wY2 / c->lp);
+        R A = SQRT((R)4 * c->power / (SFX(K_EPS0) * SFX(K_C) * PI * np * c->waist * c->waist_y));
+        CPX MY = SFX(cmk)((R)1, -etaY);
+        CPX ampe = SFX(rdivc)(A, SFX(cmul)(SFX(csqrt)(MX), SFX(csqrt)(MY)));
+        CPX deny = SFX(cscale)(MY, wY2);
+        for (int y = 0; y < c->ny; ++y)
+            for (int x = 0; x < c->nx; ++x) {
+                R ax = ((R)x - uX) * c->dx, ay = ((R)y - uY) * c->dy;
+                CPX arg = SFX(cadd)(SFX(rdivc)(-(ax * ax), den), SFX(rdivc)(-(ay * ay), deny));
+                pump[(size_t)y * c->nx + x] = SFX(cmul)(ampe, SFX(cexpc)(arg));
+            }
+        return;
+    }
     for (int y = 0; y < c->ny; ++y)
         for (int x = 0; x < c->nx; ++x) {
             R ax = ((R)x - uX) * c->dx, ay = ((R)y - uY) * c->dy;

@@ -137,3 +137,20 @@ def test_nonfinite_result_is_reported():
     with pytest.raises(shg.ShgError) as e:
         shg.solve_batch_device(ps, outs, [torch.empty_like(t) for t in outs])
     assert e.value.status == P.SHG_ERR_NONFINITE and "instance 1" in str(e.value)
+
+
+@pytest.mark.parametrize("n", [64, 256, 512])
+def test_elliptical_beam_matches_oracle(n):
+    """The elliptical pump (waist_y != waist) through the fused (64, 256) and multi-pass (512)
+    marches against the oracle; waist_y == waist is the round beam bit for bit."""
+    p = P.workload(n, 9, 6000.0, 15.0, 25.0, 2500.0, 31.0, precision=64).replace(waist_y=40.0)
+    p.lx = p.ly = 12 * 40.0
+    r = shg.solve(p)
+    rc, pump, sig, st, _ = O.solve(p)
+    assert rc == 0
+    assert rel_l2(r.pump, pump) <= 1e-10 and rel_l2(r.signal, sig) <= 1e-10
+    assert abs(r.sh_power - st.sh_power) <= 1e-12 * st.sh_power
+    round0 = shg.solve(p.replace(waist_y=0.0))
+    same = shg.solve(p.replace(waist_y=p.waist))
+    assert np.array_equal(round0.signal, same.signal) and np.array_equal(round0.pump, same.pump)
+    assert abs(round0.sh_power - r.sh_power) > 1e-3 * r.sh_power  # the ellipticity matters

@@ -70,3 +70,16 @@ def test_reference_fp32_error_vs_fp64():
     z64, _ = load("plain64_c1")
     e = rel_l2(z32["signal"], z64["signal"])
     assert 1e-6 < e < 1e-1
+
+
+@pytest.mark.parametrize("waist_y", [0.0, 45.0, 20.0])
+def test_initial_pump_carries_the_pump_power(waist_y):
+    """setPump's normalisation (Efields.h:99): the z = 0 pump carries the pump power, for the
+    round beam and for the elliptical variant (normalised with waist * waist_y)."""
+    p = P.workload(128, 12, 8000.0, 10.0, 30.0, 2000.0, 30.0, precision=64).replace(waist_y=waist_y)
+    p.lx = p.ly = 12 * max(p.waist, waist_y)
+    pump = O.set_pump(p, p.temp).reshape(p.ny, p.nx)
+    n = P.sellmeier(p.lambda_p, p.temp)
+    dx, dy = p.lx / (p.nx - 1), p.ly / (p.ny - 1)
+    power = 0.5 * P.EPS0 * P.C_UM_PS * n * float(np.sum(np.abs(pump) ** 2)) * dx * dy
+    assert abs(power - p.power) <= 1e-9 * p.power

@@ -15,6 +15,15 @@
 // NX tab-separated values at 20 significant digits (src/headers/Files.h:69-90); Tfinal_<z>.dat
 // per z plane for thermal runs with save_temperature = 1 (Files.h:169-188); and the elapsed
 // time appended to GPUTime_NZ_<NZ>_N_<NX>_T.txt (src/cuSHG.cu:90-107).
+//
+//   cushg --sweep <powers> <waists> <oven temperatures> <save_only_last> <save_temperature> [options]
+//
+// is the sweep script src/cuSHG.sh:43-105: the three comma-separated lists play ARG1, ARG2
+// and ARG3, every combination is a run, and each run's files go into the script's folder
+// sPPLT_P_<power>_W_T1_<temperature>_WAIST_<waist>/ with its report in <folder>/<folder>.txt.
+// Plain runs that keep only the last slice go through one batched call (shg_solve_batch);
+// the others run one after another.
+#include <sys/stat.h>
 #include <sys/time.h>
 
 #include <cstdio>
@@ -23,6 +32,7 @@
 #include <fstream>
 #include <iomanip>
 #include <iostream>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -60,12 +70,25 @@ void save_tensor(const R* t, int nx, int ny, int nz, const std::string& name) {
 
 int usage() {
     std::cerr << "usage: cushg <power W> <waist um> <oven temperature C> <save_only_last 0|1> "
-                 "<save_temperature 0|1> [options]\n";
+                 "<save_temperature 0|1> [options]\n"
+                 "       cushg --sweep <powers> <waists> <oven temperatures> <save_only_last 0|1> "
+                 "<save_temperature 0|1> [options]   (comma-separated lists)\n";
     return 2;
 }
 
+// The run's report line (the stdout of the reference's run).
+std::string report(const shg_params& p, const shg_stats& st) {
+    std::ostringstream o;
+    o << "SH power = " << std::setprecision(12) << st.sh_power << " W, pump power = " << st.pump_power
+      << " W, steps = " << st.steps;
+    if (p.thermal) o << ", Jacobi sweeps = " << st.jacobi_sweeps << ", outer iterations = " << st.outer_iterations;
+    o << ", device time = " << st.device_ms << " ms";
+    return o.str();
+}
+
+// One run; its files go to directory prefix `dir` ("" or "<folder>/").
 template <typename R>
-int run(const shg_params& p, bool save_only_last, bool save_temperature) {
+int run(const shg_params& p, bool save_only_last, bool save_temperature, const std::string& dir, std::string* line) {
     const size_t plane = (size_t)p.nx * p.ny;
     const size_t planes = save_only_last ? 1 : (size_t)p.nz;
     std::vector<R> pump(2 * plane * planes), sig(2 * plane * planes);
@@ -79,37 +102,24 @@ int run(const shg_params& p, bool save_only_last, bool save_temperature) {
         return 1;
     }
     if (save_only_last) {
-        save_complex(pump.data(), p.nx, p.ny, "Pump_out");
-        save_complex(sig.data(), p.nx, p.ny, "Signal_out");
+        save_complex(pump.data(), p.nx, p.ny, dir + "Pump_out");
+        save_complex(sig.data(), p.nx, p.ny, dir + "Signal_out");
     } else {
         for (int s = 0; s < p.nz; ++s) {
-            save_complex(pump.data() + 2 * plane * s, p.nx, p.ny, "Pump_" + std::to_string(s));
-            save_complex(sig.data() + 2 * plane * s, p.nx, p.ny, "Signal_" + std::to_string(s));
+            save_complex(pump.data() + 2 * plane * s, p.nx, p.ny, dir + "Pump_" + std::to_string(s));
+            save_complex(sig.data() + 2 * plane * s, p.nx, p.ny, dir + "Signal_" + std::to_string(s));
         }
     }
-    if (!T.empty()) save_tensor(T.data(), p.nx, p.ny, p.nz, "Tfinal");
-    std::cout << "SH power = " << std::setprecision(12) << st.sh_power << " W, pump power = " << st.pump_power
-              << " W, steps = " << st.steps;
-    if (p.thermal) std::cout << ", Jacobi sweeps = " << st.jacobi_sweeps << ", outer iterations = " << st.outer_iterations;
-    std::cout << ", device time = " << st.device_ms << " ms" << std::endl;
+    if (!T.empty()) save_tensor(T.data(), p.nx, p.ny, p.nz, dir + "Tfinal");
+    *line = report(p, st);
     return 0;
 }
 
-}  // namespace
-
-int main(int argc, char** argv) {
-    if (argc < 6) return usage();
-    shg_params p;
-    shg_default_params(&p);
-    // positional argv of src/cuSHG.cu:46-58
-    p.power = std::atof(argv[1]);
-    p.waist = std::atof(argv[2]);
-    p.temp = std::atof(argv[3]);
-    p.t_peltier = std::atof(argv[3]);
-    const bool save_only_last = std::atoi(argv[4]) != 0;
-    const bool save_temperature = std::atoi(argv[5]) != 0;
+// Options after the positional arguments: the reference's compile-time constants
+// (src/cuSHG.cu:11-13, src/headers/Crystal.h:19-52).  Returns 0 or the usage status.
+int parse_options(int argc, char** argv, int first, shg_params& p) {
     bool focus_given = false;
-    for (int i = 6; i < argc; ++i) {
+    for (int i = first; i < argc; ++i) {
         const std::string a = argv[i];
         auto val = [&](double& dst) {
             if (i + 1 >= argc) { usage(); std::exit(2); }
@@ -156,16 +166,128 @@ int main(int argc, char** argv) {
         }
     }
     if (!focus_given) p.focus = 0.5 * p.lz;  // src/cuSHG.cu:48
+    return 0;
+}
+
+std::vector<std::string> split(const std::string& s) {
+    std::vector<std::string> out;
+    std::stringstream ss(s);
+    std::string item;
+    while (std::getline(ss, item, ','))
+        if (!item.empty()) out.push_back(item);
+    return out;
+}
+
+void time_record(const shg_params& p, double el) {
+    std::ofstream tf("GPUTime_NZ_" + std::to_string(p.nz) + "_N_" + std::to_string(p.nx) + "_T.txt", std::ios::app);
+    if (tf.is_open()) tf << el << std::endl;
+}
+
+// The sweep of src/cuSHG.sh:58-105: every (power, waist, temperature) combination, in the
+// script's loop order, each run's files in its folder.
+int sweep(int argc, char** argv) {
+    if (argc < 7) return usage();
+    const std::vector<std::string> powers = split(argv[2]), waists = split(argv[3]), temps = split(argv[4]);
+    const bool save_only_last = std::atoi(argv[5]) != 0;
+    const bool save_temperature = std::atoi(argv[6]) != 0;
+    shg_params base;
+    shg_default_params(&base);
+    if (int rc = parse_options(argc, argv, 7, base)) return rc;
+    struct Point { shg_params p; std::string folder; };
+    std::vector<Point> pts;
+    for (const auto& P : powers)
+        for (const auto& W : waists)
+            for (const auto& T : temps) {
+                shg_params q = base;
+                q.power = std::atof(P.c_str());
+                q.waist = std::atof(W.c_str());
+                q.temp = q.t_peltier = std::atof(T.c_str());
+                pts.push_back({q, "sPPLT_P_" + P + "_W_T1_" + T + "_WAIST_" + W});  // cuSHG.sh:81
+            }
+    const double t0 = seconds();
+    std::vector<std::string> lines(pts.size());
+    if (save_only_last && !base.thermal) {
+        // one batched call for the whole sweep
+        const size_t n = pts.size();
+        const size_t plane = 2 * (size_t)base.nx * base.ny;
+        const bool f32 = base.precision == 32;
+        std::vector<double> pd(f32 ? 0 : 2 * n * plane);
+        std::vector<float> pf(f32 ? 2 * n * plane : 0);
+        std::vector<shg_params> ps(n);
+        std::vector<void*> pp(n), sp(n);
+        for (size_t i = 0; i < n; ++i) {
+            ps[i] = pts[i].p;
+            pp[i] = f32 ? (void*)(pf.data() + 2 * i * plane) : (void*)(pd.data() + 2 * i * plane);
+            sp[i] = f32 ? (void*)(pf.data() + (2 * i + 1) * plane) : (void*)(pd.data() + (2 * i + 1) * plane);
+        }
+        std::vector<double> power(n);
+        shg_status rc = shg_solve_batch(ps.data(), (int32_t)n, pp.data(), sp.data(), power.data());
+        if (rc != SHG_OK) {
+            std::cerr << "cushg: " << shg_status_string(rc) << ": " << shg_last_error() << std::endl;
+            return 1;
+        }
+        for (size_t i = 0; i < n; ++i) {
+            mkdir(pts[i].folder.c_str(), 0755);
+            const std::string dir = pts[i].folder + "/";
+            if (f32) {
+                save_complex((const float*)pp[i], base.nx, base.ny, dir + "Pump_out");
+                save_complex((const float*)sp[i], base.nx, base.ny, dir + "Signal_out");
+            } else {
+                save_complex((const double*)pp[i], base.nx, base.ny, dir + "Pump_out");
+                save_complex((const double*)sp[i], base.nx, base.ny, dir + "Signal_out");
+            }
+            std::ostringstream o;
+            o << "SH power = " << std::setprecision(12) << power[i] << " W (batched sweep of " << n << " runs)";
+            lines[i] = o.str();
+        }
+    } else {
+        for (size_t i = 0; i < pts.size(); ++i) {
+            mkdir(pts[i].folder.c_str(), 0755);
+            const int rc = base.precision == 32
+                               ? run<float>(pts[i].p, save_only_last, save_temperature, pts[i].folder + "/", &lines[i])
+                               : run<double>(pts[i].p, save_only_last, save_temperature, pts[i].folder + "/", &lines[i]);
+            if (rc) return rc;
+        }
+    }
+    const double el = seconds() - t0;
+    for (size_t i = 0; i < pts.size(); ++i) {
+        const Point& pt = pts[i];
+        std::ofstream f(pt.folder + "/" + pt.folder + ".txt");
+        f << "Power = " << pt.p.power << " W, beam waist = " << pt.p.waist << " um, oven temperature = " << pt.p.temp
+          << " C\n" << lines[i] << "\n";
+        std::cout << pt.folder << ": " << lines[i] << std::endl;
+    }
+    std::cout << "time elapsed " << el << " seconds for " << pts.size() << " runs" << std::endl;
+    time_record(base, el);
+    return 0;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    if (argc >= 2 && std::string(argv[1]) == "--sweep") return sweep(argc, argv);
+    if (argc < 6) return usage();
+    shg_params p;
+    shg_default_params(&p);
+    // positional argv of src/cuSHG.cu:46-58
+    p.power = std::atof(argv[1]);
+    p.waist = std::atof(argv[2]);
+    p.temp = std::atof(argv[3]);
+    p.t_peltier = std::atof(argv[3]);
+    const bool save_only_last = std::atoi(argv[4]) != 0;
+    const bool save_temperature = std::atoi(argv[5]) != 0;
+    if (int rc = parse_options(argc, argv, 6, p)) return rc;
     std::cout << "Pump power = " << p.power << " W, beam waist = " << p.waist << " um, focal distance = " << p.focus
               << " um, oven temperature = " << p.temp << " C, grid = " << p.nx << " x " << p.ny << " x " << p.nz
               << (p.thermal ? ", thermal" : "") << std::endl;
     const double t0 = seconds();
-    const int rc = p.precision == 32 ? run<float>(p, save_only_last, save_temperature)
-                                     : run<double>(p, save_only_last, save_temperature);
+    std::string line;
+    const int rc = p.precision == 32 ? run<float>(p, save_only_last, save_temperature, "", &line)
+                                     : run<double>(p, save_only_last, save_temperature, "", &line);
     if (rc != 0) return rc;
+    std::cout << line << std::endl;
     const double el = seconds() - t0;
     std::cout << "time elapsed " << el << " seconds" << std::endl;
-    std::ofstream tf("GPUTime_NZ_" + std::to_string(p.nz) + "_N_" + std::to_string(p.nx) + "_T.txt", std::ios::app);
-    if (tf.is_open()) tf << el << std::endl;
+    time_record(p, el);
     return 0;
 }

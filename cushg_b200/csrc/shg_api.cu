@@ -371,6 +371,62 @@ shg_status shg_heat_sweeps_device(const shg_params* p, void* temperature_dev, co
     return heat_sweeps_device(q, temperature_dev, q_dev, sweeps, (cudaStream_t)stream);
 }
 
+shg_status shg_solve_batch(const shg_params* params, int32_t count, void* const* pump_out, void* const* signal_out,
+                           double* sh_power_out) {
+    clear_error();
+    if (!params || count < 0) return fail(SHG_ERR_INVALID, "params is NULL or count < 0");
+    for (int i = 0; i < count; ++i) {
+        shg_status st = shg_check_params(&params[i]);
+        if (st != SHG_OK) return fail(st, "instance %d: %s", i, g_last_error.c_str());
+        if (params[i].thermal) return fail(SHG_ERR_UNSUPPORTED, "instance %d: batched runs are plain (thermal == 0)", i);
+        if (params[i].precision != params[0].precision)
+            return fail(SHG_ERR_INVALID, "instance %d: all instances must share one precision", i);
+    }
+    if (count == 0) return SHG_OK;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(SHG_ERR_NO_DEVICE, "no CUDA device visible");
+    }
+    std::vector<size_t> off(2 * (size_t)count + 1, 0);
+    for (int i = 0; i < count; ++i) {
+        const size_t plane = (size_t)params[i].nx * params[i].ny * complex_bytes(params[i]);
+        off[2 * i + 1] = off[2 * i] + ((pump_out && pump_out[i]) ? plane : 0);
+        off[2 * i + 2] = off[2 * i + 1] + ((signal_out && signal_out[i]) ? plane : 0);
+    }
+    cudaStream_t s = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
+    char* buf = nullptr;
+    shg_status rc = SHG_OK;
+    do {
+        if (off.back() && (e = cudaMallocAsync((void**)&buf, off.back(), s)) != cudaSuccess) {
+            rc = cuda_fail(e, "cudaMallocAsync");
+            break;
+        }
+        std::vector<void*> dp(count, nullptr), ds(count, nullptr);
+        for (int i = 0; i < count; ++i) {
+            if (off[2 * i + 1] > off[2 * i]) dp[i] = buf + off[2 * i];
+            if (off[2 * i + 2] > off[2 * i + 1]) ds[i] = buf + off[2 * i + 1];
+        }
+        if ((rc = plain_solve_batch(params, count, dp.data(), ds.data(), sh_power_out, s)) != SHG_OK) break;
+        for (int i = 0; i < count && rc == SHG_OK; ++i) {
+            if (dp[i] && (e = cudaMemcpyAsync(pump_out[i], dp[i], off[2 * i + 1] - off[2 * i], cudaMemcpyDeviceToHost, s)) !=
+                             cudaSuccess)
+                rc = cuda_fail(e, "cudaMemcpyAsync D2H");
+            if (ds[i] &&
+                (e = cudaMemcpyAsync(signal_out[i], ds[i], off[2 * i + 2] - off[2 * i + 1], cudaMemcpyDeviceToHost, s)) !=
+                    cudaSuccess)
+                rc = cuda_fail(e, "cudaMemcpyAsync D2H");
+        }
+        if (rc == SHG_OK && (e = cudaStreamSynchronize(s)) != cudaSuccess) rc = cuda_fail(e, "cudaStreamSynchronize");
+    } while (0);
+    if (buf) cudaFreeAsync(buf, s);
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+    return rc;
+}
+
 shg_status shg_solve_batch_device(const shg_params* params, int32_t count, void* const* pump_out_dev,
                                   void* const* signal_out_dev, double* sh_power_out, void* stream_) {
     clear_error();

@@ -26,7 +26,7 @@ EXPORTS = (
     "shg_default_params", "shg_check_params", "shg_steps", "shg_solve", "shg_solve_slices", "shg_solve_device",
     "shg_solve_batch_device", "shg_solve_batch_device_noalloc", "shg_grad", "shg_sh_power", "shg_last_error",
     "shg_status_string", "shg_version", "shg_heat_sweeps_device", "shg_batch_plan_create", "shg_batch_plan_launch",
-    "shg_batch_plan_powers", "shg_batch_plan_destroy", "shg_autotune", "shg_grad_batch",
+    "shg_batch_plan_powers", "shg_batch_plan_destroy", "shg_autotune", "shg_grad_batch", "shg_solve_batch",
 )
 
 
@@ -82,6 +82,9 @@ def lib() -> ctypes.CDLL:
         L.shg_solve_batch_device.argtypes = [P, ctypes.c_int32, ctypes.POINTER(vp), ctypes.POINTER(vp),
                                              ctypes.POINTER(ctypes.c_double), vp]
         L.shg_solve_batch_device.restype = ctypes.c_int
+        L.shg_solve_batch.argtypes = [P, ctypes.c_int32, ctypes.POINTER(vp), ctypes.POINTER(vp),
+                                      ctypes.POINTER(ctypes.c_double)]
+        L.shg_solve_batch.restype = ctypes.c_int
         L.shg_solve_batch_device_noalloc.argtypes = L.shg_solve_batch_device.argtypes
         L.shg_solve_batch_device_noalloc.restype = ctypes.c_int
         L.shg_grad.argtypes = [P, ctypes.POINTER(ctypes.c_double), ctypes.c_int32, ctypes.POINTER(ShgGradResult)]
@@ -214,6 +217,21 @@ def heat_sweeps_device(p: ShgParams, temperature, q, sweeps: int, stream=None) -
     s = None if stream is None else ctypes.c_void_p(stream)
     _check(lib().shg_heat_sweeps_device(ctypes.byref(p), ctypes.c_void_p(temperature.data_ptr()),
                                         ctypes.c_void_p(q.data_ptr()), int(sweeps), s))
+
+
+def solve_batch(ps: list[ShgParams]) -> tuple[list[np.ndarray], list[np.ndarray], np.ndarray]:
+    """Batch of plain instances with host buffers (shg_solve_batch): returns the pump and SH
+    fields (numpy arrays) and the SH powers."""
+    n = len(ps)
+    arr = (ShgParams * n)(*ps)
+    vp = ctypes.c_void_p
+    pumps = [np.empty((p.ny, p.nx), dtype=p.complex_dtype) for p in ps]
+    sigs = [np.empty((p.ny, p.nx), dtype=p.complex_dtype) for p in ps]
+    power = np.zeros(n, dtype=np.float64)
+    _check(lib().shg_solve_batch(arr, n, (vp * n)(*[vp(a.ctypes.data) for a in pumps]),
+                                 (vp * n)(*[vp(a.ctypes.data) for a in sigs]),
+                                 power.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+    return pumps, sigs, power
 
 
 def _dptr(a):

@@ -196,6 +196,14 @@ SHG_API shg_status shg_solve_batch_device(const shg_params* params, int32_t coun
                                   double* sh_power_out, void* stream);
 
 /*
+ * shg_solve_batch_device with host buffers: pump_out[i] / signal_out[i] are host arrays of
+ * nx_i*ny_i complex (or NULL entries), sh_power_out a host array of `count` doubles or NULL.
+ * Synchronous.  The sweep of src/cuSHG.sh:58-94 as one call.
+ */
+SHG_API shg_status shg_solve_batch(const shg_params* params, int32_t count, void* const* pump_out,
+                                   void* const* signal_out, double* sh_power_out);
+
+/*
  * Batch plans: the batched march of shg_solve_batch_device captured once into a CUDA graph,
  * with its descriptors, work-queue counters and power slots allocated at creation, then
  * replayed by shg_batch_plan_launch with one graph launch (no host work per replay).  For

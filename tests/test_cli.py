@@ -97,3 +97,25 @@ def test_cli_every_slice_files(tmp_path):
     for s in range(p.nz):
         sig = read_matrix(tmp_path / f"Signal_{s}_r.dat") + 1j * read_matrix(tmp_path / f"Signal_{s}_i.dat")
         assert np.allclose(sig, sig_s[s], rtol=0, atol=1e-18 + 1e-15 * np.abs(sig_s[s]).max())
+
+
+@pytest.mark.gpu
+def test_cli_sweep_mode_writes_the_script_folders(tmp_path):
+    """cushg --sweep replaces src/cuSHG.sh: every (power, waist, temperature) combination runs
+    (one batched call), and each run's Pump_out / Signal_out files land in the script's
+    sPPLT_P_<P>_W_T1_<T>_WAIST_<W> folder, equal to the single run of that point."""
+    base = P.workload(64, 12, 6000.0, 10.0, 25.0, 3000.0, 30.0, precision=64)
+    extra = cli_args(base)[6:]  # every option, as for a single run
+    r = subprocess.run([CLI, "--sweep", "10,20", "25", "30,35.5", "1", "0"] + extra, cwd=tmp_path,
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    for pw in ("10", "20"):
+        for t in ("30", "35.5"):
+            folder = tmp_path / f"sPPLT_P_{pw}_W_T1_{t}_WAIST_25"
+            assert (folder / f"{folder.name}.txt").exists()
+            p = base.replace(power=float(pw), temp=float(t), t_peltier=float(t))
+            ref = shg.solve(p)
+            got = read_matrix(folder / "Signal_out_r.dat") + 1j * read_matrix(folder / "Signal_out_i.dat")
+            assert np.array_equal(got, ref.signal), (pw, t)
+            gotp = read_matrix(folder / "Pump_out_r.dat") + 1j * read_matrix(folder / "Pump_out_i.dat")
+            assert np.array_equal(gotp, ref.pump), (pw, t)

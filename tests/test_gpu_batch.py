@@ -117,3 +117,15 @@ def test_autotune_rejects_unbuilt_class():
     with pytest.raises(shg.ShgError) as e:
         shg.autotune(32, 100)
     assert e.value.status == P.SHG_ERR_UNSUPPORTED
+
+
+def test_host_buffer_batch_equals_device_batch():
+    import torch
+    ps = sweep(64, 9, seed=21)
+    pumps, sigs, power = shg.solve_batch(ps)
+    dp, ds = device_outputs(ps)
+    pw = shg.solve_batch_device(ps, dp, ds)
+    torch.cuda.synchronize()
+    assert np.array_equal(power, pw)
+    for i in range(len(ps)):
+        assert np.array_equal(sigs[i], ds[i].cpu().numpy()) and np.array_equal(pumps[i], dp[i].cpu().numpy())

@@ -42,6 +42,8 @@ FP32_LANES_PER_SM = 128
 # bench (`--steps 2 --warmup 3 --no-cpu-baseline --no-autotune`, metrics dram__bytes_read.sum
 # and dram__bytes_write.sum); the fields stay on chip, so this is descriptors and outputs
 SWEEP_256_DRAM_BYTES_PER_LAUNCH = 14.30e6
+# bytes of one instance descriptor the batch call uploads (shg::InstDesc)
+INST_DESC_BYTES = 376
 
 
 def flops_per_point_step(n: int) -> float:
@@ -190,24 +192,22 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     times = [a.elapsed_time(b) for a, b in evs]
     ms = sum(times) / len(times)
 
-    # end to end through the public API: parameter sets in (host), SH powers and both
-    # output fields back into pinned host memory, every step
+    # end to end through the C ABI with host buffers (shg_solve_batch): parameter sets in,
+    # SH powers and both output fields back into pinned host memory every step, each
+    # grid-size class's fields copied as soon as its march ends
     host_p = [torch.empty((p.ny, p.nx), dtype=cdt, pin_memory=True) for p in ps]
     host_s = [torch.empty((p.ny, p.nx), dtype=cdt, pin_memory=True) for p in ps]
+    shg.solve_batch(ps, host_p, host_s)  # untimed: the call's own set-up
     e2e_t = []
-    for k in range(max(2, args.steps // 2)):
+    for k in range(max(3, args.steps // 2)):
         flush.fill_(k & 0xFF)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        powers = shg.solve_batch_device(ps, pumps, sigs, stream=sptr, want_power=True)
-        for i in range(len(ps)):
-            host_p[i].copy_(pumps[i], non_blocking=True)
-            host_s[i].copy_(sigs[i], non_blocking=True)
-        torch.cuda.synchronize()
+        shg.solve_batch(ps, host_p, host_s)
         e2e_t.append(time.perf_counter() - t0)
     e2e_ms = 1e3 * statistics.median(e2e_t)
-    d2h = sum(2 * p.nx * p.ny * (8 if args.precision == 32 else 16) for p in ps) + 8 * len(ps)
-    h2d = len(ps) * 256  # instance descriptors
+    d2h = sum(2 * p.nx * p.ny * (8 if args.precision == 32 else 16) for p in ps) + 16 * len(ps)
+    h2d = len(ps) * INST_DESC_BYTES
 
     # the dominant kernel alone: the largest grid-size class as one launch on this stream,
     # timed with CUDA events (the sweep runs the classes concurrently on forked streams)

@@ -160,7 +160,7 @@ shg_status grad_batch(const shg_params* ps, int count, const double* const* poli
     shg_status rc = SHG_OK;
     cudaEvent_t t0 = nullptr, t1 = nullptr;
     do {
-        if ((e = cudaMallocAsync((void**)&buf, total, s)) != cudaSuccess) { rc = cuda_fail(e, "cudaMallocAsync"); break; }
+        if ((e = dev_alloc((void**)&buf, total, s)) != cudaSuccess) { rc = cuda_fail(e, "cudaMallocAsync"); break; }
         std::vector<InstDesc> hd(count);
         std::vector<AdjDesc> ha(count);
         char* q = buf + b_desc + b_adesc;

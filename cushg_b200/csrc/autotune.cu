@@ -63,7 +63,7 @@ extern "C" shg_status shg_autotune(int32_t precision, int32_t n, shg_tune_result
     shg_status rc = SHG_OK;
     double rate[16] = {0};
     do {
-        if ((e = cudaMallocAsync(&buf, sizeof(InstDesc) * (size_t)count + 256, s)) != cudaSuccess) {
+        if ((e = dev_alloc((void**)&buf, sizeof(InstDesc) * (size_t)count + 256, s)) != cudaSuccess) {
             rc = cuda_fail(e, "cudaMallocAsync");
             break;
         }

@@ -72,7 +72,7 @@ shg_status plain_solve_device(const shg_params& p, const void* signal_in, void* 
     cudaError_t e;
     void* buf = nullptr;
     const size_t bytes = sizeof(InstDesc) + 2 * sizeof(double);
-    if ((e = cudaMallocAsync(&buf, bytes, stream)) != cudaSuccess) return cuda_fail(e, "cudaMallocAsync");
+    if ((e = dev_alloc((void**)&buf, bytes, stream)) != cudaSuccess) return cuda_fail(e, "cudaMallocAsync");
     InstDesc* dd = reinterpret_cast<InstDesc*>(buf);
     double* pw = reinterpret_cast<double*>(reinterpret_cast<char*>(buf) + sizeof(InstDesc));
     d.power_out = pw;
@@ -164,17 +164,44 @@ static BatchLayout batch_layout(const shg_params* params, int count, void* const
     return L;
 }
 
+// Device-to-host copies of a group's output fields (host arrays indexed by batch slot),
+// enqueued on the stream that ran the group so that they overlap the other groups' marches.
+struct HostOutputs {
+    void* const* pump;
+    void* const* signal;
+};
+
+static cudaError_t copy_group_outputs(const BatchLayout& L, const BatchLayout::Group& G, const HostOutputs* ho,
+                                      size_t cbytes, cudaStream_t s) {
+    if (!ho) return cudaSuccess;
+    cudaError_t e = cudaSuccess;
+    for (int k = G.begin; k < G.end && e == cudaSuccess; ++k) {
+        const InstDesc& d = L.descs[k];
+        const size_t bytes = (size_t)d.n * d.n * cbytes;
+        if (ho->pump && ho->pump[d.slot] && d.pump_out)
+            e = cudaMemcpyAsync(ho->pump[d.slot], d.pump_out, bytes, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess && ho->signal && ho->signal[d.slot] && d.signal_out)
+            e = cudaMemcpyAsync(ho->signal[d.slot], d.signal_out, bytes, cudaMemcpyDeviceToHost, s);
+    }
+    return e;
+}
+
 // Enqueue the batched march on `stream`: zero the groups' work-queue counters, then one
 // persistent launch per group, the groups on the fork streams `fs` (joined back into
-// `stream`) when there are several.  Capturable into a CUDA graph.
+// `stream`) when there are several, each followed on its stream by the copies of its outputs
+// to the host when `ho` is given.  Capturable into a CUDA graph (without host copies).
 static cudaError_t enqueue_batch(const BatchLayout& L, const InstDesc* dd, int* queues, cudaStream_t stream,
-                                 cudaStream_t* fs, cudaEvent_t* ev, int nfork) {
+                                 cudaStream_t* fs, cudaEvent_t* ev, int nfork, const HostOutputs* ho = nullptr,
+                                 size_t cbytes = 0) {
     cudaError_t e;
     const int ng = (int)L.groups.size();
     if ((e = cudaMemsetAsync(queues, 0, sizeof(int) * (size_t)ng, stream)) != cudaSuccess) return e;
-    if (ng == 1)
-        return run_variant(L.groups[0].v, dd + L.groups[0].begin, L.descs.data() + L.groups[0].begin,
-                           L.groups[0].end - L.groups[0].begin, queues, stream);
+    if (ng == 1) {
+        if ((e = run_variant(L.groups[0].v, dd + L.groups[0].begin, L.descs.data() + L.groups[0].begin,
+                             L.groups[0].end - L.groups[0].begin, queues, stream)) != cudaSuccess)
+            return e;
+        return copy_group_outputs(L, L.groups[0], ho, cbytes, stream);
+    }
     const int nf = std::min(ng, nfork);
     if ((e = cudaEventRecord(ev[nfork], stream)) != cudaSuccess) return e;
     for (int g = 0; g < nf; ++g)
@@ -182,7 +209,8 @@ static cudaError_t enqueue_batch(const BatchLayout& L, const InstDesc* dd, int* 
     for (int g = 0; g < ng; ++g) {
         const BatchLayout::Group& G = L.groups[g];
         if ((e = run_variant(G.v, dd + G.begin, L.descs.data() + G.begin, G.end - G.begin, queues + g, fs[g % nf])) !=
-            cudaSuccess)
+                cudaSuccess ||
+            (e = copy_group_outputs(L, G, ho, cbytes, fs[g % nf])) != cudaSuccess)
             return e;
     }
     for (int g = 0; g < nf; ++g) {
@@ -197,11 +225,12 @@ static size_t batch_bytes(int count) {
 }
 
 shg_status plain_solve_batch(const shg_params* params, int count, void* const* pump_out, void* const* signal_out,
-                             double* sh_power_out, cudaStream_t stream) {
+                             double* sh_power_out, cudaStream_t stream, void* const* pump_host,
+                             void* const* signal_host) {
     if (count == 0) return SHG_OK;
     cudaError_t e;
     void* buf = nullptr;
-    if ((e = cudaMallocAsync(&buf, batch_bytes(count), stream)) != cudaSuccess) return cuda_fail(e, "cudaMallocAsync");
+    if ((e = dev_alloc((void**)&buf, batch_bytes(count), stream)) != cudaSuccess) return cuda_fail(e, "cudaMallocAsync");
     InstDesc* dd = reinterpret_cast<InstDesc*>(buf);
     double* pw = reinterpret_cast<double*>(dd + count);
     int* queues = reinterpret_cast<int*>(pw + 2 * (size_t)count);
@@ -218,7 +247,10 @@ shg_status plain_solve_batch(const shg_params* params, int count, void* const* p
         cudaGetDevice(&dev);
         ForkStreams* f = nullptr;
         if ((e = fork_streams(dev, &f)) != cudaSuccess) { rc = cuda_fail(e, "stream pool"); break; }
-        if ((e = enqueue_batch(L, dd, queues, stream, f->s, f->ev, ForkStreams::kMax)) != cudaSuccess) {
+        const HostOutputs ho = {pump_host, signal_host};
+        const bool copies = pump_host || signal_host;
+        if ((e = enqueue_batch(L, dd, queues, stream, f->s, f->ev, ForkStreams::kMax, copies ? &ho : nullptr,
+                               complex_bytes(params[0]))) != cudaSuccess) {
             rc = cuda_fail(e, "launch ssfm_plain_kernel");
             break;
         }

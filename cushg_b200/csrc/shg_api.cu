@@ -13,6 +13,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -41,6 +42,36 @@ shg_status cuda_fail(cudaError_t e, const char* what) {
 }
 
 void clear_error() { g_last_error.clear(); }
+
+cudaError_t dev_alloc(void** ptr, size_t bytes, cudaStream_t s) {
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if ((e = cudaStreamIsCapturing(s, &cap)) != cudaSuccess) return e;
+    // inside a stream capture the allocation becomes a graph memory node
+    if (dev < 0 || dev >= 64 || cap != cudaStreamCaptureStatusNone) return cudaMallocAsync(ptr, bytes, s);
+    cudaMemPool_t pool;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (!pools[dev]) {
+            cudaMemPoolProps props = {};
+            props.allocType = cudaMemAllocationTypePinned;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = dev;
+            if ((e = cudaMemPoolCreate(&pools[dev], &props)) != cudaSuccess) {
+                pools[dev] = nullptr;
+                return e;
+            }
+            unsigned long long keep = kPoolKeepBytes;
+            cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        pool = pools[dev];
+    }
+    return cudaMallocFromPoolAsync(ptr, bytes, pool, s);
+}
 
 // Physical constants, src/headers/Crystal.h:19-21 (µm, ps, W, V).
 const double kPi = 3.14159265358979323846;
@@ -272,10 +303,10 @@ static shg_status solve_host(const shg_params* p, const void* signal_in, void* p
     void *din = nullptr, *dp = nullptr, *ds = nullptr, *dT = nullptr;
     shg_status rc = SHG_OK;
     do {
-        if (signal_in && (e = cudaMallocAsync(&din, plane, s)) != cudaSuccess) { rc = cuda_fail(e, "cudaMallocAsync"); break; }
-        if (pump_out && (e = cudaMallocAsync(&dp, outb, s)) != cudaSuccess) { rc = cuda_fail(e, "cudaMallocAsync"); break; }
-        if (signal_out && (e = cudaMallocAsync(&ds, outb, s)) != cudaSuccess) { rc = cuda_fail(e, "cudaMallocAsync"); break; }
-        if (temperature_out && p->thermal && (e = cudaMallocAsync(&dT, tbytes, s)) != cudaSuccess) {
+        if (signal_in && (e = dev_alloc((void**)&din, plane, s)) != cudaSuccess) { rc = cuda_fail(e, "cudaMallocAsync"); break; }
+        if (pump_out && (e = dev_alloc((void**)&dp, outb, s)) != cudaSuccess) { rc = cuda_fail(e, "cudaMallocAsync"); break; }
+        if (signal_out && (e = dev_alloc((void**)&ds, outb, s)) != cudaSuccess) { rc = cuda_fail(e, "cudaMallocAsync"); break; }
+        if (temperature_out && p->thermal && (e = dev_alloc((void**)&dT, tbytes, s)) != cudaSuccess) {
             rc = cuda_fail(e, "cudaMallocAsync");
             break;
         }
@@ -341,7 +372,7 @@ shg_status shg_sh_power(const shg_params* p, const double* poling, double* sh_po
     shg_status rc = SHG_OK;
     do {
         if (poling) {
-            if ((e = cudaMallocAsync((void**)&dpol, sizeof(double) * nsteps, s)) != cudaSuccess ||
+            if ((e = dev_alloc((void**)&dpol, sizeof(double) * nsteps, s)) != cudaSuccess ||
                 (e = cudaMemcpyAsync(dpol, poling, sizeof(double) * nsteps, cudaMemcpyHostToDevice, s)) != cudaSuccess) {
                 rc = cuda_fail(e, "poling upload");
                 break;
@@ -400,7 +431,7 @@ shg_status shg_solve_batch(const shg_params* params, int32_t count, void* const*
     char* buf = nullptr;
     shg_status rc = SHG_OK;
     do {
-        if (off.back() && (e = cudaMallocAsync((void**)&buf, off.back(), s)) != cudaSuccess) {
+        if (off.back() && (e = dev_alloc((void**)&buf, off.back(), s)) != cudaSuccess) {
             rc = cuda_fail(e, "cudaMallocAsync");
             break;
         }
@@ -409,17 +440,11 @@ shg_status shg_solve_batch(const shg_params* params, int32_t count, void* const*
             if (off[2 * i + 1] > off[2 * i]) dp[i] = buf + off[2 * i];
             if (off[2 * i + 2] > off[2 * i + 1]) ds[i] = buf + off[2 * i + 1];
         }
-        if ((rc = plain_solve_batch(params, count, dp.data(), ds.data(), sh_power_out, s)) != SHG_OK) break;
-        for (int i = 0; i < count && rc == SHG_OK; ++i) {
-            if (dp[i] && (e = cudaMemcpyAsync(pump_out[i], dp[i], off[2 * i + 1] - off[2 * i], cudaMemcpyDeviceToHost, s)) !=
-                             cudaSuccess)
-                rc = cuda_fail(e, "cudaMemcpyAsync D2H");
-            if (ds[i] &&
-                (e = cudaMemcpyAsync(signal_out[i], ds[i], off[2 * i + 2] - off[2 * i + 1], cudaMemcpyDeviceToHost, s)) !=
-                    cudaSuccess)
-                rc = cuda_fail(e, "cudaMemcpyAsync D2H");
-        }
-        if (rc == SHG_OK && (e = cudaStreamSynchronize(s)) != cudaSuccess) rc = cuda_fail(e, "cudaStreamSynchronize");
+        // each grid-size class's outputs are copied as soon as its march ends, overlapping the others
+        if ((rc = plain_solve_batch(params, count, dp.data(), ds.data(), sh_power_out, s, pump_out, signal_out)) !=
+            SHG_OK)
+            break;
+        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) rc = cuda_fail(e, "cudaStreamSynchronize");
     } while (0);
     if (buf) cudaFreeAsync(buf, s);
     cudaStreamSynchronize(s);

@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <mutex>
 
+#include "shg_host.h"
 #include "ssfm_multipass.cuh"
 #include "ssfm_variants.h"
 
@@ -34,7 +35,7 @@ cudaError_t mp_march(const InstDesc* dev_descs, const InstDesc* host_descs, int 
     int max_steps = 0;
     for (int i = 0; i < count; ++i) max_steps = std::max(max_steps, (int)host_descs[i].nsteps);
     MpLayout L = mp_layout<T, N>(nullptr, max_steps, THERM);
-    cudaError_t e = cudaMallocAsync((void**)&L.base, L.stride * (size_t)count, s);
+    cudaError_t e = dev_alloc((void**)&L.base, L.stride * (size_t)count, s);
     if (e != cudaSuccess) return e;
     const dim3 rgrid(Cfg::RPART, count), cgrid(N / Cfg::CW, 2, count);
     mp_setup_kernel<T, N><<<count, 256, 0, s>>>(dev_descs, L);

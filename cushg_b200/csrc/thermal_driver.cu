@@ -84,7 +84,7 @@ shg_status thermal_run(const shg_params& p, const void* signal_in, void* pump_ou
     const size_t bytes = 6 * arr + sizeof(double) * (npart + 4) + sizeof(InstDesc) + 256;
     cudaError_t e;
     char* buf = nullptr;
-    if ((e = cudaMallocAsync((void**)&buf, bytes, s)) != cudaSuccess) return cuda_fail(e, "cudaMallocAsync");
+    if ((e = dev_alloc((void**)&buf, bytes, s)) != cudaSuccess) return cuda_fail(e, "cudaMallocAsync");
     R* Ta = reinterpret_cast<R*>(buf);
     R* Tb = Ta + nt;
     R* Q = Tb + nt;
@@ -278,7 +278,7 @@ shg_status heat_run(const shg_params& p, R* T, const R* Q, int64_t sweeps, cudaS
     const int depth = sweep_depth(p);
     cudaError_t e;
     char* buf = nullptr;
-    if ((e = cudaMallocAsync((void**)&buf, arr + 256, s)) != cudaSuccess) return cuda_fail(e, "cudaMallocAsync");
+    if ((e = dev_alloc((void**)&buf, arr + 256, s)) != cudaSuccess) return cuda_fail(e, "cudaMallocAsync");
     R* other = reinterpret_cast<R*>(buf);
     unsigned* tb_err = reinterpret_cast<unsigned*>(buf + arr);
     shg_status rc = SHG_OK;

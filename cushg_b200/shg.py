@@ -219,17 +219,25 @@ def heat_sweeps_device(p: ShgParams, temperature, q, sweeps: int, stream=None) -
                                         ctypes.c_void_p(q.data_ptr()), int(sweeps), s))
 
 
-def solve_batch(ps: list[ShgParams]) -> tuple[list[np.ndarray], list[np.ndarray], np.ndarray]:
-    """Batch of plain instances with host buffers (shg_solve_batch): returns the pump and SH
-    fields (numpy arrays) and the SH powers."""
+def _host_ptr(a):
+    """Address of a host array: a numpy array or a (pinned) CPU torch tensor."""
+    return a.data_ptr() if hasattr(a, "data_ptr") else a.ctypes.data
+
+
+def solve_batch(ps: list[ShgParams], pumps=None, sigs=None):
+    """Batch of plain instances with host buffers (shg_solve_batch).  pumps / sigs: host arrays
+    to fill (numpy arrays or pinned torch tensors, one per instance) or None to allocate numpy
+    arrays.  Returns (pumps, sigs, SH powers)."""
     n = len(ps)
     arr = (ShgParams * n)(*ps)
     vp = ctypes.c_void_p
-    pumps = [np.empty((p.ny, p.nx), dtype=p.complex_dtype) for p in ps]
-    sigs = [np.empty((p.ny, p.nx), dtype=p.complex_dtype) for p in ps]
+    if pumps is None:
+        pumps = [np.empty((p.ny, p.nx), dtype=p.complex_dtype) for p in ps]
+    if sigs is None:
+        sigs = [np.empty((p.ny, p.nx), dtype=p.complex_dtype) for p in ps]
     power = np.zeros(n, dtype=np.float64)
-    _check(lib().shg_solve_batch(arr, n, (vp * n)(*[vp(a.ctypes.data) for a in pumps]),
-                                 (vp * n)(*[vp(a.ctypes.data) for a in sigs]),
+    _check(lib().shg_solve_batch(arr, n, (vp * n)(*[vp(_host_ptr(a)) for a in pumps]),
+                                 (vp * n)(*[vp(_host_ptr(a)) for a in sigs]),
                                  power.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
     return pumps, sigs, power
 

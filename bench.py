@@ -392,7 +392,7 @@ def run_thermal(args) -> dict:
     vox = p.nx * p.ny * p.nz
     out = {"metric": "thermal solve (Jacobi voxel-sweeps/s)",
            "workload": f"thermal {p.nx}x{p.ny}x{p.nz} FP{p.precision}", "status": status,
-           "jacobi_block": p.jacobi_block or 4, "wall_s": wall, "clocks": clk.summary()}
+           "jacobi_block": p.jacobi_block or "auto (1)", "wall_s": wall, "clocks": clk.summary()}
     if st is not None:
         out.update({"device_ms": st.device_ms, "jacobi_sweeps": st.jacobi_sweeps, "outer_iterations": st.outer_iterations,
                     "sh_power_w": st.sh_power, "value": vox * st.jacobi_sweeps / (st.device_ms * 1e-3),

@@ -343,8 +343,9 @@ __global__ void __launch_bounds__(NT, MINB)
                 for (int ph = 0; ph < 5; ++ph) {
                     if (ph == 2) {
                         // pointwise: the two RK4 applications around the step boundary (the second
-                        // half of step s, then the first half of step s+1)
-#pragma unroll 1
+                        // half of step s, then the first half of step s+1); two points interleaved
+                        // for instruction-level parallelism (about 1 % faster at 128-256)
+#pragma unroll 2
                         for (int k = 0; k < R2; ++k) {
                             const int x = n1 + 16 * k;
                             const int o = sidx<N, R2, SW>(lr, x);

@@ -19,11 +19,11 @@ namespace {
 struct AdjVariant {
     int precision, n, cluster, threads;
     size_t smem;
-    cudaError_t (*launch)(const InstDesc*, const AdjDesc*, int count, cudaStream_t);
+    cudaError_t (*launch)(const InstDesc*, const AdjDesc*, int count, int phase, int round, cudaStream_t);
 };
 
 template <typename T, int N, int C, int NT>
-cudaError_t launch_adjoint(const InstDesc* d, const AdjDesc* a, int count, cudaStream_t stream) {
+cudaError_t launch_adjoint(const InstDesc* d, const AdjDesc* a, int count, int phase, int round, cudaStream_t stream) {
     using Cfg = PlainCfg<T, N, C, NT, false>;
     auto kern = ssfm_adjoint_kernel<T, N, C, NT>;
     static std::once_flag once;
@@ -46,7 +46,7 @@ cudaError_t launch_adjoint(const InstDesc* d, const AdjDesc* a, int count, cudaS
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = C > 1 ? 1 : 0;
-    return cudaLaunchKernelEx(&cfg, kern, d, a);
+    return cudaLaunchKernelEx(&cfg, kern, d, a, phase, round);
 }
 
 #define SHG_ADJ(T, PREC, N, C, NT) {PREC, N, C, NT, PlainCfg<T, N, C, NT, false>::smem_bytes, &launch_adjoint<T, N, C, NT>}
@@ -142,10 +142,10 @@ shg_status grad_batch(const shg_params* ps, int count, const double* const* poli
         J.a.inv2h[2] = 1.0 / (2 * hT);
         size_t o = 0;
         J.off_ckpt = o; o += up((size_t)J.M * 2 * NN * cb);
-        J.off_seg = o;  o += 3 * up((size_t)J.K * 2 * NN * cb);
+        J.off_seg = o;  o += 3 * up((size_t)2 * J.K * 2 * NN * cb);  // two buffers each
         J.off_lam = o;  o += up(2 * NN * cb);
         J.off_z = o;    o += up(sizeof(double) * J.nsteps);
-        J.off_part = o; o += up(sizeof(double) * C * kAdjAcc);
+        J.off_part = o; o += up(sizeof(double) * (J.M + 1) * C * kAdjAcc);
         J.off_phi = o;  o += up(sizeof(double) * (size_t)J.nsteps * C);
         J.off_pol = o;  o += up(sizeof(double) * J.nsteps);
         J.bytes = o;
@@ -159,6 +159,8 @@ shg_status grad_batch(const shg_params* ps, int count, const double* const* poli
     char* buf = nullptr;
     shg_status rc = SHG_OK;
     cudaEvent_t t0 = nullptr, t1 = nullptr;
+    cudaStream_t s2 = nullptr;
+    std::vector<cudaEvent_t> evs;
     do {
         if ((e = dev_alloc((void**)&buf, total, s)) != cudaSuccess) { rc = cuda_fail(e, "cudaMallocAsync"); break; }
         std::vector<InstDesc> hd(count);
@@ -168,8 +170,8 @@ shg_status grad_batch(const shg_params* ps, int count, const double* const* poli
             GradJob& J = jobs[i];
             J.a.ckpt = q + J.off_ckpt;
             J.a.seg_a2 = q + J.off_seg;
-            J.a.seg_x = q + J.off_seg + up((size_t)J.K * 2 * NN * cb);
-            J.a.seg_y = q + J.off_seg + 2 * up((size_t)J.K * 2 * NN * cb);
+            J.a.seg_x = q + J.off_seg + up((size_t)2 * J.K * 2 * NN * cb);
+            J.a.seg_y = q + J.off_seg + 2 * up((size_t)2 * J.K * 2 * NN * cb);
             J.a.lam = q + J.off_lam;
             J.a.zs = reinterpret_cast<const double*>(q + J.off_z);
             J.a.part = reinterpret_cast<double*>(q + J.off_part);
@@ -198,10 +200,36 @@ shg_status grad_batch(const shg_params* ps, int count, const double* const* poli
             rc = cuda_fail(e, "cudaMemcpyAsync");
             break;
         }
+        // the forward launch, then per round r the adjoint march of segment M-1-r on `s`
+        // and, concurrently on `s2`, the re-march of segment M-2-r into the other buffer:
+        // a re-march waits for the adjoint march that last read its buffer (round r-1), an
+        // adjoint march for the re-march of its segment (round r-1)
+        int mmax = 0;
+        for (const GradJob& J : jobs) mmax = std::max(mmax, J.M);
+        evs.resize(2 * (size_t)mmax + 1);
+        for (auto& ev : evs)
+            if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) break;
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking);
+        if (e != cudaSuccess) { rc = cuda_fail(e, "adjoint streams"); break; }
+        cudaEvent_t* eB = evs.data();
+        cudaEvent_t* eR = evs.data() + mmax;
+        cudaEvent_t& eF = evs[2 * (size_t)mmax];
         cudaEventCreate(&t0);
         cudaEventCreate(&t1);
         cudaEventRecord(t0, s);
-        if ((e = v->launch(dd, da, count, s)) != cudaSuccess) { rc = cuda_fail(e, "launch ssfm_adjoint_kernel"); break; }
+        if ((e = v->launch(dd, da, count, kAdjForward, 0, s)) == cudaSuccess && (e = cudaEventRecord(eF, s)) == cudaSuccess)
+            e = cudaStreamWaitEvent(s2, eF, 0);
+        for (int r = 0; r < mmax && e == cudaSuccess; ++r) {
+            if (r + 1 < mmax) {
+                if (r >= 1 && (e = cudaStreamWaitEvent(s2, eB[r - 1], 0)) != cudaSuccess) break;
+                if ((e = v->launch(dd, da, count, kAdjRemarch, r, s2)) != cudaSuccess) break;
+                if ((e = cudaEventRecord(eR[r], s2)) != cudaSuccess) break;
+            }
+            if (r >= 1 && (e = cudaStreamWaitEvent(s, eR[r - 1], 0)) != cudaSuccess) break;
+            if ((e = v->launch(dd, da, count, kAdjBackward, r, s)) != cudaSuccess) break;
+            if ((e = cudaEventRecord(eB[r], s)) != cudaSuccess) break;
+        }
+        if (e != cudaSuccess) { rc = cuda_fail(e, "launch ssfm_adjoint_kernel"); break; }
         cudaEventRecord(t1, s);
         if ((e = cudaStreamSynchronize(s)) != cudaSuccess) { rc = cuda_fail(e, "adjoint march"); break; }
         float ms = 0.f;
@@ -209,7 +237,7 @@ shg_status grad_batch(const shg_params* ps, int count, const double* const* poli
         for (int i = 0; i < count && rc == SHG_OK; ++i) {
             const GradJob& J = jobs[i];
             const shg_params& p = ps[i];
-            std::vector<double> part((size_t)C * kAdjAcc), phi((size_t)J.nsteps * C);
+            std::vector<double> part((size_t)(J.M + 1) * C * kAdjAcc), phi((size_t)J.nsteps * C);
             if ((e = cudaMemcpy(part.data(), J.a.part, sizeof(double) * part.size(), cudaMemcpyDeviceToHost)) !=
                     cudaSuccess ||
                 (e = cudaMemcpy(phi.data(), J.a.phi, sizeof(double) * phi.size(), cudaMemcpyDeviceToHost)) != cudaSuccess) {
@@ -217,8 +245,9 @@ shg_status grad_batch(const shg_params* ps, int count, const double* const* poli
                 break;
             }
             double A[kAdjAcc] = {0};
-            for (int c = 0; c < C; ++c)
-                for (int k = 0; k < kAdjAcc; ++k) A[k] += part[(size_t)c * kAdjAcc + k];
+            for (int slot = 0; slot <= J.M; ++slot)
+                for (int c = 0; c < C; ++c)
+                    for (int k = 0; k < kAdjAcc; ++k) A[k] += part[((size_t)slot * C + c) * kAdjAcc + k];
             // temperature derivatives of the scalar constants (central differences in FP64)
             const double lp = p.lambda_p, ls = 0.5 * lp, T = p.temp, h = 1e-3;
             const double np = sellmeier(lp, T), ns = sellmeier(ls, T);
@@ -257,6 +286,12 @@ shg_status grad_batch(const shg_params* ps, int count, const double* const* poli
     if (t1) cudaEventDestroy(t1);
     if (buf) cudaFreeAsync(buf, s);
     cudaStreamSynchronize(s);
+    if (s2) {
+        cudaStreamSynchronize(s2);
+        cudaStreamDestroy(s2);
+    }
+    for (cudaEvent_t ev : evs)
+        if (ev) cudaEventDestroy(ev);
     cudaStreamDestroy(s);
     e = cudaGetLastError();
     if (rc == SHG_OK && e != cudaSuccess) rc = cuda_fail(e, "adjoint");

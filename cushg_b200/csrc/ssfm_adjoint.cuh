@@ -17,6 +17,9 @@
 //      propagated spectra of each step of the segment (the last segment's come from step 1
 //      directly); then march the adjoint back through the segment; the adjoint fields are
 //      parked in global memory between segments.
+// Each phase is a launch (kAdjForward, kAdjRemarch, kAdjBackward, one round of segments
+// per launch), the segment buffers are double-buffered by segment parity, so the host can
+// run the re-march of segment m-1 on other SMs while the adjoint march of segment m runs.
 // Parameter sensitivities are accumulated on the way: the stage coefficients' dependence
 // on κ, Δk, the two-photon term and the poling phase (RK4 adjoint), the propagator phases'
 // dependence on n(T) (adjoint diffraction, with the stored spectra), and the initial pump's
@@ -42,16 +45,21 @@ enum {
     kAdjAcc = 10
 };
 
+// launch phases of ssfm_adjoint_kernel
+enum { kAdjForward = 0, kAdjRemarch = 1, kAdjBackward = 2 };
+
 struct AdjDesc {
     int32_t K;          // checkpoint interval (steps)
     int32_t M;          // number of checkpoints (x_{mK}, m = 0..M-1)
     void* ckpt;         // M x 2 x n*n complex (pump, SH) before step mK, natural layout
-    void* seg_a2;       // K x 2 x n*n: fields after the diffraction of each step of a segment
-    void* seg_x;        // K x 2 x n*n: fields before each step of a segment
-    void* seg_y;        // K x 2 x n*n: propagated spectra of each step (CB order: fy*n + column)
+    void* seg_a2;       // 2 x K x 2 x n*n: fields after the diffraction of each step of a segment
+    void* seg_x;        // 2 x K x 2 x n*n: fields before each step of a segment
+    void* seg_y;        // 2 x K x 2 x n*n: propagated spectra of each step (CB order: fy*n + column)
+                        // (two buffers each, the one of segment m at parity m & 1)
     void* lam;          // 2 x n*n: adjoint fields between segments
     const double* zs;   // nsteps: z at the start of each step (the forward's accumulation)
-    double* part;       // [C][kAdjAcc] per-CTA accumulators
+    double* part;       // [M + 1][C][kAdjAcc] per-CTA accumulators: slot 0 the forward launch,
+                        // slot 1 + m the adjoint march of segment m
     double* phi;        // [nsteps][C] per-CTA dJ/dφ_s
     double pert[6][4];  // pump (amp_re, amp_im, den_re, den_im) at waist±hw, focus±hf, T±hT
     double inv2h[3];    // 1 / (2 h) of those differences
@@ -136,7 +144,8 @@ __device__ __forceinline__ void rk4_vjp(cx<T> p, cx<T> s, const cx<T>* cf, T hap
 
 template <typename T, int N, int C, int NT>
 __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __restrict__ descs,
-                                                             const AdjDesc* __restrict__ adescs) {
+                                                             const AdjDesc* __restrict__ adescs, int phase,
+                                                             int round) {
     using Cfg = PlainCfg<T, N, C, NT, false>;
     constexpr int R2 = Cfg::R2, SW = Cfg::SW;
     constexpr int JA = Cfg::JA, JB = Cfg::JB, JCA = Cfg::JCA, JCB = Cfg::JCB;
@@ -164,9 +173,16 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
     const int nsteps = d.nsteps;
     const int K = a.K;
     const T hap = (T)d.hap, has = (T)d.has, qs = (T)d.qs, dz6 = (T)(d.dz / 6.0);
+    // segment of this launch: round r runs the adjoint march of segment M-1-r and the
+    // re-march of segment M-2-r (the forward launch covers segment M-1); instances with
+    // fewer segments have nothing to do in the late rounds
+    const int m = phase == kAdjForward ? a.M - 1 : (phase == kAdjBackward ? a.M - 1 - round : a.M - 2 - round);
+    if (m < 0) return;
+    const size_t seg_stride = (size_t)K * 2 * NN;
+    const size_t seg_off = (size_t)(m & 1) * seg_stride;
     V* ckpt = reinterpret_cast<V*>(a.ckpt);
-    V* seg_a2 = reinterpret_cast<V*>(a.seg_a2);
-    V* seg_y = reinterpret_cast<V*>(a.seg_y);
+    V* seg_a2 = reinterpret_cast<V*>(a.seg_a2) + seg_off;
+    V* seg_y = reinterpret_cast<V*>(a.seg_y) + seg_off;
     V* lam = reinterpret_cast<V*>(a.lam);
 
     auto cluster_sync = [&]() {
@@ -180,7 +196,7 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
     // accumulators (kAcc*), kept as scalars so that nothing is indexed at run time
     double acc_kp = 0.0, acc_ks = 0.0, acc_dk = 0.0, acc_qs = 0.0, acc_pp = 0.0, acc_ps = 0.0;
     double acc_g0w = 0.0, acc_g0f = 0.0, acc_g0T = 0.0, acc_j = 0.0;
-    V* seg_x = reinterpret_cast<V*>(a.seg_x);
+    V* seg_x = reinterpret_cast<V*>(a.seg_x) + seg_off;
 
     // ---- plane transfers between shared memory and global (natural layout) ------------
     auto load_planes = [&](const V* gp, const V* gs) {
@@ -536,12 +552,11 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
 
     // ============================ the computation ======================================
     // One call site each for march and backward (keeps them inlined, with the accumulators
-    // in registers): the last segment's iteration runs the full forward march first.
+    // in registers).
     const int last_sb = (a.M - 1) * K;
-    for (int m = a.M - 1; m >= 0; --m) {
-        const int sb = m * K, se = min(sb + K, nsteps);
-        const bool first = (m == a.M - 1);
-        if (first) {
+    const int sb = m * K, se = min(sb + K, nsteps);
+    if (phase != kAdjBackward) {
+        if (phase == kAdjForward) {
             // x_0: the pump of setPump, SH = 0
             for (int e = tid; e < Cfg::PLANE; e += NT) {
                 const int lr = e / N, x = e % N;
@@ -550,37 +565,41 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
                 Ss[sidx<N, R2, SW>(lr, x)] = mk<T>((T)0, (T)0);
             }
         } else {
-            store_planes(lam, lam + NN);
-            __syncthreads();
             load_planes(ckpt + (size_t)m * 2 * NN, ckpt + ((size_t)m * 2 + 1) * NN);
         }
         __syncthreads();
-        // full march (keeping checkpoints and the last segment, ending in the adjoint seed),
-        // or the re-march of segment m
-        march(first ? 0 : sb, se, first, first ? last_sb : sb, first);
-        cluster_sync();
-        if (!first) {
-            load_planes(lam, lam + NN);
-            __syncthreads();
-        }
+        // the full march (keeping checkpoints and the last segment, ending in the adjoint
+        // seed), or the re-march of segment m
+        const bool fwd = phase == kAdjForward;
+        march(fwd ? 0 : sb, se, fwd, fwd ? last_sb : sb, fwd);
+        if (!fwd) return;
+        store_planes(lam, lam + NN);
+    } else {
+        load_planes(lam, lam + NN);
+        __syncthreads();
         backward(sb, se);
-    }
-    __syncthreads();
-    // dJ/dθ of the initial pump: Re <λ0_P, dP0/dθ>, dP0/dθ by central differences of the
-    // closed form (waist, focus, T)
-    for (int e = tid; e < Cfg::PLANE; e += NT) {
-        const int lr = e / N, x = e % N, y = crank + C * lr;
-        const V l0 = Ps[sidx<N, R2, SW>(lr, x)];
+        __syncthreads();
+        if (m > 0) {
+            store_planes(lam, lam + NN);
+        } else {
+            // dJ/dθ of the initial pump: Re <λ0_P, dP0/dθ>, dP0/dθ by central differences of
+            // the closed form (waist, focus, T)
+            for (int e = tid; e < Cfg::PLANE; e += NT) {
+                const int lr = e / N, x = e % N, y = crank + C * lr;
+                const V l0 = Ps[sidx<N, R2, SW>(lr, x)];
 #pragma unroll 1
-        for (int q = 0; q < 3; ++q) {
-            const double2 pp = pump_value(d, x, y, a.pert[2 * q][0], a.pert[2 * q][1], a.pert[2 * q][2], a.pert[2 * q][3]);
-            const double2 pm =
-                pump_value(d, x, y, a.pert[2 * q + 1][0], a.pert[2 * q + 1][1], a.pert[2 * q + 1][2], a.pert[2 * q + 1][3]);
-            const double dre = (pp.x - pm.x) * a.inv2h[q], dim = (pp.y - pm.y) * a.inv2h[q];
-            const double v = (double)l0.x * dre + (double)l0.y * dim;
-            if (q == 0) acc_g0w += v;
-            else if (q == 1) acc_g0f += v;
-            else acc_g0T += v;
+                for (int q = 0; q < 3; ++q) {
+                    const double2 pp =
+                        pump_value(d, x, y, a.pert[2 * q][0], a.pert[2 * q][1], a.pert[2 * q][2], a.pert[2 * q][3]);
+                    const double2 pm = pump_value(d, x, y, a.pert[2 * q + 1][0], a.pert[2 * q + 1][1],
+                                                  a.pert[2 * q + 1][2], a.pert[2 * q + 1][3]);
+                    const double dre = (pp.x - pm.x) * a.inv2h[q], dim = (pp.y - pm.y) * a.inv2h[q];
+                    const double v = (double)l0.x * dre + (double)l0.y * dim;
+                    if (q == 0) acc_g0w += v;
+                    else if (q == 1) acc_g0f += v;
+                    else acc_g0T += v;
+                }
+            }
         }
     }
     // per-CTA accumulators, block-reduced in a fixed order
@@ -595,7 +614,8 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
         if (tid == 0) {
             double t = 0.0;
             for (int w = 0; w < NT / 32; ++w) t += wred[w];
-            a.part[(size_t)crank * kAdjAcc + i] = t;
+            const size_t slot = phase == kAdjForward ? 0 : 1 + (size_t)m;
+            a.part[(slot * C + crank) * kAdjAcc + i] = t;
         }
         __syncthreads();
     }

@@ -407,7 +407,8 @@ def run_thermal_batch(args) -> dict:
     full thermal run through shg_solve_device with a fixed cost per optical-thermal update:
     `--thermal-fixed-sweeps` Jacobi sweeps (FP64 residual of the last one reported) in each of
     `--thermal-outer` outer iterations.  Jacobi to max|ΔT| < 1e-6 K at this size needs on the
-    order of 1e6 sweeps per outer iteration, beyond a bench budget."""
+    order of 1e6 sweeps per outer iteration, beyond a bench budget.  Each instance also gets
+    dJ/dT_oven through its temperature field (shg_thermal_grad), unless --no-thermal-grad."""
     import torch
     from cushg_b200 import shg
 
@@ -417,14 +418,21 @@ def run_thermal_batch(args) -> dict:
         for p in ps:
             p = p.replace(conv_rule=P.SHG_CONV_FIXED, max_sweeps=args.thermal_fixed_sweeps, max_outer=args.thermal_outer,
                           precision=32)
-            pump = torch.empty((p.ny, p.nx), dtype=torch.complex64, device="cuda")
-            sig = torch.empty_like(pump)
-            st = shg.solve_device(p, pump, sig)
-            runs.append({"oven_c": round(p.temp, 2), "sh_power_w": st.sh_power, "device_ms": st.device_ms,
-                         "sweeps": st.jacobi_sweeps, "last_max_dT_K": st.last_residual})
-            jac_vox += float(p.nx * p.ny * p.nz) * st.jacobi_sweeps
-            opt_pts += float(p.nx * p.ny * p.nz) * st.outer_iterations
-            del pump, sig
+            if args.no_thermal_grad:
+                pump = torch.empty((p.ny, p.nx), dtype=torch.complex64, device="cuda")
+                sig = torch.empty_like(pump)
+                st = shg.solve_device(p, pump, sig)
+                runs.append({"oven_c": round(p.temp, 2), "sh_power_w": st.sh_power, "device_ms": st.device_ms,
+                             "sweeps": st.jacobi_sweeps, "last_max_dT_K": st.last_residual})
+                sweeps, outer = st.jacobi_sweeps, st.outer_iterations
+                del pump, sig
+            else:
+                g = shg.thermal_grad(p)
+                runs.append({"oven_c": round(p.temp, 2), "sh_power_w": g["sh_power"], "dJ_dToven_w_per_k": g["d_temp"],
+                             "device_ms": g["device_ms"], "sweeps": g["jacobi_sweeps"]})
+                sweeps, outer = g["jacobi_sweeps"], g["outer_iterations"]
+            jac_vox += float(p.nx * p.ny * p.nz) * sweeps
+            opt_pts += float(p.nx * p.ny * p.nz) * outer
             torch.cuda.synchronize()
     total_ms = sum(r["device_ms"] for r in runs)
     return {"metric": "thermal batch device time", "value": total_ms, "unit": "ms", "higher_is_better": False,
@@ -568,6 +576,7 @@ def main() -> int:
     ap.add_argument("--thermal-count", type=int, default=8)
     ap.add_argument("--thermal-fixed-sweeps", type=int, default=200)
     ap.add_argument("--thermal-outer", type=int, default=2)
+    ap.add_argument("--no-thermal-grad", action="store_true", help="thermal-batch: the runs without dJ/dT_oven")
     ap.add_argument("--jacobi-sweeps", type=int, default=400)
     ap.add_argument("--thermal-side", type=int, default=0)
     ap.add_argument("--thermal-nz", type=int, default=0)

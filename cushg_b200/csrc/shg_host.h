@@ -3,6 +3,8 @@
 
 #include <cuda_runtime.h>
 
+#include <functional>
+
 #include "../../include/shg.h"
 #include "shg_internal.h"
 
@@ -38,9 +40,26 @@ shg_status plain_solve_batch(const shg_params* params, int count, void* const* p
                              void* const* signal_host = nullptr);
 
 // thermal runs (thermal_driver.cu)
+// State of the last optical pass of a thermal run, handed to a ThermalHook before the run
+// frees its buffers: the temperature the pass used, its per-voxel optics (working real type),
+// its descriptor (host copy and device copy), the Jacobi sweeps of the whole run and the
+// centre temperature T(NX/2, NY/2, 0).
+struct ThermalState {
+    const void* T;
+    const void* np;
+    const void* ns;
+    const void* dk;
+    const InstDesc* desc;
+    const InstDesc* desc_dev;
+    int64_t sweeps;
+    double Tc;
+};
+using ThermalHook = std::function<shg_status(const ThermalState&, cudaStream_t)>;
+
 shg_status thermal_solve_device(const shg_params& p, const void* signal_in, void* pump_out, void* signal_out,
                                 void* temperature_out, shg_stats* stats, cudaStream_t stream,
-                                void* slices_p = nullptr, void* slices_s = nullptr);
+                                void* slices_p = nullptr, void* slices_s = nullptr,
+                                const ThermalHook* hook = nullptr);
 shg_status heat_sweeps_device(const shg_params& p, void* temperature, const void* q, int64_t sweeps,
                               cudaStream_t stream);
 

@@ -61,6 +61,31 @@ __global__ void optics_kernel(const R* __restrict__ T, R* __restrict__ dk, R* __
     }
 }
 
+// Derivatives of the per-voxel optics with respect to the oven temperature: u = dT/dT_oven at
+// every voxel times dn/dT and dΔk/dT (central differences over ±1e-3 K in FP64).
+template <typename R>
+__global__ void optics_tangent_kernel(const R* __restrict__ T, const R* __restrict__ u, R* __restrict__ ddk,
+                                      R* __restrict__ dnp, R* __restrict__ dns, size_t total, double lp,
+                                      double period) {
+    const double ls = 0.5 * lp, pi = 3.14159265358979323846, h = 1e-3;
+    const double a = 2.2e-6, b = -5.9e-9;
+    auto dk_of = [&](double t) {
+        const double d = t - 25.;
+        return 2 * pi * (2 * sellmeier_dev(lp, t) / lp - sellmeier_dev(ls, t) / ls + 1 / (period * (1. + a * d + b * (d * d))));
+    };
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const double t = (double)T[i], w = (double)u[i] / (2 * h);
+        ddk[i] = (R)((dk_of(t + h) - dk_of(t - h)) * w);
+        dnp[i] = (R)((sellmeier_dev(lp, t + h) - sellmeier_dev(lp, t - h)) * w);
+        dns[i] = (R)((sellmeier_dev(ls, t + h) - sellmeier_dev(ls, t - h)) * w);
+    }
+}
+
+template <typename R>
+__global__ void fill_kernel(R* __restrict__ a, size_t total, R v) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) a[i] = v;
+}
+
 // One Jacobi sweep Ti -> Tf.  Thread block (32, 8) over (x, y), one z plane per grid z.
 // Voxels the reference never writes (the Dirichlet faces) are left untouched, which with
 // two buffers initialised alike keeps them at the oven temperature in both.
@@ -215,6 +240,21 @@ cudaError_t launch_optics(const R* T, R* dk, R* np, R* ns, const shg_params& p, 
     return cudaGetLastError();
 }
 
+template <typename R>
+cudaError_t launch_optics_tangent(const R* T, const R* u, R* ddk, R* dnp, R* dns, const shg_params& p, cudaStream_t s) {
+    const size_t total = (size_t)p.nx * p.nx * p.nz;
+    const int blocks = (int)std::min<size_t>((total + 255) / 256, 148 * 16);
+    optics_tangent_kernel<R><<<blocks, 256, 0, s>>>(T, u, ddk, dnp, dns, total, p.lambda_p, p.period);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_fill(R* a, size_t total, R v, cudaStream_t s) {
+    const int blocks = (int)std::min<size_t>((total + 255) / 256, 148 * 16);
+    fill_kernel<R><<<blocks, 256, 0, s>>>(a, total, v);
+    return cudaGetLastError();
+}
+
 size_t jacobi_partials(const shg_params& p) {
     return (size_t)((p.nx + 31) / 32) * ((p.nx + 7) / 8) * p.nz;
 }
@@ -249,6 +289,12 @@ template cudaError_t launch_thermal_init<float>(float*, float*, float*, const sh
 template cudaError_t launch_thermal_init<double>(double*, double*, double*, const shg_params&, cudaStream_t);
 template cudaError_t launch_optics<float>(const float*, float*, float*, float*, const shg_params&, cudaStream_t);
 template cudaError_t launch_optics<double>(const double*, double*, double*, double*, const shg_params&, cudaStream_t);
+template cudaError_t launch_optics_tangent<float>(const float*, const float*, float*, float*, float*, const shg_params&,
+                                                  cudaStream_t);
+template cudaError_t launch_optics_tangent<double>(const double*, const double*, double*, double*, double*,
+                                                   const shg_params&, cudaStream_t);
+template cudaError_t launch_fill<float>(float*, size_t, float, cudaStream_t);
+template cudaError_t launch_fill<double>(double*, size_t, double, cudaStream_t);
 template cudaError_t launch_jacobi<float>(const float*, float*, const float*, const JacobiCoef<float>&, int, bool, int,
                                           double*, double*, cudaStream_t);
 template cudaError_t launch_jacobi<double>(const double*, double*, const double*, const JacobiCoef<double>&, int, bool,

@@ -26,6 +26,10 @@ struct JacobiCoef {
 template <typename R> JacobiCoef<R> make_jacobi_coef(const shg_params& p);
 template <typename R> cudaError_t launch_thermal_init(R* Ta, R* Tb, R* Q, const shg_params& p, cudaStream_t s);
 template <typename R> cudaError_t launch_optics(const R* T, R* dk, R* np, R* ns, const shg_params& p, cudaStream_t s);
+// u * (dΔk/dT, dn_p/dT, dn_s/dT) at every voxel (u = dT/dT_oven)
+template <typename R>
+cudaError_t launch_optics_tangent(const R* T, const R* u, R* ddk, R* dnp, R* dns, const shg_params& p, cudaStream_t s);
+template <typename R> cudaError_t launch_fill(R* a, size_t total, R v, cudaStream_t s);
 // one sweep Ti -> Tf; with resid, also the convergence value of that sweep into *out
 template <typename R>
 cudaError_t launch_jacobi(const R* Ti, R* Tf, const R* Q, const JacobiCoef<R>& k, int boundary, bool resid, int rule,

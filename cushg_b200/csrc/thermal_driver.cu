@@ -74,7 +74,8 @@ cudaError_t run_sweeps(R*& cur, R*& nxt, const R* Ta, const SweepMaps<R>& m, con
 
 template <typename R>
 shg_status thermal_run(const shg_params& p, const void* signal_in, void* pump_out, void* signal_out,
-                       void* temperature_out, shg_stats* stats, cudaStream_t s, void* slices_p, void* slices_s) {
+                       void* temperature_out, shg_stats* stats, cudaStream_t s, void* slices_p, void* slices_s,
+                       const ThermalHook* hook) {
     const PlainVariant* v = find_plain_variant(p.precision, p.nx, 1, p.march);
     if (!v) return fail(SHG_ERR_UNSUPPORTED, "no thermal kernel for grid side %d", p.nx);
     const int n = p.nx, nz = p.nz;
@@ -111,6 +112,8 @@ shg_status thermal_run(const shg_params& p, const void* signal_in, void* pump_ou
     const int depth = sweep_depth(p);
     int64_t total = 0;
     int outer = 0;
+    InstDesc last_d;
+    double last_Tc = 0.0;
     double last = 0.0;
     R* cur = Ta;  // holds the latest temperature (the reference's Tinic == Tfinal after its copy)
     R* nxt = Tb;
@@ -232,10 +235,16 @@ shg_status thermal_run(const shg_params& p, const void* signal_in, void* pump_ou
                 break;
             }
             if ((e = run_variant(v, ddesc, &d, 1, nullptr, s)) != cudaSuccess) { rc = cuda_fail(e, "thermal optical pass"); break; }
+            last_d = d;
+            last_Tc = Tc;
             ++outer;
             if (p.conv_rule != SHG_CONV_FIXED && counter == 1 && g != 0) break;  // Solver.h:367
         }
         if (rc != SHG_OK) break;
+        if (hook && outer > 0) {
+            const ThermalState st = {cur, NP, NS, DK, &last_d, ddesc, total, last_Tc};
+            if ((rc = (*hook)(st, s)) != SHG_OK) break;
+        }
         if (temperature_out &&
             (e = cudaMemcpyAsync(temperature_out, cur, arr, cudaMemcpyDeviceToDevice, s)) != cudaSuccess) {
             rc = cuda_fail(e, "temperature out");
@@ -327,10 +336,12 @@ shg_status heat_sweeps_device(const shg_params& p, void* temperature, const void
 
 shg_status thermal_solve_device(const shg_params& p, const void* signal_in, void* pump_out, void* signal_out,
                                 void* temperature_out, shg_stats* stats, cudaStream_t stream, void* slices_p,
-                                void* slices_s) {
+                                void* slices_s, const ThermalHook* hook) {
     if (p.precision == 32)
-        return thermal_run<float>(p, signal_in, pump_out, signal_out, temperature_out, stats, stream, slices_p, slices_s);
-    return thermal_run<double>(p, signal_in, pump_out, signal_out, temperature_out, stats, stream, slices_p, slices_s);
+        return thermal_run<float>(p, signal_in, pump_out, signal_out, temperature_out, stats, stream, slices_p, slices_s,
+                                  hook);
+    return thermal_run<double>(p, signal_in, pump_out, signal_out, temperature_out, stats, stream, slices_p, slices_s,
+                               hook);
 }
 
 }  // namespace shg

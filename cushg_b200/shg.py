@@ -27,7 +27,15 @@ EXPORTS = (
     "shg_solve_batch_device", "shg_solve_batch_device_noalloc", "shg_grad", "shg_sh_power", "shg_last_error",
     "shg_status_string", "shg_version", "shg_heat_sweeps_device", "shg_batch_plan_create", "shg_batch_plan_launch",
     "shg_batch_plan_powers", "shg_batch_plan_destroy", "shg_autotune", "shg_grad_batch", "shg_solve_batch",
+    "shg_thermal_grad",
 )
+
+
+class ShgThermalGradResult(ctypes.Structure):
+    """``shg_thermal_grad_result`` of include/shg.h."""
+    _fields_ = [("sh_power", ctypes.c_double), ("d_temp", ctypes.c_double),
+                ("sh_power_tangent_march", ctypes.c_double), ("device_ms", ctypes.c_double),
+                ("stats", ShgStats), ("reserved", ctypes.c_double * 4)]
 
 
 class ShgTuneResult(ctypes.Structure):
@@ -105,6 +113,8 @@ def lib() -> ctypes.CDLL:
         L.shg_batch_plan_powers.restype = ctypes.c_int
         L.shg_batch_plan_destroy.argtypes = [vp]
         L.shg_batch_plan_destroy.restype = None
+        L.shg_thermal_grad.argtypes = [P, ctypes.POINTER(ShgThermalGradResult)]
+        L.shg_thermal_grad.restype = ctypes.c_int
         L.shg_autotune.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ShgTuneResult)]
         L.shg_autotune.restype = ctypes.c_int
         L.shg_last_error.restype = ctypes.c_char_p
@@ -362,6 +372,15 @@ class BatchPlan:
             self.close()
         except Exception:
             pass
+
+
+def thermal_grad(p: ShgParams) -> dict:
+    """shg_thermal_grad: a thermal run and dJ/dT_oven through its temperature field."""
+    r = ShgThermalGradResult()
+    _check(lib().shg_thermal_grad(ctypes.byref(p), ctypes.byref(r)))
+    return {"sh_power": r.sh_power, "d_temp": r.d_temp, "sh_power_tangent_march": r.sh_power_tangent_march,
+            "device_ms": r.device_ms, "jacobi_sweeps": r.stats.jacobi_sweeps,
+            "outer_iterations": r.stats.outer_iterations}
 
 
 def autotune(precision: int, n: int) -> dict:

@@ -311,6 +311,29 @@ SHG_API shg_status shg_grad(const shg_params* p, const double* poling, int32_t c
 SHG_API shg_status shg_grad_batch(const shg_params* params, int32_t count, const double* const* poling,
                                   int32_t checkpoint_every, shg_grad_result* out);
 
+/* Result of shg_thermal_grad. */
+typedef struct shg_thermal_grad_result {
+    double sh_power;               /* SH output power of the thermal run [W] */
+    double d_temp;                 /* dJ/dT_oven [W/K] through the converged temperature field */
+    double sh_power_tangent_march; /* J as the tangent march recomputes it (a consistency check) */
+    double device_ms;              /* device time of the run and its tangent */
+    shg_stats stats;               /* the thermal run's report */
+    double reserved[4];
+} shg_thermal_grad_result;
+
+/*
+ * A thermal run (thermal == 1, as shg_solve) and the derivative of its SH output power with
+ * respect to the oven temperature, i.e. temp and t_peltier moved together (the reference
+ * passes argv[3] as both, src/cuSHG.cu:51-53).  Forward mode: the temperature field's
+ * derivative is the homogeneous Jacobi iteration from a field of ones over the run's total
+ * sweep count (recomputed, not stored), then a tangent-linear march of the last optical pass
+ * through the per-voxel n_p, n_s, Δk and the centre-voxel pump and propagators.  The heat
+ * source Q is held fixed in the derivative: first order in the optical-thermal coupling, exact
+ * when Q does not depend on the oven temperature.  Grid sides 256 and 512, round beams.
+ * Synchronous.  No counterpart in the reference.
+ */
+SHG_API shg_status shg_thermal_grad(const shg_params* p, shg_thermal_grad_result* out);
+
 /* SH output power of a plain run with an optional per-step poling phase (as shg_grad),
  * forward only.  Host, synchronous. */
 SHG_API shg_status shg_sh_power(const shg_params* p, const double* poling, double* sh_power);

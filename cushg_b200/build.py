@@ -28,7 +28,7 @@ CLI_SRC = os.path.join(CSRC, "cli", "cushg_main.cpp")
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
-         "-I", os.path.join(ROOT, "include"), "--diag-suppress", "177"]
+         "-I", os.path.join(ROOT, "include")]
 
 
 def _headers() -> list[str]:

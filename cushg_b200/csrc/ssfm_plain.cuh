@@ -259,7 +259,7 @@ template <typename T, int N, int C, int NT, bool THERM, int MINB = 1>
 __global__ void __launch_bounds__(NT, MINB)
     ssfm_plain_kernel(const InstDesc* __restrict__ descs, int count, int* __restrict__ queue) {
     using Cfg = PlainCfg<T, N, C, NT, THERM>;
-    constexpr int R2 = Cfg::R2, RL = Cfg::RL, SW = Cfg::SW;
+    constexpr int R2 = Cfg::R2, SW = Cfg::SW;
     constexpr int JA = Cfg::JA, JB = Cfg::JB, JCA = Cfg::JCA, JCB = Cfg::JCB;
     constexpr int CPR = 16 / C;  // column sub-rows per n1 of this CTA
     using V = cx<T>;

@@ -4,7 +4,7 @@
 //   kernelSetTemperature / kernelSetBottomOvensTemperature / kernelSetOvenSurrounded
 //       -> thermal_init_kernel
 //   kernelHeatEquationTopOpen / kernelHeatEquationOvenSurrounded (one Jacobi sweep)
-//       -> jacobi_zb_kernel (unchecked sweeps) and jacobi_kernel (the checked sweep of each
+//       -> jacobi_zb2_kernel (unchecked sweeps) and jacobi_kernel (the checked sweep of each
 //          window); Ti -> Tf, the reference's Tf -> Ti device copy after every sweep becomes
 //          a ping-pong of two buffers
 //   kernelDifSquareVectors + thrust::reduce (checkConvergence)
@@ -130,41 +130,70 @@ __global__ void __launch_bounds__(256) jacobi_kernel(const R* __restrict__ Ti, R
     }
 }
 
-// One unchecked Jacobi sweep Ti -> Tf, z-blocked: thread (x, y) updates the column of up to
-// ZB planes z0..z0+ZB-1, keeping T at z-1, z and z+1 in registers as it walks up, so each
-// voxel costs one new load of the centre column and the four lateral neighbours (through
-// L1), and the boundary classification and index arithmetic are paid once per column step
-// instead of per neighbour.  Every voxel is computed by jacobi_point from the same operands
-// as in jacobi_kernel.  Thread block (32, 8), grid (n/32, n/8, nz/ZB).
+// Unchecked Jacobi sweeps Ti -> Tf, z-blocked: a thread walks a column of ZB planes,
+// keeping T at z-1, z and z+1 in registers as it goes up, so each voxel costs one new load of
+// the centre column and its lateral neighbours, and the boundary classification and index
+// arithmetic are paid once per column step.
 //
-// Used for FP32, where the one-voxel kernel is bound by instruction issue (91 thread
-// instructions per voxel, DRAM at 34 % of peak at 256x256x400): 104.5 -> 88.7 us per sweep
-// there, 249 -> 203 us at 512x512x250.  FP64 sweeps are already memory-bound and lose
-// parallelism here (64 -> 78 us at 256x256x200), so they keep jacobi_kernel.
+// One voxel per thread with every neighbour loaded was bound by instruction issue in FP32 (91
+// thread instructions per voxel, DRAM at 34 % of peak at 256x256x400).  Measured per sweep:
+//   FP32 512x512x250: 249 us (one voxel) -> 203 (z-blocked) -> 166 (z-blocked, pairs), 4.7 TB/s
+//   FP64 512x512x250: 318 us (one voxel) -> 282 (z-blocked, pairs), 5.6 TB/s
+//   FP64 128x128x200 (L2-resident): 16.6 -> 14.5 us
 constexpr int kJacobiZB = 8;
 
+// The z-blocked sweep with two x-adjacent voxels per thread: the centre column, its y
+// neighbours and Q are read as float2 / double2 (rows are 8- / 16-byte aligned since n is
+// even), the x neighbours outside the pair as scalars.  Each voxel is still jacobi_point of
+// the same operands.  Thread block (32, 8) covers 64 x 8 voxels; grid (n/64, n/8, nz/ZB).
+template <typename R> struct pair_t;
+template <> struct pair_t<float> { using type = float2; };
+template <> struct pair_t<double> { using type = double2; };
+
 template <typename R, int BOUND>
-__global__ void __launch_bounds__(256) jacobi_zb_kernel(const R* __restrict__ Ti, R* __restrict__ Tf,
-                                                        const R* __restrict__ Q, JacobiCoef<R> k) {
+__global__ void __launch_bounds__(256) jacobi_zb2_kernel(const R* __restrict__ Ti, R* __restrict__ Tf,
+                                                         const R* __restrict__ Q, JacobiCoef<R> k) {
+    using R2 = typename pair_t<R>::type;
     const int n = k.n, nz = k.nz;
-    const int x = blockIdx.x * 32 + threadIdx.x;
+    const int x = 2 * (blockIdx.x * 32 + threadIdx.x);
     const int y = blockIdx.y * 8 + threadIdx.y;
     if (x >= n || y >= n) return;
     const int z0 = blockIdx.z * kJacobiZB, z1 = min(nz, z0 + kJacobiZB);
     const size_t sy = (size_t)n, sz = (size_t)n * n;
     size_t i = (size_t)z0 * sz + (size_t)y * sy + x;
-    R below = z0 > 0 ? Ti[i - sz] : (R)0;
-    R cur = Ti[i];
+    auto ld2 = [&](size_t j) { return *reinterpret_cast<const R2*>(Ti + j); };
+    R2 zero2;
+    zero2.x = zero2.y = (R)0;
+    R2 below = z0 > 0 ? ld2(i - sz) : zero2;
+    R2 cur = ld2(i);
 #pragma unroll 2
     for (int z = z0; z < z1; ++z, i += sz) {
-        const R above = z + 1 < nz ? Ti[i + sz] : (R)0;
-        auto get = [&](int dx, int dy, int dz) -> R {
-            if (dz > 0) return above;
-            if (dz < 0) return below;
-            return Ti[i + (ptrdiff_t)dy * sy + dx];
+        const R2 above = z + 1 < nz ? ld2(i + sz) : zero2;
+        const R2 ym = y > 0 ? ld2(i - sy) : zero2, yp = y + 1 < n ? ld2(i + sy) : zero2;
+        const R xm = x > 0 ? Ti[i - 1] : (R)0, xp = x + 2 < n ? Ti[i + 2] : (R)0;
+        const R2 q = *reinterpret_cast<const R2*>(Q + i);
+        auto get0 = [&](int dx, int dy, int dz) -> R {
+            if (dz) return dz > 0 ? above.x : below.x;
+            if (dy) return dy > 0 ? yp.x : ym.x;
+            return dx > 0 ? cur.y : xm;
         };
-        R v;
-        if (jacobi_point<R, BOUND>(x, y, z, k, Q[i], get, &v)) Tf[i] = v;
+        auto get1 = [&](int dx, int dy, int dz) -> R {
+            if (dz) return dz > 0 ? above.y : below.y;
+            if (dy) return dy > 0 ? yp.y : ym.y;
+            return dx > 0 ? xp : cur.x;
+        };
+        R v0, v1;
+        const bool w0 = jacobi_point<R, BOUND>(x, y, z, k, q.x, get0, &v0);
+        const bool w1 = jacobi_point<R, BOUND>(x + 1, y, z, k, q.y, get1, &v1);
+        if (w0 && w1) {
+            R2 o;
+            o.x = v0;
+            o.y = v1;
+            *reinterpret_cast<R2*>(Tf + i) = o;
+        } else {
+            if (w0) Tf[i] = v0;
+            if (w1) Tf[i + 1] = v1;
+        }
         below = cur;
         cur = above;
     }
@@ -264,12 +293,13 @@ cudaError_t launch_jacobi(const R* Ti, R* Tf, const R* Q, const JacobiCoef<R>& k
                           double* partial, double* out, cudaStream_t s) {
     dim3 block(32, 8, 1);
     dim3 grid((k.n + 31) / 32, (k.n + 7) / 8, k.nz);
-    if (!resid && sizeof(R) == 4) {
-        const dim3 zgrid(grid.x, grid.y, (k.nz + kJacobiZB - 1) / kJacobiZB);
+    if (!resid) {
+        // n is even (shg_check_params), so the voxel pairs tile every row
+        const dim3 zgrid((k.n + 63) / 64, grid.y, (k.nz + kJacobiZB - 1) / kJacobiZB);
         if (boundary == SHG_BOUNDARY_OVEN_SURROUNDED)
-            jacobi_zb_kernel<R, SHG_BOUNDARY_OVEN_SURROUNDED><<<zgrid, block, 0, s>>>(Ti, Tf, Q, k);
+            jacobi_zb2_kernel<R, SHG_BOUNDARY_OVEN_SURROUNDED><<<zgrid, block, 0, s>>>(Ti, Tf, Q, k);
         else
-            jacobi_zb_kernel<R, SHG_BOUNDARY_TOP_OPEN><<<zgrid, block, 0, s>>>(Ti, Tf, Q, k);
+            jacobi_zb2_kernel<R, SHG_BOUNDARY_TOP_OPEN><<<zgrid, block, 0, s>>>(Ti, Tf, Q, k);
         return cudaGetLastError();
     }
     if (boundary == SHG_BOUNDARY_OVEN_SURROUNDED) {

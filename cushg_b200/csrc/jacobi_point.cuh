@@ -15,6 +15,13 @@
 
 namespace shg {
 
+// The inner-point update (Tfield.h:113-115) from the six neighbours and Q; jacobi_point's inner
+// branch, and the fast path of kernels that know a voxel is inner.
+template <typename R>
+__device__ __forceinline__ R jacobi_inner(R xp, R xm, R yp, R ym, R zp, R zm, R q, const JacobiCoef<R>& k) {
+    return k.L2 * ((xp + xm) * k.idx2 + (yp + ym) * k.idy2 + (zp + zm) * k.idz2 + q * k.iK);
+}
+
 // get(dx, dy, dz) returns the current temperature of voxel (x+dx, y+dy, z+dz); only
 // neighbours inside the grid are asked for.  q is Q at (x, y, z).  Returns false (and
 // leaves *v alone) for voxels the reference never writes.
@@ -25,8 +32,7 @@ __device__ __forceinline__ bool jacobi_point(int x, int y, int z, const JacobiCo
     if (BOUND == SHG_BOUNDARY_TOP_OPEN) {
         if (y == 0) return false;  // Dirichlet face at the oven temperature
         if (xi && yi && zi) {      // inner points (Tfield.h:113-115)
-            *v = k.L2 * ((get(1, 0, 0) + get(-1, 0, 0)) * k.idx2 + (get(0, 1, 0) + get(0, -1, 0)) * k.idy2 +
-                         (get(0, 0, 1) + get(0, 0, -1)) * k.idz2 + q * k.iK);
+            *v = jacobi_inner<R>(get(1, 0, 0), get(-1, 0, 0), get(0, 1, 0), get(0, -1, 0), get(0, 0, 1), get(0, 0, -1), q, k);
         } else if (!xi && yi && zi) {  // faces x = 0 / x = Lx (Tfield.h:119-125)
             const int xn = x == 0 ? 1 : -1;
             *v = (get(xn, 0, 0) + k.ax * (get(0, 1, 0) + get(0, -1, 0)) + k.bx * (get(0, 0, 1) + get(0, 0, -1)) +
@@ -55,8 +61,7 @@ __device__ __forceinline__ bool jacobi_point(int x, int y, int z, const JacobiCo
     } else {
         if (!(xi && yi)) return false;  // lateral faces held at the oven temperature
         if (zi) {
-            *v = k.L2 * ((get(1, 0, 0) + get(-1, 0, 0)) * k.idx2 + (get(0, 1, 0) + get(0, -1, 0)) * k.idy2 +
-                         (get(0, 0, 1) + get(0, 0, -1)) * k.idz2 + q * k.iK);
+            *v = jacobi_inner<R>(get(1, 0, 0), get(-1, 0, 0), get(0, 1, 0), get(0, -1, 0), get(0, 0, 1), get(0, 0, -1), q, k);
         } else {  // z faces (Tfield.h:229-236)
             const int zn = z == 0 ? 1 : -1;
             *v = (get(0, 0, zn) + k.az * (get(1, 0, 0) + get(-1, 0, 0)) + k.bz * (get(0, 1, 0) + get(0, -1, 0)) +

@@ -166,6 +166,8 @@ __global__ void __launch_bounds__(256) jacobi_zb2_kernel(const R* __restrict__ T
     zero2.x = zero2.y = (R)0;
     R2 below = z0 > 0 ? ld2(i - sz) : zero2;
     R2 cur = ld2(i);
+    // both voxels of the pair are inner in x and y (a pair starts at an even x)
+    const bool inner_xy = x >= 2 && x + 3 < n && y >= 1 && y + 1 < n;
 #pragma unroll 2
     for (int z = z0; z < z1; ++z, i += sz) {
         const R2 above = z + 1 < nz ? ld2(i + sz) : zero2;
@@ -183,8 +185,15 @@ __global__ void __launch_bounds__(256) jacobi_zb2_kernel(const R* __restrict__ T
             return dx > 0 ? xp : cur.x;
         };
         R v0, v1;
-        const bool w0 = jacobi_point<R, BOUND>(x, y, z, k, q.x, get0, &v0);
-        const bool w1 = jacobi_point<R, BOUND>(x + 1, y, z, k, q.y, get1, &v1);
+        bool w0 = true, w1 = true;
+        if (inner_xy && z >= 1 && z + 1 < nz) {
+            // inner voxels: jacobi_point's inner branch without the classification
+            v0 = jacobi_inner<R>(cur.y, xm, yp.x, ym.x, above.x, below.x, q.x, k);
+            v1 = jacobi_inner<R>(xp, cur.x, yp.y, ym.y, above.y, below.y, q.y, k);
+        } else {
+            w0 = jacobi_point<R, BOUND>(x, y, z, k, q.x, get0, &v0);
+            w1 = jacobi_point<R, BOUND>(x + 1, y, z, k, q.y, get1, &v1);
+        }
         if (w0 && w1) {
             R2 o;
             o.x = v0;

@@ -412,6 +412,9 @@ def run_thermal_batch(args) -> dict:
     import torch
     from cushg_b200 import shg
 
+    # each 512 x 512 x 1000 FP32 instance uses about 11 GB of workspace: keep it in the
+    # library's pool from one instance to the next (read when the pool is first created)
+    os.environ.setdefault("SHG_POOL_KEEP_MB", "16384")
     ps = P.config_thermal_512(args.thermal_count)
     runs, jac_vox, opt_pts = [], 0.0, 0.0
     with ClockSampler(0) as clk:

@@ -12,6 +12,7 @@
 #include <complex>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -66,6 +67,11 @@ cudaError_t dev_alloc(void** ptr, size_t bytes, cudaStream_t s) {
                 return e;
             }
             unsigned long long keep = kPoolKeepBytes;
+            if (const char* env = std::getenv("SHG_POOL_KEEP_MB")) {
+                char* end = nullptr;
+                const unsigned long long mb = std::strtoull(env, &end, 10);
+                if (end != env) keep = mb << 20;
+            }
             cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &keep);
         }
         pool = pools[dev];

@@ -17,9 +17,10 @@ shg_status cuda_fail(cudaError_t e, const char* what);
 void clear_error();
 
 // Stream-ordered device memory from the library's own pool on the current device, which keeps
-// up to kPoolKeepBytes between calls instead of handing it back at every synchronisation
-// (the default pool's release threshold is 0, so a repeated call would map its workspace
-// again each time).
+// up to kPoolKeepBytes (or SHG_POOL_KEEP_MB megabytes from the environment, read when the
+// pool is created) between calls instead of handing it back at every synchronisation (the
+// default pool's release threshold is 0, so a repeated call would map its workspace again
+// each time).
 constexpr unsigned long long kPoolKeepBytes = 2ull << 30;
 // Inside a stream capture it falls back to cudaMallocAsync (a graph memory node).
 cudaError_t dev_alloc(void** ptr, size_t bytes, cudaStream_t s);

@@ -394,7 +394,8 @@ def run_thermal(args) -> dict:
            "workload": f"thermal {p.nx}x{p.ny}x{p.nz} FP{p.precision}", "status": status,
            "jacobi_block": p.jacobi_block or "auto (1)", "wall_s": wall, "clocks": clk.summary()}
     if st is not None:
-        out.update({"device_ms": st.device_ms, "jacobi_sweeps": st.jacobi_sweeps, "outer_iterations": st.outer_iterations,
+        out.update({"device_ms": st.device_ms, "jacobi_ms": st.jacobi_ms, "optics_ms": st.optics_ms,
+                    "jacobi_sweeps": st.jacobi_sweeps, "outer_iterations": st.outer_iterations,
                     "sh_power_w": st.sh_power, "value": vox * st.jacobi_sweeps / (st.device_ms * 1e-3),
                     "unit": "voxel-sweeps/s",
                     "jacobi_gbs_algorithmic": 3 * (p.precision // 8) * vox * st.jacobi_sweeps / (st.device_ms * 1e-3) / 1e9})

@@ -102,6 +102,11 @@ shg_status thermal_run(const shg_params& p, const void* signal_in, void* pump_ou
     cudaEvent_t t0 = nullptr, t1 = nullptr;
     cudaEventCreate(&t0);
     cudaEventCreate(&t1);
+    // per-phase timing: the Jacobi loop of an outer iteration runs between ej[0] and ej[1],
+    // its optics and optical pass between ej[1] and ej[2]
+    cudaEvent_t ej[3] = {nullptr, nullptr, nullptr};
+    for (auto& ev : ej) cudaEventCreate(&ev);
+    double jacobi_ms = 0.0, optics_ms = 0.0;
     cudaEventRecord(t0, s);
     const JacobiCoef<R> k = make_jacobi_coef<R>(p);
     // Solver.h:332: tol = 5e-4 / TSIZE in the working precision
@@ -125,6 +130,7 @@ shg_status thermal_run(const shg_params& p, const void* signal_in, void* pump_ou
         for (int g = 0; g < max_outer && rc == SHG_OK; ++g) {
             double red = 1.0, aux = -1.0;
             int64_t counter = 0;
+            cudaEventRecord(ej[0], s);
             if (p.conv_rule == SHG_CONV_FIXED) {
                 // exactly max_sweeps sweeps; the last one reports max |Tf - Ti|
                 if ((e = run_sweeps<R>(cur, nxt, Ta, maps, Q, k, p.boundary, depth, max_sweeps - 1, tb_err, s)) !=
@@ -198,6 +204,7 @@ shg_status thermal_run(const shg_params& p, const void* signal_in, void* pump_ou
             total += counter;
             last = red;
             if (rc != SHG_OK) break;
+            cudaEventRecord(ej[1], s);
             // optical pass from the converged temperature
             if ((e = launch_optics<R>(cur, DK, NP, NS, p, s)) != cudaSuccess) { rc = cuda_fail(e, "optics"); break; }
             R tc_h = 0;
@@ -238,6 +245,13 @@ shg_status thermal_run(const shg_params& p, const void* signal_in, void* pump_ou
             last_d = d;
             last_Tc = Tc;
             ++outer;
+            cudaEventRecord(ej[2], s);
+            if ((e = cudaEventSynchronize(ej[2])) != cudaSuccess) { rc = cuda_fail(e, "thermal optical pass"); break; }
+            float a = 0.f, b = 0.f;
+            cudaEventElapsedTime(&a, ej[0], ej[1]);
+            cudaEventElapsedTime(&b, ej[1], ej[2]);
+            jacobi_ms += a;
+            optics_ms += b;
             if (p.conv_rule != SHG_CONV_FIXED && counter == 1 && g != 0) break;  // Solver.h:367
         }
         if (rc != SHG_OK) break;
@@ -268,6 +282,8 @@ shg_status thermal_run(const shg_params& p, const void* signal_in, void* pump_ou
             stats->steps = nz;
             stats->last_residual = last;
             stats->device_ms = ms;
+            stats->jacobi_ms = jacobi_ms;
+            stats->optics_ms = optics_ms;
             if (!std::isfinite(h[0]) || !std::isfinite(h[1]))
                 rc = fail(SHG_ERR_NONFINITE, "SH / pump power %g / %g", h[0], h[1]);
         }
@@ -275,6 +291,7 @@ shg_status thermal_run(const shg_params& p, const void* signal_in, void* pump_ou
     cudaFreeAsync(buf, s);
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
+    for (cudaEvent_t ev : ej) cudaEventDestroy(ev);
     e = cudaGetLastError();
     if (rc == SHG_OK && e != cudaSuccess) rc = cuda_fail(e, "thermal run");
     return rc;

@@ -97,7 +97,7 @@ class ShgStats(ctypes.Structure):
         ("sh_power", ctypes.c_double), ("pump_power", ctypes.c_double),
         ("jacobi_sweeps", ctypes.c_int64), ("outer_iterations", ctypes.c_int32),
         ("steps", ctypes.c_int32), ("last_residual", ctypes.c_double),
-        ("device_ms", ctypes.c_double),
+        ("device_ms", ctypes.c_double), ("jacobi_ms", ctypes.c_double), ("optics_ms", ctypes.c_double),
     ]
 
 

@@ -141,6 +141,9 @@ typedef struct shg_stats {
     int32_t steps;            /* SSFM steps marched per optical pass */
     double last_residual;     /* last Jacobi convergence value */
     double device_ms;         /* device time of the call (CUDA events) */
+    double jacobi_ms;         /* thermal runs: device time of the Jacobi sweeps and checks */
+    double optics_ms;         /* thermal runs: device time of the per-voxel optics and optical
+                                 passes (plain runs: 0; device_ms is the march) */
 } shg_stats;
 
 /* Fill *p with the reference's compile-time defaults (cuSHG.cu:11-13, Crystal.h:19-52,

@@ -21,9 +21,9 @@ _lib = None
 
 def build(force: bool = False) -> str:
     """Compile liboracle.so with the Makefile next to this file."""
-    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < max(
-        os.path.getmtime(os.path.join(HERE, f)) for f in ("shg_oracle.c", "shg_oracle_impl.h")
-    ):
+    deps = [os.path.join(HERE, f) for f in ("shg_oracle.c", "shg_oracle_impl.h")]
+    deps.append(os.path.join(os.path.dirname(HERE), "include", "shg.h"))  # the shared parameter / stats structs
+    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < max(os.path.getmtime(d) for d in deps):
         subprocess.run(["make", "-s", "-C", HERE], check=True)
     return LIB_PATH
 

@@ -427,13 +427,17 @@ def run_thermal_batch(args) -> dict:
                 sig = torch.empty_like(pump)
                 st = shg.solve_device(p, pump, sig)
                 runs.append({"oven_c": round(p.temp, 2), "sh_power_w": st.sh_power, "device_ms": st.device_ms,
+                             "jacobi_ms": st.jacobi_ms, "optics_ms": st.optics_ms,
                              "sweeps": st.jacobi_sweeps, "last_max_dT_K": st.last_residual})
                 sweeps, outer = st.jacobi_sweeps, st.outer_iterations
                 del pump, sig
             else:
                 g = shg.thermal_grad(p)
+                # jacobi_ms / optics_ms: the forward run's heat solve and per-voxel optics; the
+                # rest of device_ms is the optical marches and the tangent (its own sweeps included)
                 runs.append({"oven_c": round(p.temp, 2), "sh_power_w": g["sh_power"], "dJ_dToven_w_per_k": g["d_temp"],
-                             "device_ms": g["device_ms"], "sweeps": g["jacobi_sweeps"]})
+                             "device_ms": g["device_ms"], "jacobi_ms": g["jacobi_ms"], "optics_ms": g["optics_ms"],
+                             "sweeps": g["jacobi_sweeps"]})
                 sweeps, outer = g["jacobi_sweeps"], g["outer_iterations"]
             jac_vox += float(p.nx * p.ny * p.nz) * sweeps
             opt_pts += float(p.nx * p.ny * p.nz) * outer

@@ -250,9 +250,10 @@ shg_status grad_batch(const shg_params* ps, int count, const double* const* poli
                     for (int k = 0; k < kAdjAcc; ++k) A[k] += part[((size_t)slot * C + c) * kAdjAcc + k];
             // temperature derivatives of the scalar constants (central differences in FP64)
             const double lp = p.lambda_p, ls = 0.5 * lp, T = p.temp, h = 1e-3;
-            const double np = sellmeier(lp, T), ns = sellmeier(ls, T);
-            const double dnp = (sellmeier(lp, T + h) - sellmeier(lp, T - h)) / (2 * h);
-            const double dns = (sellmeier(ls, T + h) - sellmeier(ls, T - h)) / (2 * h);
+            const int cr = p.crystal;
+            const double np = sellmeier(cr, lp, T), ns = sellmeier(cr, ls, T);
+            const double dnp = (sellmeier(cr, lp, T + h) - sellmeier(cr, lp, T - h)) / (2 * h);
+            const double dns = (sellmeier(cr, ls, T + h) - sellmeier(cr, ls, T - h)) / (2 * h);
             const double ddk = (delta_k(p, T + h) - delta_k(p, T - h)) / (2 * h);
             const InstDesc& d = J.d;
             const double Jp = d.pw_s * A[kAccJ];

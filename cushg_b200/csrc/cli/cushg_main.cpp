@@ -4,7 +4,7 @@
 //         [--nx N] [--nz NZ] [--lx um] [--ly um] [--lz um] [--focus um] [--waist-y um] [--t-inf C]
 //         [--deff um/V] [--period um] [--alpha-p 1/um] [--alpha-s 1/um] [--beta-s um/W]
 //         [--rho-p rad] [--rho-s rad] [--kappa W/(um K)] [--h-conv W/(um^2 K)] [--lambda um]
-//         [--thermal] [--precision 32|64] [--boundary top-open|oven-surrounded]
+//         [--thermal] [--precision 32|64] [--boundary top-open|oven-surrounded] [--crystal spplt|ppln]
 //         [--max-outer N] [--check-every N] [--tol value] [--conv reference|maxabs]
 //
 // The five positional arguments are the reference's argv (src/cuSHG.cu:46-58); the options
@@ -156,6 +156,14 @@ int parse_options(int argc, char** argv, int first, shg_params& p) {
             if (i + 1 >= argc) return usage();
             const std::string b = argv[++i];
             p.boundary = b == "oven-surrounded" ? SHG_BOUNDARY_OVEN_SURROUNDED : SHG_BOUNDARY_TOP_OPEN;
+        } else if (a == "--crystal") {
+            if (i + 1 >= argc) return usage();
+            const std::string b = argv[++i];
+            if (b != "spplt" && b != "ppln") {
+                std::cerr << "cushg: --crystal takes spplt or ppln" << std::endl;
+                return usage();
+            }
+            p.crystal = b == "ppln" ? SHG_CRYSTAL_MGO_PPLN : SHG_CRYSTAL_MGO_SPPLT;
         } else if (a == "--conv") {
             if (i + 1 >= argc) return usage();
             const std::string b = argv[++i];

@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "../../include/shg.h"
+#include "crystal.cuh"
 #include "shg_host.h"
 #include "shg_internal.h"
 #include "ssfm_variants.h"
@@ -84,23 +85,11 @@ const double kPi = 3.14159265358979323846;
 const double kC = 299792458 * 1E6 / 1E12;
 const double kEps0 = 8.8541878128E-12 * 1E12 / 1E6;
 
-// Sellmeier equation of MgO:sPPLT (Bruner et al.), src/headers/Crystal.h:54-70.
-double sellmeier(double L, double T) {
-    const double A = 4.502483, B = 0.007294, C = 0.185087, D = -0.02357;
-    const double E = 0.073423, F = 0.199595, G = 0.001, H = 7.99724;
-    const double TK = T + 273.15;
-    const double b = 3.483933e-8 * (TK * TK);
-    const double c = 1.607839e-8 * (TK * TK);
-    const double L2 = L * L;
-    return std::sqrt(A + (B + b) / (L2 - (C + c) * (C + c)) + E / (L2 - F * F) + G / (L2 - H * H) + D * L2);
-}
+// Extraordinary index of the chosen crystal (crystal.cuh; sPPLT: src/headers/Crystal.h:54-70).
+double sellmeier(int crystal, double L, double T) { return crystal_n(crystal, L, T); }
 
 // Δk at temperature T with the grating's thermal expansion (PhaseMatching.h:47-85).
-double delta_k(const shg_params& p, double T) {
-    const double lp = p.lambda_p, ls = 0.5 * lp;
-    const double a = 2.2e-6, b = -5.9e-9, d = T - 25.;
-    return 2 * kPi * (2 * sellmeier(lp, T) / lp - sellmeier(ls, T) / ls + 1 / (p.period * (1. + a * d + b * (d * d))));
-}
+double delta_k(const shg_params& p, double T) { return crystal_delta_k(p.crystal, p.lambda_p, p.period, T); }
 
 // Constants of one plain optical pass at uniform temperature Tc (the reference reads
 // T at voxel (NX/2, NY/2, 0) for the pump and propagators, Efields.h:88,124).
@@ -110,7 +99,7 @@ InstDesc make_plain_desc(const shg_params& p, double Tc, double T_dk) {
     const double dx = p.lx / (p.nx - 1), dy = p.ly / (p.ny - 1), dz = p.lz / (p.nz - 1);
     const double lp = p.lambda_p, ls = 0.5 * lp;
     const double dQ = 2.0 * p.deff / kPi;
-    const double np = sellmeier(lp, Tc), ns = sellmeier(ls, Tc);
+    const double np = sellmeier(p.crystal, lp, Tc), ns = sellmeier(p.crystal, ls, Tc);
     d.n = p.nx;
     d.nsteps = shg_steps(&p);
     d.out_after = p.thermal ? d.nsteps - 1 : d.nsteps;
@@ -234,7 +223,8 @@ static shg_status check_params_impl(const shg_params* p, bool need_kernel) {
     if (!(p->waist > 0) || p->power < 0 || !(p->period > 0)) return fail(SHG_ERR_INVALID, "waist/power/period");
     if (p->waist_y < 0) return fail(SHG_ERR_INVALID, "waist_y must be >= 0 (0: round beam)");
     if (p->alpha_p < 0 || p->alpha_s < 0 || p->beta_s < 0) return fail(SHG_ERR_INVALID, "negative absorption");
-    if (p->crystal != SHG_CRYSTAL_MGO_SPPLT) return fail(SHG_ERR_UNSUPPORTED, "unknown crystal %d", p->crystal);
+    if (p->crystal != SHG_CRYSTAL_MGO_SPPLT && p->crystal != SHG_CRYSTAL_MGO_PPLN)
+        return fail(SHG_ERR_UNSUPPORTED, "unknown crystal %d", p->crystal);
     if (p->thermal) {
         if (!(p->kappa > 0) || p->h_conv < 0) return fail(SHG_ERR_INVALID, "kappa must be > 0, h_conv >= 0");
         if (p->boundary != SHG_BOUNDARY_TOP_OPEN && p->boundary != SHG_BOUNDARY_OVEN_SURROUNDED)

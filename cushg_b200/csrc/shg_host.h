@@ -25,7 +25,7 @@ constexpr unsigned long long kPoolKeepBytes = 2ull << 30;
 // Inside a stream capture it falls back to cudaMallocAsync (a graph memory node).
 cudaError_t dev_alloc(void** ptr, size_t bytes, cudaStream_t s);
 
-double sellmeier(double L, double T);
+double sellmeier(int crystal, double L, double T);
 double delta_k(const shg_params& p, double T);
 InstDesc make_plain_desc(const shg_params& p, double Tc, double T_dk);
 size_t complex_bytes(const shg_params& p);

@@ -13,6 +13,7 @@
 //       -> optics_kernel (Δk, n_p, n_s per voxel, once per optical pass)
 #include <cuda_runtime.h>
 
+#include "crystal.cuh"
 #include "jacobi_point.cuh"
 #include "shg_host.h"
 #include "thermal.h"
@@ -34,30 +35,16 @@ __global__ void thermal_init_kernel(R* Ta, R* Tb, R* Q, int n, int nz, R temp, R
     }
 }
 
-// Sellmeier of MgO:sPPLT (Crystal.h:54-70) in FP64 on the device.
-__device__ __forceinline__ double sellmeier_dev(double L, double T) {
-    const double A = 4.502483, B = 0.007294, C = 0.185087, D = -0.02357;
-    const double E = 0.073423, F = 0.199595, G = 0.001, H = 7.99724;
-    const double TK = T + 273.15;
-    const double b = 3.483933e-8 * (TK * TK);
-    const double c = 1.607839e-8 * (TK * TK);
-    const double L2 = L * L;
-    return sqrt(A + (B + b) / (L2 - (C + c) * (C + c)) + E / (L2 - F * F) + G / (L2 - H * H) + D * L2);
-}
-
-// Δk (PhaseMatching.h:47-65), n(λp, T) and n(λs, T) at every voxel, in FP64.
+// Δk (PhaseMatching.h:47-65), n(λp, T) and n(λs, T) at every voxel, in FP64 (crystal.cuh).
 template <typename R>
 __global__ void optics_kernel(const R* __restrict__ T, R* __restrict__ dk, R* __restrict__ np, R* __restrict__ ns,
-                              size_t total, double lp, double period) {
-    const double ls = 0.5 * lp, pi = 3.14159265358979323846;
-    const double a = 2.2e-6, b = -5.9e-9;
+                              size_t total, double lp, double period, int crystal) {
+    const double ls = 0.5 * lp;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
         const double t = (double)T[i];
-        const double npv = sellmeier_dev(lp, t), nsv = sellmeier_dev(ls, t);
-        const double d = t - 25.;
-        dk[i] = (R)(2 * pi * (2 * npv / lp - nsv / ls + 1 / (period * (1. + a * d + b * (d * d)))));
-        np[i] = (R)npv;
-        ns[i] = (R)nsv;
+        dk[i] = (R)crystal_delta_k(crystal, lp, period, t);
+        np[i] = (R)crystal_n(crystal, lp, t);
+        ns[i] = (R)crystal_n(crystal, ls, t);
     }
 }
 
@@ -66,18 +53,13 @@ __global__ void optics_kernel(const R* __restrict__ T, R* __restrict__ dk, R* __
 template <typename R>
 __global__ void optics_tangent_kernel(const R* __restrict__ T, const R* __restrict__ u, R* __restrict__ ddk,
                                       R* __restrict__ dnp, R* __restrict__ dns, size_t total, double lp,
-                                      double period) {
-    const double ls = 0.5 * lp, pi = 3.14159265358979323846, h = 1e-3;
-    const double a = 2.2e-6, b = -5.9e-9;
-    auto dk_of = [&](double t) {
-        const double d = t - 25.;
-        return 2 * pi * (2 * sellmeier_dev(lp, t) / lp - sellmeier_dev(ls, t) / ls + 1 / (period * (1. + a * d + b * (d * d))));
-    };
+                                      double period, int crystal) {
+    const double ls = 0.5 * lp, h = 1e-3;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
         const double t = (double)T[i], w = (double)u[i] / (2 * h);
-        ddk[i] = (R)((dk_of(t + h) - dk_of(t - h)) * w);
-        dnp[i] = (R)((sellmeier_dev(lp, t + h) - sellmeier_dev(lp, t - h)) * w);
-        dns[i] = (R)((sellmeier_dev(ls, t + h) - sellmeier_dev(ls, t - h)) * w);
+        ddk[i] = (R)((crystal_delta_k(crystal, lp, period, t + h) - crystal_delta_k(crystal, lp, period, t - h)) * w);
+        dnp[i] = (R)((crystal_n(crystal, lp, t + h) - crystal_n(crystal, lp, t - h)) * w);
+        dns[i] = (R)((crystal_n(crystal, ls, t + h) - crystal_n(crystal, ls, t - h)) * w);
     }
 }
 
@@ -274,7 +256,7 @@ template <typename R>
 cudaError_t launch_optics(const R* T, R* dk, R* np, R* ns, const shg_params& p, cudaStream_t s) {
     const size_t total = (size_t)p.nx * p.nx * p.nz;
     const int blocks = (int)std::min<size_t>((total + 255) / 256, 148 * 16);
-    optics_kernel<R><<<blocks, 256, 0, s>>>(T, dk, np, ns, total, p.lambda_p, p.period);
+    optics_kernel<R><<<blocks, 256, 0, s>>>(T, dk, np, ns, total, p.lambda_p, p.period, p.crystal);
     return cudaGetLastError();
 }
 
@@ -282,7 +264,7 @@ template <typename R>
 cudaError_t launch_optics_tangent(const R* T, const R* u, R* ddk, R* dnp, R* dns, const shg_params& p, cudaStream_t s) {
     const size_t total = (size_t)p.nx * p.nx * p.nz;
     const int blocks = (int)std::min<size_t>((total + 255) / 256, 148 * 16);
-    optics_tangent_kernel<R><<<blocks, 256, 0, s>>>(T, u, ddk, dnp, dns, total, p.lambda_p, p.period);
+    optics_tangent_kernel<R><<<blocks, 256, 0, s>>>(T, u, ddk, dnp, dns, total, p.lambda_p, p.period, p.crystal);
     return cudaGetLastError();
 }
 

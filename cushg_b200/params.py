@@ -31,6 +31,8 @@ SHG_CONV_FIXED = 2
 SHG_MARCH_AUTO = 0
 SHG_MARCH_FUSED = 1
 SHG_MARCH_MULTIPASS = 2
+SHG_CRYSTAL_MGO_SPPLT = 0
+SHG_CRYSTAL_MGO_PPLN = 1
 
 # physical constants of src/headers/Crystal.h:19-21 (µm, ps, W, V)
 C_UM_PS = 299792458 * 1e6 / 1e12
@@ -101,8 +103,16 @@ class ShgStats(ctypes.Structure):
     ]
 
 
-def sellmeier(lam_um: float, temp_c: float) -> float:
-    """Extraordinary index of MgO:sPPLT (Bruner et al.), src/headers/Crystal.h:54-70."""
+def sellmeier(lam_um: float, temp_c: float, crystal: int = SHG_CRYSTAL_MGO_SPPLT) -> float:
+    """Extraordinary index of MgO:sPPLT (Bruner et al.), src/headers/Crystal.h:54-70, or with
+    ``crystal = SHG_CRYSTAL_MGO_PPLN`` of 5 mol% MgO:PPLN (Gayer et al., Appl. Phys. B 91, 343
+    (2008))."""
+    if crystal == SHG_CRYSTAL_MGO_PPLN:
+        f = (temp_c - 24.5) * (temp_c + 570.82)
+        l2 = lam_um * lam_um
+        p = 0.2020 + 6.113e-8 * f
+        return math.sqrt(5.756 + 2.860e-6 * f + (0.0983 + 4.700e-8 * f) / (l2 - p * p)
+                         + (189.32 + 1.516e-4 * f) / (l2 - 12.52 * 12.52) - 1.32e-2 * l2)
     A, B, C, D = 4.502483, 0.007294, 0.185087, -0.02357
     E, F, G, H = 0.073423, 0.199595, 0.001, 7.99724
     tk = temp_c + 273.15
@@ -112,13 +122,16 @@ def sellmeier(lam_um: float, temp_c: float) -> float:
     return math.sqrt(A + (B + b) / (l2 - (C + c) ** 2) + E / (l2 - F * F) + G / (l2 - H * H) + D * l2)
 
 
-def qpm_period(temp_c: float, lambda_p: float = 1.064) -> float:
-    """Grating period that zeroes Δk of src/headers/PhaseMatching.h:47-85 at ``temp_c``
-    (including the grating's thermal expansion α = 2.2e-6, β = -5.9e-9)."""
+def qpm_period(temp_c: float, lambda_p: float = 1.064, crystal: int = SHG_CRYSTAL_MGO_SPPLT) -> float:
+    """Grating period that zeroes Δk of src/headers/PhaseMatching.h:47-85 at ``temp_c``,
+    including the grating's thermal expansion (sPPLT α = 2.2e-6, β = -5.9e-9; MgO:PPLN
+    α = 1.54e-5, β = 5.3e-9)."""
     ls = 0.5 * lambda_p
     d = temp_c - 25.0
-    expansion = 1.0 + 2.2e-6 * d + (-5.9e-9) * d * d
-    return 1.0 / ((sellmeier(ls, temp_c) / ls - 2.0 * sellmeier(lambda_p, temp_c) / lambda_p) * expansion)
+    a, b = (1.54e-5, 5.3e-9) if crystal == SHG_CRYSTAL_MGO_PPLN else (2.2e-6, -5.9e-9)
+    expansion = 1.0 + a * d + b * d * d
+    return 1.0 / ((sellmeier(ls, temp_c, crystal) / ls - 2.0 * sellmeier(lambda_p, temp_c, crystal) / lambda_p)
+                  * expansion)
 
 
 def reference_defaults() -> ShgParams:
@@ -244,7 +257,7 @@ class Result:
 def sh_power_of(p: ShgParams, signal: np.ndarray, temp: float | None = None) -> float:
     """SH power Σ ½ ε0 c n_s |S|² dx dy (n_s at ``temp``, default p.temp), summed in double."""
     t = p.temp if temp is None else temp
-    ns = sellmeier(0.5 * p.lambda_p, t)
+    ns = sellmeier(0.5 * p.lambda_p, t, p.crystal)
     dx = p.lx / (p.nx - 1)
     dy = p.ly / (p.ny - 1)
     return float(0.5 * EPS0 * C_UM_PS * ns * np.sum(np.abs(signal.astype(np.complex128)) ** 2) * dx * dy)

@@ -380,7 +380,8 @@ def thermal_grad(p: ShgParams) -> dict:
     _check(lib().shg_thermal_grad(ctypes.byref(p), ctypes.byref(r)))
     return {"sh_power": r.sh_power, "d_temp": r.d_temp, "sh_power_tangent_march": r.sh_power_tangent_march,
             "device_ms": r.device_ms, "jacobi_sweeps": r.stats.jacobi_sweeps,
-            "outer_iterations": r.stats.outer_iterations}
+            "outer_iterations": r.stats.outer_iterations, "jacobi_ms": r.stats.jacobi_ms,
+            "optics_ms": r.stats.optics_ms}
 
 
 def autotune(precision: int, n: int) -> dict:

@@ -75,7 +75,9 @@ enum {
 
 /* Crystals (Sellmeier equations). */
 enum {
-    SHG_CRYSTAL_MGO_SPPLT = 0 /* Bruner et al., src/headers/Crystal.h:54-70 */
+    SHG_CRYSTAL_MGO_SPPLT = 0, /* Bruner et al., src/headers/Crystal.h:54-70 */
+    SHG_CRYSTAL_MGO_PPLN = 1   /* 5 mol% MgO:PPLN, Gayer et al. 2008; named in the reference's
+                                  README.md:52, absent from its Crystal.h */
 };
 
 typedef struct shg_params {

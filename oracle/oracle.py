@@ -46,6 +46,8 @@ def lib():
         L.shgo_batch_plain.restype = ctypes.c_int
         L.shgo_sellmeier_d.argtypes = [ctypes.c_double, ctypes.c_double]
         L.shgo_sellmeier_d.restype = ctypes.c_double
+        L.shgo_crystal_n.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double]
+        L.shgo_crystal_n.restype = ctypes.c_double
         L.shgo_delta_k.argtypes = [P, ctypes.c_double]
         L.shgo_delta_k.restype = ctypes.c_double
         L.shgo_set_pump.argtypes = [P, ctypes.c_double, vp]
@@ -110,8 +112,8 @@ def batch_plain(ps: list[ShgParams], steps: list[int] | None = None, nthreads: i
     return out
 
 
-def sellmeier(lam: float, temp: float) -> float:
-    return float(lib().shgo_sellmeier_d(lam, temp))
+def sellmeier(lam: float, temp: float, crystal: int = 0) -> float:
+    return float(lib().shgo_crystal_n(crystal, lam, temp))
 
 
 def delta_k(p: ShgParams, temp: float) -> float:

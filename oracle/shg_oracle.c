@@ -52,13 +52,31 @@ static double shgo_sellmeier_any(double L, double T, int single) {
     return sqrt(A + Bb / (L2 - Cc * Cc) + E / (L2 - F * F) + G / (L2 - H * H) + D * L2);
 }
 
+/* 5 mol% MgO:PPLN, extraordinary index (Gayer et al., Appl. Phys. B 91, 343 (2008)):
+ * n^2 = a1 + b1 f + (a2 + b2 f)/(L^2 - (a3 + b3 f)^2) + (a4 + b4 f)/(L^2 - a5^2) - a6 L^2,
+ * f = (T - 24.5)(T + 570.82).  The reference has no code for this crystal, so both
+ * precisions evaluate it in double. */
+static double shgo_ppln(double L, double T) {
+    const double a1 = 5.756, a2 = 0.0983, a3 = 0.2020, a4 = 189.32, a5 = 12.52, a6 = 1.32e-2;
+    const double b1 = 2.860e-6, b2 = 4.700e-8, b3 = 6.113e-8, b4 = 1.516e-4;
+    const double f = (T - 24.5) * (T + 570.82);
+    const double L2 = L * L, p = a3 + b3 * f;
+    return sqrt(a1 + b1 * f + (a2 + b2 * f) / (L2 - p * p) + (a4 + b4 * f) / (L2 - a5 * a5) - a6 * L2);
+}
+
 double shgo_sellmeier_d(double L, double T) { return shgo_sellmeier_any(L, T, 0); }
-static double shgo_sellmeier_s(double L, double T) { return shgo_sellmeier_any(L, T, 1); }
+/* n(L, T) of crystal SHG_CRYSTAL_* in double */
+double shgo_crystal_n(int crystal, double L, double T) {
+    return crystal == SHG_CRYSTAL_MGO_PPLN ? shgo_ppln(L, T) : shgo_sellmeier_any(L, T, 0);
+}
+static double shgo_crystal_n_s(int crystal, double L, double T) {
+    return crystal == SHG_CRYSTAL_MGO_PPLN ? shgo_ppln(L, T) : shgo_sellmeier_any(L, T, 1);
+}
 
 /* ---- double instantiation ---- */
 #define R double
 #define SFX(name) name##_f64
-#define SELLMEIER shgo_sellmeier_d
+#define SELLMEIER shgo_crystal_n
 #define COS cos
 #define SIN sin
 #define EXP exp
@@ -77,7 +95,7 @@ static double shgo_sellmeier_s(double L, double T) { return shgo_sellmeier_any(L
 /* ---- float instantiation (the reference's own precision, src/cuSHG.cu:7-8) ---- */
 #define R float
 #define SFX(name) name##_f32
-#define SELLMEIER shgo_sellmeier_s
+#define SELLMEIER shgo_crystal_n_s
 #define COS cosf
 #define SIN sinf
 #define EXP expf
@@ -166,7 +184,7 @@ int shgo_batch_plain(const shg_params* ps, int count, const int* steps, double* 
             optics_f32 o; optics_init_f32(&o, &c, c.temp);
             set_pump_f32(&c, c.temp, P);
             cwes_plain_f32(&c, &o, st, NULL, P, S);
-            if (sh_power) sh_power[i] = power_of_f32(&c, S, NULL, sellmeier_f32(c.ls, c.temp));
+            if (sh_power) sh_power[i] = power_of_f32(&c, S, NULL, sellmeier_f32(&c, c.ls, c.temp));
             optics_free_f32(&o); free(P); free(S);
         } else {
             cfg_f64 c; make_cfg_f64(p, &c);
@@ -175,7 +193,7 @@ int shgo_batch_plain(const shg_params* ps, int count, const int* steps, double* 
             optics_f64 o; optics_init_f64(&o, &c, c.temp);
             set_pump_f64(&c, c.temp, P);
             cwes_plain_f64(&c, &o, st, NULL, P, S);
-            if (sh_power) sh_power[i] = power_of_f64(&c, S, NULL, sellmeier_f64(c.ls, c.temp));
+            if (sh_power) sh_power[i] = power_of_f64(&c, S, NULL, sellmeier_f64(&c, c.ls, c.temp));
             optics_free_f64(&o); free(P); free(S);
         }
     }
@@ -228,5 +246,5 @@ void shgo_set_q(const shg_params* p, const double* T, const double* P, const dou
 
 double shgo_sh_power(const shg_params* p, const double* S, double temp) {
     cfg_f64 c; make_cfg_f64(p, &c);
-    return power_of_f64(&c, (const cpx_f64*)S, NULL, sellmeier_f64(c.ls, temp));
+    return power_of_f64(&c, (const cpx_f64*)S, NULL, sellmeier_f64(&c, c.ls, temp));
 }

@@ -48,12 +48,6 @@ static const R SFX(K_PI) = (R)3.14159265358979323846;
 static const R SFX(K_C) = (R)(299792458 * 1E6 / 1E12);
 static const R SFX(K_EPS0) = (R)(8.8541878128E-12 * 1E12 / 1E6);
 
-/* Sellmeier equation of MgO:sPPLT (Bruner et al.), Crystal.h:54-70, rounded
- * to real_t like the reference's n(L, T). */
-static R SFX(sellmeier)(R L, R T) {
-    return (R)SELLMEIER((double)L, (double)T);
-}
-
 typedef struct {
     int nx, ny, nz;
     R lx, ly, lz, dx, dy, dz;
@@ -62,7 +56,14 @@ typedef struct {
     R kappa, hconv;
     R power, waist, focus, temp, t_inf, t_peltier;
     R waist_y; /* <= 0 or == waist: round beam */
+    int crystal; /* SHG_CRYSTAL_* */
 } SFX(cfg);
+
+/* Extraordinary index of the run's crystal (sPPLT: Crystal.h:54-70), rounded to real_t like
+ * the reference's n(L, T). */
+static R SFX(sellmeier)(const SFX(cfg)* c, R L, R T) {
+    return (R)SELLMEIER(c->crystal, (double)L, (double)T);
+}
 
 /* Grid steps dx = LX/(NX-1) etc., Crystal.h:34-36; dQ = 2 deff/π, Crystal.h:41. */
 static void SFX(make_cfg)(const shg_params* p, SFX(cfg)* c) {
@@ -82,6 +83,7 @@ static void SFX(make_cfg)(const shg_params* p, SFX(cfg)* c) {
     c->power = (R)p->power; c->waist = (R)p->waist; c->focus = (R)p->focus;
     c->waist_y = (R)p->waist_y;
     c->temp = (R)p->temp; c->t_inf = (R)p->t_inf; c->t_peltier = (R)p->t_peltier;
+    c->crystal = p->crystal;
 }
 
 /* ------------------------------------------------------------------------- */
@@ -174,7 +176,7 @@ static void SFX(fft2)(const SFX(fftplan)* pl, CPX* a, int n, int inverse) {
  * uX = NX/2 (not (NX-1)/2), n at the temperature of voxel (NX/2, NY/2, 0). */
 static void SFX(set_pump)(const SFX(cfg)* c, R Tc, CPX* pump) {
     const R PI = SFX(K_PI);
-    R np = SFX(sellmeier)(c->lp, Tc);
+    R np = SFX(sellmeier)(c, c->lp, Tc);
     R uX = (R)0.5 * (R)c->nx, uY = (R)0.5 * (R)c->ny;
     R wX2 = c->waist * c->waist;
     R zRX = PI * np * wX2 / c->lp;
@@ -216,8 +218,8 @@ static void SFX(set_pump)(const SFX(cfg)* c, R Tc, CPX* pump) {
 static void SFX(set_propagators)(const SFX(cfg)* c, R Tc, CPX* prop_p, CPX* prop_s) {
     const R PI = SFX(K_PI);
     int nx = c->nx, ny = c->ny;
-    R kp = (R)2 * PI * SFX(sellmeier)(c->lp, Tc) / c->lp;
-    R ks = (R)2 * PI * SFX(sellmeier)(c->ls, Tc) / c->ls;
+    R kp = (R)2 * PI * SFX(sellmeier)(c, c->lp, Tc) / c->lp;
+    R ks = (R)2 * PI * SFX(sellmeier)(c, c->ls, Tc) / c->ls;
     R dfX = (R)1 / c->dx / (R)nx, dfY = (R)1 / c->dy / (R)ny;
     R uX = (R)0.5 * (R)nx, uY = (R)0.5 * (R)ny;
     R tp = TAN(c->rho_p), ts = TAN(c->rho_s);
@@ -236,12 +238,14 @@ static void SFX(set_propagators)(const SFX(cfg)* c, R Tc, CPX* prop_p, CPX* prop
 
 /* Phase mismatch at one temperature, kernelSetInicialDKConstant /
  * kernelSetInicialDKThermal (PhaseMatching.h:47-85), with the grating's
- * thermal expansion α = 2.2e-6, β = -5.9e-9. */
+ * thermal expansion: sPPLT α = 2.2e-6, β = -5.9e-9 (PhaseMatching.h:53,75);
+ * MgO:PPLN α = 1.54e-5, β = 5.3e-9 (lithium niobate). */
 static R SFX(delta_k)(const SFX(cfg)* c, R T) {
     const R PI = SFX(K_PI);
-    const R a = (R)2.2e-6, b = (R)-5.9e-9;
+    const int ln = c->crystal == SHG_CRYSTAL_MGO_PPLN;
+    const R a = ln ? (R)1.54e-5 : (R)2.2e-6, b = ln ? (R)5.3e-9 : (R)-5.9e-9;
     R d = T - (R)25.;
-    return (R)2 * PI * ((R)2 * SFX(sellmeier)(c->lp, T) / c->lp - SFX(sellmeier)(c->ls, T) / c->ls +
+    return (R)2 * PI * ((R)2 * SFX(sellmeier)(c, c->lp, T) / c->lp - SFX(sellmeier)(c, c->ls, T) / c->ls +
                         (R)1 / (c->Lambda * ((R)1. + a * d + b * (d * d))));
 }
 
@@ -323,7 +327,7 @@ static void SFX(rk4_thermal)(const SFX(cfg)* c, const R* T, const R* dkint, int 
     const R* Ts = T + (size_t)s * n;
 #pragma omp parallel for schedule(static) if (shgo_threads > 1) num_threads(shgo_threads)
     for (int i = 0; i < n; ++i) {
-        SFX(pointc) k = SFX(point_consts)(c, SFX(sellmeier)(c->lp, Ts[i]), SFX(sellmeier)(c->ls, Ts[i]), 1);
+        SFX(pointc) k = SFX(point_consts)(c, SFX(sellmeier)(c, c->lp, Ts[i]), SFX(sellmeier)(c, c->ls, Ts[i]), 1);
         SFX(rk4_point)(c, &k, dkint[i] * a0 / b, dkint[i] * a1 / b, dkint[i] * a2 / b, &P[i], &S[i]);
     }
 }
@@ -464,7 +468,7 @@ static void SFX(set_q)(const SFX(cfg)* c, const R* T, const CPX* P, const CPX* S
     R* Qs = Q + (size_t)s * n;
     const R C0 = SFX(K_C), E0 = SFX(K_EPS0);
     for (int i = 0; i < n; ++i) {
-        R np = SFX(sellmeier)(c->lp, Ts[i]), ns = SFX(sellmeier)(c->ls, Ts[i]);
+        R np = SFX(sellmeier)(c, c->lp, Ts[i]), ns = SFX(sellmeier)(c, c->ls, Ts[i]);
         R Is = (R)0.5 * C0 * E0 * ns * SFX(abs2)(S[i]);
         Qs[i] = c->alpha_p * (R)0.5 * C0 * E0 * np * SFX(abs2)(P[i]) + c->alpha_s * (R)0.5 * C0 * E0 * ns * SFX(abs2)(S[i]) +
                 c->beta_s * (Is * Is);
@@ -502,7 +506,7 @@ static void SFX(ssfm_plain)(const SFX(optics)* o, const SFX(pointc)* k, R dk, R 
 
 /* Plain CWES: nsteps steps from z = 0, z accumulated as z += dz (Solver.h:303). */
 static void SFX(cwes_plain)(const SFX(cfg)* c, const SFX(optics)* o, int nsteps, const double* poling, CPX* P, CPX* S) {
-    SFX(pointc) k = SFX(point_consts)(c, SFX(sellmeier)(c->lp, c->temp), SFX(sellmeier)(c->ls, c->temp), 0);
+    SFX(pointc) k = SFX(point_consts)(c, SFX(sellmeier)(c, c->lp, c->temp), SFX(sellmeier)(c, c->ls, c->temp), 0);
     R dk = SFX(delta_k)(c, c->temp);
     R z = (R)0.0;
     for (int s = 0; s < nsteps; ++s) {
@@ -538,8 +542,8 @@ static int SFX(solve_plain)(const shg_params* p, const R* signal_in, const doubl
     if (signal_out) memcpy(signal_out, S, sizeof(CPX) * n);
     if (st) {
         memset(st, 0, sizeof(*st));
-        st->sh_power = SFX(power_of)(&c, S, NULL, SFX(sellmeier)(c.ls, c.temp));
-        st->pump_power = SFX(power_of)(&c, P, NULL, SFX(sellmeier)(c.lp, c.temp));
+        st->sh_power = SFX(power_of)(&c, S, NULL, SFX(sellmeier)(&c, c.ls, c.temp));
+        st->pump_power = SFX(power_of)(&c, P, NULL, SFX(sellmeier)(&c, c.lp, c.temp));
         st->steps = steps;
         st->outer_iterations = 1;
     }
@@ -639,7 +643,7 @@ static int SFX(solve_thermal)(const shg_params* p, const R* signal_in, R* pump_o
     if (st) {
         memset(st, 0, sizeof(*st));
         const R* Tl = Tf + (size_t)(nz - 1) * n;
-        for (size_t i = 0; i < n; ++i) { nsmap[i] = SFX(sellmeier)(c.ls, Tl[i]); npmap[i] = SFX(sellmeier)(c.lp, Tl[i]); }
+        for (size_t i = 0; i < n; ++i) { nsmap[i] = SFX(sellmeier)(&c, c.ls, Tl[i]); npmap[i] = SFX(sellmeier)(&c, c.lp, Tl[i]); }
         st->sh_power = SFX(power_of)(&c, Sout, nsmap, 0);
         st->pump_power = SFX(power_of)(&c, Pout, npmap, 0);
         st->jacobi_sweeps = total_sweeps;

@@ -28,6 +28,13 @@ template <typename T> __device__ __forceinline__ cx<T> mulc(cx<T> a, cx<T> b) {
 }
 template <typename T> __device__ __forceinline__ cx<T> scale(cx<T> a, T s) { return mk<T>(a.x * s, a.y * s); }
 
+// FP32 complex add / sub as one packed two-lane instruction each (sm_100 f32x2).  Both
+// lanes round to nearest like the scalar pair; a - b is fma(b, -1, a), exact in the product.
+template <> __device__ __forceinline__ float2 add<float>(float2 a, float2 b) { return __fadd2_rn(a, b); }
+template <> __device__ __forceinline__ float2 sub<float>(float2 a, float2 b) {
+    return __ffma2_rn(b, make_float2(-1.f, -1.f), a);
+}
+
 // cos / sin of 2π m / 16 and 2π m / 12 as literals (m in [0, M)).
 __host__ __device__ constexpr double cos16(int m) {
     return m == 0 ? 1.0 : m == 1 ? 0.923879532511286756128 : m == 2 ? 0.707106781186547524401

@@ -53,9 +53,11 @@ struct PlainCfg {
     // dynamic shared memory: P, S planes, twiddles + 4 propagator vectors (multiplier
     // tables), 2x6 coefficients, reduction scratch
     // (thermal: plus the running Δk prefix of this CTA's points, FP64)
+    // (plain FP32: plus the packed RK4 stage constants, 2 steps x 3 phases of Rk4Pack)
     static constexpr size_t smem_bytes = sizeof(cx<T>) * (2 * (size_t)PLANE + 12) + sizeof(mult<T>) * 5 * (size_t)N +
                                          sizeof(double) * (2 * (NT / 32) + 4) +
-                                         (THERM ? sizeof(double) * (size_t)PLANE : 0);
+                                         (THERM ? sizeof(double) * (size_t)PLANE
+                                                : (sizeof(T) == 4 ? 6 * sizeof(float2) * 6 : 0));
 };
 
 // physical offset of logical position p of local row lr
@@ -101,6 +103,85 @@ __device__ __forceinline__ void rk4_point(cx<T>& P, cx<T>& S, const cx<T>* cf, T
     as = add<T>(as, ks);
     P = mk<T>(p.x + ap.x * dz6, p.y + ap.y * dz6);
     S = mk<T>(s.x + as.x * dz6, s.y + as.y * dz6);
+}
+
+// Two points of the FP32 RK4 at once in packed two-lane arithmetic (sm_100 f32x2): the real
+// parts of the two points share one register pair, the imaginary parts another, and each
+// packed instruction does the work of two scalar ones.  The per-phase stage constants are
+// held with each value in both lanes (Rk4Pack, written by stage_pack).  The operations and
+// their order are those of dadz / rk4_point; only where the compiler would choose to fuse
+// a multiply into an add is fixed here.
+struct Cx2 {
+    float2 r, i;
+};
+struct Rk4Pack {
+    float2 cpr, cpi, ncpi, csr, csi, ncsi;  // cP, cS and the negated imaginary parts
+};
+
+__device__ __forceinline__ float2 bc2(float v) { return make_float2(v, v); }
+
+__device__ __forceinline__ void dadz_pair(const Cx2& p, const Cx2& s, const Rk4Pack& k, float2 nhap, float2 nhas,
+                                          float2 nqs, Cx2& dp, Cx2& ds) {
+    const float2 npi = __fmul2_rn(bc2(-1.f), p.i);
+    // sp = s conj(p)
+    const float2 spr = __ffma2_rn(s.i, p.i, __fmul2_rn(s.r, p.r));
+    const float2 spi = __ffma2_rn(s.r, npi, __fmul2_rn(s.i, p.r));
+    // dP = cP sp - 0.5 αp P
+    const float2 tpr = __ffma2_rn(k.ncpi, spi, __fmul2_rn(k.cpr, spr));
+    const float2 tpi = __ffma2_rn(k.cpi, spr, __fmul2_rn(k.cpr, spi));
+    dp.r = __ffma2_rn(nhap, p.r, tpr);
+    dp.i = __ffma2_rn(nhap, p.i, tpi);
+    // pp = P^2
+    const float2 ppr = __ffma2_rn(p.i, npi, __fmul2_rn(p.r, p.r));
+    const float2 ppi = __fmul2_rn(__fadd2_rn(p.r, p.r), p.i);
+    // dS = cS pp - (0.5 αs + qs |S|^2) S
+    const float2 tsr = __ffma2_rn(k.ncsi, ppi, __fmul2_rn(k.csr, ppr));
+    const float2 tsi = __ffma2_rn(k.csi, ppr, __fmul2_rn(k.csr, ppi));
+    const float2 ng = __ffma2_rn(nqs, __ffma2_rn(s.i, s.i, __fmul2_rn(s.r, s.r)), nhas);
+    ds.r = __ffma2_rn(ng, s.r, tsr);
+    ds.i = __ffma2_rn(ng, s.i, tsi);
+}
+
+// rk4_point for two points; k[0..2]: the stage phases z, z + dz/4, z + dz/2
+__device__ __forceinline__ void rk4_pair(Cx2& P, Cx2& S, const Rk4Pack* k, float2 nhap, float2 nhas, float2 nqs,
+                                         float2 dz6) {
+    const float2 half = bc2(0.5f), two = bc2(2.f);
+    const Cx2 p = P, s = S;
+    Cx2 kp, ks, ap, as, xp, xs;
+    dadz_pair(p, s, k[0], nhap, nhas, nqs, kp, ks);
+    ap = kp;
+    as = ks;
+#pragma unroll
+    for (int st = 0; st < 2; ++st) {
+        xp.r = __ffma2_rn(half, kp.r, p.r);
+        xp.i = __ffma2_rn(half, kp.i, p.i);
+        xs.r = __ffma2_rn(half, ks.r, s.r);
+        xs.i = __ffma2_rn(half, ks.i, s.i);
+        dadz_pair(xp, xs, k[1], nhap, nhas, nqs, kp, ks);
+        ap.r = __ffma2_rn(two, kp.r, ap.r);
+        ap.i = __ffma2_rn(two, kp.i, ap.i);
+        as.r = __ffma2_rn(two, ks.r, as.r);
+        as.i = __ffma2_rn(two, ks.i, as.i);
+    }
+    xp.r = __fadd2_rn(p.r, kp.r);
+    xp.i = __fadd2_rn(p.i, kp.i);
+    xs.r = __fadd2_rn(s.r, ks.r);
+    xs.i = __fadd2_rn(s.i, ks.i);
+    dadz_pair(xp, xs, k[2], nhap, nhas, nqs, kp, ks);
+    ap.r = __fadd2_rn(ap.r, kp.r);
+    ap.i = __fadd2_rn(ap.i, kp.i);
+    as.r = __fadd2_rn(as.r, ks.r);
+    as.i = __fadd2_rn(as.i, ks.i);
+    P.r = __ffma2_rn(ap.r, dz6, p.r);
+    P.i = __ffma2_rn(ap.i, dz6, p.i);
+    S.r = __ffma2_rn(as.r, dz6, s.r);
+    S.i = __ffma2_rn(as.i, dz6, s.i);
+}
+
+// the packed constants of phase j from the scalar ones (cf[j] = cP, cf[3 + j] = cS)
+__device__ __forceinline__ void stage_pack(const float2* cf, int j, Rk4Pack* kp) {
+    const float2 cp = cf[j], cs = cf[3 + j];
+    kp[j] = Rk4Pack{bc2(cp.x), bc2(cp.y), bc2(-cp.y), bc2(cs.x), bc2(cs.y), bc2(-cs.y)};
 }
 
 // stage coefficients of the plain dAdz of step s at position z: phases (z + dz*{0, 1/4,
@@ -276,6 +357,9 @@ __global__ void __launch_bounds__(NT, MINB)
     W* pys = pyp + N;            // SH   propagator, y factor
     double* red = reinterpret_cast<double*>(pys + N);  // [2*(NT/32)] + [4]
     double* dkint = red + 2 * (NT / 32) + 4;           // thermal: [RL*N] running Δk prefix
+    // plain FP32: packed RK4 stage constants [2][3], in the place of the thermal prefix
+    Rk4Pack* kpk = reinterpret_cast<Rk4Pack*>(dkint);
+    constexpr bool PACK = !THERM && sizeof(T) == 4;
 
     const int tid = threadIdx.x;
     const int crank = (C > 1) ? (int)cg::this_cluster().block_rank() : 0;
@@ -305,7 +389,10 @@ __global__ void __launch_bounds__(NT, MINB)
 
         // ---- tables -----------------------------------------------------------------
         init_tables<T, N>(d, tw, pxp, pxs, pyp, pys, tid, NT);
-        if (!THERM && tid < 3) stage_coef<T>(d, 0, 0.0, tid, coef);
+        if (!THERM && tid < 3) {
+            stage_coef<T>(d, 0, 0.0, tid, coef);
+            if constexpr (PACK) stage_pack(coef, tid, kpk);
+        }
 
         // ---- initial fields: setPump (Efields.h:84-119), SH = 0 or given ---------------
         const V* sin_g = reinterpret_cast<const V*>(d.signal_in);
@@ -343,8 +430,41 @@ __global__ void __launch_bounds__(NT, MINB)
                 for (int ph = 0; ph < 5; ++ph) {
                     if (ph == 2) {
                         // pointwise: the two RK4 applications around the step boundary (the second
-                        // half of step s, then the first half of step s+1); two points interleaved
-                        // for instruction-level parallelism (about 1 % faster at 128-256)
+                        // half of step s, then the first half of step s+1)
+                        if constexpr (PACK) {
+                            if (mode == 1 && s + 1 >= d.nslices) {
+                                // a middle step that records nothing: two points at a time in
+                                // packed arithmetic
+                                const Rk4Pack* kprev = kpk + 3 * (s & 1);
+                                const Rk4Pack* knext = kpk + 3 * ((s + 1) & 1);
+                                const float2 nhap = bc2(-hap), nhas = bc2(-has), nqs = bc2(-qs), dzz = bc2(dz6);
+#pragma unroll 1
+                                for (int k = 0; k + 1 < R2; k += 2) {
+                                    const int o0 = sidx<N, R2, SW>(lr, n1 + 16 * k);
+                                    const int o1 = sidx<N, R2, SW>(lr, n1 + 16 * k + 16);
+                                    const V p0 = Ps[o0], q0 = Ss[o0], p1 = Ps[o1], q1 = Ss[o1];
+                                    Cx2 P{make_float2(p0.x, p1.x), make_float2(p0.y, p1.y)};
+                                    Cx2 S{make_float2(q0.x, q1.x), make_float2(q0.y, q1.y)};
+                                    rk4_pair(P, S, kprev, nhap, nhas, nqs, dzz);
+                                    rk4_pair(P, S, knext, nhap, nhas, nqs, dzz);
+                                    Ps[o0] = make_float2(P.r.x, P.i.x);
+                                    Ps[o1] = make_float2(P.r.y, P.i.y);
+                                    Ss[o0] = make_float2(S.r.x, S.i.x);
+                                    Ss[o1] = make_float2(S.r.y, S.i.y);
+                                }
+                                if constexpr (R2 & 1) {
+                                    const int o = sidx<N, R2, SW>(lr, n1 + 16 * (R2 - 1));
+                                    V p = Ps[o], q = Ss[o];
+                                    rk4_point<T>(p, q, cf_prev, hap, has, qs, dz6);
+                                    rk4_point<T>(p, q, cf_next, hap, has, qs, dz6);
+                                    Ps[o] = p;
+                                    Ss[o] = q;
+                                }
+                                continue;
+                            }
+                        }
+                        // otherwise point by point, two interleaved for instruction-level
+                        // parallelism
 #pragma unroll 2
                         for (int k = 0; k < R2; ++k) {
                             const int x = n1 + 16 * k;
@@ -493,7 +613,10 @@ __global__ void __launch_bounds__(NT, MINB)
             __syncthreads();
             pass_ca(false);
             cluster_sync();
-            if (!THERM && tid < 3 && s + 1 < nsteps) stage_coef<T>(d, s + 1, z + d.dz, tid, cf_nxt);
+            if (!THERM && tid < 3 && s + 1 < nsteps) {
+                stage_coef<T>(d, s + 1, z + d.dz, tid, cf_nxt);
+                if constexpr (PACK) stage_pack(cf_nxt, tid, kpk + 3 * ((s + 1) & 1));
+            }
             pass_cb();
             cluster_sync();
             pass_ca(true);

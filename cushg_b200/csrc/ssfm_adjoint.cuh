@@ -142,6 +142,113 @@ __device__ __forceinline__ void rk4_vjp(cx<T> p, cx<T> s, const cx<T>* cf, T hap
     gs = add<T>(gs, hs);
 }
 
+// dadz_vjp for two points at once in packed FP32 (see rk4_pair): the same terms, lane 0 the
+// first point and lane 1 the second; the five sensitivities are accumulated per lane.
+// Constant pairs: nhap = -hap, nhas = -has, nqs = -qs, n2qs = -2 qs, inc in both lanes.
+__device__ __forceinline__ void dadz_vjp_pair(const Cx2& p, const Cx2& s, const Rk4Pack& K, float2 nhap, float2 nhas,
+                                              float2 nqs, float2 n2qs, const Cx2& gdp, const Cx2& gds, Cx2& gp,
+                                              Cx2& gs, float2 inc, float2* sens) {
+    const float2 m1 = bc2(-1.f), two = bc2(2.f);
+    const float2 npi = __fmul2_rn(m1, p.i), nsi = __fmul2_rn(m1, s.i);
+    const float2 ngdpi = __fmul2_rn(m1, gdp.i), ngdsr = __fmul2_rn(m1, gds.r), ngdsi = __fmul2_rn(m1, gds.i);
+    // t = cP s conj(p)
+    const float2 spr = __ffma2_rn(s.i, p.i, __fmul2_rn(s.r, p.r));
+    const float2 spi = __ffma2_rn(s.r, npi, __fmul2_rn(s.i, p.r));
+    const float2 tr = __ffma2_rn(K.ncpi, spi, __fmul2_rn(K.cpr, spr));
+    const float2 ti = __ffma2_rn(K.cpi, spr, __fmul2_rn(K.cpr, spi));
+    // u = cS p^2
+    const float2 ppr = __ffma2_rn(p.i, npi, __fmul2_rn(p.r, p.r));
+    const float2 ppi = __fmul2_rn(__fadd2_rn(p.r, p.r), p.i);
+    const float2 ur = __ffma2_rn(K.ncsi, ppi, __fmul2_rn(K.csr, ppr));
+    const float2 ui = __ffma2_rn(K.csi, ppr, __fmul2_rn(K.csr, ppi));
+    const float2 a2 = __ffma2_rn(s.i, s.i, __fmul2_rn(s.r, s.r));
+    // g_p += -hap g_dP + (cP s) conj(g_dP) + 2 g_dS conj(cS p)
+    const float2 cps_r = __ffma2_rn(K.ncpi, s.i, __fmul2_rn(K.cpr, s.r));
+    const float2 cps_i = __ffma2_rn(K.cpi, s.r, __fmul2_rn(K.cpr, s.i));
+    const float2 ar = __ffma2_rn(cps_i, gdp.i, __fmul2_rn(cps_r, gdp.r));
+    const float2 ai = __ffma2_rn(cps_r, ngdpi, __fmul2_rn(cps_i, gdp.r));
+    const float2 csp_r = __ffma2_rn(K.ncsi, p.i, __fmul2_rn(K.csr, p.r));
+    const float2 csp_i = __ffma2_rn(K.csi, p.r, __fmul2_rn(K.csr, p.i));
+    const float2 br = __ffma2_rn(gds.i, csp_i, __fmul2_rn(gds.r, csp_r));
+    const float2 bi = __ffma2_rn(ngdsr, csp_i, __fmul2_rn(gds.i, csp_r));
+    gp.r = __ffma2_rn(two, br, __fadd2_rn(__ffma2_rn(nhap, gdp.r, gp.r), ar));
+    gp.i = __ffma2_rn(two, bi, __fadd2_rn(__ffma2_rn(nhap, gdp.i, gp.i), ai));
+    // g_s += (p conj(cP)) g_dP + (-has - 2 qs |s|^2) g_dS - qs s^2 conj(g_dS)
+    const float2 pcc_r = __ffma2_rn(p.i, K.cpi, __fmul2_rn(p.r, K.cpr));
+    const float2 pcc_i = __ffma2_rn(p.r, K.ncpi, __fmul2_rn(p.i, K.cpr));
+    const float2 cr = __ffma2_rn(pcc_i, ngdpi, __fmul2_rn(pcc_r, gdp.r));
+    const float2 ci = __ffma2_rn(pcc_i, gdp.r, __fmul2_rn(pcc_r, gdp.i));
+    const float2 ssr = __ffma2_rn(s.i, nsi, __fmul2_rn(s.r, s.r));
+    const float2 ssi = __fmul2_rn(__fadd2_rn(s.r, s.r), s.i);
+    const float2 er = __ffma2_rn(ssi, gds.i, __fmul2_rn(ssr, gds.r));
+    const float2 ei = __ffma2_rn(ssr, ngdsi, __fmul2_rn(ssi, gds.r));
+    const float2 h = __ffma2_rn(n2qs, a2, nhas);
+    gs.r = __ffma2_rn(nqs, er, __ffma2_rn(h, gds.r, __fadd2_rn(gs.r, cr)));
+    gs.i = __ffma2_rn(nqs, ei, __ffma2_rn(h, gds.i, __fadd2_rn(gs.i, ci)));
+    // sensitivities
+    const float2 e1 = __ffma2_rn(ngdpi, tr, __fmul2_rn(gdp.r, ti));
+    const float2 e2 = __ffma2_rn(ngdsi, ur, __fmul2_rn(gds.r, ui));
+    const float2 eph = __ffma2_rn(m1, e2, e1);
+    sens[0] = __fadd2_rn(sens[0], __ffma2_rn(gdp.i, ti, __fmul2_rn(gdp.r, tr)));
+    sens[1] = __fadd2_rn(sens[1], __ffma2_rn(gds.i, ui, __fmul2_rn(gds.r, ur)));
+    sens[2] = __ffma2_rn(eph, inc, sens[2]);
+    sens[3] = __ffma2_rn(__fmul2_rn(m1, a2), __ffma2_rn(gds.i, s.i, __fmul2_rn(gds.r, s.r)), sens[3]);
+    sens[4] = __fadd2_rn(sens[4], eph);
+}
+
+// rk4_vjp for two points at once in packed FP32; k[0..2] the stage phases (see rk4_pair)
+__device__ __forceinline__ void rk4_vjp_pair(const Cx2& p, const Cx2& s, const Rk4Pack* k, float2 nhap, float2 nhas,
+                                             float2 nqs, float2 n2qs, float2 dz6, Cx2& gp, Cx2& gs, float2* sens) {
+    const float2 half = bc2(0.5f), z0 = bc2(0.f);
+    auto axpy = [](float2 a, const Cx2& x, const Cx2& y) {  // a x + y
+        return Cx2{__ffma2_rn(a, x.r, y.r), __ffma2_rn(a, x.i, y.i)};
+    };
+    auto sum = [](const Cx2& x, const Cx2& y) { return Cx2{__fadd2_rn(x.r, y.r), __fadd2_rn(x.i, y.i)}; };
+    auto scl = [](const Cx2& x, float2 a) { return Cx2{__fmul2_rn(x.r, a), __fmul2_rn(x.i, a)}; };
+    Cx2 k1p, k1s, k2p, k2s, k3p, k3s;
+    dadz_pair(p, s, k[0], nhap, nhas, nqs, k1p, k1s);
+    const Cx2 u2p = axpy(half, k1p, p), u2s = axpy(half, k1s, s);
+    dadz_pair(u2p, u2s, k[1], nhap, nhas, nqs, k2p, k2s);
+    const Cx2 u3p = axpy(half, k2p, p), u3s = axpy(half, k2s, s);
+    dadz_pair(u3p, u3s, k[1], nhap, nhas, nqs, k3p, k3s);
+    const Cx2 u4p = sum(p, k3p), u4s = sum(s, k3s);
+    const Cx2 gop = gp, gos = gs;
+    const float2 dz3 = __fadd2_rn(dz6, dz6);
+    Cx2 g3p = scl(gop, dz3), g3s = scl(gos, dz3);
+    Cx2 g2p = g3p, g2s = g3s;
+    Cx2 g1p = scl(gop, dz6), g1s = scl(gos, dz6);
+    Cx2 hp{z0, z0}, hs{z0, z0};
+    dadz_vjp_pair(u4p, u4s, k[2], nhap, nhas, nqs, n2qs, g1p, g1s, hp, hs, bc2(0.5f), sens);  // g_k4 = dz6 g
+    gp = sum(gop, hp);
+    gs = sum(gos, hs);
+    g3p = sum(g3p, hp);
+    g3s = sum(g3s, hs);
+    hp = Cx2{z0, z0};
+    hs = Cx2{z0, z0};
+    dadz_vjp_pair(u3p, u3s, k[1], nhap, nhas, nqs, n2qs, g3p, g3s, hp, hs, bc2(0.25f), sens);
+    gp = sum(gp, hp);
+    gs = sum(gs, hs);
+    g2p = axpy(half, hp, g2p);
+    g2s = axpy(half, hs, g2s);
+    hp = Cx2{z0, z0};
+    hs = Cx2{z0, z0};
+    dadz_vjp_pair(u2p, u2s, k[1], nhap, nhas, nqs, n2qs, g2p, g2s, hp, hs, bc2(0.25f), sens);
+    gp = sum(gp, hp);
+    gs = sum(gs, hs);
+    g1p = axpy(half, hp, g1p);
+    g1s = axpy(half, hs, g1s);
+    hp = Cx2{z0, z0};
+    hs = Cx2{z0, z0};
+    dadz_vjp_pair(p, s, k[0], nhap, nhas, nqs, n2qs, g1p, g1s, hp, hs, z0, sens);
+    gp = sum(gp, hp);
+    gs = sum(gs, hs);
+}
+
+// (a0, a1), (b0, b1) of two complex values as one packed pair and back
+__device__ __forceinline__ Cx2 pack2(float2 a, float2 b) { return Cx2{make_float2(a.x, b.x), make_float2(a.y, b.y)}; }
+__device__ __forceinline__ float2 lane0(const Cx2& v) { return make_float2(v.r.x, v.i.x); }
+__device__ __forceinline__ float2 lane1(const Cx2& v) { return make_float2(v.r.y, v.i.y); }
+
 template <typename T, int N, int C, int NT>
 __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __restrict__ descs,
                                                              const AdjDesc* __restrict__ adescs, int phase,
@@ -164,6 +271,10 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
     W* pyp = pxs + N;
     W* pys = pyp + N;
     double* red = reinterpret_cast<double*>(pys + N);  // [2*(NT/32)] + [4]
+    // FP32: the packed RK4 stage constants [2][3] by step parity (after the reduction area)
+    Rk4Pack* kpk = reinterpret_cast<Rk4Pack*>(red + 2 * (NT / 32) + 4);
+    constexpr bool PACK = sizeof(T) == 4;
+    constexpr int KP = PACK ? (R2 & ~1) : 0;  // points of a job that go in packed pairs
 
     const int tid = threadIdx.x;
     const int crank = (C > 1) ? (int)cg::this_cluster().block_rank() : 0;
@@ -359,8 +470,14 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
     };
 
     auto coefs = [&](int s) {  // stage coefficients of step s into its parity slot
-        if (tid < 3) stage_coef<T>(d, s, a.zs[s], tid, coef + 6 * (s & 1));
+        if (tid < 3) {
+            stage_coef<T>(d, s, a.zs[s], tid, coef + 6 * (s & 1));
+            if constexpr (PACK) stage_pack(coef + 6 * (s & 1), tid, kpk + 3 * (s & 1));
+        }
     };
+    // the per-instance constants in both lanes (FP32)
+    const float2 nhap2 = bc2(-(float)hap), nhas2 = bc2(-(float)has), nqs2 = bc2(-(float)qs);
+    const float2 n2qs2 = bc2(-2.f * (float)qs), dz62 = bc2((float)dz6);
 
     // ---- forward march over steps [sb, se) from the fields in shared memory ------------
     // ckpt_mode: keep x_{mK} as checkpoints.  Steps s >= seg_from keep x_s, a2_s and their
@@ -376,8 +493,20 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
         // first half of step sb, forward row stage
         for (int j = tid; j < JA; j += NT) {
             const int n1 = j & 15, lr = j >> 4;
+            if constexpr (PACK) {
 #pragma unroll 1
-            for (int k = 0; k < R2; ++k) {
+                for (int k = 0; k < KP; k += 2) {
+                    const int o0 = sidx<N, R2, SW>(lr, n1 + 16 * k), o1 = sidx<N, R2, SW>(lr, n1 + 16 * k + 16);
+                    Cx2 P = pack2(Ps[o0], Ps[o1]), S = pack2(Ss[o0], Ss[o1]);
+                    rk4_pair(P, S, kpk + 3 * (sb & 1), nhap2, nhas2, nqs2, dz62);
+                    Ps[o0] = lane0(P);
+                    Ps[o1] = lane1(P);
+                    Ss[o0] = lane0(S);
+                    Ss[o1] = lane1(S);
+                }
+            }
+#pragma unroll 1
+            for (int k = KP; k < R2; ++k) {
                 const int o = sidx<N, R2, SW>(lr, n1 + 16 * k);
                 V p = Ps[o], q = Ss[o];
                 rk4_point<T>(p, q, coef + 6 * (sb & 1), hap, has, qs, dz6);
@@ -406,8 +535,57 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
                 const int n1 = j & 15, lr = j >> 4;
 #pragma unroll 1
                 for (int f = 0; f < 2; ++f) row_a(f ? Ss : Ps, lr, n1, true);
+                if constexpr (PACK) {
+                    // the loop below for points k and k + 1 at once
 #pragma unroll 1
-                for (int k = 0; k < R2; ++k) {
+                    for (int k = 0; k < KP; k += 2) {
+                        const int x = n1 + 16 * k;
+                        const int o0 = sidx<N, R2, SW>(lr, x), o1 = sidx<N, R2, SW>(lr, x + 16);
+                        const size_t g0 = (size_t)(crank + C * lr) * N + x, g1 = g0 + 16;
+                        const V p0 = Ps[o0], q0 = Ss[o0], p1 = Ps[o1], q1 = Ss[o1];
+                        if (keep) {
+                            const size_t b = (size_t)(s - seg_from) * 2 * NN;
+                            seg_a2[b + g0] = p0;
+                            seg_a2[b + g1] = p1;
+                            seg_a2[b + NN + g0] = q0;
+                            seg_a2[b + NN + g1] = q1;
+                        }
+                        if (last && !seed) continue;
+                        Cx2 P = pack2(p0, p1), S = pack2(q0, q1);
+                        rk4_pair(P, S, kpk + 3 * (s & 1), nhap2, nhas2, nqs2, dz62);  // x_{s+1}
+                        if (s + 1 == nsteps) {
+                            const V e0 = lane0(S), e1 = lane1(S);
+                            acc_j += (double)e0.x * e0.x + (double)e0.y * e0.y;
+                            acc_j += (double)e1.x * e1.x + (double)e1.y * e1.y;
+                            Ps[o0] = mk<T>(0, 0);
+                            Ps[o1] = mk<T>(0, 0);
+                            Ss[o0] = mk<T>((T)(2.0 * d.pw_s * e0.x), (T)(2.0 * d.pw_s * e0.y));
+                            Ss[o1] = mk<T>((T)(2.0 * d.pw_s * e1.x), (T)(2.0 * d.pw_s * e1.y));
+                            continue;
+                        }
+                        if (ckpt_mode && (s + 1) % K == 0) {
+                            const size_t b = (size_t)((s + 1) / K) * 2 * NN;
+                            ckpt[b + g0] = lane0(P);
+                            ckpt[b + g1] = lane1(P);
+                            ckpt[b + NN + g0] = lane0(S);
+                            ckpt[b + NN + g1] = lane1(S);
+                        }
+                        if (s + 1 >= seg_from) {
+                            const size_t b = (size_t)(s + 1 - seg_from) * 2 * NN;
+                            seg_x[b + g0] = lane0(P);
+                            seg_x[b + g1] = lane1(P);
+                            seg_x[b + NN + g0] = lane0(S);
+                            seg_x[b + NN + g1] = lane1(S);
+                        }
+                        rk4_pair(P, S, kpk + 3 * ((s + 1) & 1), nhap2, nhas2, nqs2, dz62);
+                        Ps[o0] = lane0(P);
+                        Ps[o1] = lane1(P);
+                        Ss[o0] = lane0(S);
+                        Ss[o1] = lane1(S);
+                    }
+                }
+#pragma unroll 1
+                for (int k = KP; k < R2; ++k) {
                     const int x = n1 + 16 * k;
                     const int o = sidx<N, R2, SW>(lr, x);
                     const size_t g = (size_t)(crank + C * lr) * N + x;
@@ -479,8 +657,28 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
         for (int j = tid; j < JA; j += NT) {
             const int n1 = j & 15, lr = j >> 4;
             T sn[5] = {0, 0, 0, 0, 0};
+            if constexpr (PACK) {
+                float2 sp[5] = {bc2(0.f), bc2(0.f), bc2(0.f), bc2(0.f), bc2(0.f)};
 #pragma unroll 1
-            for (int k = 0; k < R2; ++k) {
+                for (int k = 0; k < KP; k += 2) {
+                    const int x = n1 + 16 * k;
+                    const int o0 = sidx<N, R2, SW>(lr, x), o1 = sidx<N, R2, SW>(lr, x + 16);
+                    const size_t g0 = (size_t)(crank + C * lr) * N + x, g1 = g0 + 16;
+                    const size_t sl = (size_t)(se - 1 - sb) * 2;
+                    Cx2 gp = pack2(Ps[o0], Ps[o1]), gs = pack2(Ss[o0], Ss[o1]);
+                    rk4_vjp_pair(pack2(seg_a2[sl * NN + g0], seg_a2[sl * NN + g1]),
+                                 pack2(seg_a2[(sl + 1) * NN + g0], seg_a2[(sl + 1) * NN + g1]),
+                                 kpk + 3 * ((se - 1) & 1), nhap2, nhas2, nqs2, n2qs2, dz62, gp, gs, sp);
+                    Ps[o0] = lane0(gp);
+                    Ps[o1] = lane1(gp);
+                    Ss[o0] = lane0(gs);
+                    Ss[o1] = lane1(gs);
+                }
+#pragma unroll
+                for (int i = 0; i < 5; ++i) sn[i] = sp[i].x + sp[i].y;
+            }
+#pragma unroll 1
+            for (int k = KP; k < R2; ++k) {
                 const int x = n1 + 16 * k;
                 const int o = sidx<N, R2, SW>(lr, x);
                 const size_t g = (size_t)(crank + C * lr) * N + x;
@@ -514,8 +712,39 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
                 T sn[5] = {0, 0, 0, 0, 0}, sn2[5] = {0, 0, 0, 0, 0};  // step s, step s-1
 #pragma unroll 1
                 for (int f = 0; f < 2; ++f) row_a(f ? Ss : Ps, lr, n1, true);
+                if constexpr (PACK) {
+                    // the loop below for points k and k + 1 at once
+                    float2 sp[5] = {bc2(0.f), bc2(0.f), bc2(0.f), bc2(0.f), bc2(0.f)};
+                    float2 sp2[5] = {bc2(0.f), bc2(0.f), bc2(0.f), bc2(0.f), bc2(0.f)};
 #pragma unroll 1
-                for (int k = 0; k < R2; ++k) {
+                    for (int k = 0; k < KP; k += 2) {
+                        const int x = n1 + 16 * k;
+                        const int o0 = sidx<N, R2, SW>(lr, x), o1 = sidx<N, R2, SW>(lr, x + 16);
+                        const size_t g0 = (size_t)(crank + C * lr) * N + x, g1 = g0 + 16;
+                        Cx2 gp = pack2(Ps[o0], Ps[o1]), gs = pack2(Ss[o0], Ss[o1]);
+                        const size_t sx_ = (size_t)(s - sb) * 2;
+                        const Cx2 xp = pack2(seg_x[sx_ * NN + g0], seg_x[sx_ * NN + g1]);
+                        const Cx2 xs = pack2(seg_x[(sx_ + 1) * NN + g0], seg_x[(sx_ + 1) * NN + g1]);
+                        rk4_vjp_pair(xp, xs, kpk + 3 * (s & 1), nhap2, nhas2, nqs2, n2qs2, dz62, gp, gs, sp);
+                        if (s > sb) {
+                            const size_t sl = (size_t)(s - 1 - sb) * 2;
+                            const Cx2 bp = pack2(seg_a2[sl * NN + g0], seg_a2[sl * NN + g1]);
+                            const Cx2 bs = pack2(seg_a2[(sl + 1) * NN + g0], seg_a2[(sl + 1) * NN + g1]);
+                            rk4_vjp_pair(bp, bs, kpk + 3 * ((s - 1) & 1), nhap2, nhas2, nqs2, n2qs2, dz62, gp, gs, sp2);
+                        }
+                        Ps[o0] = lane0(gp);
+                        Ps[o1] = lane1(gp);
+                        Ss[o0] = lane0(gs);
+                        Ss[o1] = lane1(gs);
+                    }
+#pragma unroll
+                    for (int i = 0; i < 5; ++i) {
+                        sn[i] = sp[i].x + sp[i].y;
+                        sn2[i] = sp2[i].x + sp2[i].y;
+                    }
+                }
+#pragma unroll 1
+                for (int k = KP; k < R2; ++k) {
                     const int x = n1 + 16 * k;
                     const int o = sidx<N, R2, SW>(lr, x);
                     const size_t g = (size_t)(crank + C * lr) * N + x;

@@ -33,8 +33,9 @@ struct MpCfg {
     static constexpr int CW = SW;                        // columns per column-pass CTA: one 128 B row segment
     static constexpr int CNT = 16 * CW;                  // column-pass threads: one (column, n1) job each
     static constexpr int RPART = N / RB;                 // row-pass CTAs per instance (power partials)
+    // (FP32: plus the packed RK4 stage constants of the two steps, 6 Rk4Pack)
     static constexpr size_t row_smem = sizeof(cx<T>) * (2 * (size_t)RB * N + 12) + sizeof(mult<T>) * N +
-                                       sizeof(double) * 2 * (RNT / 32);
+                                       sizeof(double) * 2 * (RNT / 32) + (sizeof(T) == 4 ? 6 * sizeof(Rk4Pack) : 0);
     static constexpr size_t col_smem = sizeof(cx<T>) * (size_t)N * CW + sizeof(mult<T>) * (2 * (size_t)N + CW);
     static_assert(N % 16 == 0 && RB * RPART == N && N % CW == 0, "bad multi-pass split");
 };
@@ -130,6 +131,9 @@ __global__ void __launch_bounds__(MpCfg<T, N>::RNT)
     double* red = reinterpret_cast<double*>(tw + N);
     const int tid = threadIdx.x, y0 = blockIdx.x * RB;
     auto cj = [](V a) { return mk<T>(a.x, -a.y); };
+    // FP32 plain: packed RK4 stage constants [2][3] (steps s, s + 1), after the reduction area
+    constexpr bool PACK = !THERM && sizeof(T) == 4;
+    Rk4Pack* kpk = reinterpret_cast<Rk4Pack*>(red + 2 * (NT / 32));
 
     for (int j = tid; j < N; j += NT) tw[j] = gtab[j];
     if (!THERM && tid < 3) {
@@ -138,6 +142,12 @@ __global__ void __launch_bounds__(MpCfg<T, N>::RNT)
         } else {
             stage_coef<T>(d, s, zs[s], tid, coef);
             if (mode == 1) stage_coef<T>(d, s + 1, zs[s + 1], tid, coef + 6);
+            if constexpr (PACK) {
+                if (mode == 1) {
+                    stage_pack(coef, tid, kpk);
+                    stage_pack(coef + 6, tid, kpk + 3);
+                }
+            }
         }
     }
     if (mode == 0) {
@@ -203,8 +213,30 @@ __global__ void __launch_bounds__(MpCfg<T, N>::RNT)
 #pragma unroll
             for (int k = 0; k < R2; ++k) F[sidx<N, R2, SW>(lr, n1 + 16 * k)] = v[k];
         }
+        int k0 = 0;
+        if constexpr (PACK) {
+            if (mode == 1 && s + 1 >= d.nslices) {
+                // a middle step that records nothing: points k and k + 1 at once in packed
+                // arithmetic (rk4_pair), the odd one out below
+                const float2 nhap = bc2(-hap), nhas = bc2(-has), nqs = bc2(-qs), dzz = bc2(dz6);
 #pragma unroll 1
-        for (int k = 0; k < R2; ++k) {
+                for (int k = 0; k + 1 < R2; k += 2) {
+                    const int o0 = sidx<N, R2, SW>(lr, n1 + 16 * k), o1 = sidx<N, R2, SW>(lr, n1 + 16 * k + 16);
+                    const V p0 = Ps[o0], q0 = Ss[o0], p1 = Ps[o1], q1 = Ss[o1];
+                    Cx2 P{make_float2(p0.x, p1.x), make_float2(p0.y, p1.y)};
+                    Cx2 S{make_float2(q0.x, q1.x), make_float2(q0.y, q1.y)};
+                    rk4_pair(P, S, kpk, nhap, nhas, nqs, dzz);
+                    rk4_pair(P, S, kpk + 3, nhap, nhas, nqs, dzz);
+                    Ps[o0] = make_float2(P.r.x, P.i.x);
+                    Ps[o1] = make_float2(P.r.y, P.i.y);
+                    Ss[o0] = make_float2(S.r.x, S.i.x);
+                    Ss[o1] = make_float2(S.r.y, S.i.y);
+                }
+                k0 = R2 & ~1;
+            }
+        }
+#pragma unroll 1
+        for (int k = k0; k < R2; ++k) {
             const int x = n1 + 16 * k;
             const int o = sidx<N, R2, SW>(lr, x);
             const size_t g = (size_t)(y0 + lr) * N + x;

@@ -41,7 +41,7 @@ FP32_LANES_PER_SM = 128
 # class (ssfm_plain_kernel<float, 256, 16, 256>), from one ncu launch-list capture of this
 # bench (`--steps 2 --warmup 3 --no-cpu-baseline --no-autotune`, metrics dram__bytes_read.sum
 # and dram__bytes_write.sum); the fields stay on chip, so this is descriptors and outputs
-SWEEP_256_DRAM_BYTES_PER_LAUNCH = 14.30e6
+SWEEP_256_DRAM_BYTES_PER_LAUNCH = 14.75e6
 # bytes of one instance descriptor the batch call uploads (shg::InstDesc)
 INST_DESC_BYTES = 376
 

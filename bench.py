@@ -158,12 +158,13 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     sptr = stream.cuda_stream
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)  # > 126 MB L2
 
-    # the launch schedule of each grid-size class, chosen on this device (untimed)
+    # the launch schedule of each grid-size class, chosen on this device by the time of this
+    # whole batch (untimed): the classes share the SMs, so a class's fastest split alone can
+    # slow the sweep
     tuned = []
     if not args.no_autotune:
-        for n in sorted({p.nx for p in ps}):
-            r = shg.autotune(args.precision, n)
-            tuned.append({"n": n, "cluster": r["cluster"], "threads": r["threads"], "candidates": r["candidates"],
+        for r in shg.autotune_batch(ps):
+            tuned.append({"n": r["n"], "cluster": r["cluster"], "threads": r["threads"], "candidates": r["candidates"],
                           "gain": r["pt_steps_per_s"] / r["default_pt_steps_per_s"]})
 
     def sweep():
@@ -574,7 +575,8 @@ def main() -> int:
     ap.add_argument("--precision", type=int, default=32, choices=[32, 64])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-autotune", action="store_true", help="use the compiled default launch schedules")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="use the compiled default launch schedules (default: shg_autotune_batch on the workload)")
     ap.add_argument("--scaling", default="weak", choices=["weak", "strong"],
                     help="weak: every rank runs its own 256-instance sweep; strong: one sweep split over the ranks")
     ap.add_argument("--class-side", type=int, default=0, help="profile case: one grid-size class only")

@@ -112,3 +112,118 @@ extern "C" shg_status shg_autotune(int32_t precision, int32_t n, shg_tune_result
     out->default_pt_steps_per_s = rate[0];
     return SHG_OK;
 }
+
+// shg_autotune_batch: the schedule of every grid-size class judged by the time of the whole
+// given batch.  The classes of a mixed batch run side by side on forked streams and share
+// the SMs, so the variant that is fastest for a class alone can slow the batch (a class that
+// fills every SM with its own CTAs holds back the clusters of the larger classes).
+// Coordinate descent from the compiled defaults: for each class, largest total work first,
+// every other compiled variant is timed with the rest fixed and kept if the batch is at
+// least 1 % faster.  A timing is the median of three runs of the batch (no field outputs,
+// SH powers kept on the device) after one untimed run.
+extern "C" shg_status shg_autotune_batch(const shg_params* params, int32_t count, shg_tune_result* out,
+                                         int32_t max_out, int32_t* n_out) {
+    clear_error();
+    if (!params || count <= 0) return fail(SHG_ERR_INVALID, "params is NULL or count <= 0");
+    if (!out || !n_out || max_out <= 0) return fail(SHG_ERR_INVALID, "out / n_out is NULL or max_out <= 0");
+    for (int i = 0; i < count; ++i) {
+        shg_status st = shg_check_params(&params[i]);
+        if (st != SHG_OK) return fail(st, "instance %d: %s", i, shg_last_error());
+        if (params[i].thermal) return fail(SHG_ERR_UNSUPPORTED, "instance %d: batched runs are plain (thermal == 0)", i);
+        if (params[i].precision != params[0].precision)
+            return fail(SHG_ERR_INVALID, "instance %d: all instances must share one precision", i);
+        if (params[i].march != SHG_MARCH_AUTO)
+            return fail(SHG_ERR_INVALID, "instance %d: the tuner chooses the march (march must be SHG_MARCH_AUTO)", i);
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(SHG_ERR_NO_DEVICE, "no CUDA device visible");
+    }
+    const int precision = params[0].precision;
+    // the classes, by total work
+    struct Cls { int n; double work; };
+    std::vector<Cls> cls;
+    double work = 0.0;
+    for (int i = 0; i < count; ++i) {
+        const double w = (double)params[i].nx * params[i].nx * shg_steps(&params[i]);
+        work += w;
+        auto it = std::find_if(cls.begin(), cls.end(), [&](const Cls& c) { return c.n == params[i].nx; });
+        if (it == cls.end()) cls.push_back({params[i].nx, w});
+        else it->work += w;
+    }
+    std::sort(cls.begin(), cls.end(), [](const Cls& a, const Cls& b) { return a.work > b.work; });
+    if ((int)cls.size() > max_out) return fail(SHG_ERR_INVALID, "the batch has %d classes, out holds %d", (int)cls.size(), max_out);
+    // start from the compiled defaults
+    std::vector<std::vector<const PlainVariant*>> cand(cls.size());
+    std::vector<int> pick(cls.size(), 0);
+    for (size_t k = 0; k < cls.size(); ++k) {
+        const PlainVariant* c[16];
+        const int nc = plain_candidates(precision, cls[k].n, c, 16);
+        cand[k].assign(c, c + nc);
+        set_plain_choice(cand[k][0]);
+    }
+    cudaStream_t s = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    shg_status rc = SHG_OK;
+    auto time_batch = [&](double* ms_out) -> shg_status {
+        float ms[4] = {0, 0, 0, 0};
+        for (int r = 0; r < 4; ++r) {
+            if ((e = cudaEventRecord(ev[0], s)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+            shg_status st = plain_solve_batch(params, count, nullptr, nullptr, nullptr, s, nullptr, nullptr);
+            if (st != SHG_OK) return st;
+            if ((e = cudaEventRecord(ev[1], s)) != cudaSuccess || (e = cudaEventSynchronize(ev[1])) != cudaSuccess ||
+                (e = cudaEventElapsedTime(&ms[r], ev[0], ev[1])) != cudaSuccess)
+                return cuda_fail(e, "tuning run");
+        }
+        std::sort(ms + 1, ms + 4);  // ms[0] is the untimed first run
+        *ms_out = ms[2];
+        return SHG_OK;
+    };
+    double t_default = 0.0, t_best = 0.0;
+    do {
+        if ((e = cudaEventCreate(&ev[0])) != cudaSuccess || (e = cudaEventCreate(&ev[1])) != cudaSuccess) {
+            rc = cuda_fail(e, "cudaEventCreate");
+            break;
+        }
+        if ((rc = time_batch(&t_default)) != SHG_OK) break;
+        t_best = t_default;
+        for (size_t k = 0; k < cls.size() && rc == SHG_OK; ++k) {
+            for (int c = 1; c < (int)cand[k].size() && rc == SHG_OK; ++c) {
+                set_plain_choice(cand[k][c]);
+                double t = 0.0;
+                if ((rc = time_batch(&t)) != SHG_OK) break;
+                if (t < 0.99 * t_best) {
+                    t_best = t;
+                    pick[k] = c;
+                }
+            }
+            set_plain_choice(cand[k][pick[k]]);
+        }
+    } while (0);
+    for (cudaEvent_t x : ev)
+        if (x) cudaEventDestroy(x);
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+    if (rc != SHG_OK) {
+        for (size_t k = 0; k < cls.size(); ++k) set_plain_choice(cand[k][0]);
+        return rc;
+    }
+    for (size_t k = 0; k < cls.size(); ++k) {
+        shg_tune_result& r = out[k];
+        std::memset(&r, 0, sizeof(r));
+        r.precision = precision;
+        r.n = cls[k].n;
+        r.cluster = cand[k][pick[k]]->cluster;
+        r.threads = cand[k][pick[k]]->threads;
+        r.candidates = (int)cand[k].size();
+        r.pt_steps_per_s = work / (t_best * 1e-3);
+        r.default_pt_steps_per_s = work / (t_default * 1e-3);
+    }
+    *n_out = (int)cls.size();
+    return SHG_OK;
+}
+
+extern "C" void shg_autotune_reset(void) { clear_plain_choices(); }

@@ -415,11 +415,26 @@ shg_status shg_solve_batch(const shg_params* params, int32_t count, void* const*
         cudaGetLastError();
         return fail(SHG_ERR_NO_DEVICE, "no CUDA device visible");
     }
+    // Page-locked host outputs are written by the march itself through their device mapping,
+    // as each instance finishes, so the transfer spreads over the whole launch; pageable ones
+    // go through a device buffer and one copy per class as soon as that class's march ends.
+    auto mapped = [](void* h) -> void* {
+        if (!h) return nullptr;
+        cudaPointerAttributes a;
+        if (cudaPointerGetAttributes(&a, h) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        return a.type == cudaMemoryTypeHost ? a.devicePointer : nullptr;
+    };
+    std::vector<void*> mp(count, nullptr), ms(count, nullptr);
     std::vector<size_t> off(2 * (size_t)count + 1, 0);
     for (int i = 0; i < count; ++i) {
         const size_t plane = (size_t)params[i].nx * params[i].ny * complex_bytes(params[i]);
-        off[2 * i + 1] = off[2 * i] + ((pump_out && pump_out[i]) ? plane : 0);
-        off[2 * i + 2] = off[2 * i + 1] + ((signal_out && signal_out[i]) ? plane : 0);
+        if (pump_out) mp[i] = mapped(pump_out[i]);
+        if (signal_out) ms[i] = mapped(signal_out[i]);
+        off[2 * i + 1] = off[2 * i] + ((pump_out && pump_out[i] && !mp[i]) ? plane : 0);
+        off[2 * i + 2] = off[2 * i + 1] + ((signal_out && signal_out[i] && !ms[i]) ? plane : 0);
     }
     cudaStream_t s = nullptr;
     cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
@@ -431,13 +446,20 @@ shg_status shg_solve_batch(const shg_params* params, int32_t count, void* const*
             rc = cuda_fail(e, "cudaMallocAsync");
             break;
         }
-        std::vector<void*> dp(count, nullptr), ds(count, nullptr);
+        std::vector<void*> dp(mp), ds(ms), hp(count, nullptr), hs(count, nullptr);
         for (int i = 0; i < count; ++i) {
-            if (off[2 * i + 1] > off[2 * i]) dp[i] = buf + off[2 * i];
-            if (off[2 * i + 2] > off[2 * i + 1]) ds[i] = buf + off[2 * i + 1];
+            if (off[2 * i + 1] > off[2 * i]) {
+                dp[i] = buf + off[2 * i];
+                hp[i] = pump_out[i];
+            }
+            if (off[2 * i + 2] > off[2 * i + 1]) {
+                ds[i] = buf + off[2 * i + 1];
+                hs[i] = signal_out[i];
+            }
         }
-        // each grid-size class's outputs are copied as soon as its march ends, overlapping the others
-        if ((rc = plain_solve_batch(params, count, dp.data(), ds.data(), sh_power_out, s, pump_out, signal_out)) !=
+        // staged outputs: each grid-size class's are copied as soon as its march ends,
+        // overlapping the others
+        if ((rc = plain_solve_batch(params, count, dp.data(), ds.data(), sh_power_out, s, hp.data(), hs.data())) !=
             SHG_OK)
             break;
         if ((e = cudaStreamSynchronize(s)) != cudaSuccess) rc = cuda_fail(e, "cudaStreamSynchronize");

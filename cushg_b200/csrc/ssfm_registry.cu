@@ -54,6 +54,11 @@ int plain_candidates(int precision, int n, const PlainVariant** out, int max) {
     return k;
 }
 
+void clear_plain_choices() {
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_chosen.clear();
+}
+
 void set_plain_choice(const PlainVariant* v) {
     std::lock_guard<std::mutex> lk(g_mu);
     for (const PlainVariant*& c : g_chosen)

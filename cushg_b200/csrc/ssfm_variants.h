@@ -66,5 +66,7 @@ const PlainVariant* find_plain_variant(int precision, int n, int thermal = 0, in
 int plain_candidates(int precision, int n, const PlainVariant** out, int max);
 // Make v the variant find_plain_variant returns for its (precision, n, thermal).
 void set_plain_choice(const PlainVariant* v);
+// forget every tuned choice: later runs use the compiled defaults
+void clear_plain_choices();
 
 }  // namespace shg

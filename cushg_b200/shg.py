@@ -27,7 +27,7 @@ EXPORTS = (
     "shg_solve_batch_device", "shg_solve_batch_device_noalloc", "shg_grad", "shg_sh_power", "shg_last_error",
     "shg_status_string", "shg_version", "shg_heat_sweeps_device", "shg_batch_plan_create", "shg_batch_plan_launch",
     "shg_batch_plan_powers", "shg_batch_plan_destroy", "shg_autotune", "shg_grad_batch", "shg_solve_batch",
-    "shg_thermal_grad",
+    "shg_thermal_grad", "shg_autotune_batch", "shg_autotune_reset",
 )
 
 
@@ -117,6 +117,11 @@ def lib() -> ctypes.CDLL:
         L.shg_thermal_grad.restype = ctypes.c_int
         L.shg_autotune.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ShgTuneResult)]
         L.shg_autotune.restype = ctypes.c_int
+        L.shg_autotune_batch.argtypes = [P, ctypes.c_int32, ctypes.POINTER(ShgTuneResult), ctypes.c_int32,
+                                         ctypes.POINTER(ctypes.c_int32)]
+        L.shg_autotune_batch.restype = ctypes.c_int
+        L.shg_autotune_reset.argtypes = []
+        L.shg_autotune_reset.restype = None
         L.shg_last_error.restype = ctypes.c_char_p
         L.shg_status_string.argtypes = [ctypes.c_int32]
         L.shg_status_string.restype = ctypes.c_char_p
@@ -230,14 +235,17 @@ def heat_sweeps_device(p: ShgParams, temperature, q, sweeps: int, stream=None) -
 
 
 def _host_ptr(a):
-    """Address of a host array: a numpy array or a (pinned) CPU torch tensor."""
+    """Address of a host array: a numpy array or a (pinned) CPU torch tensor; None for None."""
+    if a is None:
+        return None
     return a.data_ptr() if hasattr(a, "data_ptr") else a.ctypes.data
 
 
 def solve_batch(ps: list[ShgParams], pumps=None, sigs=None):
     """Batch of plain instances with host buffers (shg_solve_batch).  pumps / sigs: host arrays
-    to fill (numpy arrays or pinned torch tensors, one per instance) or None to allocate numpy
-    arrays.  Returns (pumps, sigs, SH powers)."""
+    to fill (numpy arrays or pinned torch tensors, one per instance, or None entries for
+    outputs not wanted) or None to allocate numpy arrays.  Pinned tensors are written by the
+    march directly.  Returns (pumps, sigs, SH powers)."""
     n = len(ps)
     arr = (ShgParams * n)(*ps)
     vp = ctypes.c_void_p
@@ -392,3 +400,21 @@ def autotune(precision: int, n: int) -> dict:
     return {"precision": r.precision, "n": r.n, "cluster": r.cluster, "threads": r.threads,
             "candidates": r.candidates, "pt_steps_per_s": r.pt_steps_per_s,
             "default_pt_steps_per_s": r.default_pt_steps_per_s}
+
+
+def autotune_reset() -> None:
+    """shg_autotune_reset: back to the compiled default schedules."""
+    lib().shg_autotune_reset()
+
+
+def autotune_batch(ps: list[ShgParams]) -> list[dict]:
+    """shg_autotune_batch: the launch schedule of every grid-size class of this batch, chosen
+    by the time of the whole batch; one dict per class (largest work first) as autotune()."""
+    n = len(ps)
+    arr = (ShgParams * n)(*ps)
+    out = (ShgTuneResult * 16)()
+    k = ctypes.c_int32(0)
+    _check(lib().shg_autotune_batch(arr, n, out, 16, ctypes.byref(k)))
+    return [{"precision": r.precision, "n": r.n, "cluster": r.cluster, "threads": r.threads,
+             "candidates": r.candidates, "pt_steps_per_s": r.pt_steps_per_s,
+             "default_pt_steps_per_s": r.default_pt_steps_per_s} for r in out[:k.value]]

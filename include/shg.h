@@ -203,7 +203,10 @@ SHG_API shg_status shg_solve_batch_device(const shg_params* params, int32_t coun
 /*
  * shg_solve_batch_device with host buffers: pump_out[i] / signal_out[i] are host arrays of
  * nx_i*ny_i complex (or NULL entries), sh_power_out a host array of `count` doubles or NULL.
- * Synchronous.  The sweep of src/cuSHG.sh:58-94 as one call.
+ * Synchronous.  The sweep of src/cuSHG.sh:58-94 as one call.  Page-locked buffers
+ * (cudaHostAlloc / cudaMallocHost / cudaHostRegister) are written by the march directly as
+ * each instance finishes; pageable ones are staged on the device and copied per grid-size
+ * class.
  */
 SHG_API shg_status shg_solve_batch(const shg_params* params, int32_t count, void* const* pump_out,
                                    void* const* signal_out, double* sh_power_out);
@@ -251,6 +254,25 @@ typedef struct shg_tune_result {
  * src/cuSHG.cu:22-23).
  */
 SHG_API shg_status shg_autotune(int32_t precision, int32_t n, shg_tune_result* out);
+
+/*
+ * Autotuner for a given mixed batch (shg_solve_batch_device arguments, all march ==
+ * SHG_MARCH_AUTO): the classes of a batch run side by side and share the SMs, so the split
+ * that is fastest for a class alone can slow the batch.  Starting from the compiled
+ * defaults, each class (largest total work first) tries its other compiled variants with the
+ * rest fixed, and keeps one that makes the whole batch at least 1 % faster on this device.
+ * The choices hold for every later plain run and batch in this process, as for
+ * shg_autotune.  out[0 .. *n_out-1]: one entry per class, largest work first, with
+ * pt_steps_per_s the batch's rate with the chosen schedule and default_pt_steps_per_s its
+ * rate with the defaults.  Synchronous (runs the batch 4 times per trial); call it before
+ * any stream capture.  No counterpart in the reference.
+ */
+SHG_API shg_status shg_autotune_batch(const shg_params* params, int32_t count, shg_tune_result* out,
+                                      int32_t max_out, int32_t* n_out);
+
+/* Forget the choices of shg_autotune / shg_autotune_batch: later runs use the compiled
+ * default schedules.  No counterpart in the reference. */
+SHG_API void shg_autotune_reset(void);
 
 /*
  * The batched plain march of shg_solve_batch_device without any device allocation.  This

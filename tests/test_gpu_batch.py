@@ -92,8 +92,15 @@ def test_plan_rejects_bad_input():
         shg.BatchPlan([P.config_plain_64(), P.config_plain_64().replace(precision=32)])
 
 
+@pytest.fixture
+def default_schedules():
+    """The tuners' choices hold for the process: put the compiled defaults back afterwards."""
+    yield
+    shg.autotune_reset()
+
+
 @pytest.mark.parametrize("precision,n", [(32, 128), (32, 256), (64, 128)])
-def test_autotune_keeps_results(precision, n):
+def test_autotune_keeps_results(precision, n, default_schedules):
     """The tuner times every compiled split of the class and keeps the fastest; the fields
     of the class are the same bits before and after, the SH power agrees to rounding."""
     import torch
@@ -113,6 +120,35 @@ def test_autotune_keeps_results(precision, n):
     assert np.allclose(pw0, pw1, rtol=1e-12 if precision == 64 else 1e-6, atol=0)
 
 
+@pytest.mark.parametrize("precision", [32, 64])
+def test_batch_autotune_keeps_results(precision, default_schedules):
+    """The batch tuner judges each class's compiled variants by the time of the whole batch and
+    keeps a change only when the batch gets faster.  The fields agree with the default
+    schedule's to the multi-pass-against-fused tolerances (FP64 relative L2 <= 1e-13, FP32
+    <= 1e-5): a fused split gives the same bits, the multi-pass march (a candidate at 256 x
+    256) differs where the compiler contracts multiply-adds differently."""
+    import torch
+    ps = sweep(precision, 24, seed=7 + precision)
+    before_p, before_s = device_outputs(ps)
+    pw0 = shg.solve_batch_device(ps, before_p, before_s)
+    res = shg.autotune_batch(ps)
+    assert sorted(r["n"] for r in res) == sorted({p.nx for p in ps})
+    for r in res:
+        assert r["precision"] == precision and r["candidates"] >= 1
+        assert r["pt_steps_per_s"] >= r["default_pt_steps_per_s"] > 0
+    after_p, after_s = device_outputs(ps)
+    pw1 = shg.solve_batch_device(ps, after_p, after_s)
+    torch.cuda.synchronize()
+    tol = 1e-13 if precision == 64 else 1e-5
+    rel = lambda a, b: float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
+    for i in range(len(ps)):
+        assert rel(after_s[i], before_s[i]) <= tol and rel(after_p[i], before_p[i]) <= tol, i
+    assert np.allclose(pw0, pw1, rtol=1e-12 if precision == 64 else 1e-5, atol=0)
+    with pytest.raises(shg.ShgError) as e:
+        shg.autotune_batch([ps[0].replace(march=P.SHG_MARCH_FUSED)])
+    assert e.value.status == P.SHG_ERR_INVALID
+
+
 def test_autotune_rejects_unbuilt_class():
     with pytest.raises(shg.ShgError) as e:
         shg.autotune(32, 100)
@@ -129,3 +165,33 @@ def test_host_buffer_batch_equals_device_batch():
     assert np.array_equal(power, pw)
     for i in range(len(ps)):
         assert np.array_equal(sigs[i], ds[i].cpu().numpy()) and np.array_equal(pumps[i], dp[i].cpu().numpy())
+
+
+@pytest.mark.parametrize("precision", [32, 64])
+def test_pinned_host_outputs_written_by_the_march(precision):
+    """Page-locked host outputs are written by the march through their device mapping, with no
+    staging copy; a batch that mixes them with pageable arrays and missing outputs, and holds
+    a 512 x 512 instance (multi-pass march), still equals the device batch bit for bit."""
+    import torch
+    ps = sweep(precision, 7, seed=33) + [P.workload(512, 5, 4000.0, 10.0, 30.0, 2000.0, 30.0, precision=precision)]
+    dt = torch.complex128 if precision == 64 else torch.complex64
+    npdt = np.complex128 if precision == 64 else np.complex64
+    pumps, sigs = [], []
+    for i, p in enumerate(ps):
+        kind = i % 3  # 0: pinned, 1: pageable numpy, 2: pinned pump only
+        if kind == 1:
+            pumps.append(np.full((p.ny, p.nx), np.nan, dtype=npdt))
+            sigs.append(np.full((p.ny, p.nx), np.nan, dtype=npdt))
+        else:
+            pumps.append(torch.full((p.ny, p.nx), float("nan"), dtype=dt).pin_memory())
+            sigs.append(None if kind == 2 else torch.full((p.ny, p.nx), float("nan"), dtype=dt).pin_memory())
+    _, _, power = shg.solve_batch(ps, pumps, sigs)
+    dp, ds = device_outputs(ps)
+    pw = shg.solve_batch_device(ps, dp, ds)
+    torch.cuda.synchronize()
+    assert np.array_equal(power, pw)
+    as_np = lambda a: a if isinstance(a, np.ndarray) else a.numpy()
+    for i in range(len(ps)):
+        assert np.array_equal(as_np(pumps[i]), dp[i].cpu().numpy()), i
+        if sigs[i] is not None:
+            assert np.array_equal(as_np(sigs[i]), ds[i].cpu().numpy()), i

@@ -393,6 +393,10 @@ shg_status shg_heat_sweeps_device(const shg_params* p, void* temperature_dev, co
     shg_status st = check_params_impl(&q, false);  // the heat solve needs no optical kernel
     if (st != SHG_OK) return st;
     if (!temperature_dev || !q_dev) return fail(SHG_ERR_INVALID, "temperature or Q is NULL");
+    // the sweep reads voxel pairs (float2 / double2): both arrays aligned to two reals
+    const uintptr_t al = 2 * (p->precision == 32 ? 4 : 8) - 1;
+    if (((uintptr_t)temperature_dev & al) || ((uintptr_t)q_dev & al))
+        return fail(SHG_ERR_INVALID, "temperature and Q must be aligned to %d bytes", (int)al + 1);
     if (sweeps < 0) return fail(SHG_ERR_INVALID, "sweeps must be >= 0");
     if (sweeps == 0) return SHG_OK;
     return heat_sweeps_device(q, temperature_dev, q_dev, sweeps, (cudaStream_t)stream);

@@ -13,6 +13,8 @@
 //       -> optics_kernel (Δk, n_p, n_s per voxel, once per optical pass)
 #include <cuda_runtime.h>
 
+#include <cstdint>
+
 #include "crystal.cuh"
 #include "jacobi_point.cuh"
 #include "shg_host.h"
@@ -190,6 +192,73 @@ __global__ void __launch_bounds__(256) jacobi_zb2_kernel(const R* __restrict__ T
     }
 }
 
+// FP32: the same sweep with four x-adjacent voxels per thread (float4 loads of the centre
+// column, its y neighbours and Q; the x neighbours outside the quad as scalars), half the
+// loads and index arithmetic per voxel of the pairs.  Launched when n is a multiple of 4 and
+// the three arrays are 16-byte aligned (launch_jacobi checks both), so the quads tile every
+// row and every float4 access is aligned; otherwise the pairs run.  Each voxel is
+// jacobi_point / jacobi_inner of the same operands as in every other sweep kernel.  Thread
+// block (32, 8) covers 128 x 8 voxels; grid (n/128, n/8, nz/ZB).
+template <int BOUND>
+__global__ void __launch_bounds__(256) jacobi_zb4_kernel(const float* __restrict__ Ti, float* __restrict__ Tf,
+                                                         const float* __restrict__ Q, JacobiCoef<float> k) {
+    using R = float;
+    const int n = k.n, nz = k.nz;
+    const int x = 4 * (blockIdx.x * 32 + threadIdx.x);
+    const int y = blockIdx.y * 8 + threadIdx.y;
+    if (x >= n || y >= n) return;
+    const int z0 = blockIdx.z * kJacobiZB, z1 = min(nz, z0 + kJacobiZB);
+    const size_t sy = (size_t)n, sz = (size_t)n * n;
+    size_t i = (size_t)z0 * sz + (size_t)y * sy + x;
+    auto ld4 = [&](size_t j) { return *reinterpret_cast<const float4*>(Ti + j); };
+    const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    auto arr = [](float4 v, R* a) { a[0] = v.x; a[1] = v.y; a[2] = v.z; a[3] = v.w; };
+    R below[4], cur[4];
+    arr(z0 > 0 ? ld4(i - sz) : zero4, below);
+    arr(ld4(i), cur);
+    // all four voxels of the quad are inner in x and y (a quad starts at a multiple of 4)
+    const bool inner_xy = x >= 4 && x + 4 < n && y >= 1 && y + 1 < n;
+#pragma unroll 1
+    for (int z = z0; z < z1; ++z, i += sz) {
+        R above[4], ym[4], yp[4], q[4], v[4];
+        arr(z + 1 < nz ? ld4(i + sz) : zero4, above);
+        arr(y > 0 ? ld4(i - sy) : zero4, ym);
+        arr(y + 1 < n ? ld4(i + sy) : zero4, yp);
+        arr(*reinterpret_cast<const float4*>(Q + i), q);
+        const R xm = x > 0 ? Ti[i - 1] : (R)0, xp = x + 4 < n ? Ti[i + 4] : (R)0;
+        bool w[4] = {true, true, true, true};
+        if (inner_xy && z >= 1 && z + 1 < nz) {
+            // inner voxels: jacobi_point's inner branch without the classification
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                v[j] = jacobi_inner<R>(j < 3 ? cur[j + 1] : xp, j > 0 ? cur[j - 1] : xm, yp[j], ym[j], above[j],
+                                       below[j], q[j], k);
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                auto get = [&](int dx, int dy, int dz) -> R {
+                    if (dz) return dz > 0 ? above[j] : below[j];
+                    if (dy) return dy > 0 ? yp[j] : ym[j];
+                    return dx > 0 ? (j < 3 ? cur[j + 1] : xp) : (j > 0 ? cur[j - 1] : xm);
+                };
+                w[j] = jacobi_point<R, BOUND>(x + j, y, z, k, q[j], get, &v[j]);
+            }
+        }
+        if (w[0] && w[1] && w[2] && w[3]) {
+            *reinterpret_cast<float4*>(Tf + i) = make_float4(v[0], v[1], v[2], v[3]);
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if (w[j]) Tf[i + j] = v[j];
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            below[j] = cur[j];
+            cur[j] = above[j];
+        }
+    }
+}
+
 // Deterministic second stage: one block sums (or maxes) the partials in a fixed order.
 __global__ void reduce_partials_kernel(const double* __restrict__ partial, size_t count, int rule, double* out) {
     __shared__ double s[256];
@@ -285,6 +354,19 @@ cudaError_t launch_jacobi(const R* Ti, R* Tf, const R* Q, const JacobiCoef<R>& k
     dim3 block(32, 8, 1);
     dim3 grid((k.n + 31) / 32, (k.n + 7) / 8, k.nz);
     if (!resid) {
+        if constexpr (sizeof(R) == 4) {
+            auto al16 = [](const void* a) { return ((uintptr_t)a & 15) == 0; };
+            if ((k.n & 3) == 0 && al16(Ti) && al16(Tf) && al16(Q)) {
+                // quads tile every row when n is a multiple of 4, and every row starts
+                // 16-byte aligned when the arrays do
+                const dim3 qgrid((k.n + 127) / 128, grid.y, (k.nz + kJacobiZB - 1) / kJacobiZB);
+                if (boundary == SHG_BOUNDARY_OVEN_SURROUNDED)
+                    jacobi_zb4_kernel<SHG_BOUNDARY_OVEN_SURROUNDED><<<qgrid, block, 0, s>>>(Ti, Tf, Q, k);
+                else
+                    jacobi_zb4_kernel<SHG_BOUNDARY_TOP_OPEN><<<qgrid, block, 0, s>>>(Ti, Tf, Q, k);
+                return cudaGetLastError();
+            }
+        }
         // n is even (shg_check_params), so the voxel pairs tile every row
         const dim3 zgrid((k.n + 63) / 64, grid.y, (k.nz + kJacobiZB - 1) / kJacobiZB);
         if (boundary == SHG_BOUNDARY_OVEN_SURROUNDED)

@@ -298,7 +298,8 @@ SHG_API shg_status shg_solve_batch_device_noalloc(const shg_params* params, int3
  *                    return; voxels the model holds fixed (Dirichlet faces) keep their value.
  *   q_dev            nx*ny*nz reals: the heat source Q.
  * Uses the grid, precision, kappa, h_conv, t_inf, boundary and jacobi_block of *p (p->thermal
- * is ignored).  Stream-ordered on `stream`; synchronises once at the end.
+ * is ignored).  Both buffers aligned to two reals (8 bytes in FP32, 16 in FP64; any cudaMalloc
+ * pointer is), else SHG_ERR_INVALID.  Stream-ordered on `stream`; synchronises once at the end.
  */
 SHG_API shg_status shg_heat_sweeps_device(const shg_params* p, void* temperature_dev, const void* q_dev,
                                           int64_t sweeps, void* stream);

@@ -118,13 +118,16 @@ def test_blocked_sweeps_are_bit_identical(precision, boundary, n, nz, check_ever
 @pytest.mark.gpu
 @pytest.mark.parametrize("precision", [64, 32])
 @pytest.mark.parametrize("boundary", [P.SHG_BOUNDARY_TOP_OPEN, P.SHG_BOUNDARY_OVEN_SURROUNDED])
-def test_heat_sweeps_match_oracle(precision, boundary):
+@pytest.mark.parametrize("n", [48, 34])
+def test_heat_sweeps_match_oracle(precision, boundary, n):
     """shg_heat_sweeps_device (the Tfield::upDate loop) against the oracle's sweep repeated,
     from a random temperature and heat source, for every sweep depth; depths agree bit for
-    bit with one sweep per launch."""
+    bit with one sweep per launch.  n = 48: FP32 sweeps take four voxels per thread; n = 34
+    (not a multiple of 4): two, and the TMA-staged depths, which need 16-byte rows, refuse
+    FP32 (SHG_ERR_UNSUPPORTED)."""
     import torch
 
-    n, nz, sweeps = 48, 21, 11
+    nz, sweeps = 21, 11
     p = P.workload(n, nz, 6000.0, 3.0, 30.0, 3000.0, 33.0, precision=precision, thermal=1)
     p.boundary = boundary
     rng = np.random.default_rng(7)
@@ -138,16 +141,42 @@ def test_heat_sweeps_match_oracle(precision, boundary):
     tdt = torch.float64 if precision == 64 else torch.float32
     q_d = torch.from_numpy(Q).to("cuda")
     outs = {}
+    rows16 = (n * T0.itemsize) % 16 == 0
     for blk in (1, 2, 3, 4, 0):
         t_d = torch.from_numpy(T0).to("cuda")
+        if blk in (2, 3, 4) and not rows16:
+            with pytest.raises(shg.ShgError) as e:
+                shg.heat_sweeps_device(p.replace(jacobi_block=blk), t_d, q_d, sweeps)
+            assert e.value.status == P.SHG_ERR_UNSUPPORTED
+            continue
         shg.heat_sweeps_device(p.replace(jacobi_block=blk), t_d, q_d, sweeps)
         torch.cuda.synchronize()
         outs[blk] = t_d.cpu().numpy()
         assert outs[blk].dtype == np.dtype(rdt) and t_d.dtype == tdt
-    for blk in (2, 3, 4, 0):
+    for blk in outs:
         assert np.array_equal(outs[blk], outs[1]), blk
     tol = 1e-12 if precision == 64 else 2e-6
     assert np.max(np.abs(outs[1] - Ti)) / np.max(np.abs(Ti)) < tol
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [64, 32])
+def test_heat_sweeps_reject_misaligned_buffers(precision):
+    """The sweep reads voxel pairs: a temperature or Q pointer not aligned to two reals is
+    refused on the host (SHG_ERR_INVALID) before anything is launched."""
+    import torch
+
+    n, nz = 32, 8
+    p = P.workload(n, nz, 6000.0, 3.0, 30.0, 3000.0, 33.0, precision=precision, thermal=1)
+    tdt = torch.float64 if precision == 64 else torch.float32
+    t_d = torch.full((nz * n * n + 1,), 30.0, dtype=tdt, device="cuda")
+    q_d = torch.zeros(nz * n * n + 1, dtype=tdt, device="cuda")
+    for t, q in ((t_d[1:], q_d[:-1]), (t_d[:-1], q_d[1:])):
+        with pytest.raises(shg.ShgError) as e:
+            shg.heat_sweeps_device(p, t, q, 3)
+        assert e.value.status == P.SHG_ERR_INVALID
+    shg.heat_sweeps_device(p, t_d[:-1], q_d[:-1], 3)  # aligned views run
+    torch.cuda.synchronize()
 
 
 @pytest.mark.gpu

@@ -25,7 +25,7 @@ cudaError_t mp_march(const InstDesc* dev_descs, const InstDesc* host_descs, int 
     static cudaError_t attr_err = cudaSuccess;
     std::call_once(once, [] {
         attr_err = cudaFuncSetAttribute(mp_row_kernel<T, N, THERM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)Cfg::row_smem);
+                                        (int)Cfg::row_smem_for(THERM));
         if (attr_err == cudaSuccess)
             attr_err = cudaFuncSetAttribute(mp_col_kernel<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)Cfg::col_smem);
@@ -39,10 +39,10 @@ cudaError_t mp_march(const InstDesc* dev_descs, const InstDesc* host_descs, int 
     if (e != cudaSuccess) return e;
     const dim3 rgrid(Cfg::RPART, count), cgrid(N / Cfg::CW, 2, count);
     mp_setup_kernel<T, N><<<count, 256, 0, s>>>(dev_descs, L);
-    mp_row_kernel<T, N, THERM><<<rgrid, Cfg::RNT, Cfg::row_smem, s>>>(dev_descs, L, -1);
+    mp_row_kernel<T, N, THERM><<<rgrid, Cfg::row_threads(THERM), Cfg::row_smem_for(THERM), s>>>(dev_descs, L, -1);
     for (int st = 0; st < max_steps; ++st) {
         mp_col_kernel<T, N><<<cgrid, Cfg::CNT, Cfg::col_smem, s>>>(dev_descs, L, st);
-        mp_row_kernel<T, N, THERM><<<rgrid, Cfg::RNT, Cfg::row_smem, s>>>(dev_descs, L, st);
+        mp_row_kernel<T, N, THERM><<<rgrid, Cfg::row_threads(THERM), Cfg::row_smem_for(THERM), s>>>(dev_descs, L, st);
     }
     mp_power_kernel<T, N><<<count, 32, 0, s>>>(dev_descs, L);
     e = cudaGetLastError();
@@ -51,7 +51,7 @@ cudaError_t mp_march(const InstDesc* dev_descs, const InstDesc* host_descs, int 
 }
 
 #define SHG_MP_VARIANT(T, PREC, N, THERM) \
-    {PREC, N, 0, MpCfg<T, N>::RNT, 1, THERM ? 1 : 0, MpCfg<T, N>::row_smem, nullptr, &mp_march<T, N, THERM>}
+    {PREC, N, 0, MpCfg<T, N>::row_threads(THERM), 1, THERM ? 1 : 0, MpCfg<T, N>::row_smem_for(THERM), nullptr, &mp_march<T, N, THERM>}
 
 const PlainVariant kTable[] = {
     SHG_MP_VARIANT(float, 32, 512, false),  SHG_MP_VARIANT(double, 64, 512, false),

@@ -37,6 +37,14 @@ struct MpCfg {
     static constexpr size_t row_smem = sizeof(cx<T>) * (2 * (size_t)RB * N + 12) + sizeof(mult<T>) * N +
                                        sizeof(double) * 2 * (RNT / 32) + (sizeof(T) == 4 ? 6 * sizeof(Rk4Pack) : 0);
     static constexpr size_t col_smem = sizeof(cx<T>) * (size_t)N * CW + sizeof(mult<T>) * (2 * (size_t)N + CW);
+    // The thermal row pass gives each (row, n1) job two threads in its pointwise work (the RK4
+    // half steps with per-voxel coefficients, by far its longest part): a single instance has
+    // only N x 16 jobs, and the pass otherwise lasts one thread's chain of R2 points.
+    __host__ __device__ static constexpr int row_px(bool therm) { return therm ? 2 : 1; }
+    __host__ __device__ static constexpr int row_threads(bool therm) { return RNT * row_px(therm); }
+    __host__ __device__ static constexpr size_t row_smem_for(bool therm) {
+        return row_smem + sizeof(double) * 2 * (RNT / 32) * (row_px(therm) - 1);
+    }
     static_assert(N % 16 == 0 && RB * RPART == N && N % CW == 0, "bad multi-pass split");
 };
 
@@ -108,10 +116,11 @@ __device__ __forceinline__ void r2_stage(cx<T> (&v)[R2], const mult<T>* tw, int 
 // s + 1 = out_after writes the outputs and this CTA's power partials; s = nsteps-1 is the
 // last).  Grid (N / RB, count).
 template <typename T, int N, bool THERM>
-__global__ void __launch_bounds__(MpCfg<T, N>::RNT)
+__global__ void __launch_bounds__(MpCfg<T, N>::row_threads(THERM))
     mp_row_kernel(const InstDesc* __restrict__ descs, MpLayout L, int s) {
     using Cfg = MpCfg<T, N>;
-    constexpr int R2 = Cfg::R2, RB = Cfg::RB, SW = Cfg::SW, NT = Cfg::RNT;
+    constexpr int R2 = Cfg::R2, RB = Cfg::RB, SW = Cfg::SW;
+    constexpr int JOBS = Cfg::RNT, PX = Cfg::row_px(THERM), NT = JOBS * PX;
     using V = cx<T>;
     using W = mult<T>;
     const InstDesc d = descs[blockIdx.y];
@@ -201,10 +210,13 @@ __global__ void __launch_bounds__(MpCfg<T, N>::RNT)
     const T hap = (T)d.hap, has = (T)d.has, qs = (T)d.qs, dz6 = (T)(d.dz / 6.0);
     double acc_s = 0.0, acc_p = 0.0;
     {
-        const int n1 = tid & 15, lr = tid >> 4;  // one (row, n1) job per thread
+        // one (row, n1) job per JOBS threads; its R2 stages on the job's first thread, its
+        // points shared by the job's PX threads (point k on thread part = k mod PX)
+        const int job = tid % JOBS, part = tid / JOBS;
+        const int n1 = job & 15, lr = job >> 4;
         double* dkint = THERM ? reinterpret_cast<double*>(wbase + L.off_dk) : nullptr;
 #pragma unroll 1
-        for (int f = 0; f < 2 && mode != 0; ++f) {
+        for (int f = 0; f < 2 && mode != 0 && part == 0; ++f) {
             V* F = f ? Ss : Ps;
             V v[R2];
 #pragma unroll
@@ -213,6 +225,7 @@ __global__ void __launch_bounds__(MpCfg<T, N>::RNT)
 #pragma unroll
             for (int k = 0; k < R2; ++k) F[sidx<N, R2, SW>(lr, n1 + 16 * k)] = v[k];
         }
+        if constexpr (PX > 1) __syncthreads();
         int k0 = 0;
         if constexpr (PACK) {
             if (mode == 1 && s + 1 >= d.nslices) {
@@ -236,7 +249,7 @@ __global__ void __launch_bounds__(MpCfg<T, N>::RNT)
             }
         }
 #pragma unroll 1
-        for (int k = k0; k < R2; ++k) {
+        for (int k = k0 + part; k < R2; k += PX) {
             const int x = n1 + 16 * k;
             const int o = sidx<N, R2, SW>(lr, x);
             const size_t g = (size_t)(y0 + lr) * N + x;
@@ -248,8 +261,9 @@ __global__ void __launch_bounds__(MpCfg<T, N>::RNT)
                 Ss[o] = q;
             }
         }
+        if constexpr (PX > 1) __syncthreads();
 #pragma unroll 1
-        for (int f = 0; f < 2 && mode != 2; ++f) {
+        for (int f = 0; f < 2 && mode != 2 && part == 0; ++f) {
             V* F = f ? Ss : Ps;
             V v[R2];
 #pragma unroll

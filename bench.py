@@ -603,8 +603,8 @@ def main() -> int:
     ap.add_argument("--thermal-fixed-sweeps", type=int, default=200)
     ap.add_argument("--thermal-outer", type=int, default=2)
     ap.add_argument("--no-thermal-grad", action="store_true", help="thermal-batch: the runs without dJ/dT_oven")
-    ap.add_argument("--thermal-concurrency", type=int, default=2,
-                    help="thermal-batch: instances run at a time from host threads (2 measured fastest)")
+    ap.add_argument("--thermal-concurrency", type=int, default=1,
+                    help="thermal-batch: instances run at a time from host threads")
     ap.add_argument("--jacobi-sweeps", type=int, default=400)
     ap.add_argument("--thermal-side", type=int, default=0)
     ap.add_argument("--thermal-nz", type=int, default=0)

@@ -37,10 +37,11 @@ struct MpCfg {
     static constexpr size_t row_smem = sizeof(cx<T>) * (2 * (size_t)RB * N + 12) + sizeof(mult<T>) * N +
                                        sizeof(double) * 2 * (RNT / 32) + (sizeof(T) == 4 ? 6 * sizeof(Rk4Pack) : 0);
     static constexpr size_t col_smem = sizeof(cx<T>) * (size_t)N * CW + sizeof(mult<T>) * (2 * (size_t)N + CW);
-    // The thermal row pass gives each (row, n1) job two threads in its pointwise work (the RK4
-    // half steps with per-voxel coefficients, by far its longest part): a single instance has
-    // only N x 16 jobs, and the pass otherwise lasts one thread's chain of R2 points.
-    __host__ __device__ static constexpr int row_px(bool therm) { return therm ? 2 : 1; }
+    // The thermal row pass gives each (row, n1) job several threads in its pointwise work (the
+    // RK4 half steps with per-voxel coefficients, by far its longest part): a single instance
+    // has only N x 16 jobs, and the pass otherwise lasts one thread's chain of R2 points.  Four
+    // in FP32 (the kernel fits the 128 registers of a 512-thread block), two in FP64.
+    __host__ __device__ static constexpr int row_px(bool therm) { return therm ? (sizeof(T) == 4 ? 4 : 2) : 1; }
     __host__ __device__ static constexpr int row_threads(bool therm) { return RNT * row_px(therm); }
     __host__ __device__ static constexpr size_t row_smem_for(bool therm) {
         return row_smem + sizeof(double) * 2 * (RNT / 32) * (row_px(therm) - 1);

@@ -122,15 +122,20 @@ __host__ __device__ inline JvpLayout jvp_layout(const MpLayout& L) {
     return J;
 }
 
+// Threads per (row, n1) job in the tangent row pass's pointwise work, as in the thermal row
+// pass (two: the tangent RK4 needs more registers than a 512-thread block allows).
+constexpr int kJvpPX = 2;
+
 // Row pass of the tangent march (one instance; grid N / RB): as mp_row_kernel's thermal pass
 // over the four planes P, S, Ṗ, Ṡ, with the JVP of the RK4 applications; the pass with
 // s + 1 = out_after sums this CTA's SH power and its derivative into the partials
 // (part[2 r], part[2 r + 1]).
 template <typename T, int N>
-__global__ void __launch_bounds__(MpCfg<T, N>::RNT)
+__global__ void __launch_bounds__(MpCfg<T, N>::RNT * kJvpPX)
     mp_row_jvp_kernel(const InstDesc* __restrict__ descs, MpLayout L, JvpLayout JL, JvpDesc jd, int s) {
     using Cfg = MpCfg<T, N>;
-    constexpr int R2 = Cfg::R2, RB = Cfg::RB, SW = Cfg::SW, NT = Cfg::RNT;
+    constexpr int R2 = Cfg::R2, RB = Cfg::RB, SW = Cfg::SW;
+    constexpr int JOBS = Cfg::RNT, PX = kJvpPX, NT = JOBS * PX;
     using V = cx<T>;
     using W = mult<T>;
     using R = T;
@@ -219,10 +224,13 @@ __global__ void __launch_bounds__(MpCfg<T, N>::RNT)
     const size_t nn = (size_t)N * N;
     double acc_j = 0.0, acc_jd = 0.0;
     {
-        const int n1 = tid & 15, lr = tid >> 4;
-        if (mode != 0) r2_pass(n1, lr, true);
+        // one (row, n1) job per JOBS threads: its R2 stages on the first, its points shared
+        const int job = tid % JOBS, part = tid / JOBS;
+        const int n1 = job & 15, lr = job >> 4;
+        if (mode != 0 && part == 0) r2_pass(n1, lr, true);
+        __syncthreads();
 #pragma unroll 1
-        for (int k = 0; k < R2; ++k) {
+        for (int k = part; k < R2; k += PX) {
             const int x = n1 + 16 * k;
             const int o = sidx<N, R2, SW>(lr, x);
             const size_t gi = (size_t)(y0 + lr) * N + x;
@@ -257,7 +265,8 @@ __global__ void __launch_bounds__(MpCfg<T, N>::RNT)
                 F4[3][o] = qd;
             }
         }
-        if (mode != 2) r2_pass(n1, lr, false);
+        __syncthreads();
+        if (mode != 2 && part == 0) r2_pass(n1, lr, false);
     }
     __syncthreads();
     if (s + 1 == d.out_after) {

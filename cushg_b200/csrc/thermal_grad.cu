@@ -33,7 +33,8 @@ namespace {
 template <typename T, int N>
 cudaError_t jvp_march(const InstDesc& d, const InstDesc* d_dev, const JvpDesc& jd, cudaStream_t s) {
     using Cfg = MpCfg<T, N>;
-    const size_t row_smem = sizeof(cx<T>) * 4 * (size_t)Cfg::RB * N + sizeof(mult<T>) * N + sizeof(double) * 2 * (Cfg::RNT / 32);
+    constexpr int row_nt = Cfg::RNT * kJvpPX;
+    const size_t row_smem = sizeof(cx<T>) * 4 * (size_t)Cfg::RB * N + sizeof(mult<T>) * N + sizeof(double) * 2 * (row_nt / 32);
     const size_t col_smem = sizeof(cx<T>) * 2 * (size_t)N * Cfg::CW + sizeof(mult<T>) * (2 * (size_t)N + Cfg::CW);
     static std::once_flag once;
     static cudaError_t attr_err = cudaSuccess;
@@ -49,10 +50,10 @@ cudaError_t jvp_march(const InstDesc& d, const InstDesc* d_dev, const JvpDesc& j
     cudaError_t e = dev_alloc((void**)&L.base, JL.stride, s);
     if (e != cudaSuccess) return e;
     mp_setup_kernel<T, N><<<1, 256, 0, s>>>(d_dev, L);
-    mp_row_jvp_kernel<T, N><<<Cfg::RPART, Cfg::RNT, row_smem, s>>>(d_dev, L, JL, jd, -1);
+    mp_row_jvp_kernel<T, N><<<Cfg::RPART, row_nt, row_smem, s>>>(d_dev, L, JL, jd, -1);
     for (int st = 0; st < d.nsteps; ++st) {
         mp_col_jvp_kernel<T, N><<<dim3(N / Cfg::CW, 2), Cfg::CNT, col_smem, s>>>(d_dev, L, JL, jd, st);
-        mp_row_jvp_kernel<T, N><<<Cfg::RPART, Cfg::RNT, row_smem, s>>>(d_dev, L, JL, jd, st);
+        mp_row_jvp_kernel<T, N><<<Cfg::RPART, row_nt, row_smem, s>>>(d_dev, L, JL, jd, st);
     }
     mp_jvp_sum_kernel<T, N><<<1, 32, 0, s>>>(d_dev, L, jd);
     e = cudaGetLastError();

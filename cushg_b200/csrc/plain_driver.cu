@@ -220,6 +220,56 @@ static cudaError_t enqueue_batch(const BatchLayout& L, const InstDesc* dd, int* 
     return cudaSuccess;
 }
 
+// Host-to-device upload of a batch's descriptors through page-locked staging.  A copy from
+// pageable memory may make the driver wait for the stream to drain before it stages the data,
+// which would hold the host until the previous batch on the stream has finished and leave the
+// GPU idle while the host prepares the next one.  A small ring of page-locked slots, each
+// reused only after the copy that last read it has completed, keeps the call asynchronous.
+// While the stream is being captured the plain copy is used.
+class PinnedStage {
+  public:
+    cudaError_t upload(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+            cudaGetLastError();
+            return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+        }
+        std::lock_guard<std::mutex> lk(mu_);
+        Slot& sl = slots_[next_];
+        next_ = (next_ + 1) % kSlots;
+        cudaError_t e;
+        if (sl.done) {
+            if ((e = cudaEventSynchronize(sl.done)) != cudaSuccess) return e;
+            cudaEventDestroy(sl.done);  // recreated below on the current device
+            sl.done = nullptr;
+        }
+        if (sl.cap < bytes) {
+            if (sl.buf) cudaFreeHost(sl.buf);
+            sl.buf = nullptr;
+            sl.cap = 0;
+            if ((e = cudaHostAlloc(&sl.buf, bytes, cudaHostAllocPortable)) != cudaSuccess) return e;
+            sl.cap = bytes;
+        }
+        std::memcpy(sl.buf, src, bytes);
+        if ((e = cudaMemcpyAsync(dst, sl.buf, bytes, cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
+        if ((e = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming)) != cudaSuccess) return e;
+        return cudaEventRecord(sl.done, s);
+    }
+
+  private:
+    static constexpr int kSlots = 4;
+    struct Slot {
+        void* buf = nullptr;
+        size_t cap = 0;
+        cudaEvent_t done = nullptr;
+    };
+    Slot slots_[kSlots];
+    int next_ = 0;
+    std::mutex mu_;
+};
+
+static PinnedStage g_desc_stage;  // process lifetime; its page-locked slots are held until exit
+
 static size_t batch_bytes(int count) {
     return sizeof(InstDesc) * (size_t)count + 2 * sizeof(double) * (size_t)count + sizeof(int) * 64;
 }
@@ -238,9 +288,8 @@ shg_status plain_solve_batch(const shg_params* params, int count, void* const* p
     shg_status rc = SHG_OK;
     do {
         if (L.groups.size() > 64) { rc = fail(SHG_ERR_UNSUPPORTED, "more than 64 kernel variants in one batch"); break; }
-        if ((e = cudaMemcpyAsync(dd, L.descs.data(), sizeof(InstDesc) * (size_t)count, cudaMemcpyHostToDevice,
-                                 stream)) != cudaSuccess) {
-            rc = cuda_fail(e, "cudaMemcpyAsync descs");
+        if ((e = g_desc_stage.upload(dd, L.descs.data(), sizeof(InstDesc) * (size_t)count, stream)) != cudaSuccess) {
+            rc = cuda_fail(e, "descriptor upload");
             break;
         }
         int dev = 0;

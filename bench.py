@@ -296,7 +296,9 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
                      "traffic": SWEEP_256_DRAM_BYTES_PER_LAUNCH if (args.precision == 32 and not args.class_side) else None,
                      "traffic_note": "DRAM bytes per launch of the 256x256 FP32 class, ncu capture of this bench",
                      "peak_source": f"nominal {B200_SMS} SMs x {lanes} lanes x 2 flop x measured median SM clock {sm_mhz:.0f} MHz",
-                     "kernel": f"ssfm_plain_kernel, {nmax}x{nmax} class ({len(dom)} instances), one launch",
+                     "kernel": f"ssfm_plain_kernel, {nmax}x{nmax} class ({len(dom)} instances), one launch, "
+                               + next((f"{t['cluster']}-CTA clusters x {t['threads']} threads (tuned)"
+                                       for t in tuned if t["n"] == nmax), "compiled default split"),
                      "launch_ms": dom_ms, "flops_per_launch": algorithmic_flops(dom),
                      "sweep": {"achieved": sweep_tflops, "frac": sweep_tflops / peak, "flops": fl,
                                "note": "all four classes, concurrent on forked streams"},

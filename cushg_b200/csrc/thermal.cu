@@ -124,7 +124,10 @@ __global__ void __launch_bounds__(256) jacobi_kernel(const R* __restrict__ Ti, R
 //   FP32 512x512x250: 249 us (one voxel) -> 203 (z-blocked) -> 166 (z-blocked, pairs), 4.7 TB/s
 //   FP64 512x512x250: 318 us (one voxel) -> 282 (z-blocked, pairs), 5.6 TB/s
 //   FP64 128x128x200 (L2-resident): 16.6 -> 14.5 us
-constexpr int kJacobiZB = 8;
+// Planes per z-block: 16.  Per sweep at 512x512x250, z-blocks of 4 / 8 / 16 planes measured
+// 145 / 142 / 141 us (FP32) and 286 / 280 / 276 us (FP64); at 128x128x200 FP64 all three take
+// 14.4 us (the 79 MB sweep streams at HBM speed either way).
+constexpr int kJacobiZB = 16;
 
 // The z-blocked sweep with two x-adjacent voxels per thread: the centre column, its y
 // neighbours and Q are read as float2 / double2 (rows are 8- / 16-byte aligned since n is

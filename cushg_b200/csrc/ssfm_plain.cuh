@@ -262,16 +262,34 @@ __device__ __forceinline__ double2 pump_value(const InstDesc& d, int x, int y, d
 // (PhaseMatching.h:27-44), in FP64.
 template <typename T>
 __device__ __forceinline__ void thermal_coef(const InstDesc& d, double dki, int sl, double np, double ns, cx<T>* cf) {
-    const double kp = d.kf_p / np, ks = d.kf_s / ns;
     const double sr = (double)sl, b = sr + 1.0;
+    if constexpr (sizeof(T) == 4) {
+        // FP32 run: the phases (up to hundreds of radians) and their reduction to [-π, π] in
+        // FP64, then sine, cosine and κ/n in FP32, accurate to the float rounding the
+        // coefficients get anyway; one FP64 division instead of five and no FP64 sincos
+        const double q = dki / b, two_pi = 6.283185307179586476925, inv_two_pi = 0.159154943091895335769;
+        const float kp = (float)d.kf_p / (float)np, ks = (float)d.kf_s / (float)ns;
 #pragma unroll
-    for (int j = 0; j < 3; ++j) {
-        const double inc = j == 0 ? 0.0 : (j == 1 ? 0.25 : 0.5);
-        const double phi = dki * (d.dz * inc + sr * d.dz) / b;
-        double sn, cs;
-        sincos(phi, &sn, &cs);
-        cf[j] = mk<T>((T)(kp * sn), (T)(kp * cs));
-        cf[3 + j] = mk<T>((T)(-ks * sn), (T)(ks * cs));
+        for (int j = 0; j < 3; ++j) {
+            const double inc = j == 0 ? 0.0 : (j == 1 ? 0.25 : 0.5);
+            const double phi = q * (d.dz * inc + sr * d.dz);
+            const float r = (float)fma(-two_pi, rint(phi * inv_two_pi), phi);
+            float sn, cs;
+            sincosf(r, &sn, &cs);
+            cf[j] = mk<T>(kp * sn, kp * cs);
+            cf[3 + j] = mk<T>(-ks * sn, ks * cs);
+        }
+    } else {
+        const double kp = d.kf_p / np, ks = d.kf_s / ns;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const double inc = j == 0 ? 0.0 : (j == 1 ? 0.25 : 0.5);
+            const double phi = dki * (d.dz * inc + sr * d.dz) / b;
+            double sn, cs;
+            sincos(phi, &sn, &cs);
+            cf[j] = mk<T>((T)(kp * sn), (T)(kp * cs));
+            cf[3 + j] = mk<T>((T)(-ks * sn), (T)(ks * cs));
+        }
     }
 }
 

@@ -86,9 +86,33 @@ __device__ __forceinline__ void rk4_jvp(cx<T>& P, cx<T>& S, cx<T>& Pd, cx<T>& Sd
 template <typename T>
 __device__ __forceinline__ void thermal_coef_jvp(const InstDesc& d, double dki, double dkid, int sl, double np,
                                                  double ns, double npd, double nsd, cx<T>* cf, cx<T>* cfd) {
+    const double sr = (double)sl, b = sr + 1.0;
+    if constexpr (sizeof(T) == 4) {
+        // FP32 run: cf exactly as thermal_coef computes it (FP64 phase and reduction, FP32
+        // sine, cosine and κ/n), so the tangent march's forward part repeats the forward
+        // march; the tangents in FP32
+        const double q = dki / b, qd = dkid / b, two_pi = 6.283185307179586476925,
+                     inv_two_pi = 0.159154943091895335769;
+        const float kp = (float)d.kf_p / (float)np, ks = (float)d.kf_s / (float)ns;
+        const float kpd = -kp * (float)npd / (float)np, ksd = -ks * (float)nsd / (float)ns;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const double inc = j == 0 ? 0.0 : (j == 1 ? 0.25 : 0.5);
+            const double zj = d.dz * inc + sr * d.dz;
+            const double phi = q * zj;
+            const float r = (float)fma(-two_pi, rint(phi * inv_two_pi), phi);
+            const float phid = (float)(qd * zj);
+            float sn, cs;
+            sincosf(r, &sn, &cs);
+            cf[j] = mk<T>(kp * sn, kp * cs);
+            cf[3 + j] = mk<T>(-ks * sn, ks * cs);
+            cfd[j] = mk<T>(kpd * sn + kp * cs * phid, kpd * cs - kp * sn * phid);
+            cfd[3 + j] = mk<T>(-ksd * sn - ks * cs * phid, ksd * cs - ks * sn * phid);
+        }
+        return;
+    }
     const double kp = d.kf_p / np, ks = d.kf_s / ns;
     const double kpd = -kp * npd / np, ksd = -ks * nsd / ns;
-    const double sr = (double)sl, b = sr + 1.0;
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
         const double inc = j == 0 ? 0.0 : (j == 1 ? 0.25 : 0.5);

@@ -216,8 +216,10 @@ __global__ void __launch_bounds__(MpCfg<T, N>::row_threads(THERM))
         const int job = tid % JOBS, part = tid / JOBS;
         const int n1 = job & 15, lr = job >> 4;
         double* dkint = THERM ? reinterpret_cast<double*>(wbase + L.off_dk) : nullptr;
+        // the R2 stages of the job's two fields: on its first thread, or with several threads
+        // per job one field each on the first two
 #pragma unroll 1
-        for (int f = 0; f < 2 && mode != 0 && part == 0; ++f) {
+        for (int f = PX > 1 ? part : 0; f < (PX > 1 ? part + 1 : 2) && f < 2 && mode != 0; ++f) {
             V* F = f ? Ss : Ps;
             V v[R2];
 #pragma unroll
@@ -264,7 +266,7 @@ __global__ void __launch_bounds__(MpCfg<T, N>::row_threads(THERM))
         }
         if constexpr (PX > 1) __syncthreads();
 #pragma unroll 1
-        for (int f = 0; f < 2 && mode != 2 && part == 0; ++f) {
+        for (int f = PX > 1 ? part : 0; f < (PX > 1 ? part + 1 : 2) && f < 2 && mode != 2; ++f) {
             V* F = f ? Ss : Ps;
             V v[R2];
 #pragma unroll

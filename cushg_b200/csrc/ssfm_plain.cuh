@@ -310,13 +310,24 @@ __device__ __forceinline__ void boundary_point(const InstDesc& d, int mode, int 
     const R* tdk = reinterpret_cast<const R*>(d.t_dk);
     R* tq = reinterpret_cast<R*>(d.t_q);
     const int h0 = mode == 0 ? 1 : 0, h1 = mode == 2 ? 1 : 2;
+    // thermal: the per-voxel optics of both half steps, read before any arithmetic through
+    // the read-only path (the march never writes them), so that they are in flight together
+    R pre_np[2] = {0, 0}, pre_ns[2] = {0, 0}, pre_dk = 0;
+    if constexpr (THERM) {
+        for (int h = h0; h < h1; ++h) {
+            const size_t gz = (size_t)(s + h) * nn + g;
+            pre_np[h] = __ldg(tnp + gz);
+            pre_ns[h] = __ldg(tns + gz);
+            if (h == 1) pre_dk = __ldg(tdk + gz);
+        }
+    }
 #pragma unroll 1
     for (int h = h0; h < h1; ++h) {
         const int sl = s + h;  // slice of this half step
         if constexpr (THERM) {
             const size_t gz = (size_t)sl * nn + g;
-            if (h == 1) *dki = (mode == 0 ? 0.0 : *dki) + (double)tdk[gz];
-            const double np = (double)tnp[gz], ns = (double)tns[gz];
+            if (h == 1) *dki = (mode == 0 ? 0.0 : *dki) + (double)pre_dk;
+            const double np = (double)pre_np[h], ns = (double)pre_ns[h];
             V cf[6];
             thermal_coef<T>(d, *dki, sl, np, ns, cf);
             rk4_point<T>(p, q, cf, hap, has, (T)(0.5 * (d.bf_s * ns)), dz6);

@@ -223,9 +223,10 @@ __global__ void __launch_bounds__(MpCfg<T, N>::RNT * kJvpPX)
             }
         }
     };
-    auto r2_pass = [&](int n1, int lr, bool inv) {
+    // the R2 stages of planes [f0, f1) of job (lr, n1)
+    auto r2_pass = [&](int n1, int lr, bool inv, int f0, int f1) {
 #pragma unroll 1
-        for (int f = 0; f < 4; ++f) {
+        for (int f = f0; f < f1; ++f) {
             V v[R2];
 #pragma unroll
             for (int k = 0; k < R2; ++k) v[k] = F4[f][sidx<N, R2, SW>(lr, n1 + 16 * k)];
@@ -251,7 +252,9 @@ __global__ void __launch_bounds__(MpCfg<T, N>::RNT * kJvpPX)
         // one (row, n1) job per JOBS threads: its R2 stages on the first, its points shared
         const int job = tid % JOBS, part = tid / JOBS;
         const int n1 = job & 15, lr = job >> 4;
-        if (mode != 0 && part == 0) r2_pass(n1, lr, true);
+        // the four planes' R2 stages split over the job's PX threads
+        const int f0 = part * 4 / PX, f1 = (part + 1) * 4 / PX;
+        if (mode != 0) r2_pass(n1, lr, true, f0, f1);
         __syncthreads();
 #pragma unroll 1
         for (int k = part; k < R2; k += PX) {
@@ -290,7 +293,7 @@ __global__ void __launch_bounds__(MpCfg<T, N>::RNT * kJvpPX)
             }
         }
         __syncthreads();
-        if (mode != 2 && part == 0) r2_pass(n1, lr, false);
+        if (mode != 2) r2_pass(n1, lr, false, f0, f1);
     }
     __syncthreads();
     if (s + 1 == d.out_after) {

@@ -93,3 +93,30 @@ def test_fixed_sweep_rule_needs_counts():
     assert shg.check_params(p) == P.SHG_ERR_INVALID
     assert shg.check_params(p.replace(max_sweeps=10, max_outer=2)) == P.SHG_OK
     assert shg.check_params(p.replace(conv_rule=3)) == P.SHG_ERR_INVALID
+
+
+def test_batch_autotune_arguments_are_checked_before_the_device():
+    """shg_autotune_batch validates its arguments on the host: a null or empty batch, a null
+    result array, a forced march and mixed precisions are SHG_ERR_INVALID; a valid batch on a
+    machine without a GPU is SHG_ERR_NO_DEVICE.  shg_autotune_reset never fails."""
+    import ctypes
+    from cushg_b200.shg import ShgTuneResult, ShgParams
+
+    L = shg.lib()
+    p = P.config_plain_64().replace(precision=32)
+    out = (ShgTuneResult * 4)()
+    n = ctypes.c_int32(0)
+
+    def call(ps, count, res=out, cap=4):
+        arr = (ShgParams * max(1, len(ps)))(*ps) if ps else None
+        return L.shg_autotune_batch(arr, count, res, cap, ctypes.byref(n))
+
+    assert call([], 0) == P.SHG_ERR_INVALID
+    assert call([p], 1, res=None) == P.SHG_ERR_INVALID
+    assert call([p], 1, cap=0) == P.SHG_ERR_INVALID
+    assert call([p.replace(march=P.SHG_MARCH_FUSED)], 1) == P.SHG_ERR_INVALID
+    assert call([p, p.replace(precision=64)], 2) == P.SHG_ERR_INVALID
+    import torch
+    if not torch.cuda.is_available():
+        assert call([p], 1) == P.SHG_ERR_NO_DEVICE
+    L.shg_autotune_reset()

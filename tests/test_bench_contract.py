@@ -29,6 +29,4 @@ def test_reference_arm_prints_one_complete_line():
     e = d["e2e"]
     assert e["value"] == d["value"] and e["unit"] == d["unit"]
     assert e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0
-    with open(os.path.join(ROOT, "BASELINE.json")) as f:
-        metric = json.load(f)["metric"]
-    assert d["metric"].split(" ")[0] in metric
+    assert d["metric"] == "batched SSFM grid-pt·steps/s"

@@ -162,7 +162,11 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     # whole batch (untimed): the classes share the SMs, so a class's fastest split alone can
     # slow the sweep
     tuned = []
-    if not args.no_autotune:
+    if args.class_side and args.class_schedule:
+        c, t = (int(v) for v in args.class_schedule.split(","))
+        shg.set_schedule(args.precision, args.class_side, c, t)
+        tuned.append({"n": args.class_side, "cluster": c, "threads": t, "candidates": 1, "gain": 1.0})
+    elif not args.no_autotune:
         for r in shg.autotune_batch(ps):
             tuned.append({"n": r["n"], "cluster": r["cluster"], "threads": r["threads"], "candidates": r["candidates"],
                           "gain": r["pt_steps_per_s"] / r["default_pt_steps_per_s"]})
@@ -600,6 +604,8 @@ def main() -> int:
     ap.add_argument("--class-side", type=int, default=0, help="profile case: one grid-size class only")
     ap.add_argument("--class-count", type=int, default=18)
     ap.add_argument("--class-nz", type=int, default=24)
+    ap.add_argument("--class-schedule", default="",
+                    help="with --class-side: the compiled split to use, as CLUSTER,THREADS (shg_set_schedule)")
     ap.add_argument("--workload", default="sweep", choices=["sweep", "thermal", "adjoint", "jacobi", "thermal-batch"])
     ap.add_argument("--thermal-count", type=int, default=8)
     ap.add_argument("--thermal-fixed-sweeps", type=int, default=200)

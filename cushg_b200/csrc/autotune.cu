@@ -227,3 +227,19 @@ extern "C" shg_status shg_autotune_batch(const shg_params* params, int32_t count
 }
 
 extern "C" void shg_autotune_reset(void) { clear_plain_choices(); }
+
+// shg_set_schedule: the compiled variant of a class chosen by its split, without timing (for
+// example a schedule that shg_autotune_batch found in an earlier process).
+extern "C" shg_status shg_set_schedule(int32_t precision, int32_t n, int32_t cluster, int32_t threads) {
+    clear_error();
+    if (precision != 32 && precision != 64) return fail(SHG_ERR_INVALID, "precision must be 32 or 64");
+    const PlainVariant* cand[16];
+    const int nc = plain_candidates(precision, n, cand, 16);
+    for (int i = 0; i < nc; ++i)
+        if (cand[i]->cluster == cluster && cand[i]->threads == threads) {
+            set_plain_choice(cand[i]);
+            return SHG_OK;
+        }
+    return fail(SHG_ERR_UNSUPPORTED, "no compiled variant of grid side %d at precision %d with %d-CTA clusters x %d threads",
+                n, precision, cluster, threads);
+}

@@ -27,7 +27,7 @@ EXPORTS = (
     "shg_solve_batch_device", "shg_solve_batch_device_noalloc", "shg_grad", "shg_sh_power", "shg_last_error",
     "shg_status_string", "shg_version", "shg_heat_sweeps_device", "shg_batch_plan_create", "shg_batch_plan_launch",
     "shg_batch_plan_powers", "shg_batch_plan_destroy", "shg_autotune", "shg_grad_batch", "shg_solve_batch",
-    "shg_thermal_grad", "shg_autotune_batch", "shg_autotune_reset",
+    "shg_thermal_grad", "shg_autotune_batch", "shg_autotune_reset", "shg_set_schedule",
 )
 
 
@@ -122,6 +122,8 @@ def lib() -> ctypes.CDLL:
         L.shg_autotune_batch.restype = ctypes.c_int
         L.shg_autotune_reset.argtypes = []
         L.shg_autotune_reset.restype = None
+        L.shg_set_schedule.argtypes = [ctypes.c_int32] * 4
+        L.shg_set_schedule.restype = ctypes.c_int
         L.shg_last_error.restype = ctypes.c_char_p
         L.shg_status_string.argtypes = [ctypes.c_int32]
         L.shg_status_string.restype = ctypes.c_char_p
@@ -405,6 +407,11 @@ def autotune(precision: int, n: int) -> dict:
 def autotune_reset() -> None:
     """shg_autotune_reset: back to the compiled default schedules."""
     lib().shg_autotune_reset()
+
+
+def set_schedule(precision: int, n: int, cluster: int, threads: int) -> None:
+    """shg_set_schedule: use the compiled variant of (precision, n) with this split."""
+    _check(lib().shg_set_schedule(int(precision), int(n), int(cluster), int(threads)))
 
 
 def autotune_batch(ps: list[ShgParams]) -> list[dict]:

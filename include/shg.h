@@ -274,6 +274,12 @@ SHG_API shg_status shg_autotune_batch(const shg_params* params, int32_t count, s
  * default schedules.  No counterpart in the reference. */
 SHG_API void shg_autotune_reset(void);
 
+/* Choose a class's compiled variant by its split (the cluster and threads fields of a
+ * shg_tune_result), without timing: e.g. to reuse a schedule that shg_autotune_batch found in
+ * an earlier process.  SHG_ERR_UNSUPPORTED if no such variant is compiled.  No counterpart in
+ * the reference. */
+SHG_API shg_status shg_set_schedule(int32_t precision, int32_t n, int32_t cluster, int32_t threads);
+
 /*
  * The batched plain march of shg_solve_batch_device without any device allocation.  This
  * entry point has no counterpart in the reference.  It is for callers that cannot allocate

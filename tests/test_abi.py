@@ -120,3 +120,13 @@ def test_batch_autotune_arguments_are_checked_before_the_device():
     if not torch.cuda.is_available():
         assert call([p], 1) == P.SHG_ERR_NO_DEVICE
     L.shg_autotune_reset()
+
+
+def test_set_schedule_finds_compiled_splits_only():
+    """shg_set_schedule looks the split up among the compiled variants (no device needed)."""
+    L = shg.lib()
+    assert L.shg_set_schedule(32, 256, 8, 256) == P.SHG_OK
+    assert L.shg_set_schedule(32, 256, 3, 256) == P.SHG_ERR_UNSUPPORTED
+    assert L.shg_set_schedule(32, 100, 1, 128) == P.SHG_ERR_UNSUPPORTED
+    assert L.shg_set_schedule(16, 256, 8, 256) == P.SHG_ERR_INVALID
+    L.shg_autotune_reset()

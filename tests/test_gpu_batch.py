@@ -149,6 +149,22 @@ def test_batch_autotune_keeps_results(precision, default_schedules):
     assert e.value.status == P.SHG_ERR_INVALID
 
 
+@pytest.mark.parametrize("cluster,threads", [(8, 256), (16, 512)])
+def test_pinned_schedule_gives_the_same_fields(cluster, threads, default_schedules):
+    """shg_set_schedule picks a compiled 256 x 256 split without timing; the per-point
+    arithmetic is the split's, so the fields are the same bits as with the default split."""
+    import torch
+    ps = [P.workload(256, 9, 4000.0, 5.0 + i, 30.0, 2000.0, 30.0, precision=32) for i in range(5)]
+    ref_p, ref_s = device_outputs(ps)
+    shg.solve_batch_device(ps, ref_p, ref_s)
+    shg.set_schedule(32, 256, cluster, threads)
+    got_p, got_s = device_outputs(ps)
+    shg.solve_batch_device(ps, got_p, got_s)
+    torch.cuda.synchronize()
+    for i in range(len(ps)):
+        assert torch.equal(got_s[i], ref_s[i]) and torch.equal(got_p[i], ref_p[i]), i
+
+
 def test_autotune_rejects_unbuilt_class():
     with pytest.raises(shg.ShgError) as e:
         shg.autotune(32, 100)

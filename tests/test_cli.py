@@ -28,6 +28,12 @@ def test_cli_usage_without_arguments():
     assert "usage" in r.stderr
 
 
+def test_cli_rejects_an_unknown_crystal():
+    r = subprocess.run([CLI, "5", "30", "40", "1", "0", "--crystal", "bbo"], capture_output=True, text=True)
+    assert r.returncode == 2
+    assert "--crystal takes spplt or ppln" in r.stderr
+
+
 def cli_args(p, save_only_last=1, save_t=0):
     a = [CLI, repr(p.power), repr(p.waist), repr(p.temp), str(save_only_last), str(save_t),
          "--nx", str(p.nx), "--nz", str(p.nz), "--lx", repr(p.lx), "--ly", repr(p.ly), "--lz", repr(p.lz),
@@ -35,6 +41,8 @@ def cli_args(p, save_only_last=1, save_t=0):
          "--alpha-p", repr(p.alpha_p), "--alpha-s", repr(p.alpha_s), "--beta-s", repr(p.beta_s),
          "--rho-p", repr(p.rho_p), "--rho-s", repr(p.rho_s), "--kappa", repr(p.kappa), "--h-conv", repr(p.h_conv),
          "--precision", str(p.precision)]
+    if p.crystal == P.SHG_CRYSTAL_MGO_PPLN:
+        a += ["--crystal", "ppln"]
     if p.thermal:
         a += ["--thermal", "--max-outer", str(p.max_outer), "--check-every", str(p.check_every)]
         if p.boundary == P.SHG_BOUNDARY_OVEN_SURROUNDED:
@@ -119,3 +127,17 @@ def test_cli_sweep_mode_writes_the_script_folders(tmp_path):
             assert np.array_equal(got, ref.signal), (pw, t)
             gotp = read_matrix(folder / "Pump_out_r.dat") + 1j * read_matrix(folder / "Pump_out_i.dat")
             assert np.array_equal(gotp, ref.pump), (pw, t)
+
+
+@pytest.mark.gpu
+def test_cli_second_crystal_matches_the_library(tmp_path):
+    """--crystal ppln selects MgO:PPLN: the .dat files hold the fields shg_solve gives for the
+    same parameters (written at 20 significant digits)."""
+    p = P.workload(64, 30, 8000.0, 20.0, 25.0, 3600.0, 40.0, precision=64)
+    p.crystal = P.SHG_CRYSTAL_MGO_PPLN
+    p.period = P.qpm_period(40.3, p.lambda_p, P.SHG_CRYSTAL_MGO_PPLN)
+    r = subprocess.run(cli_args(p), cwd=tmp_path, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    sig = read_matrix(tmp_path / "Signal_out_r.dat") + 1j * read_matrix(tmp_path / "Signal_out_i.dat")
+    ref = shg.solve(p).signal
+    assert np.linalg.norm(sig - ref) / np.linalg.norm(ref) <= 1e-12

@@ -421,8 +421,10 @@ def run_thermal_batch(args) -> dict:
     from cushg_b200 import shg
 
     # each 512 x 512 x 1000 FP32 instance uses about 11 GB of workspace: keep it in the
-    # library's pool from one instance to the next (read when the pool is first created)
+    # library's pool from one instance to the next (read when the pool is first created), and
+    # grow the pool to it before the timed runs (set-up, as an application would at start)
     os.environ.setdefault("SHG_POOL_KEEP_MB", "16384")
+    shg.reserve_device_memory(12 << 30)
     ps = P.config_thermal_512(args.thermal_count)
     ps = [p.replace(conv_rule=P.SHG_CONV_FIXED, max_sweeps=args.thermal_fixed_sweeps, max_outer=args.thermal_outer,
                     precision=32) for p in ps]

@@ -45,9 +45,14 @@ shg_status cuda_fail(cudaError_t e, const char* what) {
 
 void clear_error() { g_last_error.clear(); }
 
+namespace {
+std::mutex g_pool_mu;
+cudaMemPool_t g_pools[64] = {};
+}  // namespace
+
 cudaError_t dev_alloc(void** ptr, size_t bytes, cudaStream_t s) {
-    static std::mutex mu;
-    static cudaMemPool_t pools[64] = {};
+    std::mutex& mu = g_pool_mu;
+    cudaMemPool_t* pools = g_pools;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
@@ -400,6 +405,44 @@ shg_status shg_heat_sweeps_device(const shg_params* p, void* temperature_dev, co
     if (sweeps < 0) return fail(SHG_ERR_INVALID, "sweeps must be >= 0");
     if (sweeps == 0) return SHG_OK;
     return heat_sweeps_device(q, temperature_dev, q_dev, sweeps, (cudaStream_t)stream);
+}
+
+shg_status shg_reserve_device_memory(int64_t bytes) {
+    clear_error();
+    if (bytes < 0) return fail(SHG_ERR_INVALID, "bytes must be >= 0");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(SHG_ERR_NO_DEVICE, "no CUDA device visible");
+    }
+    if (bytes == 0) return SHG_OK;
+    cudaStream_t s = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
+    void* p = nullptr;
+    shg_status rc = SHG_OK;
+    if ((e = dev_alloc(&p, (size_t)bytes, s)) != cudaSuccess) {
+        rc = cuda_fail(e, "reserve");
+    } else {
+        // keep at least the reserved bytes in the pool from now on
+        int dev = 0;
+        cudaGetDevice(&dev);
+        {
+            std::lock_guard<std::mutex> lk(g_pool_mu);
+            if (dev >= 0 && dev < 64 && g_pools[dev]) {
+                unsigned long long keep = 0;
+                cudaMemPoolGetAttribute(g_pools[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+                if (keep < (unsigned long long)bytes) {
+                    keep = (unsigned long long)bytes;
+                    cudaMemPoolSetAttribute(g_pools[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+                }
+            }
+        }
+        cudaFreeAsync(p, s);
+        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) rc = cuda_fail(e, "reserve");
+    }
+    cudaStreamDestroy(s);
+    return rc;
 }
 
 shg_status shg_solve_batch(const shg_params* params, int32_t count, void* const* pump_out, void* const* signal_out,

@@ -28,6 +28,7 @@ EXPORTS = (
     "shg_status_string", "shg_version", "shg_heat_sweeps_device", "shg_batch_plan_create", "shg_batch_plan_launch",
     "shg_batch_plan_powers", "shg_batch_plan_destroy", "shg_autotune", "shg_grad_batch", "shg_solve_batch",
     "shg_thermal_grad", "shg_autotune_batch", "shg_autotune_reset", "shg_set_schedule",
+    "shg_reserve_device_memory",
 )
 
 
@@ -124,6 +125,8 @@ def lib() -> ctypes.CDLL:
         L.shg_autotune_reset.restype = None
         L.shg_set_schedule.argtypes = [ctypes.c_int32] * 4
         L.shg_set_schedule.restype = ctypes.c_int
+        L.shg_reserve_device_memory.argtypes = [ctypes.c_int64]
+        L.shg_reserve_device_memory.restype = ctypes.c_int
         L.shg_last_error.restype = ctypes.c_char_p
         L.shg_status_string.argtypes = [ctypes.c_int32]
         L.shg_status_string.restype = ctypes.c_char_p
@@ -407,6 +410,11 @@ def autotune(precision: int, n: int) -> dict:
 def autotune_reset() -> None:
     """shg_autotune_reset: back to the compiled default schedules."""
     lib().shg_autotune_reset()
+
+
+def reserve_device_memory(nbytes: int) -> None:
+    """shg_reserve_device_memory: grow the library's pool to hold nbytes and keep them."""
+    _check(lib().shg_reserve_device_memory(int(nbytes)))
 
 
 def set_schedule(precision: int, n: int, cluster: int, threads: int) -> None:

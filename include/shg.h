@@ -270,6 +270,13 @@ SHG_API shg_status shg_autotune(int32_t precision, int32_t n, shg_tune_result* o
 SHG_API shg_status shg_autotune_batch(const shg_params* params, int32_t count, shg_tune_result* out,
                                       int32_t max_out, int32_t* n_out);
 
+/* Grow the library's device memory pool on the current device to hold `bytes`, and keep at
+ * least that much from now on (raises the keep threshold of SHG_POOL_KEEP_MB).  Later calls
+ * draw their workspace from it without mapping new memory: a 512 x 512 x 1000 thermal run
+ * takes about 11 GB, and growing the pool to that is most of a first run's extra time.
+ * Synchronous.  No counterpart in the reference. */
+SHG_API shg_status shg_reserve_device_memory(int64_t bytes);
+
 /* Forget the choices of shg_autotune / shg_autotune_batch: later runs use the compiled
  * default schedules.  No counterpart in the reference. */
 SHG_API void shg_autotune_reset(void);

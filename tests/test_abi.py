@@ -130,3 +130,11 @@ def test_set_schedule_finds_compiled_splits_only():
     assert L.shg_set_schedule(32, 100, 1, 128) == P.SHG_ERR_UNSUPPORTED
     assert L.shg_set_schedule(16, 256, 8, 256) == P.SHG_ERR_INVALID
     L.shg_autotune_reset()
+
+
+def test_reserve_device_memory_checks_its_argument():
+    import torch
+    L = shg.lib()
+    assert L.shg_reserve_device_memory(-1) == P.SHG_ERR_INVALID
+    if not torch.cuda.is_available():
+        assert L.shg_reserve_device_memory(1 << 20) == P.SHG_ERR_NO_DEVICE

@@ -88,3 +88,12 @@ def test_long_march_at_the_largest_side():
     r64 = shg.solve(p.replace(precision=64))
     assert rel_l2(r32.signal, r64.signal) <= 1e-4
     assert abs(r32.sh_power - r64.sh_power) <= 1e-4 * r64.sh_power
+
+
+def test_reserved_pool_serves_later_runs():
+    """shg_reserve_device_memory grows the library's pool; runs after it give the same bits."""
+    p = P.workload(128, 12, 6000.0, 10.0, 30.0, 3000.0, 30.0, precision=32)
+    before = shg.solve(p)
+    shg.reserve_device_memory(1 << 30)
+    after = shg.solve(p)
+    assert np.array_equal(before.signal, after.signal) and before.sh_power == after.sh_power

@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(256) jacobi_zb2_kernel(const R* __restrict__ T
         const R2 above = z + 1 < nz ? ld2(i + sz) : zero2;
         const R2 ym = y > 0 ? ld2(i - sy) : zero2, yp = y + 1 < n ? ld2(i + sy) : zero2;
         const R xm = x > 0 ? Ti[i - 1] : (R)0, xp = x + 2 < n ? Ti[i + 2] : (R)0;
-        const R2 q = *reinterpret_cast<const R2*>(Q + i);
+        const R2 q = Q ? *reinterpret_cast<const R2*>(Q + i) : zero2;  // Q null: no heat source
         auto get0 = [&](int dx, int dy, int dz) -> R {
             if (dz) return dz > 0 ? above.x : below.x;
             if (dy) return dy > 0 ? yp.x : ym.x;
@@ -227,7 +227,7 @@ __global__ void __launch_bounds__(256) jacobi_zb4_kernel(const float* __restrict
         arr(z + 1 < nz ? ld4(i + sz) : zero4, above);
         arr(y > 0 ? ld4(i - sy) : zero4, ym);
         arr(y + 1 < n ? ld4(i + sy) : zero4, yp);
-        arr(*reinterpret_cast<const float4*>(Q + i), q);
+        arr(Q ? *reinterpret_cast<const float4*>(Q + i) : zero4, q);  // Q null: no heat source
         const R xm = x > 0 ? Ti[i - 1] : (R)0, xp = x + 4 < n ? Ti[i + 4] : (R)0;
         bool w[4] = {true, true, true, true};
         if (inner_xy && z >= 1 && z + 1 < nz) {

@@ -301,7 +301,9 @@ template <typename R>
 shg_status heat_run(const shg_params& p, R* T, const R* Q, int64_t sweeps, cudaStream_t s) {
     const int n = p.nx, nz = p.nz;
     const size_t nt = (size_t)n * n * nz, arr = sizeof(R) * nt;
-    const int depth = sweep_depth(p);
+    // Q null (no heat source, the sweeps read none): one sweep per launch, whose kernels
+    // take a null Q as zero
+    const int depth = Q ? sweep_depth(p) : 1;
     cudaError_t e;
     char* buf = nullptr;
     if ((e = dev_alloc((void**)&buf, arr + 256, s)) != cudaSuccess) return cuda_fail(e, "cudaMallocAsync");

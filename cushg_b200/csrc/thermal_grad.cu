@@ -68,24 +68,23 @@ shg_status thermal_tangent(const shg_params& p, const ThermalState& st, double* 
     const size_t nt = (size_t)p.nx * p.nx * p.nz, arr = sizeof(R) * nt;
     cudaError_t e;
     char* buf = nullptr;
-    if ((e = dev_alloc((void**)&buf, 5 * arr + 256, s)) != cudaSuccess) return cuda_fail(e, "cudaMallocAsync");
+    if ((e = dev_alloc((void**)&buf, 4 * arr + 256, s)) != cudaSuccess) return cuda_fail(e, "cudaMallocAsync");
     R* u = reinterpret_cast<R*>(buf);
-    R* zero = u + nt;
-    R* ddk = zero + nt;
+    R* ddk = u + nt;
     R* dnp = ddk + nt;
     R* dns = dnp + nt;
     double* dout = reinterpret_cast<double*>(dns + nt);
     shg_status rc = SHG_OK;
     do {
-        // 1. u = dT/dT_o: the homogeneous sweeps from a field of ones
-        if ((e = launch_fill<R>(u, nt, (R)1, s)) != cudaSuccess ||
-            (e = cudaMemsetAsync(zero, 0, arr, s)) != cudaSuccess) {
+        // 1. u = dT/dT_o: the homogeneous sweeps from a field of ones (no heat source: the
+        // sweeps read no Q)
+        if ((e = launch_fill<R>(u, nt, (R)1, s)) != cudaSuccess) {
             rc = cuda_fail(e, "tangent set-up");
             break;
         }
         shg_params q = p;
         q.t_inf = 0.0;
-        if (st.sweeps > 0 && (rc = heat_sweeps_device(q, u, zero, st.sweeps, s)) != SHG_OK) break;
+        if (st.sweeps > 0 && (rc = heat_sweeps_device(q, u, nullptr, st.sweeps, s)) != SHG_OK) break;
         // 2. per-voxel tangents of the optics
         if ((e = launch_optics_tangent<R>(reinterpret_cast<const R*>(st.T), u, ddk, dnp, dns, p, s)) != cudaSuccess) {
             rc = cuda_fail(e, "optics tangent");

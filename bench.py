@@ -527,7 +527,8 @@ def run_adjoint(args) -> dict:
     """Adjoint workload (outside the default sweep line): gradients of the SH power of the
     256x256 / nz = 400 FP32 run (20 mm, 30 W, w0 = 35 µm, focus 0.4 L, 30 °C) with respect to
     waist, focus, oven temperature and a 399-entry poling-phase vector drawn from N(0, 0.1 rad),
-    checkpoints every 20 steps.
+    with the library's checkpoint choice (about sqrt(steps) for one gradient; every step for a
+    batch that fills the GPU) unless --checkpoint-every sets one.
 
     value: gradients/s of a batch of `--adjoint-batch` such instances (poling seeds 0..B-1) in
     one shg_grad_batch launch; grad_over_forward: that batch's time over the batched forward
@@ -567,7 +568,8 @@ def run_adjoint(args) -> dict:
     pols = [polv(i) for i in range(B)]
     for _ in range(max(1, args.warmup - 2)):
         shg.grad_batch(ps, pols, checkpoint_every=kk)
-    gb = [shg.grad_batch(ps, pols, checkpoint_every=kk)[0]["device_ms"] for _ in range(args.steps)]
+    gbr = [shg.grad_batch(ps, pols, checkpoint_every=kk)[0] for _ in range(args.steps)]
+    gb = [r["device_ms"] for r in gbr]
     pumps = [torch.empty((p.ny, p.nx), dtype=cdt, device="cuda") for _ in range(B)]
     sigs = [torch.empty_like(t) for t in pumps]
     stream = torch.cuda.current_stream()
@@ -584,7 +586,8 @@ def run_adjoint(args) -> dict:
         fb.append(a.elapsed_time(b))
     gbm, fbm = statistics.median(gb), statistics.median(fb)
     return {"metric": "adjoint grads/s", "value": B * 1e3 / gbm, "unit": "gradients/s",
-            "workload": f"{B} x (256x256 nz={p.nz}, 3 scalars + {nst}-vector), checkpoints every {g['checkpoint_every']}",
+            "workload": f"{B} x (256x256 nz={p.nz}, 3 scalars + {nst}-vector), checkpoints every "
+                        f"{gbr[0]['checkpoint_every']} steps (single gradient: every {g['checkpoint_every']})",
             "precision": p.precision, "batch": B, "batch_grad_ms": gbm, "batch_forward_ms": fbm,
             "grad_over_forward": gbm / fbm,
             "single": {"grad_ms": gm, "forward_ms": fm, "grad_over_forward": gm / fm},
@@ -618,7 +621,8 @@ def main() -> int:
     ap.add_argument("--jacobi-sweeps", type=int, default=400)
     ap.add_argument("--thermal-side", type=int, default=0)
     ap.add_argument("--thermal-nz", type=int, default=0)
-    ap.add_argument("--checkpoint-every", type=int, default=20)
+    ap.add_argument("--checkpoint-every", type=int, default=0,
+                    help="adjoint checkpoint interval (0: the library's choice)")
     ap.add_argument("--adjoint-nz", type=int, default=0, help="adjoint workload with this nz (profiling case)")
     ap.add_argument("--adjoint-batch", type=int, default=18, help="instances of the batched gradient")
     ap.add_argument("--thermal-max-sweeps", type=int, default=0)

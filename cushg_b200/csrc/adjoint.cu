@@ -89,6 +89,7 @@ struct GradJob {
     AdjDesc a;
     int nsteps, K, M;
     size_t off_ckpt, off_seg, off_lam, off_z, off_part, off_phi, off_pol;  // in the instance's workspace
+    size_t seg_bytes;  // one segment array: two buffers, or one when a single segment holds the march
     size_t bytes;
 };
 
@@ -116,19 +117,31 @@ shg_status grad_batch(const shg_params* ps, int count, const double* const* poli
     const size_t NN = (size_t)p0.nx * p0.nx;
     const size_t cb = complex_bytes(p0);
     auto up = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    // workspace of one instance with checkpoints every K steps
+    auto layout = [&](GradJob& J, int K) {
+        J.K = K;
+        J.M = (J.nsteps + K - 1) / K;
+        J.a.K = J.K;
+        J.a.M = J.M;
+        size_t o = 0;
+        J.off_ckpt = o; o += up((size_t)J.M * 2 * NN * cb);
+        // segment m uses buffer m & 1, so a single segment needs no second buffer
+        J.seg_bytes = up((size_t)(J.M > 1 ? 2 : 1) * J.K * 2 * NN * cb);
+        J.off_seg = o;  o += 3 * J.seg_bytes;
+        J.off_lam = o;  o += up(2 * NN * cb);
+        J.off_z = o;    o += up(sizeof(double) * J.nsteps);
+        J.off_part = o; o += up(sizeof(double) * (J.M + 1) * C * kAdjAcc);
+        J.off_phi = o;  o += up(sizeof(double) * (size_t)J.nsteps * C);
+        J.off_pol = o;  o += up(sizeof(double) * J.nsteps);
+        J.bytes = o;
+    };
     std::vector<GradJob> jobs(count);
-    size_t total = 0;
     for (int i = 0; i < count; ++i) {
         const shg_params& p = ps[i];
         GradJob& J = jobs[i];
         J.nsteps = shg_steps(&p);
-        J.K = checkpoint_every > 0 ? std::min(checkpoint_every, J.nsteps)
-                                   : std::max(1, (int)std::lround(std::sqrt((double)J.nsteps)));
-        J.M = (J.nsteps + J.K - 1) / J.K;
         J.d = make_plain_desc(p, p.temp, p.temp);
         std::memset(&J.a, 0, sizeof(J.a));
-        J.a.K = J.K;
-        J.a.M = J.M;
         // central differences of the closed-form pump
         const double hw = 1e-5 * p.waist, hf = 1e-5 * std::max(std::fabs(p.focus), p.lz), hT = 1e-3;
         pump_params(p, p.waist + hw, p.focus, p.temp, J.a.pert[0]);
@@ -140,16 +153,32 @@ shg_status grad_batch(const shg_params* ps, int count, const double* const* poli
         J.a.inv2h[0] = 1.0 / (2 * hw);
         J.a.inv2h[1] = 1.0 / (2 * hf);
         J.a.inv2h[2] = 1.0 / (2 * hT);
-        size_t o = 0;
-        J.off_ckpt = o; o += up((size_t)J.M * 2 * NN * cb);
-        J.off_seg = o;  o += 3 * up((size_t)2 * J.K * 2 * NN * cb);  // two buffers each
-        J.off_lam = o;  o += up(2 * NN * cb);
-        J.off_z = o;    o += up(sizeof(double) * J.nsteps);
-        J.off_part = o; o += up(sizeof(double) * (J.M + 1) * C * kAdjAcc);
-        J.off_phi = o;  o += up(sizeof(double) * (size_t)J.nsteps * C);
-        J.off_pol = o;  o += up(sizeof(double) * J.nsteps);
-        J.bytes = o;
-        total += o;
+    }
+    // checkpoint_every <= 0: a batch whose clusters cover every SM keeps every step's fields
+    // (one segment, no re-march) when they fit in half the free device memory, since such a
+    // batch leaves no idle SMs for the re-march to overlap on; a smaller batch, or one too
+    // large for that, keeps about sqrt(steps) checkpoints and re-marches on a second stream
+    int nsm = 0;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, 0) != cudaSuccess) {
+        cudaGetLastError();
+        nsm = 0;
+    }
+    bool keep_all = false;
+    if (checkpoint_every <= 0 && nsm > 0 && (size_t)count * C >= (size_t)nsm) {
+        size_t need = 0, fr = 0, tot = 0;
+        for (GradJob& J : jobs) {
+            layout(J, J.nsteps);
+            need += J.bytes;
+        }
+        if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) keep_all = need <= fr / 2;
+        else cudaGetLastError();
+    }
+    size_t total = 0;
+    for (GradJob& J : jobs) {
+        layout(J, checkpoint_every > 0 ? std::min(checkpoint_every, J.nsteps)
+                  : keep_all          ? J.nsteps
+                                      : std::max(1, (int)std::lround(std::sqrt((double)J.nsteps))));
+        total += J.bytes;
     }
     const size_t b_desc = up(sizeof(InstDesc) * (size_t)count), b_adesc = up(sizeof(AdjDesc) * (size_t)count);
     total += b_desc + b_adesc;
@@ -170,8 +199,8 @@ shg_status grad_batch(const shg_params* ps, int count, const double* const* poli
             GradJob& J = jobs[i];
             J.a.ckpt = q + J.off_ckpt;
             J.a.seg_a2 = q + J.off_seg;
-            J.a.seg_x = q + J.off_seg + up((size_t)2 * J.K * 2 * NN * cb);
-            J.a.seg_y = q + J.off_seg + 2 * up((size_t)2 * J.K * 2 * NN * cb);
+            J.a.seg_x = q + J.off_seg + J.seg_bytes;
+            J.a.seg_y = q + J.off_seg + 2 * J.seg_bytes;
             J.a.lam = q + J.off_lam;
             J.a.zs = reinterpret_cast<const double*>(q + J.off_z);
             J.a.part = reinterpret_cast<double*>(q + J.off_part);

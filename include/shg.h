@@ -336,7 +336,8 @@ typedef struct shg_grad_result {
  * model is the reference's scheme.  poling: NULL or shg_steps(p) phases [rad], a per-step
  * phase of the QPM grating added to the mismatch phase of that step's RK4 stages (zero for
  * the reference's uniform grating).  checkpoint_every: fields are kept every that many steps
- * and re-marched in between (<= 0: about sqrt(steps)).  Host buffers, synchronous.
+ * and re-marched in between (<= 0: about sqrt(steps); >= steps: every step is kept and
+ * nothing is re-marched).  Host buffers, synchronous.
  */
 SHG_API shg_status shg_grad(const shg_params* p, const double* poling, int32_t checkpoint_every,
                             shg_grad_result* out);
@@ -346,8 +347,10 @@ SHG_API shg_status shg_grad(const shg_params* p, const double* poling, int32_t c
  * sweeps and optimisers that need many gradients at once.  All instances share precision and
  * grid side (nz and every other parameter may differ).  poling: NULL, or an array of `count`
  * pointers each NULL or to shg_steps(&params[i]) phases.  out[i] as for shg_grad (its
- * d_poling, if set, receives instance i's vector); device_ms is the whole launch.  No
- * counterpart in the reference.
+ * d_poling, if set, receives instance i's vector); device_ms is the whole launch.
+ * checkpoint_every <= 0 keeps every step's fields (no re-march) when the batch's clusters
+ * cover every SM and its workspace fits in half the free device memory, else about
+ * sqrt(steps); out[i].checkpoint_every says which.  No counterpart in the reference.
  */
 SHG_API shg_status shg_grad_batch(const shg_params* params, int32_t count, const double* const* poling,
                                   int32_t checkpoint_every, shg_grad_result* out);

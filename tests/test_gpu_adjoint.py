@@ -119,3 +119,23 @@ def test_grad_batch_equals_single_gradients():
         for key in ("sh_power", "d_waist", "d_focus", "d_temp"):
             assert g[key] == ref[key], key
         assert np.array_equal(g["d_poling"], ref["d_poling"])
+
+
+def test_batch_filling_the_gpu_keeps_every_step():
+    """With checkpoint_every <= 0, a batch whose clusters cover every SM keeps every step's
+    fields (no re-march), a small batch about sqrt(steps); both give the gradients of an
+    explicit interval to round-off."""
+    ps, pols = [], []
+    for i in range(160):
+        p = case(64, nz=13).replace(power=10.0 + 0.1 * i)
+        ps.append(p)
+        pols.append(poling_vector(p, seed=i))
+    auto = shg.grad_batch(ps, pols)
+    fixed = shg.grad_batch(ps, pols, checkpoint_every=3)
+    for a, f in zip(auto, fixed):
+        assert a["checkpoint_every"] == a["steps"] == 12 and f["checkpoint_every"] == 3
+        for key in ("sh_power", "d_waist", "d_focus", "d_temp"):
+            assert abs(a[key] - f[key]) <= 1e-12 * abs(f[key]) + 1e-300, key
+        assert np.allclose(a["d_poling"], f["d_poling"], rtol=0, atol=1e-12 * np.abs(f["d_poling"]).max())
+    small = shg.grad_batch(ps[:2], pols[:2])
+    assert all(r["checkpoint_every"] == 3 for r in small)  # round(sqrt(12))

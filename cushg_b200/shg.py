@@ -286,7 +286,9 @@ def grad(p: ShgParams, poling: np.ndarray | None = None, checkpoint_every: int =
 
 def grad_batch(ps: list[ShgParams], polings=None, checkpoint_every: int = 0) -> list[dict]:
     """Gradients of many plain runs in one launch (shg_grad_batch); polings: None or a list of
-    per-instance poling vectors (entries may be None).  Returns one dict per instance as grad."""
+    per-instance poling vectors (entries may be None).  checkpoint_every <= 0: every step's
+    fields are kept when the batch covers every SM and they fit in half the free device
+    memory, else about sqrt(steps).  Returns one dict per instance as grad."""
     n = len(ps)
     arr = (ShgParams * n)(*ps)
     DP = ctypes.POINTER(ctypes.c_double)

@@ -309,6 +309,28 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
     double acc_g0w = 0.0, acc_g0f = 0.0, acc_g0T = 0.0, acc_j = 0.0;
     V* seg_x = reinterpret_cast<V*>(a.seg_x) + seg_off;
 
+    // L2 prefetch of what adjoint step s of the segment from sb reads from global memory:
+    // x_s, the stored spectra of step s and (s > sb) a2_{s-1}, each two planes in one
+    // contiguous block. Each CTA of the cluster fetches its 1/C share of each block in 4 KB
+    // bulk prefetches (16-byte aligned: a share is a multiple of 256 bytes), so the loads of
+    // the point loop and of the column pass find it in L2 one step later.
+    auto prefetch_step = [&](int s, int sb) {
+        constexpr size_t kPair = 2 * (size_t)N * N * sizeof(V), kShare = kPair / C, kChunk = 4096;
+        constexpr int kChunks = (int)((kShare + kChunk - 1) / kChunk);
+        static_assert(kShare % 16 == 0, "bulk prefetch needs 16-byte multiples");
+        for (int i = tid; i < 3 * kChunks; i += NT) {
+            const int arr = i / kChunks, ch = i % kChunks;
+            const int slot = arr == 2 ? s - 1 - sb : s - sb;
+            if (slot < 0 || slot >= K) continue;
+            const V* blk = arr == 0 ? seg_x : (arr == 1 ? seg_y : seg_a2);
+            const char* src = reinterpret_cast<const char*>(blk) + (size_t)slot * kPair + (size_t)crank * kShare +
+                              (size_t)ch * kChunk;
+            const size_t rem = kShare - (size_t)ch * kChunk;
+            const unsigned bytes = (unsigned)(rem < kChunk ? rem : kChunk);
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+        }
+    };
+
     // ---- plane transfers between shared memory and global (natural layout) ------------
     auto load_planes = [&](const V* gp, const V* gs) {
         for (int e = tid; e < Cfg::PLANE; e += NT) {
@@ -650,6 +672,7 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
 
     // ---- adjoint march back over [sb, se) from lambda_se in shared memory ---------------
     auto backward = [&](int sb, int se) {
+        prefetch_step(se - 1, sb);
         coefs(se - 1);
         __syncthreads();
         double phi_cur = 0.0;  // this thread's part of Φ_s for the step being finished
@@ -695,6 +718,7 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
         }
         __syncthreads();
         for (int s = se - 1; s >= sb; --s) {
+            if (s > sb) prefetch_step(s - 1, sb);
             pass_rb(false);
             __syncthreads();
             pass_ca(false);

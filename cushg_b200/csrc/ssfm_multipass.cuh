@@ -113,6 +113,18 @@ __device__ __forceinline__ void r2_stage(cx<T> (&v)[R2], const mult<T>* tw, int 
     }
 }
 
+// L2 prefetch of `bytes` of global memory from p, in 4 KB bulk prefetches issued by threads
+// i, i + n, ... of the block; nothing when p or bytes is not a multiple of 16 (a bulk
+// prefetch needs both).  A prefetch only warms L2: it never changes what a load returns.
+__device__ __forceinline__ void l2_prefetch(const void* p, size_t bytes, int i, int n) {
+    const char* c = reinterpret_cast<const char*>(p);
+    if (((reinterpret_cast<uintptr_t>(c) | bytes) & 15) != 0) return;
+    for (size_t o = (size_t)i * 4096; o < bytes; o += (size_t)n * 4096) {
+        const unsigned b = (unsigned)(bytes - o < 4096 ? bytes - o : 4096);
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(c + o), "r"(b) : "memory");
+    }
+}
+
 // Row pass of step s (s = -1: the first pass, which builds the initial fields; the pass with
 // s + 1 = out_after writes the outputs and this CTA's power partials; s = nsteps-1 is the
 // last).  Grid (N / RB, count).
@@ -145,6 +157,16 @@ __global__ void __launch_bounds__(MpCfg<T, N>::row_threads(THERM))
     constexpr bool PACK = !THERM && sizeof(T) == 4;
     Rk4Pack* kpk = reinterpret_cast<Rk4Pack*>(red + 2 * (NT / 32));
 
+    if constexpr (THERM) {
+        // step s reads slices s and s + 1 of the per-voxel optics; slice s + 1 is cold in
+        // HBM. Warm this CTA's rows of slice s + 2 for the next row pass.
+        if (s + 2 < d.nsteps) {
+            const size_t off = (size_t)(s + 2) * N * N + (size_t)y0 * N, rb = sizeof(T) * RB * N;
+            l2_prefetch(reinterpret_cast<const T*>(d.t_np) + off, rb, tid, NT);
+            l2_prefetch(reinterpret_cast<const T*>(d.t_ns) + off, rb, tid, NT);
+            l2_prefetch(reinterpret_cast<const T*>(d.t_dk) + off, rb, tid, NT);
+        }
+    }
     for (int j = tid; j < N; j += NT) tw[j] = gtab[j];
     if (!THERM && tid < 3) {
         if (mode == 0) {

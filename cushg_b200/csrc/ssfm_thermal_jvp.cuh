@@ -182,6 +182,14 @@ __global__ void __launch_bounds__(MpCfg<T, N>::RNT * kJvpPX)
     double* red = reinterpret_cast<double*>(tw + N);
     const int tid = threadIdx.x, y0 = blockIdx.x * RB;
     auto cj = [](V a) { return mk<T>(a.x, -a.y); };
+    if (s + 2 < d.nsteps) {
+        // step s reads slices s and s + 1 of the optics and their tangents; warm this CTA's
+        // rows of slice s + 2 in L2 for the next row pass
+        const size_t off = (size_t)(s + 2) * N * N + (size_t)y0 * N, rb = sizeof(R) * RB * N;
+        const void* arrs[6] = {d.t_np, d.t_ns, d.t_dk, jd.dnp, jd.dns, jd.ddk};
+#pragma unroll
+        for (int a = 0; a < 6; ++a) l2_prefetch(reinterpret_cast<const R*>(arrs[a]) + off, rb, tid, NT);
+    }
     for (int j = tid; j < N; j += NT) tw[j] = gtab[j];
     if (mode == 0) {
         // setPump at T_c and its tangent (central difference of the closed form times u_c)

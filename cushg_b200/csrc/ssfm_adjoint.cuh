@@ -468,7 +468,7 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
                             } else {
                                 // dJ/dθ_f = Re(conj(Λ) i Y): Λ = this spectrum / N^2, Y = stored D X,
                                 // stored as D X / N^2 -> Re(conj(u) i Ystored)
-                                const V yv = ybuf[yo];
+                                const V yv = __ldcs(&ybuf[yo]);  // read once: evict first
                                 const T c = u[k1].y * yv.x - u[k1].x * yv.y;
                                 const T sy = (T)(fy < N / 2 ? fy : fy - N);
                                 wsum += c * (fxq + dfy2 * (sy * sy));
@@ -689,8 +689,8 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
                     const size_t g0 = (size_t)(crank + C * lr) * N + x, g1 = g0 + 16;
                     const size_t sl = (size_t)(se - 1 - sb) * 2;
                     Cx2 gp = pack2(Ps[o0], Ps[o1]), gs = pack2(Ss[o0], Ss[o1]);
-                    rk4_vjp_pair(pack2(seg_a2[sl * NN + g0], seg_a2[sl * NN + g1]),
-                                 pack2(seg_a2[(sl + 1) * NN + g0], seg_a2[(sl + 1) * NN + g1]),
+                    rk4_vjp_pair(pack2(__ldcs(&seg_a2[sl * NN + g0]), __ldcs(&seg_a2[sl * NN + g1])),
+                                 pack2(__ldcs(&seg_a2[(sl + 1) * NN + g0]), __ldcs(&seg_a2[(sl + 1) * NN + g1])),
                                  kpk + 3 * ((se - 1) & 1), nhap2, nhas2, nqs2, n2qs2, dz62, gp, gs, sp);
                     Ps[o0] = lane0(gp);
                     Ps[o1] = lane1(gp);
@@ -707,7 +707,7 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
                 const size_t g = (size_t)(crank + C * lr) * N + x;
                 const size_t sl = (size_t)(se - 1 - sb) * 2;
                 V gp = Ps[o], gs = Ss[o];
-                rk4_vjp<T>(seg_a2[sl * NN + g], seg_a2[(sl + 1) * NN + g], coef + 6 * ((se - 1) & 1), hap, has, qs, dz6,
+                rk4_vjp<T>(__ldcs(&seg_a2[sl * NN + g]), __ldcs(&seg_a2[(sl + 1) * NN + g]), coef + 6 * ((se - 1) & 1), hap, has, qs, dz6,
                            gp, gs, sn);
                 Ps[o] = gp;
                 Ss[o] = gs;
@@ -747,13 +747,13 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
                         const size_t g0 = (size_t)(crank + C * lr) * N + x, g1 = g0 + 16;
                         Cx2 gp = pack2(Ps[o0], Ps[o1]), gs = pack2(Ss[o0], Ss[o1]);
                         const size_t sx_ = (size_t)(s - sb) * 2;
-                        const Cx2 xp = pack2(seg_x[sx_ * NN + g0], seg_x[sx_ * NN + g1]);
-                        const Cx2 xs = pack2(seg_x[(sx_ + 1) * NN + g0], seg_x[(sx_ + 1) * NN + g1]);
+                        const Cx2 xp = pack2(__ldcs(&seg_x[sx_ * NN + g0]), __ldcs(&seg_x[sx_ * NN + g1]));
+                        const Cx2 xs = pack2(__ldcs(&seg_x[(sx_ + 1) * NN + g0]), __ldcs(&seg_x[(sx_ + 1) * NN + g1]));
                         rk4_vjp_pair(xp, xs, kpk + 3 * (s & 1), nhap2, nhas2, nqs2, n2qs2, dz62, gp, gs, sp);
                         if (s > sb) {
                             const size_t sl = (size_t)(s - 1 - sb) * 2;
-                            const Cx2 bp = pack2(seg_a2[sl * NN + g0], seg_a2[sl * NN + g1]);
-                            const Cx2 bs = pack2(seg_a2[(sl + 1) * NN + g0], seg_a2[(sl + 1) * NN + g1]);
+                            const Cx2 bp = pack2(__ldcs(&seg_a2[sl * NN + g0]), __ldcs(&seg_a2[sl * NN + g1]));
+                            const Cx2 bs = pack2(__ldcs(&seg_a2[(sl + 1) * NN + g0]), __ldcs(&seg_a2[(sl + 1) * NN + g1]));
                             rk4_vjp_pair(bp, bs, kpk + 3 * ((s - 1) & 1), nhap2, nhas2, nqs2, n2qs2, dz62, gp, gs, sp2);
                         }
                         Ps[o0] = lane0(gp);
@@ -775,12 +775,12 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
                     V gp = Ps[o], gs = Ss[o];
                     // x_s and (inside the segment) a2_{s-1} from the segment buffers
                     const size_t sx_ = (size_t)(s - sb) * 2;
-                    const V xp = seg_x[sx_ * NN + g], xs = seg_x[(sx_ + 1) * NN + g];
+                    const V xp = __ldcs(&seg_x[sx_ * NN + g]), xs = __ldcs(&seg_x[(sx_ + 1) * NN + g]);
                     V bp = mk<T>(0, 0), bs = mk<T>(0, 0);
                     if (s > sb) {
                         const size_t sl = (size_t)(s - 1 - sb) * 2;
-                        bp = seg_a2[sl * NN + g];
-                        bs = seg_a2[(sl + 1) * NN + g];
+                        bp = __ldcs(&seg_a2[sl * NN + g]);
+                        bs = __ldcs(&seg_a2[(sl + 1) * NN + g]);
                     }
                     rk4_vjp<T>(xp, xs, coef + 6 * (s & 1), hap, has, qs, dz6, gp, gs, sn);
                     if (s > sb) {

@@ -158,8 +158,9 @@ shg_status grad_batch(const shg_params* ps, int count, const double* const* poli
     // (one segment, no re-march) when they fit in half the free device memory, since such a
     // batch leaves no idle SMs for the re-march to overlap on; a smaller batch, or one too
     // large for that, keeps about sqrt(steps) checkpoints and re-marches on a second stream
-    int nsm = 0;
-    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, 0) != cudaSuccess) {
+    int nsm = 0, dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
         cudaGetLastError();
         nsm = 0;
     }

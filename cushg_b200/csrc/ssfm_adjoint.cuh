@@ -464,7 +464,7 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
                             const size_t yo = (size_t)fy * N + x;
                             if (!adjoint) {
                                 u[k1] = mulw(mulw(u[k1], py[fy]), px);
-                                if (ybuf) ybuf[yo] = u[k1];
+                                if (ybuf) __stcs(&ybuf[yo], u[k1]);  // read by a later launch: evict first
                             } else {
                                 // dJ/dθ_f = Re(conj(Λ) i Y): Λ = this spectrum / N^2, Y = stored D X,
                                 // stored as D X / N^2 -> Re(conj(u) i Ystored)
@@ -567,10 +567,10 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
                         const V p0 = Ps[o0], q0 = Ss[o0], p1 = Ps[o1], q1 = Ss[o1];
                         if (keep) {
                             const size_t b = (size_t)(s - seg_from) * 2 * NN;
-                            seg_a2[b + g0] = p0;
-                            seg_a2[b + g1] = p1;
-                            seg_a2[b + NN + g0] = q0;
-                            seg_a2[b + NN + g1] = q1;
+                            __stcs(&seg_a2[b + g0], p0);
+                            __stcs(&seg_a2[b + g1], p1);
+                            __stcs(&seg_a2[b + NN + g0], q0);
+                            __stcs(&seg_a2[b + NN + g1], q1);
                         }
                         if (last && !seed) continue;
                         Cx2 P = pack2(p0, p1), S = pack2(q0, q1);
@@ -587,17 +587,17 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
                         }
                         if (ckpt_mode && (s + 1) % K == 0) {
                             const size_t b = (size_t)((s + 1) / K) * 2 * NN;
-                            ckpt[b + g0] = lane0(P);
-                            ckpt[b + g1] = lane1(P);
-                            ckpt[b + NN + g0] = lane0(S);
-                            ckpt[b + NN + g1] = lane1(S);
+                            __stcs(&ckpt[b + g0], lane0(P));
+                            __stcs(&ckpt[b + g1], lane1(P));
+                            __stcs(&ckpt[b + NN + g0], lane0(S));
+                            __stcs(&ckpt[b + NN + g1], lane1(S));
                         }
                         if (s + 1 >= seg_from) {
                             const size_t b = (size_t)(s + 1 - seg_from) * 2 * NN;
-                            seg_x[b + g0] = lane0(P);
-                            seg_x[b + g1] = lane1(P);
-                            seg_x[b + NN + g0] = lane0(S);
-                            seg_x[b + NN + g1] = lane1(S);
+                            __stcs(&seg_x[b + g0], lane0(P));
+                            __stcs(&seg_x[b + g1], lane1(P));
+                            __stcs(&seg_x[b + NN + g0], lane0(S));
+                            __stcs(&seg_x[b + NN + g1], lane1(S));
                         }
                         rk4_pair(P, S, kpk + 3 * ((s + 1) & 1), nhap2, nhas2, nqs2, dz62);
                         Ps[o0] = lane0(P);
@@ -613,8 +613,8 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
                     const size_t g = (size_t)(crank + C * lr) * N + x;
                     V p = Ps[o], q = Ss[o];
                     if (keep) {
-                        seg_a2[((size_t)(s - seg_from) * 2) * NN + g] = p;
-                        seg_a2[((size_t)(s - seg_from) * 2 + 1) * NN + g] = q;
+                        __stcs(&seg_a2[((size_t)(s - seg_from) * 2) * NN + g], p);
+                        __stcs(&seg_a2[((size_t)(s - seg_from) * 2 + 1) * NN + g], q);
                     }
                     if (last && !seed) continue;
                     rk4_point<T>(p, q, coef + 6 * (s & 1), hap, has, qs, dz6);  // x_{s+1}
@@ -626,12 +626,12 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
                         continue;
                     }
                     if (ckpt_mode && (s + 1) % K == 0) {
-                        ckpt[((size_t)((s + 1) / K) * 2) * NN + g] = p;
-                        ckpt[((size_t)((s + 1) / K) * 2 + 1) * NN + g] = q;
+                        __stcs(&ckpt[((size_t)((s + 1) / K) * 2) * NN + g], p);
+                        __stcs(&ckpt[((size_t)((s + 1) / K) * 2 + 1) * NN + g], q);
                     }
                     if (s + 1 >= seg_from) {
-                        seg_x[((size_t)(s + 1 - seg_from) * 2) * NN + g] = p;
-                        seg_x[((size_t)(s + 1 - seg_from) * 2 + 1) * NN + g] = q;
+                        __stcs(&seg_x[((size_t)(s + 1 - seg_from) * 2) * NN + g], p);
+                        __stcs(&seg_x[((size_t)(s + 1 - seg_from) * 2 + 1) * NN + g], q);
                     }
                     rk4_point<T>(p, q, coef + 6 * ((s + 1) & 1), hap, has, qs, dz6);
                     Ps[o] = p;

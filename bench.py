@@ -144,6 +144,9 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
 
     ps = workload_params(args, rank)
+    if args.precision == 32 and args.fp32_guard > 0:
+        # instances whose predicted FP32 SH field error exceeds the guard run the FP64 march
+        ps = [p.replace(fp32_guard=args.fp32_guard) for p in ps]
     total_pts = world * point_steps(ps)
     if args.scaling == "strong" and not args.class_side:
         # one sweep (seed 0) split across the ranks, greedy by cost; no data-path collective
@@ -180,6 +183,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
 
     # device-timed region: inputs (descriptors) already resident after warm-up... the
     # descriptor upload is part of every call; the fields never leave the chip
+    # each step starts from an idle device after an L2 flush, like the end-to-end calls below,
+    # and both take the median over their steps
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     if dist is not None:
         dist.barrier()
@@ -187,15 +192,16 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     with ClockSampler(local_rank) as clk:
         for k in range(args.steps):
             flush.fill_(k & 0xFF)
+            torch.cuda.synchronize()
             evs[k][0].record(stream)
             sweep()
             evs[k][1].record(stream)
-        torch.cuda.synchronize()
+            torch.cuda.synchronize()
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
     times = [a.elapsed_time(b) for a, b in evs]
-    ms = sum(times) / len(times)
+    ms = statistics.median(times)
 
     # end to end through the C ABI with host buffers (shg_solve_batch): parameter sets in,
     # SH powers and both output fields back into pinned host memory every step, each
@@ -204,7 +210,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     host_s = [torch.empty((p.ny, p.nx), dtype=cdt, pin_memory=True) for p in ps]
     shg.solve_batch(ps, host_p, host_s)  # untimed: the call's own set-up
     e2e_t = []
-    for k in range(max(3, args.steps // 2)):
+    for k in range(args.steps):
         flush.fill_(k & 0xFF)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -265,7 +271,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     # accuracy of this precision against the FP64 path on the same sweep
     err = None
     if args.precision == 32 and not args.class_side:
-        ps64 = [p.replace(precision=64) for p in ps]
+        ps64 = [p.replace(precision=64, fp32_guard=0.0) for p in ps]
         p32 = shg.solve_batch_device(ps, None, None, stream=sptr)
         p64 = shg.solve_batch_device(ps64, None, None, stream=sptr)
         rel = np.abs(p32 - p64) / np.abs(p64)
@@ -312,11 +318,120 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     }
     if err is not None:
         out["fp32_error_vs_fp64"] = err
+    if args.precision == 32 and args.fp32_guard > 0:
+        prom = [p for p in ps if shg.fp32_error_estimate(p) > args.fp32_guard]
+        out["config"]["fp32_guard"] = {
+            "guard": args.fp32_guard, "instances_on_fp64_march": len(prom),
+            "point_steps_on_fp64_march_frac": point_steps(prom) / point_steps(ps),
+            "note": "instances whose predicted FP32 SH field error (shg_fp32_error_estimate) exceeds the guard "
+                    "run the FP64 march with FP32 outputs; the rest, and all transforms of the rest, run in FP32"}
+    if world == 1 and not args.class_side and args.precision == 32 and not args.no_extras:
+        # the rest of the metric: the plain per-instance FP64 path on the same sweep, and the
+        # adjoint gradients of the 256 x 256 / nz = 400 configuration
+        out["fp64_plain_per_instance"] = fp64_per_instance(ps, value)
+        out["adjoint"] = adjoint_figures(32, args.adjoint_batch, 5, 3, args.checkpoint_every)
     if args.class_side:
         out["config"]["workload"] = f"{len(ps)} instances of {args.class_side}x{args.class_side}, nz = {args.class_nz}"
     if not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(ps, args.precision)
     return out
+
+
+def fp64_per_instance(ps, fp32_batch_value: float, count: int = 32) -> dict:
+    """The plain FP64 path run per instance (one shg_solve_device call per instance, as the
+    reference runs one process per point) over a stride sample of the sweep: pt-steps/s from
+    the calls' device times, and the FP32 batch's rate over it."""
+    import torch
+    from cushg_b200 import shg
+
+    sample = [p.replace(precision=64) for p in sample_stride(ps, count)]
+    bufs = {}
+    for p in sample:
+        if p.nx not in bufs:
+            bufs[p.nx] = (torch.empty((p.ny, p.nx), dtype=torch.complex128, device="cuda"),
+                          torch.empty((p.ny, p.nx), dtype=torch.complex128, device="cuda"))
+    for p in sample[:4]:
+        shg.solve_device(p, *bufs[p.nx])
+    torch.cuda.synchronize()
+    dev_ms = sum(shg.solve_device(p, *bufs[p.nx]).device_ms for p in sample)
+    v = point_steps(sample) / (dev_ms * 1e-3)
+    single = P.config_adjoint().replace(precision=64)
+    b = (torch.empty((256, 256), dtype=torch.complex128, device="cuda"),
+         torch.empty((256, 256), dtype=torch.complex128, device="cuda"))
+    for _ in range(3):
+        shg.solve_device(single, *b)
+    t256 = statistics.median(shg.solve_device(single, *b).device_ms for _ in range(5))
+    return {"value": v, "unit": "grid-pt·steps/s", "sample": f"{len(sample)} of the sweep's instances (stride), "
+                                                               "one call each, summed device time",
+            "fp32_batch_over_fp64_per_instance": fp32_batch_value / v,
+            "n256_nz400_ms": t256, "n256_nz400_pt_steps_per_s": 256 * 256 * 399 / (t256 * 1e-3)}
+
+
+def adjoint_figures(precision: int, batch: int, steps: int, warmup: int, checkpoint_every: int = 0,
+                    nz: int = 0) -> dict:
+    """Gradients of the SH power of the 256x256 / nz = 400 run (20 mm, 30 W, w0 = 35 µm, focus
+    0.4 L, 30 °C) with respect to waist, focus, oven temperature and a 399-entry poling-phase
+    vector drawn from N(0, 0.1 rad): a batch of `batch` such instances (poling seeds 0..B-1) in
+    one shg_grad_batch call against the batched forward march of the same instances (both fill
+    the GPU, so this is the cost ratio), and one instance's latency against its forward march.
+    Medians of device times over `steps` runs after `warmup`."""
+    import torch
+    from cushg_b200 import shg
+
+    p = P.config_adjoint().replace(precision=precision)
+    if nz:
+        p = p.replace(nz=nz)
+    nst = p.nz - 1
+    kk = checkpoint_every
+    cdt = torch.complex64 if p.precision == 32 else torch.complex128
+
+    def polv(seed):
+        return np.random.default_rng(seed).normal(0.0, 0.1, size=nst)
+
+    # single instance: latency
+    pol = polv(0)
+    for _ in range(warmup):
+        shg.grad(p, pol, checkpoint_every=kk)
+    g_ms = []
+    for _ in range(steps):
+        g = shg.grad(p, pol, checkpoint_every=kk)
+        g_ms.append(g["device_ms"])
+    pump = torch.empty((p.ny, p.nx), dtype=cdt, device="cuda")
+    sig = torch.empty_like(pump)
+    for _ in range(warmup):
+        shg.solve_device(p, pump, sig)
+    f_ms = [shg.solve_device(p, pump, sig).device_ms for _ in range(steps)]
+    gm, fm = statistics.median(g_ms), statistics.median(f_ms)
+
+    # batch: throughput and cost ratio
+    ps = [p] * batch
+    pols = [polv(i) for i in range(batch)]
+    for _ in range(max(1, warmup - 2)):
+        shg.grad_batch(ps, pols, checkpoint_every=kk)
+    gbr = [shg.grad_batch(ps, pols, checkpoint_every=kk)[0] for _ in range(steps)]
+    gb = [r["device_ms"] for r in gbr]
+    pumps = [torch.empty((p.ny, p.nx), dtype=cdt, device="cuda") for _ in range(batch)]
+    sigs = [torch.empty_like(t) for t in pumps]
+    stream = torch.cuda.current_stream()
+    for _ in range(warmup):
+        shg.solve_batch_device(ps, pumps, sigs, stream=stream.cuda_stream, want_power=False)
+    torch.cuda.synchronize()
+    fb = []
+    for _ in range(steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        shg.solve_batch_device(ps, pumps, sigs, stream=stream.cuda_stream, want_power=False)
+        b.record(stream)
+        torch.cuda.synchronize()
+        fb.append(a.elapsed_time(b))
+    gbm, fbm = statistics.median(gb), statistics.median(fb)
+    return {"value": batch * 1e3 / gbm, "unit": "gradients/s",
+            "workload": f"{batch} x (256x256 nz={p.nz}, 3 scalars + {nst}-vector), checkpoints every "
+                        f"{gbr[0]['checkpoint_every']} steps (single gradient: every {g['checkpoint_every']})",
+            "precision": p.precision, "batch": batch, "batch_grad_ms": gbm, "batch_forward_ms": fbm,
+            "grad_over_forward": gbm / fbm,
+            "single": {"grad_ms": gm, "forward_ms": fm, "grad_over_forward": gm / fm},
+            "sh_power_w": g["sh_power"], "d_waist": g["d_waist"], "d_focus": g["d_focus"], "d_temp": g["d_temp"]}
 
 
 def cpu_baseline(ps, precision: int, count: int = 24) -> dict:
@@ -416,18 +531,47 @@ def run_thermal_batch(args) -> dict:
     `--thermal-fixed-sweeps` Jacobi sweeps (FP64 residual of the last one reported) in each of
     `--thermal-outer` outer iterations.  Jacobi to max|ΔT| < 1e-6 K at this size needs on the
     order of 1e6 sweeps per outer iteration, beyond a bench budget.  Each instance also gets
-    dJ/dT_oven through its temperature field (shg_thermal_grad), unless --no-thermal-grad."""
+    dJ/dT_oven through its temperature field, unless --no-thermal-grad.  `--thermal-mode batch`
+    (default): all instances in one shg_thermal_batch call (optical and tangent passes batched);
+    `sequential`: one shg_solve_device / shg_thermal_grad call per instance."""
     import torch
     from cushg_b200 import shg
 
     # each 512 x 512 x 1000 FP32 instance uses about 11 GB of workspace: keep it in the
     # library's pool from one instance to the next (read when the pool is first created), and
     # grow the pool to it before the timed runs (set-up, as an application would at start)
-    os.environ.setdefault("SHG_POOL_KEEP_MB", "16384")
-    shg.reserve_device_memory(12 << 30)
     ps = P.config_thermal_512(args.thermal_count)
     ps = [p.replace(conv_rule=P.SHG_CONV_FIXED, max_sweeps=args.thermal_fixed_sweeps, max_outer=args.thermal_outer,
                     precision=32) for p in ps]
+    if args.thermal_mode == "batch":
+        # all instances in one shg_thermal_batch call: every instance's buffers and tangent at
+        # once (about 11.5 GB each at 512 x 512 x 1000 FP32), in the pool before timing
+        os.environ.setdefault("SHG_POOL_KEEP_MB", str(12 * 1024 * len(ps) + 4096))
+        shg.reserve_device_memory((12 << 30) * len(ps))
+        grad = not args.no_thermal_grad
+        for _ in range(1):  # warm-up on two instances: kernel loading, pool growth
+            shg.thermal_batch([q.replace(max_sweeps=2, nz=20) for q in ps[:2]], grad=grad)
+        torch.cuda.synchronize()
+        with ClockSampler(0) as clk:
+            t0 = time.perf_counter()
+            stats, dt = shg.thermal_batch(ps, grad=grad)
+            torch.cuda.synchronize()
+            wall_ms = 1e3 * (time.perf_counter() - t0)
+        runs = []
+        for i, (p, st) in enumerate(zip(ps, stats)):
+            r = {"oven_c": round(p.temp, 2), "sh_power_w": st.sh_power, "sweeps": st.jacobi_sweeps,
+                 "jacobi_ms": st.jacobi_ms, "optics_ms": st.optics_ms, "last_max_dT_K": st.last_residual}
+            if dt is not None:
+                r["dJ_dToven_w_per_k"] = float(dt[i])
+            runs.append(r)
+        return {"metric": "thermal batch time", "value": stats[0].device_ms, "unit": "ms", "higher_is_better": False,
+                "timing": "device time of one shg_thermal_batch call (CUDA events)", "wall_ms": wall_ms,
+                "mode": "batch", "with_gradient": grad,
+                "workload": f"{len(ps)} x thermal 512x512x1000 FP32, {args.thermal_outer} outer x "
+                            f"{args.thermal_fixed_sweeps} Jacobi sweeps each",
+                "instances": runs, "clocks": clk.summary()}
+    os.environ.setdefault("SHG_POOL_KEEP_MB", "16384")
+    shg.reserve_device_memory(12 << 30)
 
     def one(p):
         if args.no_thermal_grad:
@@ -524,74 +668,12 @@ def run_jacobi(args) -> dict:
 
 
 def run_adjoint(args) -> dict:
-    """Adjoint workload (outside the default sweep line): gradients of the SH power of the
-    256x256 / nz = 400 FP32 run (20 mm, 30 W, w0 = 35 µm, focus 0.4 L, 30 °C) with respect to
-    waist, focus, oven temperature and a 399-entry poling-phase vector drawn from N(0, 0.1 rad),
-    with the library's checkpoint choice (about sqrt(steps) for one gradient; every step for a
-    batch that fills the GPU) unless --checkpoint-every sets one.
-
-    value: gradients/s of a batch of `--adjoint-batch` such instances (poling seeds 0..B-1) in
-    one shg_grad_batch launch; grad_over_forward: that batch's time over the batched forward
-    march of the same instances (both fill the GPU, so this is the cost ratio).  The single
-    instance's latency against its forward march is reported beside it."""
-    import torch
-    from cushg_b200 import shg
-
-    p = P.config_adjoint().replace(precision=args.precision)
-    if args.adjoint_nz:
-        p = p.replace(nz=args.adjoint_nz)
-    nst = p.nz - 1
-    kk = args.checkpoint_every
-    cdt = torch.complex64 if p.precision == 32 else torch.complex128
-
-    def polv(seed):
-        return np.random.default_rng(seed).normal(0.0, 0.1, size=nst)
-
-    # single instance: latency
-    pol = polv(0)
-    for _ in range(args.warmup):
-        shg.grad(p, pol, checkpoint_every=kk)
-    g_ms = []
-    for _ in range(args.steps):
-        g = shg.grad(p, pol, checkpoint_every=kk)
-        g_ms.append(g["device_ms"])
-    pump = torch.empty((p.ny, p.nx), dtype=cdt, device="cuda")
-    sig = torch.empty_like(pump)
-    for _ in range(args.warmup):
-        shg.solve_device(p, pump, sig)
-    f_ms = [shg.solve_device(p, pump, sig).device_ms for _ in range(args.steps)]
-    gm, fm = statistics.median(g_ms), statistics.median(f_ms)
-
-    # batch: throughput and cost ratio
-    B = args.adjoint_batch
-    ps = [p] * B
-    pols = [polv(i) for i in range(B)]
-    for _ in range(max(1, args.warmup - 2)):
-        shg.grad_batch(ps, pols, checkpoint_every=kk)
-    gbr = [shg.grad_batch(ps, pols, checkpoint_every=kk)[0] for _ in range(args.steps)]
-    gb = [r["device_ms"] for r in gbr]
-    pumps = [torch.empty((p.ny, p.nx), dtype=cdt, device="cuda") for _ in range(B)]
-    sigs = [torch.empty_like(t) for t in pumps]
-    stream = torch.cuda.current_stream()
-    for _ in range(args.warmup):
-        shg.solve_batch_device(ps, pumps, sigs, stream=stream.cuda_stream, want_power=False)
-    torch.cuda.synchronize()
-    fb = []
-    for _ in range(args.steps):
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        shg.solve_batch_device(ps, pumps, sigs, stream=stream.cuda_stream, want_power=False)
-        b.record(stream)
-        torch.cuda.synchronize()
-        fb.append(a.elapsed_time(b))
-    gbm, fbm = statistics.median(gb), statistics.median(fb)
-    return {"metric": "adjoint grads/s", "value": B * 1e3 / gbm, "unit": "gradients/s",
-            "workload": f"{B} x (256x256 nz={p.nz}, 3 scalars + {nst}-vector), checkpoints every "
-                        f"{gbr[0]['checkpoint_every']} steps (single gradient: every {g['checkpoint_every']})",
-            "precision": p.precision, "batch": B, "batch_grad_ms": gbm, "batch_forward_ms": fbm,
-            "grad_over_forward": gbm / fbm,
-            "single": {"grad_ms": gm, "forward_ms": fm, "grad_over_forward": gm / fm},
-            "sh_power_w": g["sh_power"], "d_waist": g["d_waist"], "d_focus": g["d_focus"], "d_temp": g["d_temp"]}
+    """Adjoint workload (outside the default sweep line; the default line carries the same
+    figures under "adjoint"): see adjoint_figures.  value: gradients/s of a batch of
+    `--adjoint-batch` instances in one shg_grad_batch launch."""
+    r = adjoint_figures(args.precision, args.adjoint_batch, args.steps, args.warmup, args.checkpoint_every,
+                        args.adjoint_nz)
+    return {"metric": "adjoint grads/s", **r}
 
 
 def main() -> int:
@@ -602,6 +684,11 @@ def main() -> int:
     ap.add_argument("--precision", type=int, default=32, choices=[32, 64])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--fp32-guard", type=float, default=5e-6,
+                    help="FP32 sweep: instances whose predicted FP32 SH field error exceeds this run the FP64 "
+                         "march (0: all FP32)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="sweep line without the FP64 per-instance and adjoint figures (profiling runs)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="use the compiled default launch schedules (default: shg_autotune_batch on the workload)")
     ap.add_argument("--scaling", default="weak", choices=["weak", "strong"],
@@ -617,7 +704,9 @@ def main() -> int:
     ap.add_argument("--thermal-outer", type=int, default=2)
     ap.add_argument("--no-thermal-grad", action="store_true", help="thermal-batch: the runs without dJ/dT_oven")
     ap.add_argument("--thermal-concurrency", type=int, default=1,
-                    help="thermal-batch: instances run at a time from host threads")
+                    help="thermal-batch, sequential mode: instances run at a time from host threads")
+    ap.add_argument("--thermal-mode", default="batch", choices=["batch", "sequential"],
+                    help="thermal-batch: one shg_thermal_batch call, or one run per instance")
     ap.add_argument("--jacobi-sweeps", type=int, default=400)
     ap.add_argument("--thermal-side", type=int, default=0)
     ap.add_argument("--thermal-nz", type=int, default=0)

@@ -26,12 +26,11 @@ template <typename T, int N, int C, int NT>
 cudaError_t launch_adjoint(const InstDesc* d, const AdjDesc* a, int count, int phase, int round, cudaStream_t stream) {
     using Cfg = PlainCfg<T, N, C, NT, false>;
     auto kern = ssfm_adjoint_kernel<T, N, C, NT>;
-    static std::once_flag once;
-    static cudaError_t attr_err = cudaSuccess;
-    std::call_once(once, [&]() {
-        attr_err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::smem_bytes);
-        if (attr_err == cudaSuccess && C > 8)
-            attr_err = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    static PerDevice<int> state;  // kernel attributes, once per device
+    const cudaError_t attr_err = state.get([&](int, int&) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::smem_bytes);
+        if (e == cudaSuccess && C > 8) e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        return e;
     });
     if (attr_err != cudaSuccess) return attr_err;
     cudaLaunchConfig_t cfg = {};

@@ -104,12 +104,10 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
         : "memory");
 }
 
-constexpr uint64_t kTbWaitNs = 2000000000ull;  // 2 s: a staged plane that takes longer is an error
-
 template <typename R, int BOUND, int TL>
 __global__ void __launch_bounds__(kTbThreads, 1)
     jacobi_tb_kernel(const __grid_constant__ CUtensorMap tmT, const __grid_constant__ CUtensorMap tmQ,
-                     R* __restrict__ Tf, const JacobiCoef<R> k, int zc, unsigned* __restrict__ err) {
+                     R* __restrict__ Tf, const JacobiCoef<R> k, int zc, unsigned* __restrict__ err, const TbWait w) {
     using Cfg = TbCfg<R, TL>;
     constexpr int W = kTbSide, PL = Cfg::PLANE;
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -133,6 +131,7 @@ __global__ void __launch_bounds__(kTbThreads, 1)
     }
     __syncthreads();
     auto issue = [&](int j) {  // thread 0: stage plane j of T and of Q
+        if (j == w.withhold) return;  // self-test: this plane's wait must run out
         const int s = (j - jb) % kTbSlots;
         mbar_expect_tx(&bar[s], 2u * (unsigned)Cfg::plane_bytes);
         tma_load_3d(sT + s * PL, &tmT, xs, ys, j, &bar[s]);
@@ -161,7 +160,7 @@ __global__ void __launch_bounds__(kTbThreads, 1)
         for (int l = TL; l > 0; --l) qr[l] = qr[l - 1];
         if (j < je) {
             const int s = (j - jb) % kTbSlots;
-            if (!mbar_wait_bounded(&bar[s], (unsigned)((j - jb) / kTbSlots) & 1u, kTbWaitNs)) timed_out = true;
+            if (!mbar_wait_bounded(&bar[s], (unsigned)((j - jb) / kTbSlots) & 1u, w.limit_ns)) timed_out = true;
             ring[0][0] = sT[s * PL + v * W + u];
             qr[0] = sQ[s * PL + v * W + u];
         }
@@ -200,7 +199,7 @@ __global__ void __launch_bounds__(kTbThreads, 1)
         // bounded chance to land before the CTA's shared memory is released
         atomicOr(err, 1u);
         for (int jj = jstop; jj < min(je, jstop + kTbAhead + 1); ++jj)
-            mbar_wait_bounded(&bar[(jj - jb) % kTbSlots], (unsigned)((jj - jb) / kTbSlots) & 1u, kTbWaitNs / 4);
+            mbar_wait_bounded(&bar[(jj - jb) % kTbSlots], (unsigned)((jj - jb) / kTbSlots) & 1u, w.limit_ns / 4);
     }
 }
 
@@ -222,22 +221,23 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 
 template <typename R, int BOUND, int TL>
 cudaError_t launch_tb(const CUtensorMap& tmT, const CUtensorMap& tmQ, R* Tf, const JacobiCoef<R>& k, unsigned* err,
-                      cudaStream_t s) {
+                      const TbWait& w, cudaStream_t s) {
     using Cfg = TbCfg<R, TL>;
     auto kern = jacobi_tb_kernel<R, BOUND, TL>;
-    static std::once_flag once;
-    static cudaError_t attr_err = cudaSuccess;
-    static int sms = 148;
-    std::call_once(once, [&]() {
-        attr_err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::smem_bytes);
-        int dev = 0;
-        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    });
+    static PerDevice<int> state;  // kernel attributes and the SM count, once per device
+    int sms = 0;
+    const cudaError_t attr_err = state.get(
+        [&](int dev, int& n) {
+            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::smem_bytes);
+            if (e == cudaSuccess) e = cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+            return e;
+        },
+        &sms);
     if (attr_err != cudaSuccess) return attr_err;
     const int tx = (k.n + Cfg::TX - 1) / Cfg::TX, ty = (k.n + Cfg::TY - 1) / Cfg::TY;
     const int zc = jacobi_tb_chunk(tx * ty, k.nz, TL, sms);
     const dim3 grid(tx, ty, (k.nz + zc - 1) / zc);
-    kern<<<grid, kTbThreads, Cfg::smem_bytes, s>>>(tmT, tmQ, Tf, k, zc, err);
+    kern<<<grid, kTbThreads, Cfg::smem_bytes, s>>>(tmT, tmQ, Tf, k, zc, err, w);
     return cudaGetLastError();
 }
 
@@ -281,18 +281,18 @@ shg_status make_tb_map(const R* base, int n, int nz, CUtensorMap* map) {
 
 template <typename R>
 cudaError_t launch_jacobi_tb(const CUtensorMap& tmT, const CUtensorMap& tmQ, R* Tf, const JacobiCoef<R>& k,
-                             int boundary, int depth, unsigned* err, cudaStream_t s) {
+                             int boundary, int depth, unsigned* err, cudaStream_t s, TbWait w) {
     if (boundary == SHG_BOUNDARY_OVEN_SURROUNDED) {
         switch (depth) {
-            case 2: return launch_tb<R, SHG_BOUNDARY_OVEN_SURROUNDED, 2>(tmT, tmQ, Tf, k, err, s);
-            case 3: return launch_tb<R, SHG_BOUNDARY_OVEN_SURROUNDED, 3>(tmT, tmQ, Tf, k, err, s);
-            case 4: return launch_tb<R, SHG_BOUNDARY_OVEN_SURROUNDED, 4>(tmT, tmQ, Tf, k, err, s);
+            case 2: return launch_tb<R, SHG_BOUNDARY_OVEN_SURROUNDED, 2>(tmT, tmQ, Tf, k, err, w, s);
+            case 3: return launch_tb<R, SHG_BOUNDARY_OVEN_SURROUNDED, 3>(tmT, tmQ, Tf, k, err, w, s);
+            case 4: return launch_tb<R, SHG_BOUNDARY_OVEN_SURROUNDED, 4>(tmT, tmQ, Tf, k, err, w, s);
         }
     } else {
         switch (depth) {
-            case 2: return launch_tb<R, SHG_BOUNDARY_TOP_OPEN, 2>(tmT, tmQ, Tf, k, err, s);
-            case 3: return launch_tb<R, SHG_BOUNDARY_TOP_OPEN, 3>(tmT, tmQ, Tf, k, err, s);
-            case 4: return launch_tb<R, SHG_BOUNDARY_TOP_OPEN, 4>(tmT, tmQ, Tf, k, err, s);
+            case 2: return launch_tb<R, SHG_BOUNDARY_TOP_OPEN, 2>(tmT, tmQ, Tf, k, err, w, s);
+            case 3: return launch_tb<R, SHG_BOUNDARY_TOP_OPEN, 3>(tmT, tmQ, Tf, k, err, w, s);
+            case 4: return launch_tb<R, SHG_BOUNDARY_TOP_OPEN, 4>(tmT, tmQ, Tf, k, err, w, s);
         }
     }
     return cudaErrorInvalidValue;
@@ -301,8 +301,67 @@ cudaError_t launch_jacobi_tb(const CUtensorMap& tmT, const CUtensorMap& tmQ, R* 
 template shg_status make_tb_map<float>(const float*, int, int, CUtensorMap*);
 template shg_status make_tb_map<double>(const double*, int, int, CUtensorMap*);
 template cudaError_t launch_jacobi_tb<float>(const CUtensorMap&, const CUtensorMap&, float*, const JacobiCoef<float>&,
-                                             int, int, unsigned*, cudaStream_t);
+                                             int, int, unsigned*, cudaStream_t, TbWait);
 template cudaError_t launch_jacobi_tb<double>(const CUtensorMap&, const CUtensorMap&, double*,
-                                              const JacobiCoef<double>&, int, int, unsigned*, cudaStream_t);
+                                              const JacobiCoef<double>&, int, int, unsigned*, cudaStream_t, TbWait);
+
+namespace {
+
+// Self-test of the bounded staging wait: two blocked sweeps of a 64 x 64 x 32 grid whose
+// plane `withhold` is never staged.
+template <typename R>
+shg_status selftest_wait(double wait_us, int withhold) {
+    constexpr int n = 64, nz = 32;
+    const size_t nt = (size_t)n * n * nz;
+    shg_params p;
+    shg_default_params(&p);
+    p.nx = p.ny = n;
+    p.nz = nz;
+    p.precision = sizeof(R) == 8 ? 64 : 32;
+    p.thermal = 1;
+    const JacobiCoef<R> k = make_jacobi_coef<R>(p);
+    char* buf = nullptr;
+    cudaError_t e = cudaMalloc((void**)&buf, 3 * sizeof(R) * nt + 256);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc");
+    R* Ta = reinterpret_cast<R*>(buf);
+    R* Tb = Ta + nt;
+    R* Q = Tb + nt;
+    unsigned* err = reinterpret_cast<unsigned*>(Q + nt);
+    shg_status rc = SHG_OK;
+    CUtensorMap mt, mq;
+    do {
+        if ((e = cudaMemset(buf, 0, 3 * sizeof(R) * nt + 256)) != cudaSuccess) { rc = cuda_fail(e, "cudaMemset"); break; }
+        if ((rc = make_tb_map<R>(Ta, n, nz, &mt)) != SHG_OK || (rc = make_tb_map<R>(Q, n, nz, &mq)) != SHG_OK) break;
+        TbWait w;
+        w.limit_ns = (uint64_t)(wait_us * 1e3);
+        w.withhold = withhold;
+        if ((e = launch_jacobi_tb<R>(mt, mq, Tb, k, SHG_BOUNDARY_TOP_OPEN, 2, err, nullptr, w)) != cudaSuccess ||
+            (e = cudaDeviceSynchronize()) != cudaSuccess) {
+            rc = cuda_fail(e, "blocked sweeps");
+            break;
+        }
+        unsigned h = 0;
+        if ((e = cudaMemcpy(&h, err, sizeof(h), cudaMemcpyDeviceToHost)) != cudaSuccess) { rc = cuda_fail(e, "cudaMemcpy"); break; }
+        if (h) rc = fail(SHG_ERR_CUDA, "a staged plane did not arrive within %g us (plane %d withheld)", wait_us, withhold);
+    } while (0);
+    cudaFree(buf);
+    return rc;
+}
+
+}  // namespace
 
 }  // namespace shg
+
+extern "C" shg_status shg_selftest_bounded_wait(int32_t precision, double wait_us, int32_t withhold_plane) {
+    using namespace shg;
+    clear_error();
+    if (precision != 32 && precision != 64) return fail(SHG_ERR_INVALID, "precision must be 32 or 64");
+    if (!(wait_us > 0) || wait_us > 1e7) return fail(SHG_ERR_INVALID, "wait_us must be in (0, 1e7]");
+    if (withhold_plane < -1 || withhold_plane >= 32) return fail(SHG_ERR_INVALID, "withhold_plane must be in -1..31");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(SHG_ERR_NO_DEVICE, "no CUDA device visible");
+    }
+    return precision == 64 ? selftest_wait<double>(wait_us, withhold_plane) : selftest_wait<float>(wait_us, withhold_plane);
+}

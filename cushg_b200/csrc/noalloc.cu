@@ -7,7 +7,7 @@
 // allocation can block or synchronise the device at an unpredictable moment, and plugin
 // hosts that forbid a library from allocating behind their back.  Such a caller still owns
 // and passes the input parameters and the output buffers; this entry point adds nothing
-// but kernel launches and copies into memory that exists since the library was loaded.
+// but kernel launches and a copy of the power slots back to the host.
 //
 // The scratch (instance descriptors and per-instance power slots) lives in g_noalloc_scratch,
 // a file-scope __device__ array of kNoAllocScratchBytes (about 23 KB) that every GPU which loads
@@ -15,17 +15,22 @@
 // instances per call.
 //
 // In host code the name g_noalloc_scratch is only a host-side stand-in for the device
-// symbol, not a device address; the address is obtained once per device with
-// cudaGetSymbolAddress while that device is current, on the first call made on it.  That
-// first call should therefore come before any stream capture.
+// symbol, not a device address.  The first call made on a device, with that device current,
+// sets that device up: it looks the array's address up with cudaGetSymbolAddress and loads
+// every kernel this entry point can launch (with CUDA's lazy module loading a kernel's code is
+// otherwise loaded at its first launch, and the driver may take device memory for it then).
+// So make the first call on each device before the host hands all free device memory to its
+// own allocator, and before any stream capture.  Later calls allocate nothing.
 //
-// All calls share the one array and it keeps the last call's contents.  Each call rewrites
-// the descriptors it uses and clears the power slots before its kernels run.  Calls whose
-// work overlaps on the GPU (concurrent calls on different streams, or from several host
-// threads) race on the array: serialise them.
+// The descriptors travel as a kernel parameter (a fixed 24 KB block, copied by the launch),
+// so no host staging buffer is involved.  All calls share the one array and it keeps the last
+// call's contents: each call rewrites the descriptors it uses and clears the power slots
+// before its marches run.  Calls whose work overlaps on the GPU (concurrent calls on
+// different streams, or from several host threads) race on the array: serialise them.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <mutex>
 
@@ -38,27 +43,55 @@ namespace shg {
 constexpr int kNoAllocMaxInstances = 64;
 constexpr size_t kNoAllocDescBytes = sizeof(InstDesc) * kNoAllocMaxInstances;
 constexpr size_t kNoAllocScratchBytes = ((kNoAllocDescBytes + 2 * sizeof(double) * kNoAllocMaxInstances + 255) / 256) * 256;
-constexpr int kNoAllocMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-static std::mutex g_noalloc_mu;
-static void* g_noalloc_addr[kNoAllocMaxDevices] = {};
+// The descriptors of one call, passed by value (kernel parameters may take up to 32 KB).
+struct NoAllocUpload {
+    InstDesc desc[kNoAllocMaxInstances];
+    int32_t count;
+};
+static_assert(sizeof(NoAllocUpload) <= 32000, "descriptor block exceeds the kernel parameter limit");
 
-// Device address of g_noalloc_scratch on the current device (set up once per device).
-static shg_status noalloc_scratch_address(void** out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
-    if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(SHG_ERR_UNSUPPORTED, "device ordinal %d too large", dev);
-    std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_addr[dev]) {
-        void* ptr = nullptr;
-        e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-        if (e != cudaSuccess || !ptr) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
-        g_noalloc_addr[dev] = ptr;
-    }
-    *out = g_noalloc_addr[dev];
+// Writes the call's descriptors into the scratch and clears its power slots.
+__global__ void noalloc_upload_kernel(__grid_constant__ const NoAllocUpload up, InstDesc* ddesc, double* dpow) {
+    const int words = (int)(sizeof(InstDesc) / sizeof(uint32_t));
+    static_assert(sizeof(InstDesc) % sizeof(uint32_t) == 0, "InstDesc is copied in 32-bit words");
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(up.desc);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(ddesc);
+    for (int i = threadIdx.x; i < up.count * words; i += blockDim.x) dst[i] = src[i];
+    for (int i = threadIdx.x; i < 2 * up.count; i += blockDim.x) dpow[i] = 0.0;
+}
+
+// Once per device: the device address of g_noalloc_scratch, and every kernel this entry point
+// launches loaded (a zero-instance launch of each fused plain variant runs its per-device
+// attribute set-up, which loads the kernel, and launches nothing).
+static PerDevice<void*> g_noalloc_device;
+
+static shg_status noalloc_setup(void** out) {
+    const cudaError_t e = g_noalloc_device.get(
+        [](int, void*& addr) {
+            void* ptr = nullptr;
+            cudaError_t r = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+            if (r != cudaSuccess) return r;
+            if (!ptr) return cudaErrorInvalidSymbol;
+            cudaFuncAttributes fa;
+            r = cudaFuncGetAttributes(&fa, noalloc_upload_kernel);
+            if (r != cudaSuccess) return r;
+            for (int prec : {32, 64}) {
+                const PlainVariant* cand[16];
+                for (int n = 16; n <= 256; n += 16) {
+                    const int k = plain_candidates(prec, n, cand, 16);
+                    for (int i = 0; i < k; ++i)
+                        if (cand[i]->launch && (r = cand[i]->launch(nullptr, 0, nullptr, nullptr)) != cudaSuccess)
+                            return r;
+                }
+            }
+            addr = ptr;
+            return cudaSuccess;
+        },
+        out);
+    if (e != cudaSuccess) return cuda_fail(e, "device set-up of the allocation-free march");
     return SHG_OK;
 }
 
@@ -84,22 +117,25 @@ extern "C" shg_status shg_solve_batch_device_noalloc(const shg_params* params, i
     }
     cudaStream_t stream = (cudaStream_t)stream_;
     void* base = nullptr;
-    shg_status rc = noalloc_scratch_address(&base);
+    shg_status rc = noalloc_setup(&base);
     if (rc != SHG_OK) return rc;
     InstDesc* ddesc = reinterpret_cast<InstDesc*>(base);
     double* dpow = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(base) + kNoAllocDescBytes);
 
-    // descriptors on the stack, grouped by kernel variant, longest march first
-    InstDesc descs[kNoAllocMaxInstances];
+    // kernel variants: the fused march only (the multi-pass march needs workspace); an
+    // automatic choice of the multi-pass march falls back to the fused one where it is built
     const PlainVariant* var[kNoAllocMaxInstances];
-    int order[kNoAllocMaxInstances];
+    int order[kNoAllocMaxInstances], out32[kNoAllocMaxInstances];
     for (int i = 0; i < count; ++i) {
         order[i] = i;
-        var[i] = find_plain_variant(params[i].precision, params[i].nx, 0, params[i].march);
-        if (var[i]->mp)
+        var[i] = plain_variant_of(params[i], &out32[i]);
+        if (var[i] && var[i]->mp && params[i].march == SHG_MARCH_AUTO)
+            var[i] = find_plain_variant(params[i].precision, params[i].nx, 0, SHG_MARCH_FUSED);
+        if (!var[i] || var[i]->mp)
             return fail(SHG_ERR_UNSUPPORTED, "instance %d: the multi-pass march (side %d) needs device workspace", i,
                         params[i].nx);
     }
+    // descriptors grouped by kernel variant, longest march first
     std::sort(order, order + count, [&](int a, int b) {
         if (var[a] != var[b]) return var[a] < var[b];
         const double ca = (double)params[a].nx * params[a].nx * shg_steps(&params[a]);
@@ -107,21 +143,22 @@ extern "C" shg_status shg_solve_batch_device_noalloc(const shg_params* params, i
         if (ca != cb) return ca > cb;
         return a < b;
     });
+    NoAllocUpload up;
+    std::memset(&up, 0, sizeof(up));
+    up.count = count;
     for (int k = 0; k < count; ++k) {
         const int i = order[k];
         InstDesc d = make_plain_desc(params[i], params[i].temp, params[i].temp);
         d.slot = i;
+        d.out32 = out32[i];
         d.pump_out = pump_out_dev ? pump_out_dev[i] : nullptr;
         d.signal_out = signal_out_dev ? signal_out_dev[i] : nullptr;
         d.power_out = dpow + 2 * (size_t)i;
-        descs[k] = d;
+        up.desc[k] = d;
     }
     cudaError_t e;
-    if ((e = cudaMemcpyAsync(ddesc, descs, sizeof(InstDesc) * (size_t)count, cudaMemcpyHostToDevice, stream)) !=
-        cudaSuccess)
-        return cuda_fail(e, "cudaMemcpyAsync descriptors");
-    if ((e = cudaMemsetAsync(dpow, 0, 2 * sizeof(double) * (size_t)count, stream)) != cudaSuccess)
-        return cuda_fail(e, "cudaMemsetAsync power slots");
+    noalloc_upload_kernel<<<1, 256, 0, stream>>>(up, ddesc, dpow);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "launch noalloc_upload_kernel");
     for (int k = 0; k < count;) {
         int j = k;
         while (j < count && var[order[j]] == var[order[k]]) ++j;
@@ -130,12 +167,18 @@ extern "C" shg_status shg_solve_batch_device_noalloc(const shg_params* params, i
         k = j;
     }
     if (sh_power_out) {
+        // {SH power, pump power} per instance; a NaN or Inf power fails the call as in the
+        // allocating batch, naming the instance
         double h[2 * kNoAllocMaxInstances];
         if ((e = cudaMemcpyAsync(h, dpow, 2 * sizeof(double) * (size_t)count, cudaMemcpyDeviceToHost, stream)) !=
                 cudaSuccess ||
             (e = cudaStreamSynchronize(stream)) != cudaSuccess)
             return cuda_fail(e, "batched march");
-        for (int i = 0; i < count; ++i) sh_power_out[i] = h[2 * i];
+        for (int i = 0; i < count; ++i) {
+            if (!std::isfinite(h[2 * i]) || !std::isfinite(h[2 * i + 1]))
+                return fail(SHG_ERR_NONFINITE, "instance %d: SH / pump power %g / %g", i, h[2 * i], h[2 * i + 1]);
+            sh_power_out[i] = h[2 * i];
+        }
     }
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "batched march");

@@ -58,9 +58,11 @@ cudaError_t fork_streams(int dev, ForkStreams** out) {
 shg_status plain_solve_device(const shg_params& p, const void* signal_in, void* pump_out, void* signal_out,
                               shg_stats* stats, cudaStream_t stream, void* slices_p, void* slices_s,
                               const double* poling_dev) {
-    const PlainVariant* v = find_plain_variant(p.precision, p.nx, 0, p.march);
+    int out32 = 0;
+    const PlainVariant* v = plain_variant_of(p, &out32);
     if (!v) return fail(SHG_ERR_UNSUPPORTED, "no kernel for grid side %d", p.nx);
     InstDesc d = make_plain_desc(p, p.temp, p.temp);
+    d.out32 = out32;
     d.signal_in = signal_in;
     d.has_signal_in = signal_in ? 1 : 0;
     d.pump_out = pump_out;
@@ -131,11 +133,12 @@ struct BatchLayout {
 
 static BatchLayout batch_layout(const shg_params* params, int count, void* const* pump_out, void* const* signal_out,
                                 double* power_slots) {
-    struct Item { const PlainVariant* v; int idx; double cost; };
+    struct Item { const PlainVariant* v; int idx; double cost; int out32; };
     std::vector<Item> items(count);
     for (int i = 0; i < count; ++i) {
-        const PlainVariant* v = find_plain_variant(params[i].precision, params[i].nx, 0, params[i].march);
-        items[i] = {v, i, (double)params[i].nx * params[i].nx * shg_steps(&params[i])};
+        int out32 = 0;
+        const PlainVariant* v = plain_variant_of(params[i], &out32);
+        items[i] = {v, i, (double)params[i].nx * params[i].nx * shg_steps(&params[i]), out32};
     }
     std::stable_sort(items.begin(), items.end(), [](const Item& a, const Item& b) {
         if (a.v != b.v) return a.v < b.v;
@@ -147,6 +150,7 @@ static BatchLayout batch_layout(const shg_params* params, int count, void* const
         const int i = items[k].idx;
         InstDesc d = make_plain_desc(params[i], params[i].temp, params[i].temp);
         d.slot = i;
+        d.out32 = items[k].out32;
         d.pump_out = pump_out ? pump_out[i] : nullptr;
         d.signal_out = signal_out ? signal_out[i] : nullptr;
         d.power_out = power_slots + 2 * (size_t)i;

@@ -23,7 +23,8 @@ struct InstDesc {
     double amp_re, amp_im, den_re, den_im;
     double ux, uy, dx, dy;
     int32_t elliptic;      // 1: elliptical pump, P = amp * exp(-ax^2 / den - ay^2 / deny)
-    int32_t pad0;
+    int32_t out32;         // FP64 march of an FP32 instance: signal_in, the outputs and the
+                           // slices are FP32 complex (the march rounds what it writes)
     double deny_re, deny_im;
     // propagator phase θ = -dz (a (dfx^2 sx^2 + dfy^2 sy^2) + b sx) per field,
     // sx, sy the signed FFT frequency indices

@@ -5,7 +5,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <mutex>
+
+#include "per_device.h"
 
 #include "ssfm_plain.cuh"
 #include "ssfm_variants.h"
@@ -27,29 +28,29 @@ cudaError_t launch_plain(const InstDesc* descs, int count, int* queue, cudaStrea
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = C > 1 ? 1 : 0;
-    // once per process: kernel attributes and the clusters that fit on the device at once
-    // (the size of a persistent launch); the device is the current one at the first call
-    static std::once_flag once;
-    static cudaError_t attr_err = cudaSuccess;
-    static int resident = 0;
-    std::call_once(once, [&]() {
-        attr_err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::smem_bytes);
-        if (attr_err == cudaSuccess && C > 8)
-            attr_err = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-        if (attr_err != cudaSuccess) return;
-        if (C > 1) {
-            cfg.gridDim = dim3(C, 1, 1);
-            attr_err = cudaOccupancyMaxActiveClusters(&resident, kern, &cfg);
-        } else {
-            int dev = 0, sms = 0, per_sm = 0;
-            attr_err = cudaGetDevice(&dev);
-            if (attr_err == cudaSuccess) attr_err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            if (attr_err == cudaSuccess)
-                attr_err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, Cfg::smem_bytes);
-            resident = sms * per_sm;
-        }
-        if (attr_err == cudaSuccess && resident < 1) attr_err = cudaErrorInvalidConfiguration;
-    });
+    // once per device: kernel attributes and the clusters that fit on the device at once
+    // (the size of a persistent launch)
+    static PerDevice<int> state;
+    int resident = 0;
+    const cudaError_t attr_err = state.get(
+        [&](int dev, int& res) {
+            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::smem_bytes);
+            if (e == cudaSuccess && C > 8) e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+            if (e != cudaSuccess) return e;
+            if (C > 1) {
+                cudaLaunchConfig_t occ = cfg;
+                occ.gridDim = dim3(C, 1, 1);
+                e = cudaOccupancyMaxActiveClusters(&res, kern, &occ);
+            } else {
+                int sms = 0, per_sm = 0;
+                e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+                if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, Cfg::smem_bytes);
+                res = sms * per_sm;
+            }
+            if (e == cudaSuccess && res < 1) e = cudaErrorInvalidConfiguration;
+            return e;
+        },
+        &resident);
     if (attr_err != cudaSuccess) return attr_err;
     if (count <= 0) return cudaSuccess;
     const int clusters = queue ? std::min(count, resident) : count;

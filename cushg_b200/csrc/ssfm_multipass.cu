@@ -21,14 +21,13 @@ namespace {
 template <typename T, int N, bool THERM>
 cudaError_t mp_march(const InstDesc* dev_descs, const InstDesc* host_descs, int count, cudaStream_t s) {
     using Cfg = MpCfg<T, N>;
-    static std::once_flag once;
-    static cudaError_t attr_err = cudaSuccess;
-    std::call_once(once, [] {
-        attr_err = cudaFuncSetAttribute(mp_row_kernel<T, N, THERM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)Cfg::row_smem_for(THERM));
-        if (attr_err == cudaSuccess)
-            attr_err = cudaFuncSetAttribute(mp_col_kernel<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)Cfg::col_smem);
+    static PerDevice<int> state;  // kernel attributes, once per device
+    const cudaError_t attr_err = state.get([](int, int&) {
+        cudaError_t e = cudaFuncSetAttribute(mp_row_kernel<T, N, THERM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)Cfg::row_smem_for(THERM));
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(mp_col_kernel<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::col_smem);
+        return e;
     });
     if (attr_err != cudaSuccess) return attr_err;
     if (count <= 0) return cudaSuccess;

@@ -257,6 +257,30 @@ __device__ __forceinline__ double2 pump_value(const InstDesc& d, int x, int y, d
     return make_double2(amp_re * er - amp_im * ei, amp_re * ei + amp_im * er);
 }
 
+// Caller buffers of an instance (signal_in, outputs, slices) hold complex values of the
+// working type, or FP32 complex when an FP64 march runs an FP32 instance (d.out32): the
+// march reads and rounds at the buffer, nothing else changes.
+template <typename T>
+__device__ __forceinline__ void put_field(const InstDesc& d, void* base, size_t i, cx<T> v) {
+    if constexpr (sizeof(T) == 8) {
+        if (d.out32) {
+            reinterpret_cast<float2*>(base)[i] = make_float2((float)v.x, (float)v.y);
+            return;
+        }
+    }
+    reinterpret_cast<cx<T>*>(base)[i] = v;
+}
+template <typename T>
+__device__ __forceinline__ cx<T> get_field(const InstDesc& d, const void* base, size_t i) {
+    if constexpr (sizeof(T) == 8) {
+        if (d.out32) {
+            const float2 v = reinterpret_cast<const float2*>(base)[i];
+            return mk<T>((T)v.x, (T)v.y);
+        }
+    }
+    return reinterpret_cast<const cx<T>*>(base)[i];
+}
+
 // Thermal stage coefficients at one voxel (Solver.h:33-55): κ = kf / n(λ, T(x,y,s)) and the
 // phase DKint (dz inc + s dz) / (s + 1), DKint the running sum of Δk over slices 0..s
 // (PhaseMatching.h:27-44), in FP64.
@@ -344,12 +368,12 @@ __device__ __forceinline__ void boundary_point(const InstDesc& d, int mode, int 
         if (h == 0 && s + 1 < d.nslices) {
             // per-slice record: the fields before step s+1 (Solver.h:289-295)
             const size_t gs = (size_t)(s + 1) * nn + g;
-            if (d.slices_p) reinterpret_cast<V*>(d.slices_p)[gs] = p;
-            if (d.slices_s) reinterpret_cast<V*>(d.slices_s)[gs] = q;
+            if (d.slices_p) put_field<T>(d, d.slices_p, gs, p);
+            if (d.slices_s) put_field<T>(d, d.slices_s, gs, q);
         }
         if (h == 0 && s + 1 == d.out_after) {
-            if (d.pump_out) reinterpret_cast<V*>(d.pump_out)[g] = p;
-            if (d.signal_out) reinterpret_cast<V*>(d.signal_out)[g] = q;
+            if (d.pump_out) put_field<T>(d, d.pump_out, g, p);
+            if (d.signal_out) put_field<T>(d, d.signal_out, g, q);
             double ws = 1.0, wp = 1.0;
             if constexpr (THERM) {
                 ws = (double)tns[(size_t)(s + 1) * nn + g];
@@ -424,15 +448,15 @@ __global__ void __launch_bounds__(NT, MINB)
         }
 
         // ---- initial fields: setPump (Efields.h:84-119), SH = 0 or given ---------------
-        const V* sin_g = reinterpret_cast<const V*>(d.signal_in);
         for (int e = tid; e < Cfg::PLANE; e += NT) {
             const int lr = e / N, x = e % N;
             const int y = crank + C * lr;
             const double2 pv = pump_value(d, x, y, d.amp_re, d.amp_im, d.den_re, d.den_im);
             Ps[sidx<N, R2, SW>(lr, x)] = mk<T>((T)pv.x, (T)pv.y);
-            Ss[sidx<N, R2, SW>(lr, x)] = d.has_signal_in ? sin_g[(size_t)y * N + x] : mk<T>((T)0, (T)0);
-            if (d.slices_p) reinterpret_cast<V*>(d.slices_p)[(size_t)y * N + x] = Ps[sidx<N, R2, SW>(lr, x)];
-            if (d.slices_s) reinterpret_cast<V*>(d.slices_s)[(size_t)y * N + x] = Ss[sidx<N, R2, SW>(lr, x)];
+            Ss[sidx<N, R2, SW>(lr, x)] = d.has_signal_in ? get_field<T>(d, d.signal_in, (size_t)y * N + x)
+                                                         : mk<T>((T)0, (T)0);
+            if (d.slices_p) put_field<T>(d, d.slices_p, (size_t)y * N + x, Ps[sidx<N, R2, SW>(lr, x)]);
+            if (d.slices_s) put_field<T>(d, d.slices_s, (size_t)y * N + x, Ss[sidx<N, R2, SW>(lr, x)]);
         }
         __syncthreads();
 
@@ -630,9 +654,18 @@ __global__ void __launch_bounds__(NT, MINB)
             }
         };
 
+        // Between the two row passes a CTA-wide barrier is needed only where a warp's RA jobs
+        // and RB jobs touch different rows.  With R2 == 16 both passes give job j the row j / 16
+        // and every thread the same jobs, so each warp owns its rows for RB, RA and RB' / RA'
+        // alike, and a warp barrier orders them.
+        auto row_sync = [&]() {
+            if constexpr (R2 == 16) __syncwarp();
+            else __syncthreads();
+        };
+
         double acc_s = 0.0, acc_p = 0.0;
         pass_ra(0, -1, coef, coef, acc_s, acc_p);
-        __syncthreads();
+        row_sync();
 
         double z = 0.0;
         for (int s = 0; s < nsteps; ++s) {
@@ -651,9 +684,9 @@ __global__ void __launch_bounds__(NT, MINB)
             pass_ca(true);
             __syncthreads();
             pass_rb(true);
-            __syncthreads();
+            row_sync();
             pass_ra(s + 1 < nsteps ? 1 : 2, s, cf_cur, cf_nxt, acc_s, acc_p);
-            __syncthreads();
+            row_sync();
             z += d.dz;
         }
 

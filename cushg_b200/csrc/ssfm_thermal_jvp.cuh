@@ -29,6 +29,8 @@ struct JvpDesc {
     double pump_scale;       // u(T_c voxel) / (2 h)
     double adot_p, adot_s;   // d a / dT_o of the propagator coefficients a = 2π²/k (pump, SH)
     double* out;             // device [2]: SH power, its derivative
+    void* q_dot;             // or null: the tangent of the heat source Q this pass emits
+                             // (Tfield.h:260-276), slice by slice like the forward march
 };
 
 // dA/dz (dadz) and its derivative along (ṗ, ṡ) and the coefficient tangents (ċP, ċS, q̇s).
@@ -150,23 +152,26 @@ __host__ __device__ inline JvpLayout jvp_layout(const MpLayout& L) {
 // pass (two: the tangent RK4 needs more registers than a 512-thread block allows).
 constexpr int kJvpPX = 2;
 
-// Row pass of the tangent march (one instance; grid N / RB): as mp_row_kernel's thermal pass
-// over the four planes P, S, Ṗ, Ṡ, with the JVP of the RK4 applications; the pass with
+// Row pass of the tangent march (grid (N / RB, instances); the workspace of instance i at
+// L.base + i * L.stride, L.stride covering the tangent planes of JL): as mp_row_kernel's thermal
+// pass over the four planes P, S, Ṗ, Ṡ, with the JVP of the RK4 applications; the pass with
 // s + 1 = out_after sums this CTA's SH power and its derivative into the partials
 // (part[2 r], part[2 r + 1]).
 template <typename T, int N>
 __global__ void __launch_bounds__(MpCfg<T, N>::RNT * kJvpPX)
-    mp_row_jvp_kernel(const InstDesc* __restrict__ descs, MpLayout L, JvpLayout JL, JvpDesc jd, int s) {
+    mp_row_jvp_kernel(const InstDesc* __restrict__ descs, MpLayout L, JvpLayout JL, const JvpDesc* __restrict__ jds,
+                      int s) {
     using Cfg = MpCfg<T, N>;
     constexpr int R2 = Cfg::R2, RB = Cfg::RB, SW = Cfg::SW;
     constexpr int JOBS = Cfg::RNT, PX = kJvpPX, NT = JOBS * PX;
     using V = cx<T>;
     using W = mult<T>;
     using R = T;
-    const InstDesc d = descs[0];
+    const InstDesc d = descs[blockIdx.y];
     if (s >= d.nsteps) return;
+    const JvpDesc jd = jds[blockIdx.y];
     const int mode = s < 0 ? 0 : (s + 1 < d.nsteps ? 1 : 2);
-    char* wbase = L.base;
+    char* wbase = L.base + (size_t)blockIdx.y * L.stride;
     V* g[4] = {reinterpret_cast<V*>(wbase), reinterpret_cast<V*>(wbase + L.off_s), reinterpret_cast<V*>(wbase + JL.off_pd),
                reinterpret_cast<V*>(wbase + JL.off_sd)};
     const W* gtab = reinterpret_cast<const W*>(wbase + L.off_tab);
@@ -284,6 +289,18 @@ __global__ void __launch_bounds__(MpCfg<T, N>::RNT * kJvpPX)
                 thermal_coef_jvp<T>(d, dkint[gi], dkind[gi], sl, np, ns, (double)dnp[gz], (double)dns[gz], cf, cfd);
                 rk4_jvp<T>(p, q, pd, qd, cf, cfd, hap, has, (T)(0.5 * (d.bf_s * ns)), (T)(0.5 * (d.bf_s * (double)dns[gz])),
                            dz6);
+                if (h == 0 && jd.q_dot) {
+                    // tangent of kernelSetQ for slice s after its step:
+                    // Q = q_p n_p |P|^2 + q_s n_s |S|^2 + βs (q_h n_s |S|^2)^2
+                    const double npd = (double)dnp[gz], nsd = (double)dns[gz];
+                    const double ap2 = (double)p.x * p.x + (double)p.y * p.y;
+                    const double as2 = (double)q.x * q.x + (double)q.y * q.y;
+                    const double ap2d = 2.0 * ((double)p.x * pd.x + (double)p.y * pd.y);
+                    const double as2d = 2.0 * ((double)q.x * qd.x + (double)q.y * qd.y);
+                    const double is = d.q_h * ns * as2, isd = d.q_h * (nsd * as2 + ns * as2d);
+                    reinterpret_cast<R*>(jd.q_dot)[gz] =
+                        (R)(d.q_p * (npd * ap2 + np * ap2d) + d.q_s * (nsd * as2 + ns * as2d) + 2.0 * d.beta_s * is * isd);
+                }
                 if (h == 0 && s + 1 == d.out_after) {
                     // J = pw sum n_s |S|^2 over the output slice, and its tangent
                     const size_t go = (size_t)(s + 1) * nn + gi;
@@ -340,18 +357,20 @@ __global__ void __launch_bounds__(MpCfg<T, N>::RNT * kJvpPX)
 
 // Column pass of the tangent march: the diffraction of one field (blockIdx.y) and of its
 // tangent over CW columns.  Ẏ = D Ẋ + i θ̇ D X with θ̇ = -dz ȧ (dfx² sx² + dfy² sy²), ȧ
-// the derivative of the propagator coefficient of that field.  Grid (N / CW, 2).
+// the derivative of the propagator coefficient of that field.  Grid (N / CW, 2, instances).
 template <typename T, int N>
 __global__ void __launch_bounds__(MpCfg<T, N>::CNT)
-    mp_col_jvp_kernel(const InstDesc* __restrict__ descs, MpLayout L, JvpLayout JL, JvpDesc jd, int s) {
+    mp_col_jvp_kernel(const InstDesc* __restrict__ descs, MpLayout L, JvpLayout JL, const JvpDesc* __restrict__ jds,
+                      int s) {
     using Cfg = MpCfg<T, N>;
     constexpr int R2 = Cfg::R2, CW = Cfg::CW, NT = Cfg::CNT;
     using V = cx<T>;
     using W = mult<T>;
-    const InstDesc d = descs[0];
+    const InstDesc d = descs[blockIdx.z];
     if (s >= d.nsteps) return;
+    const double adot = blockIdx.y ? jds[blockIdx.z].adot_s : jds[blockIdx.z].adot_p;
     const int f = blockIdx.y;
-    char* wbase = L.base;
+    char* wbase = L.base + (size_t)blockIdx.z * L.stride;
     V* F = reinterpret_cast<V*>(wbase + (f ? L.off_s : 0));
     V* Fd = reinterpret_cast<V*>(wbase + (f ? JL.off_sd : JL.off_pd));
     const W* gtab = reinterpret_cast<const W*>(wbase + L.off_tab);
@@ -387,7 +406,6 @@ __global__ void __launch_bounds__(MpCfg<T, N>::CNT)
     col_stage(tile, false);
     col_stage(tiled, false);
     __syncthreads();
-    const double adot = f ? jd.adot_s : jd.adot_p;
     for (int j = tid; j < R2 * CW; j += NT) {
         const int c = j % CW, k2 = j / CW;
         const int x = x0 + c;
@@ -435,18 +453,20 @@ __global__ void __launch_bounds__(MpCfg<T, N>::CNT)
     }
 }
 
-// SH power and its derivative from the row-pass partials (fixed order), times pw_s.
+// SH power and its derivative from the row-pass partials (fixed order), times pw_s; one
+// block per instance.
 template <typename T, int N>
-__global__ void mp_jvp_sum_kernel(const InstDesc* __restrict__ descs, MpLayout L, JvpDesc jd) {
+__global__ void mp_jvp_sum_kernel(const InstDesc* __restrict__ descs, MpLayout L, const JvpDesc* __restrict__ jds) {
     if (threadIdx.x != 0) return;
-    const double* part = reinterpret_cast<const double*>(L.base + L.off_part);
+    const int i = blockIdx.x;
+    const double* part = reinterpret_cast<const double*>(L.base + (size_t)i * L.stride + L.off_part);
     double a = 0.0, b = 0.0;
     for (int r = 0; r < MpCfg<T, N>::RPART; ++r) {
         a += part[2 * r];
         b += part[2 * r + 1];
     }
-    jd.out[0] = a * descs[0].pw_s;
-    jd.out[1] = b * descs[0].pw_s;
+    jds[i].out[0] = a * descs[i].pw_s;
+    jds[i].out[1] = b * descs[i].pw_s;
 }
 
 }  // namespace shg

@@ -51,17 +51,17 @@ __global__ void optics_kernel(const R* __restrict__ T, R* __restrict__ dk, R* __
 }
 
 // Derivatives of the per-voxel optics with respect to the oven temperature: u = dT/dT_oven at
-// every voxel times dn/dT and dΔk/dT (central differences over ±1e-3 K in FP64).
+// every voxel times dn/dT and dΔk/dT, both in closed form (crystal.cuh), in FP64.
 template <typename R>
 __global__ void optics_tangent_kernel(const R* __restrict__ T, const R* __restrict__ u, R* __restrict__ ddk,
                                       R* __restrict__ dnp, R* __restrict__ dns, size_t total, double lp,
                                       double period, int crystal) {
-    const double ls = 0.5 * lp, h = 1e-3;
+    const double ls = 0.5 * lp;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
-        const double t = (double)T[i], w = (double)u[i] / (2 * h);
-        ddk[i] = (R)((crystal_delta_k(crystal, lp, period, t + h) - crystal_delta_k(crystal, lp, period, t - h)) * w);
-        dnp[i] = (R)((crystal_n(crystal, lp, t + h) - crystal_n(crystal, lp, t - h)) * w);
-        dns[i] = (R)((crystal_n(crystal, ls, t + h) - crystal_n(crystal, ls, t - h)) * w);
+        const double t = (double)T[i], w = (double)u[i];
+        ddk[i] = (R)(crystal_ddk_dT(crystal, lp, period, t) * w);
+        dnp[i] = (R)(crystal_dn_dT(crystal, lp, t) * w);
+        dns[i] = (R)(crystal_dn_dT(crystal, ls, t) * w);
     }
 }
 

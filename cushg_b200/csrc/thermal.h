@@ -41,8 +41,14 @@ size_t jacobi_partials(const shg_params& p);
 // staged plane never arrived.
 int jacobi_tb_chunk(int tiles, int nz, int depth, int sms);
 template <typename R> shg_status make_tb_map(const R* base, int n, int nz, CUtensorMap* map);
+// Bound of each wait for a staged plane (2 s by default: a plane that takes longer is an
+// error), and a plane never staged (the self-test of that bound; -1: none).
+struct TbWait {
+    uint64_t limit_ns = 2000000000ull;
+    int withhold = -1;
+};
 template <typename R>
 cudaError_t launch_jacobi_tb(const CUtensorMap& tmT, const CUtensorMap& tmQ, R* Tf, const JacobiCoef<R>& k,
-                             int boundary, int depth, unsigned* err, cudaStream_t s);
+                             int boundary, int depth, unsigned* err, cudaStream_t s, TbWait w = TbWait());
 
 }  // namespace shg

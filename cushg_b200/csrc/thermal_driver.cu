@@ -19,6 +19,7 @@
 #include <cmath>
 #include <cstring>
 #include <utility>
+#include <vector>
 
 #include "shg_host.h"
 #include "ssfm_variants.h"
@@ -72,223 +73,292 @@ cudaError_t run_sweeps(R*& cur, R*& nxt, const R* Ta, const SweepMaps<R>& m, con
     return cudaSuccess;
 }
 
+// One instance of a thermal run: its buffers, its Jacobi state and its latest optical pass.
 template <typename R>
-shg_status thermal_run(const shg_params& p, const void* signal_in, void* pump_out, void* signal_out,
-                       void* temperature_out, shg_stats* stats, cudaStream_t s, void* slices_p, void* slices_s,
-                       const ThermalHook* hook) {
-    const PlainVariant* v = find_plain_variant(p.precision, p.nx, 1, p.march);
-    if (!v) return fail(SHG_ERR_UNSUPPORTED, "no thermal kernel for grid side %d", p.nx);
-    const int n = p.nx, nz = p.nz;
-    const size_t nt = (size_t)n * n * nz;
-    const size_t arr = sizeof(R) * nt;
-    const size_t npart = jacobi_partials(p);
-    const size_t bytes = 6 * arr + sizeof(double) * (npart + 4) + sizeof(InstDesc) + 256;
-    cudaError_t e;
+struct ThermalInst {
+    const shg_params* p = nullptr;
+    const void* signal_in = nullptr;
+    void *pump_out = nullptr, *signal_out = nullptr, *slices_p = nullptr, *slices_s = nullptr;
     char* buf = nullptr;
-    if ((e = dev_alloc((void**)&buf, bytes, s)) != cudaSuccess) return cuda_fail(e, "cudaMallocAsync");
-    R* Ta = reinterpret_cast<R*>(buf);
-    R* Tb = Ta + nt;
-    R* Q = Tb + nt;
-    R* DK = Q + nt;
-    R* NP = DK + nt;
-    R* NS = NP + nt;
-    double* partial = reinterpret_cast<double*>(NS + nt);
-    double* resid = partial + npart;   // [0] convergence value, [1] staging-error word
-    double* power = resid + 2;         // [2]
-    InstDesc* ddesc = reinterpret_cast<InstDesc*>(((uintptr_t)(power + 2) + 255) & ~(uintptr_t)255);
-    unsigned* tb_err = reinterpret_cast<unsigned*>(resid + 1);  // set by a blocked sweep whose staging timed out
+    R *Ta = nullptr, *Tb = nullptr, *Q = nullptr, *DK = nullptr, *NP = nullptr, *NS = nullptr;
+    double *partial = nullptr, *resid = nullptr, *power = nullptr;
+    unsigned* tb_err = nullptr;
+    R *cur = nullptr, *nxt = nullptr;  // cur holds the latest temperature (the reference's Tinic == Tfinal)
+    SweepMaps<R> maps;
+    JacobiCoef<R> k;
+    double tol = 0.0;
+    int check_every = 0, max_outer = 0, depth = 1;
+    int64_t max_sweeps = 0;
+    int64_t total = 0, counter = 0;  // sweeps of the run, of the current outer iteration
+    int outer = 0;
+    double last = 0.0, Tc = 0.0;
+    bool done = false;
+    InstDesc d;  // descriptor of the latest optical pass
+    double jacobi_ms = 0.0, optics_ms = 0.0;
+};
 
+// Buffers and initial temperature of one instance (T = temp, oven faces = t_peltier, Q = 0,
+// Solver.h:319-323).
+template <typename R>
+shg_status ti_setup(ThermalInst<R>& t, cudaStream_t s) {
+    const shg_params& p = *t.p;
+    const int n = p.nx, nz = p.nz;
+    const size_t nt = (size_t)n * n * nz, arr = sizeof(R) * nt;
+    const size_t npart = jacobi_partials(p);
+    const size_t bytes = 6 * arr + sizeof(double) * (npart + 4) + 256;
+    cudaError_t e;
+    if ((e = dev_alloc((void**)&t.buf, bytes, s)) != cudaSuccess) return cuda_fail(e, "cudaMallocAsync");
+    t.Ta = reinterpret_cast<R*>(t.buf);
+    t.Tb = t.Ta + nt;
+    t.Q = t.Tb + nt;
+    t.DK = t.Q + nt;
+    t.NP = t.DK + nt;
+    t.NS = t.NP + nt;
+    t.partial = reinterpret_cast<double*>(t.NS + nt);
+    t.resid = t.partial + npart;                            // [0] convergence value, [1] staging-error word
+    t.power = t.resid + 2;                                  // [2]
+    t.tb_err = reinterpret_cast<unsigned*>(t.resid + 1);    // set by a blocked sweep whose staging timed out
+    t.k = make_jacobi_coef<R>(p);
+    // Solver.h:332: tol = 5e-4 / TSIZE in the working precision
+    t.tol = p.jacobi_tol > 0 ? p.jacobi_tol : (double)(R)(5e-4 / (double)nt);
+    t.check_every = p.check_every > 0 ? p.check_every : 5000;
+    t.max_sweeps = p.max_sweeps > 0 ? p.max_sweeps : ((int64_t)1 << 40);
+    t.max_outer = p.max_outer > 0 ? p.max_outer : 20;
+    t.depth = sweep_depth(p);
+    t.cur = t.Ta;
+    t.nxt = t.Tb;
+    shg_status rc;
+    if (t.depth > 1 && (rc = make_sweep_maps<R>(t.Ta, t.Tb, t.Q, n, nz, &t.maps)) != SHG_OK) return rc;
+    if ((e = cudaMemsetAsync(t.resid, 0, 2 * sizeof(double), s)) != cudaSuccess) return cuda_fail(e, "memset");
+    if ((e = launch_thermal_init<R>(t.Ta, t.Tb, t.Q, p, s)) != cudaSuccess) return cuda_fail(e, "thermal init");
+    return SHG_OK;
+}
+
+// The Jacobi loop of one outer iteration (Solver.h:335-355): the convergence value is taken on
+// the first sweep of every window of check_every sweeps; a value equal to the previous check
+// counts as converged; the rest of each window runs unchecked, `depth` sweeps per launch.
+// FIXED rule: exactly max_sweeps sweeps, the last one reporting max |Tf - Ti|.
+template <typename R>
+shg_status ti_jacobi(ThermalInst<R>& t, cudaStream_t s) {
+    const shg_params& p = *t.p;
+    const size_t nt = (size_t)p.nx * p.nx * p.nz;
+    cudaError_t e;
+    double red = 1.0, aux = -1.0;
+    int64_t counter = 0;
+    // one checked sweep: its convergence value and the staging-error word
+    auto checked = [&](int rule, double* out) -> shg_status {
+        if ((e = launch_jacobi<R>(t.cur, t.nxt, t.Q, t.k, p.boundary, true, rule, t.partial, t.resid, s)) != cudaSuccess)
+            return cuda_fail(e, "jacobi sweep");
+        std::swap(t.cur, t.nxt);
+        double h[2] = {0.0, 0.0};
+        if ((e = cudaMemcpyAsync(h, t.resid, sizeof(h), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(s)) != cudaSuccess)
+            return cuda_fail(e, "jacobi residual");
+        unsigned staged_err = 0;
+        std::memcpy(&staged_err, &h[1], sizeof(staged_err));
+        if (staged_err) return fail(SHG_ERR_CUDA, "blocked Jacobi sweep: a staged plane did not arrive");
+        *out = h[0];
+        return SHG_OK;
+    };
     shg_status rc = SHG_OK;
+    if (p.conv_rule == SHG_CONV_FIXED) {
+        if ((e = run_sweeps<R>(t.cur, t.nxt, t.Ta, t.maps, t.Q, t.k, p.boundary, t.depth, t.max_sweeps - 1, t.tb_err, s)) !=
+            cudaSuccess)
+            return cuda_fail(e, "jacobi sweep");
+        if ((rc = checked(SHG_CONV_MAXABS, &red)) != SHG_OK) return rc;
+        counter = t.max_sweeps;
+        if (!std::isfinite(red))
+            return fail(SHG_ERR_NONFINITE, "Jacobi residual is %g after %lld sweeps", red, (long long)counter);
+    }
+    while (p.conv_rule != SHG_CONV_FIXED && red >= t.tol) {
+        if (counter >= t.max_sweeps)
+            return fail(SHG_ERR_NOT_CONVERGED, "Jacobi: %lld sweeps without reaching %g (last %g)", (long long)counter,
+                        t.tol, red);
+        double h0 = 0.0;
+        if ((rc = checked(p.conv_rule, &h0)) != SHG_OK) return rc;
+        if (counter > 0) aux = red;
+        red = p.conv_rule == SHG_CONV_MAXABS ? h0 : (double)(R)(std::sqrt((R)h0) / (R)(double)nt);
+        if (!std::isfinite(red))
+            return fail(SHG_ERR_NONFINITE, "Jacobi residual is %g after %lld sweeps", red, (long long)counter);
+        if (red == aux) red = 0.5 * t.tol;
+        ++counter;
+        if (red < t.tol) break;
+        const int64_t left = std::min<int64_t>(t.check_every - 1, t.max_sweeps - counter);
+        if ((e = run_sweeps<R>(t.cur, t.nxt, t.Ta, t.maps, t.Q, t.k, p.boundary, t.depth, left, t.tb_err, s)) !=
+            cudaSuccess)
+            return cuda_fail(e, "jacobi sweep");
+        counter += std::max<int64_t>(left, 0);
+    }
+    t.counter = counter;
+    t.total += counter;
+    t.last = red;
+    return SHG_OK;
+}
+
+// Δk, n_p, n_s from T and the descriptor of the optical pass from T(NX/2, NY/2, 0)
+// (Solver.h:359-365), into t.d (host).
+template <typename R>
+shg_status ti_optics(ThermalInst<R>& t, cudaStream_t s) {
+    const shg_params& p = *t.p;
+    const int n = p.nx, nz = p.nz;
+    cudaError_t e;
+    if ((e = launch_optics<R>(t.cur, t.DK, t.NP, t.NS, p, s)) != cudaSuccess) return cuda_fail(e, "optics");
+    R tc_h = 0;
+    const size_t ic = (size_t)(n / 2) * n + n / 2;  // IDX(NX/2, NY/2, 0)
+    if ((e = cudaMemcpyAsync(&tc_h, t.cur + ic, sizeof(R), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(s)) != cudaSuccess)
+        return cuda_fail(e, "read T");
+    t.Tc = (double)tc_h;
+    InstDesc d = make_plain_desc(p, t.Tc, t.Tc);
+    const double dQ = 2.0 * p.deff / kPi, lp = p.lambda_p, ls = 0.5 * lp;
+    d.kf_p = 1.0 * kPi * dQ / lp;
+    d.kf_s = 0.5 * kPi * dQ / ls;
+    d.bf_s = p.beta_s * 0.5 * kEps0 * kC;
+    d.q_p = p.alpha_p * 0.5 * kC * kEps0;
+    d.q_s = p.alpha_s * 0.5 * kC * kEps0;
+    d.q_h = 0.5 * kC * kEps0;
+    d.beta_s = p.beta_s;
+    d.t_np = t.NP;
+    d.t_ns = t.NS;
+    d.t_dk = t.DK;
+    d.t_q = t.Q;
+    d.pw_s = d.pw_p = 0.5 * kEps0 * kC * d.dx * d.dy;
+    d.signal_in = t.signal_in;
+    d.has_signal_in = t.signal_in ? 1 : 0;
+    d.pump_out = t.pump_out;
+    d.signal_out = t.signal_out;
+    d.power_out = t.power;
+    d.slices_p = t.slices_p;
+    d.slices_s = t.slices_s;
+    d.nslices = (t.slices_p || t.slices_s) ? nz : 0;
+    t.d = d;
+    return SHG_OK;
+}
+
+// The thermal runs of `count` parameter sets (one grid side, precision and nz) in lockstep:
+// each outer iteration runs every instance's Jacobi loop, then the optical passes of all
+// instances still iterating as ONE launch sequence of the thermal march over them (a grid over
+// the instances), then `hook` with their states.  An instance stops after its last pass
+// (Solver.h:367, or max_outer); the others continue.  count == 1 is shg_solve's thermal run.
+template <typename R>
+shg_status thermal_batch_run(const shg_params* ps, int count, const void* const* signal_in, void* const* pump_out,
+                             void* const* signal_out, void* const* temperature_out, shg_stats* stats, cudaStream_t s,
+                             void* slices_p, void* slices_s, const ThermalBatchHook* hook) {
+    const shg_params& p0 = ps[0];
+    const PlainVariant* v = find_plain_variant(p0.precision, p0.nx, 1, p0.march);
+    if (!v) return fail(SHG_ERR_UNSUPPORTED, "no thermal kernel for grid side %d", p0.nx);
+    const size_t arr = sizeof(R) * (size_t)p0.nx * p0.nx * p0.nz;
+    std::vector<ThermalInst<R>> ti(count);
+    std::vector<InstDesc> hd(count);
+    std::vector<ThermalState> states(count);
+    std::vector<int> act(count);
+    InstDesc* dd = nullptr;
+    shg_status rc = SHG_OK;
+    cudaError_t e;
     cudaEvent_t t0 = nullptr, t1 = nullptr;
     cudaEventCreate(&t0);
     cudaEventCreate(&t1);
-    // per-phase timing: the Jacobi loop of an outer iteration runs between ej[0] and ej[1],
-    // its optics and optical pass between ej[1] and ej[2]
+    // per-phase timing: an instance's Jacobi loop between ej[0] and ej[1], the optics and the
+    // batched optical pass between ej[1] and ej[2]
     cudaEvent_t ej[3] = {nullptr, nullptr, nullptr};
     for (auto& ev : ej) cudaEventCreate(&ev);
-    double jacobi_ms = 0.0, optics_ms = 0.0;
     cudaEventRecord(t0, s);
-    const JacobiCoef<R> k = make_jacobi_coef<R>(p);
-    // Solver.h:332: tol = 5e-4 / TSIZE in the working precision
-    const double tol = p.jacobi_tol > 0 ? p.jacobi_tol : (double)(R)(5e-4 / (double)nt);
-    const int check_every = p.check_every > 0 ? p.check_every : 5000;
-    const int64_t max_sweeps = p.max_sweeps > 0 ? p.max_sweeps : ((int64_t)1 << 40);
-    const int max_outer = p.max_outer > 0 ? p.max_outer : 20;
-    const int depth = sweep_depth(p);
-    int64_t total = 0;
-    int outer = 0;
-    InstDesc last_d;
-    double last_Tc = 0.0;
-    double last = 0.0;
-    R* cur = Ta;  // holds the latest temperature (the reference's Tinic == Tfinal after its copy)
-    R* nxt = Tb;
-    SweepMaps<R> maps;
     do {
-        if (depth > 1 && (rc = make_sweep_maps<R>(Ta, Tb, Q, n, nz, &maps)) != SHG_OK) break;
-        if ((e = cudaMemsetAsync(resid, 0, 2 * sizeof(double), s)) != cudaSuccess) { rc = cuda_fail(e, "memset"); break; }
-        if ((e = launch_thermal_init<R>(Ta, Tb, Q, p, s)) != cudaSuccess) { rc = cuda_fail(e, "thermal init"); break; }
-        for (int g = 0; g < max_outer && rc == SHG_OK; ++g) {
-            double red = 1.0, aux = -1.0;
-            int64_t counter = 0;
-            cudaEventRecord(ej[0], s);
-            if (p.conv_rule == SHG_CONV_FIXED) {
-                // exactly max_sweeps sweeps; the last one reports max |Tf - Ti|
-                if ((e = run_sweeps<R>(cur, nxt, Ta, maps, Q, k, p.boundary, depth, max_sweeps - 1, tb_err, s)) !=
-                        cudaSuccess ||
-                    (e = launch_jacobi<R>(cur, nxt, Q, k, p.boundary, true, SHG_CONV_MAXABS, partial, resid, s)) !=
-                        cudaSuccess) {
-                    rc = cuda_fail(e, "jacobi sweep");
-                    break;
-                }
-                std::swap(cur, nxt);
-                double h[2] = {0.0, 0.0};
-                if ((e = cudaMemcpyAsync(h, resid, sizeof(h), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
-                    (e = cudaStreamSynchronize(s)) != cudaSuccess) {
-                    rc = cuda_fail(e, "jacobi residual");
-                    break;
-                }
-                unsigned staged_err = 0;
-                std::memcpy(&staged_err, &h[1], sizeof(staged_err));
-                if (staged_err) {
-                    rc = fail(SHG_ERR_CUDA, "blocked Jacobi sweep: a staged plane did not arrive");
-                    break;
-                }
-                red = h[0];
-                counter = max_sweeps;
-                if (!std::isfinite(red)) {
-                    rc = fail(SHG_ERR_NONFINITE, "Jacobi residual is %g after %lld sweeps", red, (long long)counter);
-                    break;
-                }
-            }
-            while (p.conv_rule != SHG_CONV_FIXED && red >= tol) {
-                if (counter >= max_sweeps) {
-                    rc = fail(SHG_ERR_NOT_CONVERGED, "Jacobi: %lld sweeps without reaching %g (last %g)",
-                              (long long)counter, tol, red);
-                    break;
-                }
-                // the checked sweep of this window
-                if ((e = launch_jacobi<R>(cur, nxt, Q, k, p.boundary, true, p.conv_rule, partial, resid, s)) != cudaSuccess) {
-                    rc = cuda_fail(e, "jacobi sweep");
-                    break;
-                }
-                std::swap(cur, nxt);
-                double h[2] = {0.0, 0.0};
-                if ((e = cudaMemcpyAsync(h, resid, sizeof(h), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
-                    (e = cudaStreamSynchronize(s)) != cudaSuccess) {
-                    rc = cuda_fail(e, "jacobi residual");
-                    break;
-                }
-                unsigned staged_err = 0;
-                std::memcpy(&staged_err, &h[1], sizeof(staged_err));
-                if (staged_err) {
-                    rc = fail(SHG_ERR_CUDA, "blocked Jacobi sweep: a staged plane did not arrive");
-                    break;
-                }
-                if (counter > 0) aux = red;
-                red = p.conv_rule == SHG_CONV_MAXABS ? h[0] : (double)(R)(std::sqrt((R)h[0]) / (R)(double)nt);
-                if (!std::isfinite(red)) {
-                    rc = fail(SHG_ERR_NONFINITE, "Jacobi residual is %g after %lld sweeps", red, (long long)counter);
-                    break;
-                }
-                if (red == aux) red = 0.5 * tol;
-                ++counter;
-                if (red < tol) break;
-                // the rest of the window, unchecked: `depth` sweeps per launch
-                const int64_t left = std::min<int64_t>(check_every - 1, max_sweeps - counter);
-                if ((e = run_sweeps<R>(cur, nxt, Ta, maps, Q, k, p.boundary, depth, left, tb_err, s)) != cudaSuccess) {
-                    rc = cuda_fail(e, "jacobi sweep");
-                    break;
-                }
-                counter += std::max<int64_t>(left, 0);
-            }
-            total += counter;
-            last = red;
-            if (rc != SHG_OK) break;
-            cudaEventRecord(ej[1], s);
-            // optical pass from the converged temperature
-            if ((e = launch_optics<R>(cur, DK, NP, NS, p, s)) != cudaSuccess) { rc = cuda_fail(e, "optics"); break; }
-            R tc_h = 0;
-            const size_t ic = (size_t)(n / 2) * n + n / 2;  // IDX(NX/2, NY/2, 0)
-            if ((e = cudaMemcpyAsync(&tc_h, cur + ic, sizeof(R), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
-                (e = cudaStreamSynchronize(s)) != cudaSuccess) {
-                rc = cuda_fail(e, "read T");
-                break;
-            }
-            const double Tc = (double)tc_h;
-            InstDesc d = make_plain_desc(p, Tc, Tc);
-            const double dQ = 2.0 * p.deff / kPi, lp = p.lambda_p, ls = 0.5 * lp;
-            d.kf_p = 1.0 * kPi * dQ / lp;
-            d.kf_s = 0.5 * kPi * dQ / ls;
-            d.bf_s = p.beta_s * 0.5 * kEps0 * kC;
-            d.q_p = p.alpha_p * 0.5 * kC * kEps0;
-            d.q_s = p.alpha_s * 0.5 * kC * kEps0;
-            d.q_h = 0.5 * kC * kEps0;
-            d.beta_s = p.beta_s;
-            d.t_np = NP;
-            d.t_ns = NS;
-            d.t_dk = DK;
-            d.t_q = Q;
-            d.pw_s = d.pw_p = 0.5 * kEps0 * kC * d.dx * d.dy;
-            d.signal_in = signal_in;
-            d.has_signal_in = signal_in ? 1 : 0;
-            d.pump_out = pump_out;
-            d.signal_out = signal_out;
-            d.power_out = power;
-            d.slices_p = slices_p;
-            d.slices_s = slices_s;
-            d.nslices = (slices_p || slices_s) ? nz : 0;
-            if ((e = cudaMemcpyAsync(ddesc, &d, sizeof(d), cudaMemcpyHostToDevice, s)) != cudaSuccess) {
-                rc = cuda_fail(e, "descriptor");
-                break;
-            }
-            if ((e = run_variant(v, ddesc, &d, 1, nullptr, s)) != cudaSuccess) { rc = cuda_fail(e, "thermal optical pass"); break; }
-            last_d = d;
-            last_Tc = Tc;
-            ++outer;
-            cudaEventRecord(ej[2], s);
-            if ((e = cudaEventSynchronize(ej[2])) != cudaSuccess) { rc = cuda_fail(e, "thermal optical pass"); break; }
-            float a = 0.f, b = 0.f;
-            cudaEventElapsedTime(&a, ej[0], ej[1]);
-            cudaEventElapsedTime(&b, ej[1], ej[2]);
-            jacobi_ms += a;
-            optics_ms += b;
-            if (p.conv_rule != SHG_CONV_FIXED && counter == 1 && g != 0) break;  // Solver.h:367
-        }
-        if (rc != SHG_OK) break;
-        if (hook && outer > 0) {
-            const ThermalState st = {cur, NP, NS, DK, &last_d, ddesc, total, last_Tc};
-            if ((rc = (*hook)(st, s)) != SHG_OK) break;
-        }
-        if (temperature_out &&
-            (e = cudaMemcpyAsync(temperature_out, cur, arr, cudaMemcpyDeviceToDevice, s)) != cudaSuccess) {
-            rc = cuda_fail(e, "temperature out");
+        if ((e = dev_alloc((void**)&dd, sizeof(InstDesc) * (size_t)count, s)) != cudaSuccess) {
+            rc = cuda_fail(e, "cudaMallocAsync");
             break;
         }
+        for (int i = 0; i < count && rc == SHG_OK; ++i) {
+            ti[i].p = &ps[i];
+            ti[i].signal_in = signal_in ? signal_in[i] : nullptr;
+            ti[i].pump_out = pump_out ? pump_out[i] : nullptr;
+            ti[i].signal_out = signal_out ? signal_out[i] : nullptr;
+            ti[i].slices_p = slices_p;
+            ti[i].slices_s = slices_s;
+            rc = ti_setup<R>(ti[i], s);
+        }
+        if (rc != SHG_OK) break;
+        for (int g = 0; rc == SHG_OK; ++g) {
+            int na = 0;
+            for (int i = 0; i < count; ++i)
+                if (!ti[i].done) act[na++] = i;
+            if (na == 0) break;
+            for (int a = 0; a < na && rc == SHG_OK; ++a) {
+                ThermalInst<R>& t = ti[act[a]];
+                cudaEventRecord(ej[0], s);
+                if ((rc = ti_jacobi<R>(t, s)) != SHG_OK) break;
+                cudaEventRecord(ej[1], s);
+                if ((e = cudaEventSynchronize(ej[1])) != cudaSuccess) { rc = cuda_fail(e, "jacobi"); break; }
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, ej[0], ej[1]);
+                t.jacobi_ms += ms;
+            }
+            if (rc != SHG_OK) break;
+            cudaEventRecord(ej[1], s);
+            for (int a = 0; a < na && rc == SHG_OK; ++a) {
+                rc = ti_optics<R>(ti[act[a]], s);
+                hd[a] = ti[act[a]].d;
+            }
+            if (rc != SHG_OK) break;
+            if ((e = cudaMemcpyAsync(dd, hd.data(), sizeof(InstDesc) * (size_t)na, cudaMemcpyHostToDevice, s)) != cudaSuccess) {
+                rc = cuda_fail(e, "descriptors");
+                break;
+            }
+            if ((e = run_variant(v, dd, hd.data(), na, nullptr, s)) != cudaSuccess) { rc = cuda_fail(e, "thermal optical pass"); break; }
+            cudaEventRecord(ej[2], s);
+            if ((e = cudaEventSynchronize(ej[2])) != cudaSuccess) { rc = cuda_fail(e, "thermal optical pass"); break; }
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ej[1], ej[2]);
+            for (int a = 0; a < na; ++a) {
+                ThermalInst<R>& t = ti[act[a]];
+                ++t.outer;
+                t.optics_ms += ms;
+                // Solver.h:367: the last pass is the one whose Jacobi loop converged at its first sweep
+                t.done = t.outer == t.max_outer || (t.p->conv_rule != SHG_CONV_FIXED && t.counter == 1 && g != 0);
+                states[a] = {t.cur, t.NP, t.NS, t.DK, &hd[a], dd + a, t.counter, t.Tc, g, t.done, act[a]};
+            }
+            if (hook && (rc = (*hook)(states.data(), na, s)) != SHG_OK) break;
+        }
+        if (rc != SHG_OK) break;
+        for (int i = 0; i < count && rc == SHG_OK; ++i) {
+            if (temperature_out && temperature_out[i] &&
+                (e = cudaMemcpyAsync(temperature_out[i], ti[i].cur, arr, cudaMemcpyDeviceToDevice, s)) != cudaSuccess)
+                rc = cuda_fail(e, "temperature out");
+        }
+        if (rc != SHG_OK) break;
         cudaEventRecord(t1, s);
         if (stats) {
-            double h[2] = {0, 0};
-            if ((e = cudaMemcpyAsync(h, power, sizeof(h), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
-                (e = cudaStreamSynchronize(s)) != cudaSuccess) {
+            std::vector<double> h(2 * (size_t)count);
+            for (int i = 0; i < count && e == cudaSuccess; ++i)
+                e = cudaMemcpyAsync(&h[2 * (size_t)i], ti[i].power, 2 * sizeof(double), cudaMemcpyDeviceToHost, s);
+            if (e != cudaSuccess || (e = cudaStreamSynchronize(s)) != cudaSuccess) {
                 rc = cuda_fail(e, "thermal run");
                 break;
             }
             float ms = 0.f;
             cudaEventElapsedTime(&ms, t0, t1);
-            std::memset(stats, 0, sizeof(*stats));
-            stats->sh_power = h[0];
-            stats->pump_power = h[1];
-            stats->jacobi_sweeps = total;
-            stats->outer_iterations = outer;
-            stats->steps = nz;
-            stats->last_residual = last;
-            stats->device_ms = ms;
-            stats->jacobi_ms = jacobi_ms;
-            stats->optics_ms = optics_ms;
-            if (!std::isfinite(h[0]) || !std::isfinite(h[1]))
-                rc = fail(SHG_ERR_NONFINITE, "SH / pump power %g / %g", h[0], h[1]);
+            for (int i = 0; i < count; ++i) {
+                shg_stats& st = stats[i];
+                std::memset(&st, 0, sizeof(st));
+                st.sh_power = h[2 * (size_t)i];
+                st.pump_power = h[2 * (size_t)i + 1];
+                st.jacobi_sweeps = ti[i].total;
+                st.outer_iterations = ti[i].outer;
+                st.steps = ps[i].nz;
+                st.last_residual = ti[i].last;
+                st.device_ms = ms;
+                st.jacobi_ms = ti[i].jacobi_ms;
+                st.optics_ms = ti[i].optics_ms;
+                if (rc == SHG_OK && (!std::isfinite(st.sh_power) || !std::isfinite(st.pump_power)))
+                    rc = count > 1 ? fail(SHG_ERR_NONFINITE, "instance %d: SH / pump power %g / %g", i, st.sh_power,
+                                          st.pump_power)
+                                   : fail(SHG_ERR_NONFINITE, "SH / pump power %g / %g", st.sh_power, st.pump_power);
+            }
         }
     } while (0);
-    cudaFreeAsync(buf, s);
+    for (auto& t : ti)
+        if (t.buf) cudaFreeAsync(t.buf, s);
+    if (dd) cudaFreeAsync(dd, s);
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
     for (cudaEvent_t ev : ej) cudaEventDestroy(ev);
@@ -356,11 +426,21 @@ shg_status heat_sweeps_device(const shg_params& p, void* temperature, const void
 shg_status thermal_solve_device(const shg_params& p, const void* signal_in, void* pump_out, void* signal_out,
                                 void* temperature_out, shg_stats* stats, cudaStream_t stream, void* slices_p,
                                 void* slices_s, const ThermalHook* hook) {
-    if (p.precision == 32)
-        return thermal_run<float>(p, signal_in, pump_out, signal_out, temperature_out, stats, stream, slices_p, slices_s,
-                                  hook);
-    return thermal_run<double>(p, signal_in, pump_out, signal_out, temperature_out, stats, stream, slices_p, slices_s,
-                               hook);
+    ThermalBatchHook bh;
+    if (hook) bh = [hook](const ThermalState* st, int, cudaStream_t s) { return (*hook)(st[0], s); };
+    return thermal_solve_batch(&p, 1, &signal_in, &pump_out, &signal_out, &temperature_out, stats, stream, slices_p,
+                               slices_s, hook ? &bh : nullptr);
+}
+
+shg_status thermal_solve_batch(const shg_params* ps, int count, const void* const* signal_in, void* const* pump_out,
+                               void* const* signal_out, void* const* temperature_out, shg_stats* stats,
+                               cudaStream_t stream, void* slices_p, void* slices_s, const ThermalBatchHook* hook) {
+    if (count <= 0) return SHG_OK;
+    if (ps[0].precision == 32)
+        return thermal_batch_run<float>(ps, count, signal_in, pump_out, signal_out, temperature_out, stats, stream,
+                                        slices_p, slices_s, hook);
+    return thermal_batch_run<double>(ps, count, signal_in, pump_out, signal_out, temperature_out, stats, stream,
+                                     slices_p, slices_s, hook);
 }
 
 }  // namespace shg

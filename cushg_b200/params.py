@@ -58,6 +58,7 @@ class ShgParams(ctypes.Structure):
         ("jacobi_tol", ctypes.c_double), ("max_sweeps", ctypes.c_int64),
         ("jacobi_block", ctypes.c_int32), ("march", ctypes.c_int32),
         ("reserved1", ctypes.c_int32), ("waist_y", ctypes.c_double),
+        ("fp32_guard", ctypes.c_double),
     ]
 
     def copy(self) -> "ShgParams":

@@ -28,7 +28,8 @@ EXPORTS = (
     "shg_status_string", "shg_version", "shg_heat_sweeps_device", "shg_batch_plan_create", "shg_batch_plan_launch",
     "shg_batch_plan_powers", "shg_batch_plan_destroy", "shg_autotune", "shg_grad_batch", "shg_solve_batch",
     "shg_thermal_grad", "shg_autotune_batch", "shg_autotune_reset", "shg_set_schedule",
-    "shg_reserve_device_memory",
+    "shg_reserve_device_memory", "shg_fp32_error_estimate", "shg_selftest_bounded_wait",
+    "shg_thermal_batch",
 )
 
 
@@ -80,6 +81,13 @@ def lib() -> ctypes.CDLL:
         L.shg_default_params.restype = None
         L.shg_check_params.argtypes = [P]
         L.shg_check_params.restype = ctypes.c_int
+        L.shg_thermal_batch.argtypes = [P, ctypes.c_int32, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp),
+                                        ctypes.POINTER(ShgStats), ctypes.POINTER(ctypes.c_double), vp]
+        L.shg_thermal_batch.restype = ctypes.c_int
+        L.shg_selftest_bounded_wait.argtypes = [ctypes.c_int32, ctypes.c_double, ctypes.c_int32]
+        L.shg_selftest_bounded_wait.restype = ctypes.c_int
+        L.shg_fp32_error_estimate.argtypes = [P]
+        L.shg_fp32_error_estimate.restype = ctypes.c_double
         L.shg_steps.argtypes = [P]
         L.shg_steps.restype = ctypes.c_int32
         L.shg_solve.argtypes = [P, vp, vp, vp, vp, ctypes.POINTER(ShgStats)]
@@ -148,6 +156,18 @@ def default_params() -> ShgParams:
 
 def check_params(p: ShgParams) -> int:
     return int(lib().shg_check_params(ctypes.byref(p)))
+
+
+def fp32_error_estimate(p: ShgParams) -> float:
+    """Predicted relative error of the FP32 SH output field (shg_fp32_error_estimate); an
+    FP32 instance with ``fp32_guard`` below it runs the FP64 march."""
+    return float(lib().shg_fp32_error_estimate(ctypes.byref(p)))
+
+
+def selftest_bounded_wait(precision: int, wait_us: float, withhold_plane: int) -> None:
+    """shg_selftest_bounded_wait: raises ShgError(SHG_ERR_CUDA) when a staged plane's wait ran
+    out."""
+    _check(lib().shg_selftest_bounded_wait(int(precision), float(wait_us), int(withhold_plane)))
 
 
 def steps(p: ShgParams) -> int:
@@ -387,6 +407,28 @@ class BatchPlan:
             self.close()
         except Exception:
             pass
+
+
+def thermal_batch(ps: list[ShgParams], pump_outs=None, signal_outs=None, temperature_outs=None, grad: bool = False,
+                  stream=None) -> tuple[list[ShgStats], np.ndarray | None]:
+    """shg_thermal_batch: thermal runs in lockstep with batched optical (and, with grad, tangent)
+    passes; outputs are device tensors (or None).  Returns the per-instance stats and, with grad,
+    dJ/dT_oven per instance."""
+    n = len(ps)
+    arr = (ShgParams * n)(*ps)
+    vp = ctypes.c_void_p
+
+    def ptrs(ts):
+        if ts is None:
+            return None
+        return (vp * n)(*[vp(t.data_ptr()) if t is not None else None for t in ts])
+
+    stats = (ShgStats * n)()
+    dt = np.zeros(n, dtype=np.float64) if grad else None
+    dp = dt.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if dt is not None else None
+    s = None if stream is None else vp(stream)
+    _check(lib().shg_thermal_batch(arr, n, ptrs(pump_outs), ptrs(signal_outs), ptrs(temperature_outs), stats, dp, s))
+    return list(stats), dt
 
 
 def thermal_grad(p: ShgParams) -> dict:

@@ -126,6 +126,15 @@ typedef struct shg_params {
      * length and focusing term in y, and Ap0 normalised with waist * waist_y so that the beam
      * carries `power` (the commented code keeps waist^2, which would not). */
     double waist_y;
+    /* FP32 plain runs only (precision 32, thermal 0, fused grid sides up to 256): the largest
+     * predicted relative error of the FP32 SH output field this instance accepts.  The FP32
+     * march rounds both fields at every step; when the crystal is far from phase matching the
+     * SH grows and cancels along the crystal, so the output is a small remainder of a larger
+     * field and its relative error grows with that ratio.  shg_fp32_error_estimate predicts
+     * it before the march.  An instance whose prediction exceeds fp32_guard runs the FP64
+     * march instead, with its outputs rounded to FP32 (same buffers, same layout).
+     * 0 (default): every FP32 instance runs in FP32.  No counterpart in the reference. */
+    double fp32_guard;
 } shg_params;
 
 enum {
@@ -159,6 +168,16 @@ SHG_API shg_status shg_check_params(const shg_params* p);
  * reference records the fields before its last step (Solver.h:283-286), so a
  * plain pass marches nz-1 steps and a thermal pass nz (its last step feeds Q). */
 SHG_API int32_t shg_steps(const shg_params* p);
+
+/* Predicted relative L2 error of the SH output field of the FP32 march against the FP64
+ * march, for a plain run of these parameters: K * c * sqrt(steps), where c is the ratio of
+ * the peak to the final magnitude of the undepleted Gaussian-beam SH amplitude
+ *   H(z) = integral_0^z e^{i Δk z'} / sqrt((1 + i (z' - f)/z_Rx) (1 + i (z' - f)/z_Ry)) dz'
+ * (the phase-mismatch cancellation along the crystal) and K the per-step rounding of the
+ * FP32 march, fitted on the 256-instance parameter sweep (grid sides 64-256).  The SH power's
+ * relative error is typically below it.  Host-only arithmetic; no counterpart in the
+ * reference. */
+SHG_API double shg_fp32_error_estimate(const shg_params* p);
 
 /*
  * Solve one instance.  Replaces Solver::run (Solver.h:311-390) with
@@ -294,10 +313,14 @@ SHG_API shg_status shg_set_schedule(int32_t precision, int32_t n, int32_t cluste
  * latency-bound loops where an allocation may block or synchronise, plugin hosts that forbid
  * it): its scratch (instance descriptors, power slots) is a fixed ~23 KB __device__ array of
  * the library, held by every GPU that loads it until exit.  Limit: count <= 64 instances
- * (larger counts return SHG_ERR_INVALID).  The first call on a device looks up that array's
- * address and should come before any stream capture.  Calls share the array: calls that
- * overlap on the GPU (other streams, other threads) race and must be serialised.
- * Arguments as shg_solve_batch_device; sh_power_out (host, may be NULL) synchronises.
+ * (larger counts return SHG_ERR_INVALID), grid sides of the fused march (up to 256).  The
+ * first call on a device sets that device up: it looks the array's address up and loads the
+ * kernels it launches, for which the CUDA driver may take device memory.  Make that first
+ * call before the host hands all free memory to its own allocator, and before any stream
+ * capture; later calls allocate nothing.  Calls share the array: calls that overlap on the
+ * GPU (other streams, other threads) race and must be serialised.
+ * Arguments as shg_solve_batch_device; sh_power_out (host, may be NULL) synchronises, and a
+ * NaN or Inf SH or pump power then returns SHG_ERR_NONFINITE naming the instance.
  */
 SHG_API shg_status shg_solve_batch_device_noalloc(const shg_params* params, int32_t count,
                                                   void* const* pump_out_dev, void* const* signal_out_dev,
@@ -316,6 +339,40 @@ SHG_API shg_status shg_solve_batch_device_noalloc(const shg_params* params, int3
  */
 SHG_API shg_status shg_heat_sweeps_device(const shg_params* p, void* temperature_dev, const void* q_dev,
                                           int64_t sweeps, void* stream);
+
+/*
+ * A batch of thermal runs: the -DTHERMAL outer loop of Solver::run (Solver.h:321-373) for each
+ * parameter set, which the reference's sweep script runs as one process per point
+ * (cuSHG.sh:58-94), marched in lockstep on `stream`.  Every outer iteration runs each
+ * instance's Jacobi loop (its own stopping rule and counts), then the optical passes of all
+ * instances still iterating as one launch sequence of the thermal march (grids over the
+ * instances), so the optical passes of small batches fill the GPU.  An instance stops after
+ * its own last pass.  Each instance's fields, temperature, powers and counts equal its
+ * shg_solve_device run bit for bit.  All instances share precision, grid side, nz and march;
+ * thermal == 1.
+ *   pump_out_dev, signal_out_dev, temperature_out_dev  arrays of count device buffers, or NULL
+ *                  (an array, or any entry of one); fields nx*ny complex, temperature nx*ny*nz.
+ *   stats          count entries, or NULL; device_ms is the whole batch's time, optics_ms the
+ *                  time of the batched optical passes the instance took part in.
+ *   d_temp_out     count doubles (host), or NULL.  With it, each instance's dJ/dT_oven as
+ *                  shg_thermal_grad computes it (grid sides 256 and 512, round beams), with the
+ *                  tangent marches of every outer iteration batched the same way.
+ * Synchronises `stream` before returning.  No counterpart in the reference.
+ */
+SHG_API shg_status shg_thermal_batch(const shg_params* params, int32_t count, void* const* pump_out_dev,
+                                     void* const* signal_out_dev, void* const* temperature_out_dev,
+                                     shg_stats* stats, double* d_temp_out, void* stream);
+
+/*
+ * Diagnostics: the bounded wait of the TMA-staged Jacobi sweeps (jacobi_block >= 2).  Runs two
+ * blocked sweeps of a 64 x 64 x 32 grid with every wait for a staged plane limited to wait_us
+ * microseconds and, with withhold_plane in 0..31, that plane's staging never issued, so its
+ * wait runs out: the kernel then stops, waits (bounded) for the loads it did issue, and
+ * reports through a status word.  Returns SHG_ERR_CUDA when a wait ran out, SHG_OK when every
+ * plane arrived (withhold_plane = -1).  The device stays usable either way.  No counterpart
+ * in the reference.
+ */
+SHG_API shg_status shg_selftest_bounded_wait(int32_t precision, double wait_us, int32_t withhold_plane);
 
 /* Gradients of the SH output power (plain runs), from shg_grad. */
 typedef struct shg_grad_result {

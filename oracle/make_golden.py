@@ -4,14 +4,16 @@ fixtures (.npz).
 TEST INFRASTRUCTURE ONLY.  Needs a GPU (the reference is CUDA-only).  Usage on the GPU
 machine, from the repository root:
 
-    python oracle/make_golden.py [--out gpurun_out/golden] [case ...]
+    python oracle/make_golden.py [--out DIR] [case ...]
 
 Each case runs `oracle/_ref/<case>/cuSHG <power> <waist> <temp> 1 <save_T>` (the argv of
 src/cuSHG.cu:46-58) in a scratch folder, then reads its ASCII outputs:
 Pump_out_{r,i}.dat and Signal_out_{r,i}.dat (NY rows of NX tab-separated values,
 src/headers/Files.h:69-90) and, for thermal cases, Tfinal_<z>.dat (src/headers/Files.h:169-202).
 The .npz holds pump, signal (complex128), T (float64, nz x ny x nx) when present, the
-parameter set as JSON, and the wall time of the run.  Copy the files into tests/golden/.
+parameter set as JSON, and the wall time of the run (for temperature grids above FULL_T_MAX
+voxels: the slices T_SLICES and FP64 sums over all voxels instead of T).  The default output
+folder is tests/golden/.
 """
 from __future__ import annotations
 
@@ -27,7 +29,11 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(HERE))
-from oracle.golden_cases import CASES  # noqa: E402
+from oracle.golden_cases import CASES, FULL_CASES, T_SLICES  # noqa: E402
+
+ALL_CASES = {**CASES, **FULL_CASES}
+# a temperature grid above this many voxels is stored as the slices T_SLICES plus sums
+FULL_T_MAX = 1 << 20
 
 
 def read_matrix(path: str, ny: int, nx: int) -> np.ndarray:
@@ -44,7 +50,7 @@ def read_matrix(path: str, ny: int, nx: int) -> np.ndarray:
 
 
 def run_case(name: str, out_dir: str, timeout: float) -> dict:
-    case = CASES[name]
+    case = ALL_CASES[name]
     p = case["params"]
     exe = os.path.join(HERE, "_ref", name, "cuSHG")
     if not os.path.exists(exe):
@@ -63,7 +69,16 @@ def run_case(name: str, out_dir: str, timeout: float) -> dict:
         arrays = {"pump": pump.astype(np.complex128), "signal": sig.astype(np.complex128)}
         if thermal:
             T = np.stack([read_matrix(os.path.join(wd, f"Tfinal_{z}.dat"), ny, nx) for z in range(nz)])
-            arrays["T"] = T
+            if T.size <= FULL_T_MAX:
+                arrays["T"] = T
+            else:
+                zs = [z for z in T_SLICES if z < nz]
+                arrays["T_z"] = np.asarray(zs, dtype=np.int64)
+                arrays["T_slices"] = T[zs]
+                arrays["T_sum"] = np.asarray(float(np.sum(T, dtype=np.float64)))
+                arrays["T_sumsq"] = np.asarray(float(np.sum(T * T, dtype=np.float64)))
+                arrays["T_min"] = np.asarray(float(T.min()))
+                arrays["T_max"] = np.asarray(float(T.max()))
         # iteration counts printed by the reference's thermal loop (Solver.h:356)
         sweeps = [int(tok.split()[0]) for tok in r.stdout.replace("\r", "\n").split("\n")
                   if tok.strip().endswith("iterations -> steady-state.")]
@@ -76,11 +91,11 @@ def run_case(name: str, out_dir: str, timeout: float) -> dict:
 
 def main() -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default="gpurun_out/golden")
+    ap.add_argument("--out", default=os.path.join(os.path.dirname(HERE), "tests", "golden"))
     ap.add_argument("--timeout", type=float, default=600.0)
     ap.add_argument("cases", nargs="*")
     a = ap.parse_args()
-    names = a.cases or list(CASES)
+    names = a.cases or list(ALL_CASES)
     rc = 0
     for n in names:
         try:

@@ -17,8 +17,11 @@ Patch set (every pattern must match, or the build stops):
   * outer optical-thermal iteration count (src/headers/Solver.h:325);
   * temperature dump at 20 significant digits (src/headers/Files.h:179).
 
-Run on this machine (needs /root/reference and nvcc, no GPU):
-    python oracle/ref_build.py            # all cases
+Run where the reference checkout and nvcc are (no GPU needed):
+    python oracle/ref_build.py [--reference DIR] [case ...]    # default: all cases
+DIR is the reference checkout (the folder holding src/cuSHG.cu).  Without --reference it is
+taken from the environment variable CUSHG_REFERENCE, else from a folder named `reference`
+beside this repository.
 The binaries travel to the GPU machine with the repository snapshot; make_golden.py runs
 them there.
 """
@@ -32,11 +35,19 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_SRC = "/root/reference/src"
+
+
+def reference_src(path: str | None = None) -> str:
+    """The reference's src/ folder: `path`, else $CUSHG_REFERENCE, else ../reference beside
+    the repository."""
+    root = path or os.environ.get("CUSHG_REFERENCE") or os.path.join(os.path.dirname(os.path.dirname(HERE)),
+                                                                      "reference")
+    return os.path.join(root, "src")
+
 OUT = os.path.join(HERE, "_ref")
 
 sys.path.insert(0, os.path.dirname(HERE))
-from oracle.golden_cases import CASES, TIMING_CASES  # noqa: E402
+from oracle.golden_cases import CASES, FULL_CASES, TIMING_CASES  # noqa: E402
 
 
 def _sub(text: str, pattern: str, repl: str, count_expected: int | None = None, flags=0) -> str:
@@ -131,11 +142,12 @@ def patch_tree(dst: str, case: dict) -> None:
     open(f, "w").write(s)
 
 
-def build_case(name: str, case: dict, nvcc: str = "nvcc") -> str:
+def build_case(name: str, case: dict, nvcc: str = "nvcc", src: str | None = None) -> str:
+    src = src or reference_src()
     dst = os.path.join(OUT, name, "src")
     if os.path.isdir(os.path.join(OUT, name)):
         shutil.rmtree(os.path.join(OUT, name))
-    shutil.copytree(REF_SRC, dst)
+    shutil.copytree(src, dst)
     patch_tree(dst, case)
     exe = os.path.join(OUT, name, "cuSHG")
     cmd = [nvcc, "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "cuSHG.cu", "-o", exe, "-lcufftw", "-lcufft"]
@@ -150,13 +162,19 @@ def build_case(name: str, case: dict, nvcc: str = "nvcc") -> str:
 
 
 def main(argv: list[str]) -> int:
-    if not os.path.isdir(REF_SRC):
-        print("reference sources not present; nothing to build")
+    import argparse
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default=None, help="reference checkout (the folder holding src/cuSHG.cu)")
+    ap.add_argument("cases", nargs="*")
+    a = ap.parse_args(argv[1:])
+    src = reference_src(a.reference)
+    if not os.path.isdir(src):
+        print(f"reference sources not present at {src}; nothing to build")
         return 0
-    allc = {**CASES, **TIMING_CASES}
-    names = argv[1:] or list(allc)
-    for n in names:
-        exe = build_case(n, allc[n])
+    allc = {**CASES, **FULL_CASES, **TIMING_CASES}
+    for n in a.cases or list(allc):
+        exe = build_case(n, allc[n], src=src)
         print("built", exe)
     return 0
 

@@ -43,7 +43,7 @@ def test_steps_follow_the_output_slice_rule():
 
 @pytest.mark.parametrize("field,value", [
     ("nx", 63), ("nz", 1), ("precision", 16), ("waist", 0.0), ("lx", -1.0), ("alpha_p", -1e-6),
-    ("power", float("nan")), ("lambda_p", 0.0),
+    ("power", float("nan")), ("lambda_p", 0.0), ("fp32_guard", -1e-5), ("fp32_guard", float("inf")),
 ])
 def test_invalid_params_are_rejected(field, value):
     p = P.config_plain_64().replace(**{field: value})
@@ -138,3 +138,18 @@ def test_reserve_device_memory_checks_its_argument():
     assert L.shg_reserve_device_memory(-1) == P.SHG_ERR_INVALID
     if not torch.cuda.is_available():
         assert L.shg_reserve_device_memory(1 << 20) == P.SHG_ERR_NO_DEVICE
+
+
+def test_fp32_error_estimate_follows_the_phase_mismatch_cancellation():
+    """shg_fp32_error_estimate is host arithmetic: the phase-matched run is well conditioned
+    (the SH grows monotonically, the estimate is K sqrt(steps) times about 1), a run far from
+    phase matching is worse, and more steps raise it as sqrt(steps)."""
+    p = P.workload(128, 201, 10000.0, 10.0, 30.0, 5000.0, P.QPM_TEMP, precision=32)
+    matched = shg.fp32_error_estimate(p)
+    assert 0 < matched < 3 * 1.3e-7 * (p.nz - 1) ** 0.5
+    far = shg.fp32_error_estimate(p.replace(temp=60.0, t_peltier=60.0))
+    assert far > 3 * matched
+    longer = shg.fp32_error_estimate(p.replace(nz=801))
+    assert abs(longer / matched - 2.0) < 1e-6
+    # an elliptical beam goes through the general envelope
+    assert shg.fp32_error_estimate(p.replace(waist_y=45.0)) > 0

@@ -204,3 +204,20 @@ def test_fixed_sweep_rule_runs_exact_counts(precision):
     assert np.max(np.abs(t_d.cpu().numpy() - r.temperature)) <= (1e-12 if precision == 64 else 1e-5)
     r2 = shg.solve(p.replace(max_outer=3), want_temperature=True)
     assert r2.stats.jacobi_sweeps == 3 * 37 and r2.stats.outer_iterations == 3
+
+
+@pytest.mark.parametrize("precision", [32, 64])
+def test_blocked_sweep_wait_runs_out_and_reports(precision):
+    """The TMA-staged sweeps bound every wait for a staged plane.  With one plane's staging
+    withheld and a 20 µs limit the wait runs out: the call returns SHG_ERR_CUDA, the device
+    stays usable, and the same sweeps with every plane staged, and a thermal run with blocked
+    sweeps, still pass."""
+    with pytest.raises(shg.ShgError) as e:
+        shg.selftest_bounded_wait(precision, 20.0, 7)
+    assert e.value.status == P.SHG_ERR_CUDA
+    assert "did not arrive" in str(e.value)
+    shg.selftest_bounded_wait(precision, 2e6, -1)
+    p = G.params_of("thermal64_n32").replace(jacobi_block=2)
+    r = shg.solve(p, want_temperature=True)
+    ref = shg.solve(p.replace(jacobi_block=1), want_temperature=True)
+    assert np.array_equal(r.temperature, ref.temperature)

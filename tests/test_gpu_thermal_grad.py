@@ -1,11 +1,12 @@
 """dJ/dT_oven of a thermal run through its temperature field (shg_thermal_grad), against
 central finite differences of the whole thermal run.
 
-With no absorption the heat source Q is zero, the temperature field depends on the oven
-temperature only through the heat equation, and the forward-mode derivative is exact: it
-must match central differences to 1e-6 relative (FP64; the run uses a fixed sweep count, so
-both sides differentiate the same procedure).  With absorption, Q's feedback is held fixed
-in the derivative, which the test bounds loosely."""
+The runs use a fixed sweep count, so both sides differentiate the same procedure.  The
+forward-mode derivative carries the tangent of the heat source Q of every optical pass into
+the next outer iteration's sweeps, so it is exact with absorption too: FP64 within 1e-6
+relative of central differences without absorption (Q = 0), within 1e-4 with absorption and
+two or three outer iterations, at 256 x 256 and 512 x 512; the FP32 derivative within 1e-3 of
+FP64 central differences."""
 import numpy as np
 import pytest
 
@@ -46,16 +47,19 @@ def test_thermal_grad_without_absorption_matches_finite_differences(n):
     assert abs(g["d_temp"] - d) <= 1e-6 * abs(d), (g["d_temp"], d)
 
 
-def test_thermal_grad_with_absorption_is_first_order():
-    p = case(256, absorb=True, outer=2)
+@pytest.mark.parametrize("n,outer", [(256, 2), (256, 3), (512, 2)])
+def test_thermal_grad_with_absorption_matches_finite_differences(n, outer):
+    p = case(n, absorb=True, outer=outer)
     g = shg.thermal_grad(p)
+    assert g["outer_iterations"] == outer
+    assert g["sh_power"] == shg.solve(p).sh_power
     d = fd(p)
-    assert np.isfinite(g["d_temp"]) and np.sign(g["d_temp"]) == np.sign(d)
-    assert abs(g["d_temp"] - d) <= 5e-2 * abs(d), (g["d_temp"], d)
+    assert abs(g["d_temp"] - d) <= 1e-4 * abs(d), (g["d_temp"], d)
 
 
-def test_thermal_grad_fp32_512():
-    p = case(512, precision=32)
+@pytest.mark.parametrize("absorb", [False, True])
+def test_thermal_grad_fp32_512(absorb):
+    p = case(512, precision=32, absorb=absorb, outer=2 if absorb else 1)
     g = shg.thermal_grad(p)
     d = fd(p.replace(precision=64))
     assert abs(g["d_temp"] - d) <= 1e-3 * abs(d), (g["d_temp"], d)

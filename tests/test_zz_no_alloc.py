@@ -48,8 +48,13 @@ def test_noalloc_batch_matches_allocating_batch_on_two_calls_in_a_row():
         ref_p, ref_s = outputs(ps)
         ref_power = shg.solve_batch_device(ps, ref_p, ref_s)
         got_p, got_s = outputs(ps)
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info()[0]
         got_power = shg.solve_batch_device_noalloc(ps, got_p, got_s)
         torch.cuda.synchronize()
+        if call > 0:
+            # after the first call's device set-up, a call takes no device memory
+            assert torch.cuda.mem_get_info()[0] == free_before
         field_tol = 1e-10 if precision == 64 else 1e-5
         power_tol = 1e-12 if precision == 64 else 1e-5
         for i in range(len(ps)):

@@ -97,10 +97,9 @@ struct ThermalInst {
     double jacobi_ms = 0.0, optics_ms = 0.0;
 };
 
-// Buffers and initial temperature of one instance (T = temp, oven faces = t_peltier, Q = 0,
-// Solver.h:319-323).
+// Buffers of one instance.
 template <typename R>
-shg_status ti_setup(ThermalInst<R>& t, cudaStream_t s) {
+shg_status ti_alloc(ThermalInst<R>& t, cudaStream_t s) {
     const shg_params& p = *t.p;
     const int n = p.nx, nz = p.nz;
     const size_t nt = (size_t)n * n * nz, arr = sizeof(R) * nt;
@@ -127,10 +126,16 @@ shg_status ti_setup(ThermalInst<R>& t, cudaStream_t s) {
     t.depth = sweep_depth(p);
     t.cur = t.Ta;
     t.nxt = t.Tb;
-    shg_status rc;
-    if (t.depth > 1 && (rc = make_sweep_maps<R>(t.Ta, t.Tb, t.Q, n, nz, &t.maps)) != SHG_OK) return rc;
+    if (t.depth > 1) return make_sweep_maps<R>(t.Ta, t.Tb, t.Q, n, nz, &t.maps);
+    return SHG_OK;
+}
+
+// Initial temperature of one instance (T = temp, oven faces = t_peltier, Q = 0, Solver.h:319-323).
+template <typename R>
+shg_status ti_init(ThermalInst<R>& t, cudaStream_t s) {
+    cudaError_t e;
     if ((e = cudaMemsetAsync(t.resid, 0, 2 * sizeof(double), s)) != cudaSuccess) return cuda_fail(e, "memset");
-    if ((e = launch_thermal_init<R>(t.Ta, t.Tb, t.Q, p, s)) != cudaSuccess) return cuda_fail(e, "thermal init");
+    if ((e = launch_thermal_init<R>(t.Ta, t.Tb, t.Q, *t.p, s)) != cudaSuccess) return cuda_fail(e, "thermal init");
     return SHG_OK;
 }
 
@@ -262,7 +267,6 @@ shg_status thermal_batch_run(const shg_params* ps, int count, const void* const*
     // batched optical pass between ej[1] and ej[2]
     cudaEvent_t ej[3] = {nullptr, nullptr, nullptr};
     for (auto& ev : ej) cudaEventCreate(&ev);
-    cudaEventRecord(t0, s);
     do {
         if ((e = dev_alloc((void**)&dd, sizeof(InstDesc) * (size_t)count, s)) != cudaSuccess) {
             rc = cuda_fail(e, "cudaMallocAsync");
@@ -275,8 +279,13 @@ shg_status thermal_batch_run(const shg_params* ps, int count, const void* const*
             ti[i].signal_out = signal_out ? signal_out[i] : nullptr;
             ti[i].slices_p = slices_p;
             ti[i].slices_s = slices_s;
-            rc = ti_setup<R>(ti[i], s);
+            rc = ti_alloc<R>(ti[i], s);
         }
+        if (rc != SHG_OK) break;
+        // the device time starts after the workspace is allocated (a pool that grows maps
+        // memory on the host's time, while the stream idles)
+        cudaEventRecord(t0, s);
+        for (int i = 0; i < count && rc == SHG_OK; ++i) rc = ti_init<R>(ti[i], s);
         if (rc != SHG_OK) break;
         for (int g = 0; rc == SHG_OK; ++g) {
             int na = 0;

@@ -19,13 +19,15 @@ namespace {
 struct AdjVariant {
     int precision, n, cluster, threads;
     size_t smem;
+    // the full kernel (every phase), and the march-only one (forward and re-march phases)
     cudaError_t (*launch)(const InstDesc*, const AdjDesc*, int count, int phase, int round, cudaStream_t);
+    cudaError_t (*launch_march)(const InstDesc*, const AdjDesc*, int count, int phase, int round, cudaStream_t);
 };
 
-template <typename T, int N, int C, int NT>
+template <typename T, int N, int C, int NT, bool MARCH_ONLY>
 cudaError_t launch_adjoint(const InstDesc* d, const AdjDesc* a, int count, int phase, int round, cudaStream_t stream) {
     using Cfg = PlainCfg<T, N, C, NT, false>;
-    auto kern = ssfm_adjoint_kernel<T, N, C, NT>;
+    auto kern = ssfm_adjoint_kernel<T, N, C, NT, MARCH_ONLY>;
     static PerDevice<int> state;  // kernel attributes, once per device
     const cudaError_t attr_err = state.get([&](int, int&) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::smem_bytes);
@@ -48,7 +50,9 @@ cudaError_t launch_adjoint(const InstDesc* d, const AdjDesc* a, int count, int p
     return cudaLaunchKernelEx(&cfg, kern, d, a, phase, round);
 }
 
-#define SHG_ADJ(T, PREC, N, C, NT) {PREC, N, C, NT, PlainCfg<T, N, C, NT, false>::smem_bytes, &launch_adjoint<T, N, C, NT>}
+#define SHG_ADJ(T, PREC, N, C, NT)                                                                         \
+    {PREC, N, C, NT, PlainCfg<T, N, C, NT, false>::smem_bytes, &launch_adjoint<T, N, C, NT, false>, \
+     &launch_adjoint<T, N, C, NT, true>}
 
 const AdjVariant kAdjVariants[] = {
     SHG_ADJ(float, 32, 32, 1, 128),  SHG_ADJ(float, 32, 64, 1, 256),   SHG_ADJ(float, 32, 128, 2, 256),
@@ -246,12 +250,15 @@ shg_status grad_batch(const shg_params* ps, int count, const double* const* poli
         cudaEventCreate(&t0);
         cudaEventCreate(&t1);
         cudaEventRecord(t0, s);
-        if ((e = v->launch(dd, da, count, kAdjForward, 0, s)) == cudaSuccess && (e = cudaEventRecord(eF, s)) == cudaSuccess)
+        // the forward and re-march phases run the march-only kernel (two CTAs per SM where its
+        // shared memory allows), the adjoint marches the full one
+        if ((e = v->launch_march(dd, da, count, kAdjForward, 0, s)) == cudaSuccess &&
+            (e = cudaEventRecord(eF, s)) == cudaSuccess)
             e = cudaStreamWaitEvent(s2, eF, 0);
         for (int r = 0; r < mmax && e == cudaSuccess; ++r) {
             if (r + 1 < mmax) {
                 if (r >= 1 && (e = cudaStreamWaitEvent(s2, eB[r - 1], 0)) != cudaSuccess) break;
-                if ((e = v->launch(dd, da, count, kAdjRemarch, r, s2)) != cudaSuccess) break;
+                if ((e = v->launch_march(dd, da, count, kAdjRemarch, r, s2)) != cudaSuccess) break;
                 if ((e = cudaEventRecord(eR[r], s2)) != cudaSuccess) break;
             }
             if (r >= 1 && (e = cudaStreamWaitEvent(s, eR[r - 1], 0)) != cudaSuccess) break;
@@ -277,13 +284,12 @@ shg_status grad_batch(const shg_params* ps, int count, const double* const* poli
             for (int slot = 0; slot <= J.M; ++slot)
                 for (int c = 0; c < C; ++c)
                     for (int k = 0; k < kAdjAcc; ++k) A[k] += part[((size_t)slot * C + c) * kAdjAcc + k];
-            // temperature derivatives of the scalar constants (central differences in FP64)
-            const double lp = p.lambda_p, ls = 0.5 * lp, T = p.temp, h = 1e-3;
+            // temperature derivatives of the scalar constants (closed form, FP64)
+            const double lp = p.lambda_p, ls = 0.5 * lp, T = p.temp;
             const int cr = p.crystal;
             const double np = sellmeier(cr, lp, T), ns = sellmeier(cr, ls, T);
-            const double dnp = (sellmeier(cr, lp, T + h) - sellmeier(cr, lp, T - h)) / (2 * h);
-            const double dns = (sellmeier(cr, ls, T + h) - sellmeier(cr, ls, T - h)) / (2 * h);
-            const double ddk = (delta_k(p, T + h) - delta_k(p, T - h)) / (2 * h);
+            const double dnp = sellmeier_dT(cr, lp, T), dns = sellmeier_dT(cr, ls, T);
+            const double ddk = delta_k_dT(p, T);
             const InstDesc& d = J.d;
             const double Jp = d.pw_s * A[kAccJ];
             double dT = 0.0;

@@ -95,6 +95,8 @@ double sellmeier(int crystal, double L, double T) { return crystal_n(crystal, L,
 
 // Δk at temperature T with the grating's thermal expansion (PhaseMatching.h:47-85).
 double delta_k(const shg_params& p, double T) { return crystal_delta_k(p.crystal, p.lambda_p, p.period, T); }
+double sellmeier_dT(int crystal, double L, double T) { return crystal_dn_dT(crystal, L, T); }
+double delta_k_dT(const shg_params& p, double T) { return crystal_ddk_dT(p.crystal, p.lambda_p, p.period, T); }
 
 // Constants of one plain optical pass at uniform temperature Tc (the reference reads
 // T at voxel (NX/2, NY/2, 0) for the pump and propagators, Efields.h:88,124).

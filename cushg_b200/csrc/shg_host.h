@@ -28,6 +28,9 @@ cudaError_t dev_alloc(void** ptr, size_t bytes, cudaStream_t s);
 
 double sellmeier(int crystal, double L, double T);
 double delta_k(const shg_params& p, double T);
+// dn/dT and dΔk/dT in closed form (crystal.cuh)
+double sellmeier_dT(int crystal, double L, double T);
+double delta_k_dT(const shg_params& p, double T);
 InstDesc make_plain_desc(const shg_params& p, double Tc, double T_dk);
 // shg_fp32_error_estimate
 double fp32_error_estimate(const shg_params& p);

@@ -249,10 +249,13 @@ __device__ __forceinline__ Cx2 pack2(float2 a, float2 b) { return Cx2{make_float
 __device__ __forceinline__ float2 lane0(const Cx2& v) { return make_float2(v.r.x, v.i.x); }
 __device__ __forceinline__ float2 lane1(const Cx2& v) { return make_float2(v.r.y, v.i.y); }
 
-template <typename T, int N, int C, int NT>
-__global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __restrict__ descs,
-                                                             const AdjDesc* __restrict__ adescs, int phase,
-                                                             int round) {
+// MARCH_ONLY: an instantiation with the forward and re-march phases only.  Without the
+// adjoint march's code it needs half the registers, so two CTAs fit on an SM where the full
+// kernel fits one; the march it runs is the same code as the full kernel's.
+template <typename T, int N, int C, int NT, bool MARCH_ONLY = false>
+__global__ void __launch_bounds__(NT, MARCH_ONLY ? 2 : 1) ssfm_adjoint_kernel(const InstDesc* __restrict__ descs,
+                                                                              const AdjDesc* __restrict__ adescs,
+                                                                              int phase, int round) {
     using Cfg = PlainCfg<T, N, C, NT, false>;
     constexpr int R2 = Cfg::R2, SW = Cfg::SW;
     constexpr int JA = Cfg::JA, JB = Cfg::JB, JCA = Cfg::JCA, JCB = Cfg::JCB;
@@ -827,7 +830,7 @@ __global__ void __launch_bounds__(NT, 1) ssfm_adjoint_kernel(const InstDesc* __r
         march(fwd ? 0 : sb, se, fwd, fwd ? last_sb : sb, fwd);
         if (!fwd) return;
         store_planes(lam, lam + NN);
-    } else {
+    } else if constexpr (!MARCH_ONLY) {
         load_planes(lam, lam + NN);
         __syncthreads();
         backward(sb, se);

@@ -95,7 +95,75 @@ struct ThermalInst {
     bool done = false;
     InstDesc d;  // descriptor of the latest optical pass
     double jacobi_ms = 0.0, optics_ms = 0.0;
+    // Graphs of `count` one-sweep launches starting from Ta (parity 0) or Tb (parity 1): a
+    // window of unchecked sweeps is a thousand launches of ~10 µs each, replayed from a graph
+    // instead of being issued one by one.
+    struct SweepGraph {
+        int64_t count = 0;
+        int parity = 0;
+        cudaGraphExec_t exec = nullptr;
+    };
+    SweepGraph graphs[4];
 };
+
+// Windows shorter than this run as plain launches.
+constexpr int64_t kSweepGraphMin = 64;
+
+// `count` unchecked one-sweep launches of instance t from a graph (captured at first use for
+// this start buffer and count, kept for the run): cur / nxt as run_sweeps leaves them.
+template <typename R>
+cudaError_t run_sweeps_graphed(ThermalInst<R>& t, int64_t count, cudaStream_t s) {
+    const shg_params& p = *t.p;
+    if (t.depth > 1 || count < kSweepGraphMin)
+        return run_sweeps<R>(t.cur, t.nxt, t.Ta, t.maps, t.Q, t.k, p.boundary, t.depth, count, t.tb_err, s);
+    const int parity = t.cur == t.Ta ? 0 : 1;
+    typename ThermalInst<R>::SweepGraph* g = nullptr;
+    for (auto& c : t.graphs)
+        if (c.exec && c.count == count && c.parity == parity) g = &c;
+    if (!g) {
+        for (auto& c : t.graphs)
+            if (!c.exec) {
+                g = &c;
+                break;
+            }
+        if (!g)  // every slot used by other counts: plain launches
+            return run_sweeps<R>(t.cur, t.nxt, t.Ta, t.maps, t.Q, t.k, p.boundary, t.depth, count, t.tb_err, s);
+        cudaStream_t cs = nullptr;
+        cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return e;
+        cudaGraph_t graph = nullptr;
+        R* a = t.cur;
+        R* b = t.nxt;
+        e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            const cudaError_t el = run_sweeps<R>(a, b, t.Ta, t.maps, t.Q, t.k, p.boundary, 1, count, t.tb_err, cs);
+            e = cudaStreamEndCapture(cs, &graph);
+            if (el != cudaSuccess) e = el;
+        }
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&g->exec, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        cudaStreamDestroy(cs);
+        if (e != cudaSuccess) {
+            g->exec = nullptr;
+            return e;
+        }
+        g->count = count;
+        g->parity = parity;
+    }
+    const cudaError_t e = cudaGraphLaunch(g->exec, s);
+    if (e != cudaSuccess) return e;
+    if (count & 1) std::swap(t.cur, t.nxt);
+    return cudaSuccess;
+}
+
+template <typename R>
+void ti_release(ThermalInst<R>& t) {
+    for (auto& c : t.graphs)
+        if (c.exec) {
+            cudaGraphExecDestroy(c.exec);
+            c.exec = nullptr;
+        }
+}
 
 // Buffers of one instance.
 template <typename R>
@@ -167,9 +235,7 @@ shg_status ti_jacobi(ThermalInst<R>& t, cudaStream_t s) {
     };
     shg_status rc = SHG_OK;
     if (p.conv_rule == SHG_CONV_FIXED) {
-        if ((e = run_sweeps<R>(t.cur, t.nxt, t.Ta, t.maps, t.Q, t.k, p.boundary, t.depth, t.max_sweeps - 1, t.tb_err, s)) !=
-            cudaSuccess)
-            return cuda_fail(e, "jacobi sweep");
+        if ((e = run_sweeps_graphed<R>(t, t.max_sweeps - 1, s)) != cudaSuccess) return cuda_fail(e, "jacobi sweep");
         if ((rc = checked(SHG_CONV_MAXABS, &red)) != SHG_OK) return rc;
         counter = t.max_sweeps;
         if (!std::isfinite(red))
@@ -189,9 +255,7 @@ shg_status ti_jacobi(ThermalInst<R>& t, cudaStream_t s) {
         ++counter;
         if (red < t.tol) break;
         const int64_t left = std::min<int64_t>(t.check_every - 1, t.max_sweeps - counter);
-        if ((e = run_sweeps<R>(t.cur, t.nxt, t.Ta, t.maps, t.Q, t.k, p.boundary, t.depth, left, t.tb_err, s)) !=
-            cudaSuccess)
-            return cuda_fail(e, "jacobi sweep");
+        if ((e = run_sweeps_graphed<R>(t, left, s)) != cudaSuccess) return cuda_fail(e, "jacobi sweep");
         counter += std::max<int64_t>(left, 0);
     }
     t.counter = counter;
@@ -365,8 +429,11 @@ shg_status thermal_batch_run(const shg_params* ps, int count, const void* const*
             }
         }
     } while (0);
-    for (auto& t : ti)
+    cudaStreamSynchronize(s);  // the graphs' launches are done before their release
+    for (auto& t : ti) {
+        ti_release<R>(t);
         if (t.buf) cudaFreeAsync(t.buf, s);
+    }
     if (dd) cudaFreeAsync(dd, s);
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);

@@ -160,15 +160,17 @@ static BatchLayout batch_layout(const shg_params* params, int count, void* const
         int j = k;
         double w = 0;
         while (j < count && items[j].v == items[k].v) w += items[j++].cost;
-        // an FP64 group (an FP64 batch, or the instances an FP32 batch's guard promotes) costs
-        // about 2.5x an FP32 group of the same point-steps: ordered by that, a small FP64
-        // group starts early instead of trailing the FP32 groups
-        if (items[k].v->precision == 64) w *= 2.5;
         L.groups.push_back({items[k].v, k, j, w});
         k = j;
     }
-    std::sort(L.groups.begin(), L.groups.end(),
-              [](const BatchLayout::Group& a, const BatchLayout::Group& b) { return a.work > b.work; });
+    // The groups an FP32 batch's guard promotes to the FP64 march go first: few instances, but
+    // each runs about 2.5x as long as in FP32, so they are the batch's longest jobs; launched
+    // last, their clusters would wait for SMs and trail the FP32 groups.  Then by total work.
+    std::sort(L.groups.begin(), L.groups.end(), [&](const BatchLayout::Group& a, const BatchLayout::Group& b) {
+        const bool pa = a.v->precision > params[0].precision, pb = b.v->precision > params[0].precision;
+        if (pa != pb) return pa;
+        return a.work > b.work;
+    });
     return L;
 }
 

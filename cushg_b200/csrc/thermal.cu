@@ -13,7 +13,6 @@
 //       -> optics_kernel (Δk, n_p, n_s per voxel, once per optical pass)
 #include <cuda_runtime.h>
 
-#include <algorithm>
 #include <cstdint>
 
 #include "crystal.cuh"
@@ -138,25 +137,18 @@ template <typename R> struct pair_t;
 template <> struct pair_t<float> { using type = float2; };
 template <> struct pair_t<double> { using type = double2; };
 
-// One work item of the paired sweep: the column of voxel pairs (x, x+1) at row y over the
-// planes [z0, z1).  CG: read T through L2 only (ld.global.cg), for a kernel that runs several
-// sweeps in one launch and must not see a stale L1 line of the buffer it wrote a sweep ago.
-template <typename R, int BOUND, bool CG>
-__device__ __forceinline__ void jacobi_pairs_column(const R* __restrict__ Ti, R* __restrict__ Tf,
-                                                    const R* __restrict__ Q, const JacobiCoef<R>& k, int x, int y,
-                                                    int z0, int z1) {
+template <typename R, int BOUND>
+__global__ void __launch_bounds__(256) jacobi_zb2_kernel(const R* __restrict__ Ti, R* __restrict__ Tf,
+                                                         const R* __restrict__ Q, JacobiCoef<R> k) {
     using R2 = typename pair_t<R>::type;
     const int n = k.n, nz = k.nz;
+    const int x = 2 * (blockIdx.x * 32 + threadIdx.x);
+    const int y = blockIdx.y * 8 + threadIdx.y;
+    if (x >= n || y >= n) return;
+    const int z0 = blockIdx.z * kJacobiZB, z1 = min(nz, z0 + kJacobiZB);
     const size_t sy = (size_t)n, sz = (size_t)n * n;
     size_t i = (size_t)z0 * sz + (size_t)y * sy + x;
-    auto ld2 = [&](size_t j) {
-        if constexpr (CG) return __ldcg(reinterpret_cast<const R2*>(Ti + j));
-        else return *reinterpret_cast<const R2*>(Ti + j);
-    };
-    auto ld1 = [&](size_t j) {
-        if constexpr (CG) return __ldcg(Ti + j);
-        else return Ti[j];
-    };
+    auto ld2 = [&](size_t j) { return *reinterpret_cast<const R2*>(Ti + j); };
     R2 zero2;
     zero2.x = zero2.y = (R)0;
     R2 below = z0 > 0 ? ld2(i - sz) : zero2;
@@ -167,7 +159,7 @@ __device__ __forceinline__ void jacobi_pairs_column(const R* __restrict__ Ti, R*
     for (int z = z0; z < z1; ++z, i += sz) {
         const R2 above = z + 1 < nz ? ld2(i + sz) : zero2;
         const R2 ym = y > 0 ? ld2(i - sy) : zero2, yp = y + 1 < n ? ld2(i + sy) : zero2;
-        const R xm = x > 0 ? ld1(i - 1) : (R)0, xp = x + 2 < n ? ld1(i + 2) : (R)0;
+        const R xm = x > 0 ? Ti[i - 1] : (R)0, xp = x + 2 < n ? Ti[i + 2] : (R)0;
         const R2 q = Q ? *reinterpret_cast<const R2*>(Q + i) : zero2;  // Q null: no heat source
         auto get0 = [&](int dx, int dy, int dz) -> R {
             if (dz) return dz > 0 ? above.x : below.x;
@@ -200,83 +192,6 @@ __device__ __forceinline__ void jacobi_pairs_column(const R* __restrict__ Ti, R*
         }
         below = cur;
         cur = above;
-    }
-}
-
-template <typename R, int BOUND>
-__global__ void __launch_bounds__(256) jacobi_zb2_kernel(const R* __restrict__ Ti, R* __restrict__ Tf,
-                                                         const R* __restrict__ Q, JacobiCoef<R> k) {
-    const int x = 2 * (blockIdx.x * 32 + threadIdx.x);
-    const int y = blockIdx.y * 8 + threadIdx.y;
-    if (x >= k.n || y >= k.n) return;
-    const int z0 = blockIdx.z * kJacobiZB, z1 = min(k.nz, z0 + kJacobiZB);
-    jacobi_pairs_column<R, BOUND, false>(Ti, Tf, Q, k, x, y, z0, z1);
-}
-
-// Several unchecked sweeps in one cooperative launch, for grids that stay in L2 (where a
-// sweep lasts ~10 µs and the launch boundary between sweeps is a sizeable part of it).  Every
-// CTA takes the same work items (a 64 x 8 tile of pair columns over zb planes) in every
-// sweep, and the CTAs meet at a grid barrier between sweeps: an arrival counter and a
-// generation word in global memory, each wait bounded by kPersistWaitNs, after which the
-// kernel sets *err and every CTA returns.  All CTAs are resident at once (cooperative launch),
-// so the barrier completes.  Sweep s reads Ta when (parity + s) is even, else Tb, and writes
-// the other.  Each voxel is the same jacobi_inner / jacobi_point of the same operands as in
-// the one-sweep kernels.
-constexpr unsigned long long kPersistWaitNs = 2000000000ull;
-
-__device__ __forceinline__ unsigned long long persist_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-template <typename R, int BOUND>
-__global__ void __launch_bounds__(256) jacobi_persist_kernel(R* __restrict__ Ta, R* __restrict__ Tb,
-                                                             const R* __restrict__ Q, JacobiCoef<R> k, int nsweeps,
-                                                             int parity, int zb, unsigned* __restrict__ bar,
-                                                             unsigned* __restrict__ err) {
-    const int n = k.n, nz = k.nz;
-    const int tiles_x = (n + 63) / 64, tiles_y = (n + 7) / 8, zblocks = (nz + zb - 1) / zb;
-    const int items = tiles_x * tiles_y * zblocks;
-    __shared__ int s_abort;
-    for (int sweep = 0; sweep < nsweeps; ++sweep) {
-        const bool from_a = ((parity + sweep) & 1) == 0;
-        const R* Ti = from_a ? Ta : Tb;
-        R* Tf = from_a ? Tb : Ta;
-        for (int it = blockIdx.x; it < items; it += gridDim.x) {
-            const int tx = it % tiles_x, ty = (it / tiles_x) % tiles_y, bz = it / (tiles_x * tiles_y);
-            const int x = 2 * (tx * 32 + threadIdx.x), y = ty * 8 + threadIdx.y;
-            if (x < n && y < n) {
-                const int z0 = bz * zb;
-                jacobi_pairs_column<R, BOUND, true>(Ti, Tf, Q, k, x, y, z0, min(nz, z0 + zb));
-            }
-        }
-        if (sweep + 1 == nsweeps) break;
-        // grid barrier
-        __syncthreads();
-        if (threadIdx.x == 0 && threadIdx.y == 0) {
-            s_abort = 0;
-            volatile unsigned* gen = bar + 1;
-            const unsigned g = *gen;
-            __threadfence();
-            if (atomicAdd(bar, 1u) == gridDim.x - 1) {
-                bar[0] = 0;
-                __threadfence();
-                atomicAdd(bar + 1, 1u);
-            } else {
-                const unsigned long long t0 = persist_ns();
-                while (*gen == g) {
-                    if (persist_ns() - t0 > kPersistWaitNs) {
-                        atomicOr(err, 1u);
-                        s_abort = 1;
-                        break;
-                    }
-                }
-            }
-            __threadfence();
-        }
-        __syncthreads();
-        if (s_abort) return;
     }
 }
 
@@ -432,39 +347,6 @@ cudaError_t launch_fill(R* a, size_t total, R v, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-// Planes per work item of the persistent sweeps: one item per resident CTA where possible.
-static int persist_zb(int n, int nz, int grid) {
-    const long cols = (long)((n + 63) / 64) * ((n + 7) / 8);
-    const long zb = (cols * nz + grid - 1) / grid;
-    return (int)std::max(1L, std::min((long)nz, zb));
-}
-
-template <typename R>
-cudaError_t launch_jacobi_persist(R* Ta, R* Tb, const R* Q, const JacobiCoef<R>& k, int boundary, int nsweeps,
-                                  int parity, unsigned* bar, unsigned* err, cudaStream_t s) {
-    auto kern = boundary == SHG_BOUNDARY_OVEN_SURROUNDED ? jacobi_persist_kernel<R, SHG_BOUNDARY_OVEN_SURROUNDED>
-                                                          : jacobi_persist_kernel<R, SHG_BOUNDARY_TOP_OPEN>;
-    static PerDevice<int> state;  // resident CTAs of the cooperative grid, once per device
-    int grid = 0;
-    cudaError_t e = state.get(
-        [&](int dev, int& g) {
-            int sms = 0, per_sm = 0;
-            cudaError_t r = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            int coop = 0;
-            if (r == cudaSuccess) r = cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
-            if (r == cudaSuccess) r = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0);
-            g = coop ? sms * per_sm : 0;
-            return r;
-        },
-        &grid);
-    if (e != cudaSuccess) return e;
-    if (grid <= 0) return cudaErrorNotSupported;
-    int zb = persist_zb(k.n, k.nz, grid);
-    JacobiCoef<R> kk = k;
-    void* args[] = {&Ta, &Tb, const_cast<R**>(&Q), &kk, &nsweeps, &parity, &zb, &bar, &err};
-    return cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(32, 8), args, 0, s);
-}
-
 size_t jacobi_partials(const shg_params& p) {
     return (size_t)((p.nx + 31) / 32) * ((p.nx + 7) / 8) * p.nz;
 }
@@ -523,9 +405,5 @@ template cudaError_t launch_jacobi<float>(const float*, float*, const float*, co
                                           double*, double*, cudaStream_t);
 template cudaError_t launch_jacobi<double>(const double*, double*, const double*, const JacobiCoef<double>&, int, bool,
                                            int, double*, double*, cudaStream_t);
-template cudaError_t launch_jacobi_persist<float>(float*, float*, const float*, const JacobiCoef<float>&, int, int, int,
-                                                  unsigned*, unsigned*, cudaStream_t);
-template cudaError_t launch_jacobi_persist<double>(double*, double*, const double*, const JacobiCoef<double>&, int, int,
-                                                   int, unsigned*, unsigned*, cudaStream_t);
 
 }  // namespace shg

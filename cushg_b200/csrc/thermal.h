@@ -35,13 +35,6 @@ template <typename R>
 cudaError_t launch_jacobi(const R* Ti, R* Tf, const R* Q, const JacobiCoef<R>& k, int boundary, bool resid, int rule,
                           double* partial, double* out, cudaStream_t s);
 size_t jacobi_partials(const shg_params& p);
-// `nsweeps` unchecked sweeps in one cooperative launch (grids that stay in L2): sweep s reads
-// Ta when (parity + s) is even, else Tb, and writes the other; bar: two zeroed words the
-// launches share (an arrival counter, left at zero, and a generation word); *err is set to 1
-// if a grid barrier wait gave up (every CTA then returns early).
-template <typename R>
-cudaError_t launch_jacobi_persist(R* Ta, R* Tb, const R* Q, const JacobiCoef<R>& k, int boundary, int nsweeps,
-                                  int parity, unsigned* bar, unsigned* err, cudaStream_t s);
 
 // Temporally blocked sweeps (jacobi_tb.cu): `depth` (2..4) sweeps Ti -> Tf in one launch,
 // with Ti and Q read through 3D TMA maps made by make_tb_map.  *err is set to 1 if a

@@ -83,7 +83,6 @@ struct ThermalInst {
     R *Ta = nullptr, *Tb = nullptr, *Q = nullptr, *DK = nullptr, *NP = nullptr, *NS = nullptr;
     double *partial = nullptr, *resid = nullptr, *power = nullptr;
     unsigned* tb_err = nullptr;
-    unsigned* bar = nullptr;  // grid-barrier words of the persistent sweeps
     R *cur = nullptr, *nxt = nullptr;  // cur holds the latest temperature (the reference's Tinic == Tfinal)
     SweepMaps<R> maps;
     JacobiCoef<R> k;
@@ -110,34 +109,11 @@ struct ThermalInst {
 // Windows shorter than this run as plain launches.
 constexpr int64_t kSweepGraphMin = 64;
 
-// Grids whose sweep streams from L2 (T, T' and Q within kPersistBytes) run a window of
-// unchecked sweeps as one cooperative launch (launch_jacobi_persist) instead of a launch per
-// sweep: there a sweep lasts ~10 µs and the boundary between launches is a sizeable part of it.
-constexpr size_t kPersistBytes = 100ull << 20;
-
-template <typename R>
-bool use_persist(const shg_params& p, int depth) {
-    return depth == 1 && 3 * sizeof(R) * (size_t)p.nx * p.nx * p.nz <= kPersistBytes;
-}
-
-// `count` unchecked one-sweep launches of instance t: one cooperative launch for an L2-sized
-// grid, else a graph of one-sweep launches (captured at first use for this start buffer and
-// count, kept for the run): cur / nxt as run_sweeps leaves them.
+// `count` unchecked one-sweep launches of instance t from a graph (captured at first use for
+// this start buffer and count, kept for the run): cur / nxt as run_sweeps leaves them.
 template <typename R>
 cudaError_t run_sweeps_graphed(ThermalInst<R>& t, int64_t count, cudaStream_t s) {
     const shg_params& p = *t.p;
-    if (count <= 0) return cudaSuccess;
-    if (use_persist<R>(p, t.depth)) {
-        while (count > 0) {
-            const int c = (int)std::min<int64_t>(count, 1 << 20);
-            const cudaError_t e =
-                launch_jacobi_persist<R>(t.Ta, t.Tb, t.Q, t.k, p.boundary, c, t.cur == t.Ta ? 0 : 1, t.bar, t.tb_err, s);
-            if (e != cudaSuccess) return e;
-            if (c & 1) std::swap(t.cur, t.nxt);
-            count -= c;
-        }
-        return cudaSuccess;
-    }
     if (t.depth > 1 || count < kSweepGraphMin)
         return run_sweeps<R>(t.cur, t.nxt, t.Ta, t.maps, t.Q, t.k, p.boundary, t.depth, count, t.tb_err, s);
     const int parity = t.cur == t.Ta ? 0 : 1;
@@ -209,7 +185,6 @@ shg_status ti_alloc(ThermalInst<R>& t, cudaStream_t s) {
     t.resid = t.partial + npart;                            // [0] convergence value, [1] staging-error word
     t.power = t.resid + 2;                                  // [2]
     t.tb_err = reinterpret_cast<unsigned*>(t.resid + 1);    // set by a blocked sweep whose staging timed out
-    t.bar = reinterpret_cast<unsigned*>(t.resid + 4);      // [2], after the power slots
     t.k = make_jacobi_coef<R>(p);
     // Solver.h:332: tol = 5e-4 / TSIZE in the working precision
     t.tol = p.jacobi_tol > 0 ? p.jacobi_tol : (double)(R)(5e-4 / (double)nt);
@@ -227,7 +202,7 @@ shg_status ti_alloc(ThermalInst<R>& t, cudaStream_t s) {
 template <typename R>
 shg_status ti_init(ThermalInst<R>& t, cudaStream_t s) {
     cudaError_t e;
-    if ((e = cudaMemsetAsync(t.resid, 0, 5 * sizeof(double), s)) != cudaSuccess) return cuda_fail(e, "memset");
+    if ((e = cudaMemsetAsync(t.resid, 0, 2 * sizeof(double), s)) != cudaSuccess) return cuda_fail(e, "memset");
     if ((e = launch_thermal_init<R>(t.Ta, t.Tb, t.Q, *t.p, s)) != cudaSuccess) return cuda_fail(e, "thermal init");
     return SHG_OK;
 }
@@ -254,7 +229,7 @@ shg_status ti_jacobi(ThermalInst<R>& t, cudaStream_t s) {
             return cuda_fail(e, "jacobi residual");
         unsigned staged_err = 0;
         std::memcpy(&staged_err, &h[1], sizeof(staged_err));
-        if (staged_err) return fail(SHG_ERR_CUDA, "Jacobi sweeps: a staged plane or a grid barrier wait gave up");
+        if (staged_err) return fail(SHG_ERR_CUDA, "blocked Jacobi sweep: a staged plane did not arrive");
         *out = h[0];
         return SHG_OK;
     };
@@ -480,31 +455,20 @@ shg_status heat_run(const shg_params& p, R* T, const R* Q, int64_t sweeps, cudaS
     if ((e = dev_alloc((void**)&buf, arr + 256, s)) != cudaSuccess) return cuda_fail(e, "cudaMallocAsync");
     R* other = reinterpret_cast<R*>(buf);
     unsigned* tb_err = reinterpret_cast<unsigned*>(buf + arr);
-    unsigned* bar = tb_err + 1;  // [2]: grid-barrier words of the persistent sweeps
     shg_status rc = SHG_OK;
     do {
         SweepMaps<R> maps;
         if (depth > 1 && (rc = make_sweep_maps<R>(T, other, Q, n, nz, &maps)) != SHG_OK) break;
         // both buffers start alike, so the voxels no sweep writes (Dirichlet faces) agree
         if ((e = cudaMemcpyAsync(other, T, arr, cudaMemcpyDeviceToDevice, s)) != cudaSuccess ||
-            (e = cudaMemsetAsync(tb_err, 0, 3 * sizeof(unsigned), s)) != cudaSuccess) {
+            (e = cudaMemsetAsync(tb_err, 0, sizeof(unsigned), s)) != cudaSuccess) {
             rc = cuda_fail(e, "heat sweeps set-up");
             break;
         }
         const JacobiCoef<R> k = make_jacobi_coef<R>(p);
         R* cur = T;
         R* nxt = other;
-        if (use_persist<R>(p, depth) && sweeps > 0) {
-            for (int64_t left = sweeps; left > 0 && e == cudaSuccess;) {
-                const int c = (int)std::min<int64_t>(left, 1 << 20);
-                e = launch_jacobi_persist<R>(T, other, Q, k, p.boundary, c, cur == T ? 0 : 1, bar, tb_err, s);
-                if (c & 1) std::swap(cur, nxt);
-                left -= c;
-            }
-        } else {
-            e = run_sweeps<R>(cur, nxt, T, maps, Q, k, p.boundary, depth, sweeps, tb_err, s);
-        }
-        if (e != cudaSuccess) {
+        if ((e = run_sweeps<R>(cur, nxt, T, maps, Q, k, p.boundary, depth, sweeps, tb_err, s)) != cudaSuccess) {
             rc = cuda_fail(e, "jacobi sweep");
             break;
         }
@@ -518,7 +482,7 @@ shg_status heat_run(const shg_params& p, R* T, const R* Q, int64_t sweeps, cudaS
             rc = cuda_fail(e, "heat sweeps");
             break;
         }
-        if (h) rc = fail(SHG_ERR_CUDA, "Jacobi sweeps: a staged plane or a grid barrier wait gave up");
+        if (h) rc = fail(SHG_ERR_CUDA, "blocked Jacobi sweep: a staged plane did not arrive");
     } while (0);
     cudaFreeAsync(buf, s);
     e = cudaGetLastError();

@@ -39,9 +39,9 @@ B200_SMS = 148
 FP32_LANES_PER_SM = 128
 # DRAM bytes (read + write) per launch of the dominant kernel of the sweep, the 256 x 256 FP32
 # class (ssfm_plain_kernel<float, 256, 16, 256>), from one ncu launch-list capture of this
-# bench (`--steps 2 --warmup 3 --no-cpu-baseline --no-autotune`, metrics dram__bytes_read.sum
+# bench (`--steps 2 --warmup 3 --no-cpu-baseline --no-autotune --no-extras`, dram__bytes_read.sum
 # and dram__bytes_write.sum); the fields stay on chip, so this is descriptors and outputs
-SWEEP_256_DRAM_BYTES_PER_LAUNCH = 14.75e6
+SWEEP_256_DRAM_BYTES_PER_LAUNCH = 9.78e6
 # bytes of one instance descriptor the batch call uploads (shg::InstDesc)
 INST_DESC_BYTES = 376
 
@@ -302,7 +302,9 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         },
         "e2e": {"value": e2e_value, "unit": "grid-pt·steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e_ms},
-        "gpu_launches": args.steps * len({p.nx for p in ps}),
+        # one persistent launch per (precision the instance runs in, grid side) group per step
+        "gpu_launches": args.steps * len({(64 if (p.fp32_guard > 0 and shg.fp32_error_estimate(p) > p.fp32_guard)
+                                           else p.precision, p.nx) for p in ps}),
         "roofline": {"bound": "fp32-issue" if args.precision == 32 else "fp64-issue", "achieved": achieved_tflops,
                      "peak": peak, "unit": "TFLOP/s", "frac": achieved_tflops / peak,
                      "traffic": SWEEP_256_DRAM_BYTES_PER_LAUNCH if (args.precision == 32 and not args.class_side) else None,

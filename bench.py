@@ -144,9 +144,6 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
 
     ps = workload_params(args, rank)
-    if args.precision == 32 and args.fp32_guard > 0:
-        # instances whose predicted FP32 SH field error exceeds the guard run the FP64 march
-        ps = [p.replace(fp32_guard=args.fp32_guard) for p in ps]
     total_pts = world * point_steps(ps)
     if args.scaling == "strong" and not args.class_side:
         # one sweep (seed 0) split across the ranks, greedy by cost; no data-path collective
@@ -154,6 +151,9 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         full = P.config_sweep(256, seed=0, precision=args.precision)
         _, ps = shard.shard(full, rank, world)
         total_pts = point_steps(full)
+    if args.precision == 32 and args.fp32_guard > 0:
+        # instances whose predicted FP32 SH field error exceeds the guard run the FP64 march
+        ps = [p.replace(fp32_guard=args.fp32_guard) for p in ps]
     cdt = torch.complex64 if args.precision == 32 else torch.complex128
     pumps = [torch.empty((p.ny, p.nx), dtype=cdt, device=dev) for p in ps]
     sigs = [torch.empty((p.ny, p.nx), dtype=cdt, device=dev) for p in ps]
@@ -279,6 +279,30 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         rel = np.abs(p32 - p64) / np.abs(p64)
         err = {"sh_power_rel_max": float(rel.max()), "sh_power_rel_median": float(np.median(rel))}
 
+    # the same sweep with every instance in FP32 (no guard): its rate and its error, beside the
+    # guarded headline (same schedules, timing as above, fewer steps)
+    unguarded = None
+    if args.precision == 32 and args.fp32_guard > 0 and not args.class_side and not args.no_extras:
+        pu = [p.replace(fp32_guard=0.0) for p in ps]
+        for _ in range(2):
+            shg.solve_batch_device(pu, pumps, sigs, stream=sptr, want_power=False)
+        tu = []
+        for k in range(max(3, args.steps // 2)):
+            flush.fill_(k & 0xFF)
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            shg.solve_batch_device(pu, pumps, sigs, stream=sptr, want_power=False)
+            b.record(stream)
+            torch.cuda.synchronize()
+            tu.append(a.elapsed_time(b))
+        wu = shg.solve_batch_device(pu, None, None, stream=sptr)
+        relu = np.abs(wu - p64) / np.abs(p64)
+        mu = statistics.median(tu)
+        unguarded = {"value": point_steps(pu) / (mu * 1e-3), "unit": "grid-pt·steps/s", "ms_per_step": mu,
+                     "sh_power_rel_max": float(relu.max()), "sh_power_rel_median": float(np.median(relu)),
+                     "instances_above_1e-5": int((relu > 1e-5).sum())}
+
     out = {
         "metric": "batched SSFM grid-pt·steps/s",
         "value": value,
@@ -322,6 +346,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     }
     if err is not None:
         out["fp32_error_vs_fp64"] = err
+    if unguarded is not None:
+        out["fp32_unguarded"] = unguarded
     if args.precision == 32 and args.fp32_guard > 0:
         prom = [p for p in ps if shg.fp32_error_estimate(p) > args.fp32_guard]
         out["config"]["fp32_guard"] = {

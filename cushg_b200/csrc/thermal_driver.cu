@@ -104,81 +104,10 @@ struct ThermalInst {
         cudaGraphExec_t exec = nullptr;
     };
     SweepGraph graphs[4];
-    const void* l2win = nullptr;  // the L2Window active during this instance's Jacobi loop, or null
 };
 
 // Windows shorter than this run as plain launches.
 constexpr int64_t kSweepGraphMin = 64;
-
-// L2 residency of an instance's Jacobi working set.  T, T' and Q are contiguous at the start
-// of its buffer; when they fit the device's persisting-L2 set-aside, the Jacobi loop runs
-// with an access-policy window over them (hit property persisting), so the sweeps read them
-// back from L2 instead of streaming them from HBM.  The set-aside is sized once per device
-// (cudaLimitPersistingL2CacheSize, a limit of this process's context); the stream's previous
-// window is restored after the loop and the persisting lines are released.
-struct L2Persist {
-    size_t max_persist = 0, max_window = 0;
-};
-
-inline cudaError_t l2_persist_limits(L2Persist* out) {
-    static PerDevice<L2Persist> state;
-    return state.get(
-        [](int dev, L2Persist& l) {
-            int mp = 0, mw = 0;
-            cudaError_t e = cudaDeviceGetAttribute(&mp, cudaDevAttrMaxPersistingL2CacheSize, dev);
-            if (e == cudaSuccess) e = cudaDeviceGetAttribute(&mw, cudaDevAttrMaxAccessPolicyWindowSize, dev);
-            if (e == cudaSuccess && mp > 0) e = cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, (size_t)mp);
-            if (e != cudaSuccess) {  // no persistence: run without a window
-                cudaGetLastError();
-                mp = mw = 0;
-            }
-            l.max_persist = (size_t)mp;
-            l.max_window = (size_t)mw;
-            return cudaSuccess;
-        },
-        out);
-}
-
-class L2Window {
-  public:
-    // A window over [base, base + bytes) on s when it fits the device's limits; else nothing.
-    L2Window(cudaStream_t s, void* base, size_t bytes) : s_(s) {
-        L2Persist l;
-        if (!s || l2_persist_limits(&l) != cudaSuccess || l.max_persist == 0 || bytes > l.max_window) return;
-        if (cudaStreamGetAttribute(s, cudaStreamAttributeAccessPolicyWindow, &old_) != cudaSuccess) {
-            cudaGetLastError();
-            return;
-        }
-        cudaStreamAttrValue v = {};
-        v.accessPolicyWindow.base_ptr = base;
-        v.accessPolicyWindow.num_bytes = bytes;
-        v.accessPolicyWindow.hitRatio = (float)std::min(1.0, (double)l.max_persist / (double)bytes);
-        v.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
-        v.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
-        if (cudaStreamSetAttribute(s, cudaStreamAttributeAccessPolicyWindow, &v) != cudaSuccess) {
-            cudaGetLastError();
-            return;
-        }
-        value_ = v;
-        set_ = true;
-    }
-    ~L2Window() {
-        if (!set_) return;
-        cudaStreamSetAttribute(s_, cudaStreamAttributeAccessPolicyWindow, &old_);
-        cudaCtxResetPersistingL2Cache();
-        cudaGetLastError();
-    }
-    // the same window on another stream (the stream a graph window is captured on)
-    void apply(cudaStream_t other) const {
-        if (set_) cudaStreamSetAttribute(other, cudaStreamAttributeAccessPolicyWindow, &value_);
-    }
-    bool active() const { return set_; }
-
-  private:
-    cudaStream_t s_;
-    bool set_ = false;
-    cudaStreamAttrValue old_ = {}, value_ = {};
-};
 
 // `count` unchecked one-sweep launches of instance t from a graph (captured at first use for
 // this start buffer and count, kept for the run): cur / nxt as run_sweeps leaves them.
@@ -202,7 +131,6 @@ cudaError_t run_sweeps_graphed(ThermalInst<R>& t, int64_t count, cudaStream_t s)
         cudaStream_t cs = nullptr;
         cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
         if (e != cudaSuccess) return e;
-        if (t.l2win) static_cast<const L2Window*>(t.l2win)->apply(cs);  // captured into the kernel nodes
         cudaGraph_t graph = nullptr;
         R* a = t.cur;
         R* b = t.nxt;
@@ -431,13 +359,7 @@ shg_status thermal_batch_run(const shg_params* ps, int count, const void* const*
             for (int a = 0; a < na && rc == SHG_OK; ++a) {
                 ThermalInst<R>& t = ti[act[a]];
                 cudaEventRecord(ej[0], s);
-                {
-                    const L2Window win(s, t.Ta, 3 * arr);  // T, T' and Q
-                    t.l2win = win.active() ? &win : nullptr;
-                    rc = ti_jacobi<R>(t, s);
-                    t.l2win = nullptr;
-                }
-                if (rc != SHG_OK) break;
+                if ((rc = ti_jacobi<R>(t, s)) != SHG_OK) break;
                 cudaEventRecord(ej[1], s);
                 if ((e = cudaEventSynchronize(ej[1])) != cudaSuccess) { rc = cuda_fail(e, "jacobi"); break; }
                 float ms = 0.f;
@@ -590,28 +512,11 @@ shg_status thermal_solve_batch(const shg_params* ps, int count, const void* cons
                                void* const* signal_out, void* const* temperature_out, shg_stats* stats,
                                cudaStream_t stream, void* slices_p, void* slices_s, const ThermalBatchHook* hook) {
     if (count <= 0) return SHG_OK;
-    // On the legacy default stream, the run goes to a stream of its own that is ordered with
-    // it (a blocking stream), so that stream attributes (the L2 window of the Jacobi loops)
-    // can be set; a thermal run synchronises before it returns in any case.
-    cudaStream_t own = nullptr;
-    if (!stream) {
-        const cudaError_t e = cudaStreamCreate(&own);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
-        stream = own;
-    }
-    shg_status rc;
     if (ps[0].precision == 32)
-        rc = thermal_batch_run<float>(ps, count, signal_in, pump_out, signal_out, temperature_out, stats, stream,
-                                      slices_p, slices_s, hook);
-    else
-        rc = thermal_batch_run<double>(ps, count, signal_in, pump_out, signal_out, temperature_out, stats, stream,
-                                       slices_p, slices_s, hook);
-    if (own) {
-        const cudaError_t e = cudaStreamSynchronize(own);
-        cudaStreamDestroy(own);
-        if (rc == SHG_OK && e != cudaSuccess) rc = cuda_fail(e, "thermal run");
-    }
-    return rc;
+        return thermal_batch_run<float>(ps, count, signal_in, pump_out, signal_out, temperature_out, stats, stream,
+                                        slices_p, slices_s, hook);
+    return thermal_batch_run<double>(ps, count, signal_in, pump_out, signal_out, temperature_out, stats, stream,
+                                     slices_p, slices_s, hook);
 }
 
 }  // namespace shg

@@ -13,7 +13,6 @@
 //       -> optics_kernel (Δk, n_p, n_s per voxel, once per optical pass)
 #include <cuda_runtime.h>
 
-#include <algorithm>
 #include <cstdint>
 
 #include "crystal.cuh"
@@ -341,137 +340,10 @@ cudaError_t launch_optics_tangent(const R* T, const R* u, R* ddk, R* dnp, R* dns
     return cudaGetLastError();
 }
 
-// Two Jacobi sweeps in one pass over memory (temporal blocking) for a strip of H full rows
-// over a chunk of planes.  A sweep at configuration 2's size (128 x 128 x 200 FP64) streams
-// its 78.6 MB from DRAM at the copy rate, so two sweeps per pass halve the bytes per sweep.
-//   * The CTA owns output rows [y0, y0 + H) of planes [z0, z1), every x.  Full rows need no
-//     x halo; the y halo is one row of the intermediate sweep and two of the input.
-//   * It streams z.  Shared memory holds a ring of three input planes (rows y0-2 .. y0+H+1)
-//     and a ring of three intermediate planes (rows y0-1 .. y0+H): step q loads input plane
-//     q+1, computes intermediate plane q, then output plane q-1, with a barrier after the load
-//     and one after the intermediate plane.
-//   * Every voxel of both sweeps is jacobi_point / jacobi_inner of the same operands as in the
-//     one-sweep kernels (voxels the model does not write keep their value), so two sweeps here
-//     give the bits of two one-sweep launches.
-template <typename R>
-struct Zf2Cfg {
-    static size_t smem(int n, int H) { return sizeof(R) * (size_t)n * (3 * (size_t)(H + 4) + 3 * (size_t)(H + 2)); }
-};
-
-template <typename R, int BOUND>
-__global__ void __launch_bounds__(256) jacobi_zf2_kernel(const R* __restrict__ Ti, R* __restrict__ Tf,
-                                                         const R* __restrict__ Q, JacobiCoef<R> k, int H, int zc) {
-    extern __shared__ __align__(16) unsigned char zf2_raw[];
-    const int n = k.n, nz = k.nz;
-    const int y0 = blockIdx.x * H, z0 = blockIdx.y * zc, z1 = min(nz, z0 + zc);
-    const int R0 = H + 4, R1 = H + 2;  // rows of an input / intermediate plane
-    R* L0 = reinterpret_cast<R*>(zf2_raw);  // [3][R0][n], row r is y = y0 - 2 + r
-    R* L1 = L0 + 3 * (size_t)R0 * n;        // [3][R1][n], row r is y = y0 - 1 + r
-    const size_t sz = (size_t)n * n;
-    const int pairs = n / 2;
-    auto l0 = [&](int z, int y) { return L0 + ((size_t)(z % 3) * R0 + (y - (y0 - 2))) * n; };
-    auto l1 = [&](int z, int y) { return L1 + ((size_t)(z % 3) * R1 + (y - (y0 - 1))) * n; };
-    // input plane z, rows y0-2 .. y0+H+1 inside the grid
-    auto load = [&](int z) {
-        const int ya = max(0, y0 - 2), yb = min(n, y0 + H + 2);
-        for (int i = threadIdx.x; i < (yb - ya) * pairs; i += blockDim.x) {
-            const int y = ya + i / pairs, x = 2 * (i % pairs);
-            *reinterpret_cast<typename pair_t<R>::type*>(l0(z, y) + x) =
-                *reinterpret_cast<const typename pair_t<R>::type*>(Ti + (size_t)z * sz + (size_t)y * n + x);
-        }
-    };
-    // one sweep of plane z, rows [ya, yb), from the ring `src` of the previous level; out(x, y,
-    // v, written) receives each voxel
-    auto sweep = [&](int z, int ya, int yb, auto src, auto out) {
-        for (int i = threadIdx.x; i < (yb - ya) * pairs; i += blockDim.x) {
-            const int y = ya + i / pairs, x0 = 2 * (i % pairs);
-            typename pair_t<R>::type q2;
-            q2.x = q2.y = (R)0;  // Q null: no heat source
-            if (Q) q2 = *reinterpret_cast<const typename pair_t<R>::type*>(Q + (size_t)z * sz + (size_t)y * n + x0);
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int x = x0 + h;
-                const R qv = h ? q2.y : q2.x;
-                auto get = [&](int dx, int dy, int dz) -> R { return src(z + dz, y + dy)[x + dx]; };
-                const R old = src(z, y)[x];
-                R v;
-                bool w;
-                if (x >= 1 && x + 1 < n && y >= 1 && y + 1 < n && z >= 1 && z + 1 < nz) {
-                    v = jacobi_inner<R>(get(1, 0, 0), get(-1, 0, 0), get(0, 1, 0), get(0, -1, 0), get(0, 0, 1),
-                                        get(0, 0, -1), qv, k);
-                    w = true;
-                } else {
-                    w = jacobi_point<R, BOUND>(x, y, z, k, qv, get, &v);
-                }
-                out(x, y, w ? v : old, w);
-            }
-        }
-    };
-    const int qa = max(0, z0 - 1), qb = min(nz, z1 + 1);  // intermediate planes needed
-    int loaded = max(0, qa - 1) - 1;                         // last input plane in the ring
-    for (int q = qa; q < qb; ++q) {
-        while (loaded < min(nz - 1, q + 1)) load(++loaded);
-        __syncthreads();
-        // intermediate plane q (sweep 1), rows y0-1 .. y0+H inside the grid
-        sweep(q, max(0, y0 - 1), min(n, y0 + H + 1), l0, [&](int x, int y, R v, bool) { l1(q, y)[x] = v; });
-        __syncthreads();
-        // output plane q-1 (sweep 2), once its intermediate neighbours q-2 .. q exist
-        const int r = q - 1;
-        if (r >= z0 && r < z1)
-            sweep(r, y0, min(n, y0 + H), l1, [&](int x, int y, R v, bool w) {
-                if (w) Tf[(size_t)r * sz + (size_t)y * n + x] = v;
-            });
-    }
-    // the last output plane, when its upper neighbour plane is past the chunk's last step
-    const int r = qb - 1;
-    if (r >= z0 && r < z1 && r == nz - 1) {
-        __syncthreads();
-        sweep(r, y0, min(n, y0 + H), l1, [&](int x, int y, R v, bool w) {
-            if (w) Tf[(size_t)r * sz + (size_t)y * n + x] = v;
-        });
-    }
-}
-
 template <typename R>
 cudaError_t launch_fill(R* a, size_t total, R v, cudaStream_t s) {
     const int blocks = (int)std::min<size_t>((total + 255) / 256, 148 * 16);
     fill_kernel<R><<<blocks, 256, 0, s>>>(a, total, v);
-    return cudaGetLastError();
-}
-
-// Rows per strip of the two-sweep pass: 8 where the two shared-memory rings fit in 200 KB, else
-// 4, else 0 (not available).
-static int zf2_rows(int n, size_t real_bytes) {
-    for (int H : {8, 4})
-        if (real_bytes * (size_t)n * (3 * (size_t)(H + 4) + 3 * (size_t)(H + 2)) <= (200u << 10)) return H;
-    return 0;
-}
-
-bool jacobi_pair_available(int n, int precision) { return zf2_rows(n, precision == 32 ? 4 : 8) > 0; }
-
-template <typename R>
-cudaError_t launch_jacobi_pair(const R* Ti, R* Tf, const R* Q, const JacobiCoef<R>& k, int boundary, cudaStream_t s) {
-    const int H = zf2_rows(k.n, sizeof(R));
-    if (!H) return cudaErrorNotSupported;
-    const size_t smem = Zf2Cfg<R>::smem(k.n, H);
-    auto kern = boundary == SHG_BOUNDARY_OVEN_SURROUNDED ? jacobi_zf2_kernel<R, SHG_BOUNDARY_OVEN_SURROUNDED>
-                                                          : jacobi_zf2_kernel<R, SHG_BOUNDARY_TOP_OPEN>;
-    static PerDevice<int> state[2];  // attributes and SM count, once per device and boundary
-    int sms = 0;
-    cudaError_t e = state[boundary == SHG_BOUNDARY_OVEN_SURROUNDED ? 1 : 0].get(
-        [&](int dev, int& m) {
-            cudaError_t r = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 << 10);
-            if (r == cudaSuccess) r = cudaDeviceGetAttribute(&m, cudaDevAttrMultiProcessorCount, dev);
-            return r;
-        },
-        &sms);
-    if (e != cudaSuccess) return e;
-    // planes per CTA: about two CTAs per SM over the grid's strips
-    const int strips = (k.n + H - 1) / H;
-    const long target = 2L * (sms > 0 ? sms : 148);
-    const int zc = (int)std::max(4L, ((long)k.nz * strips + target - 1) / target);
-    const dim3 grid(strips, (k.nz + zc - 1) / zc);
-    kern<<<grid, 256, smem, s>>>(Ti, Tf, Q, k, H, zc);
     return cudaGetLastError();
 }
 
@@ -533,9 +405,5 @@ template cudaError_t launch_jacobi<float>(const float*, float*, const float*, co
                                           double*, double*, cudaStream_t);
 template cudaError_t launch_jacobi<double>(const double*, double*, const double*, const JacobiCoef<double>&, int, bool,
                                            int, double*, double*, cudaStream_t);
-template cudaError_t launch_jacobi_pair<float>(const float*, float*, const float*, const JacobiCoef<float>&, int,
-                                               cudaStream_t);
-template cudaError_t launch_jacobi_pair<double>(const double*, double*, const double*, const JacobiCoef<double>&, int,
-                                                cudaStream_t);
 
 }  // namespace shg

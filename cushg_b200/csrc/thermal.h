@@ -35,12 +35,6 @@ template <typename R>
 cudaError_t launch_jacobi(const R* Ti, R* Tf, const R* Q, const JacobiCoef<R>& k, int boundary, bool resid, int rule,
                           double* partial, double* out, cudaStream_t s);
 size_t jacobi_partials(const shg_params& p);
-// Two unchecked sweeps Ti -> Tf in one pass (temporal blocking over strips of full rows), the
-// bits of two one-sweep launches; cudaErrorNotSupported where its shared-memory rings do not
-// fit (jacobi_pair_available).
-bool jacobi_pair_available(int n, int precision);
-template <typename R>
-cudaError_t launch_jacobi_pair(const R* Ti, R* Tf, const R* Q, const JacobiCoef<R>& k, int boundary, cudaStream_t s);
 
 // Temporally blocked sweeps (jacobi_tb.cu): `depth` (2..4) sweeps Ti -> Tf in one launch,
 // with Ti and Q read through 3D TMA maps made by make_tb_map.  *err is set to 1 if a

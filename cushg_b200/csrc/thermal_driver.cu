@@ -35,13 +35,9 @@ namespace {
 // (512x512x250 FP64): 16.6 vs 28.9 us per sweep at 128x128x200 FP64, 325 vs 357 us at
 // 512x512x250 FP64.  The blocked kernel is issue-bound (halo recomputation, one barrier per
 // plane), not memory-bound.
-//
-// Automatic (jacobi_block = 0): two sweeps per launch through the full-row pass of
-// launch_jacobi_pair where it fits, which halves the DRAM bytes per sweep; 1: one sweep per
-// launch; 2..4: the TMA-staged blocked kernel.  Every choice gives the same bits.
 int sweep_depth(const shg_params& p) {
     if (p.jacobi_block > 0) return p.jacobi_block;
-    return jacobi_pair_available(p.nx, p.precision) ? 0 : 1;
+    return 1;
 }
 
 // TMA maps of the two temperature buffers and Q for the blocked sweeps.
@@ -64,11 +60,9 @@ template <typename R>
 cudaError_t run_sweeps(R*& cur, R*& nxt, const R* Ta, const SweepMaps<R>& m, const R* Q, const JacobiCoef<R>& k,
                        int boundary, int depth, int64_t count, unsigned* tb_err, cudaStream_t s) {
     while (count > 0) {
-        const int t = depth == 0 ? (int)std::min<int64_t>(2, count) : (int)std::min<int64_t>(depth, count);
+        const int t = (int)std::min<int64_t>(depth, count);
         cudaError_t e;
-        if (depth == 0 && t == 2)
-            e = launch_jacobi_pair<R>(cur, nxt, Q, k, boundary, s);
-        else if (t >= 2)
+        if (t >= 2)
             e = launch_jacobi_tb<R>(cur == Ta ? m.a : m.b, m.q, nxt, k, boundary, t, tb_err, s);
         else
             e = launch_jacobi<R>(cur, nxt, Q, k, boundary, false, 0, nullptr, nullptr, s);
@@ -142,7 +136,7 @@ cudaError_t run_sweeps_graphed(ThermalInst<R>& t, int64_t count, cudaStream_t s)
         R* b = t.nxt;
         e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
-            const cudaError_t el = run_sweeps<R>(a, b, t.Ta, t.maps, t.Q, t.k, p.boundary, t.depth, count, t.tb_err, cs);
+            const cudaError_t el = run_sweeps<R>(a, b, t.Ta, t.maps, t.Q, t.k, p.boundary, 1, count, t.tb_err, cs);
             e = cudaStreamEndCapture(cs, &graph);
             if (el != cudaSuccess) e = el;
         }
@@ -158,9 +152,7 @@ cudaError_t run_sweeps_graphed(ThermalInst<R>& t, int64_t count, cudaStream_t s)
     }
     const cudaError_t e = cudaGraphLaunch(g->exec, s);
     if (e != cudaSuccess) return e;
-    // the buffer swaps run_sweeps makes: one per launch (a launch is two sweeps at depth 0)
-    const int64_t swaps = t.depth == 0 ? count / 2 + (count & 1) : count;
-    if (swaps & 1) std::swap(t.cur, t.nxt);
+    if (count & 1) std::swap(t.cur, t.nxt);
     return cudaSuccess;
 }
 
@@ -457,7 +449,7 @@ shg_status heat_run(const shg_params& p, R* T, const R* Q, int64_t sweeps, cudaS
     const size_t nt = (size_t)n * n * nz, arr = sizeof(R) * nt;
     // Q null (no heat source, the sweeps read none): one sweep per launch, whose kernels
     // take a null Q as zero
-    const int depth = (Q || sweep_depth(p) <= 1) ? sweep_depth(p) : 1;
+    const int depth = Q ? sweep_depth(p) : 1;
     cudaError_t e;
     char* buf = nullptr;
     if ((e = dev_alloc((void**)&buf, arr + 256, s)) != cudaSuccess) return cuda_fail(e, "cudaMallocAsync");

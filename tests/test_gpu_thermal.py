@@ -94,9 +94,8 @@ def test_thermal_fp32_against_fp64_oracle():
 @pytest.mark.parametrize("boundary", [P.SHG_BOUNDARY_TOP_OPEN, P.SHG_BOUNDARY_OVEN_SURROUNDED])
 @pytest.mark.parametrize("n,nz,check_every", [(64, 50, 8), (32, 23, 7), (128, 40, 30)])
 def test_blocked_sweeps_are_bit_identical(precision, boundary, n, nz, check_every):
-    """Fusing sweeps (automatic: two per launch through the full-row pass; 2, 3 or 4 per launch
-    through the TMA-staged kernel) gives the same temperatures, fields and sweep counts, bit
-    for bit, as one sweep per launch.  The grids
+    """Fusing 2, 3 or 4 sweeps per launch (TMA-staged temporal blocking) gives the same
+    temperatures, fields and sweep counts, bit for bit, as one sweep per launch.  The grids
     leave partial tiles at the +x / +y edges and split z into chunks; check windows of
     check_every - 1 unchecked sweeps leave remainders of 1, 2 and 3 sweeps."""
     p = P.workload(n, nz, 6000.0, 3.0, 30.0, 3000.0, 33.0, precision=precision, thermal=1)

@@ -531,8 +531,13 @@ def run_thermal(args) -> dict:
         p = p.replace(nz=args.thermal_nz)
     if args.thermal_max_sweeps:
         p = p.replace(max_sweeps=args.thermal_max_sweeps)
-    p = p.replace(jacobi_block=args.jacobi_block, precision=args.thermal_precision)
+    direct = args.heat_solver == "direct"
+    p = p.replace(jacobi_block=args.jacobi_block, precision=args.thermal_precision,
+                  heat_solver=P.SHG_HEAT_DIRECT if direct else P.SHG_HEAT_JACOBI)
     cdt = torch.complex128 if p.precision == 64 else torch.complex64
+    if direct:  # operator transforms (computed once per process) and kernels before timing
+        wp = torch.empty((p.ny, p.nx), dtype=cdt, device="cuda")
+        shg.solve_device(p.replace(max_outer=1), wp, torch.empty_like(wp))
     pump = torch.empty((p.ny, p.nx), dtype=cdt, device="cuda")
     sig = torch.empty_like(pump)
     with ClockSampler(0) as clk:
@@ -548,7 +553,15 @@ def run_thermal(args) -> dict:
     out = {"metric": "thermal solve (Jacobi voxel-sweeps/s)",
            "workload": f"thermal {p.nx}x{p.ny}x{p.nz} FP{p.precision}", "status": status,
            "jacobi_block": p.jacobi_block or "auto (1)", "wall_s": wall, "clocks": clk.summary()}
-    if st is not None:
+    if st is not None and direct:
+        out.update({"metric": "thermal solve time", "heat_solver": "direct", "value": st.device_ms, "unit": "ms",
+                    "higher_is_better": False, "device_ms": st.device_ms, "heat_solve_ms": st.jacobi_ms,
+                    "optics_ms": st.optics_ms, "outer_iterations": st.outer_iterations, "sh_power_w": st.sh_power,
+                    "last_max_dT_K": st.last_residual,
+                    "note": "each outer iteration's temperature is the Jacobi sweeps' fixed point; last_max_dT_K "
+                            "is max |ΔT| of one FP64 sweep applied to the last one"})
+        out.pop("jacobi_block")
+    elif st is not None:
         out.update({"device_ms": st.device_ms, "jacobi_ms": st.jacobi_ms, "optics_ms": st.optics_ms,
                     "jacobi_sweeps": st.jacobi_sweeps, "outer_iterations": st.outer_iterations,
                     "sh_power_w": st.sh_power, "value": vox * st.jacobi_sweeps / (st.device_ms * 1e-3),
@@ -574,16 +587,28 @@ def run_thermal_batch(args) -> dict:
     # library's pool from one instance to the next (read when the pool is first created), and
     # grow the pool to it before the timed runs (set-up, as an application would at start)
     ps = P.config_thermal_512(args.thermal_count)
-    ps = [p.replace(conv_rule=P.SHG_CONV_FIXED, max_sweeps=args.thermal_fixed_sweeps, max_outer=args.thermal_outer,
-                    precision=32) for p in ps]
+    direct = args.heat_solver == "direct"
+    if direct:  # the stated rule: max|ΔT| < 1e-6 K every outer iteration, at most 5 of them
+        ps = [p.replace(precision=32, heat_solver=P.SHG_HEAT_DIRECT) for p in ps]
+        label = (f"{len(ps)} x thermal 512x512x1000 FP32, heat equation solved to the Jacobi fixed point "
+                 f"(direct, FP64) every outer iteration, <= {ps[0].max_outer} outer iterations, "
+                 f"max|ΔT| < {ps[0].jacobi_tol:g} K")
+    else:
+        ps = [p.replace(conv_rule=P.SHG_CONV_FIXED, max_sweeps=args.thermal_fixed_sweeps,
+                        max_outer=args.thermal_outer, precision=32) for p in ps]
+        label = (f"{len(ps)} x thermal 512x512x1000 FP32, {args.thermal_outer} outer x "
+                 f"{args.thermal_fixed_sweeps} Jacobi sweeps each")
     if args.thermal_mode == "batch":
         # all instances in one shg_thermal_batch call: every instance's buffers and tangent at
         # once (about 11.5 GB each at 512 x 512 x 1000 FP32), in the pool before timing
-        os.environ.setdefault("SHG_POOL_KEEP_MB", str(12 * 1024 * len(ps) + 4096))
-        shg.reserve_device_memory((12 << 30) * len(ps))
+        extra = (5 << 30) if direct else 0  # the direct solve's two FP64 volumes (4.2 GB)
+        os.environ.setdefault("SHG_POOL_KEEP_MB", str(12 * 1024 * len(ps) + 4096 + (extra >> 20)))
+        shg.reserve_device_memory((12 << 30) * len(ps) + extra)
         grad = not args.no_thermal_grad
-        for _ in range(1):  # warm-up on two instances: kernel loading, pool growth
-            shg.thermal_batch([q.replace(max_sweeps=2, nz=20) for q in ps[:2]], grad=grad)
+        for _ in range(1):  # warm-up on two instances: kernel loading, pool growth, operator transforms
+            shg.thermal_batch([q.replace(max_sweeps=2, max_outer=2, nz=20) for q in ps[:2]], grad=grad)
+            if direct:
+                shg.thermal_batch([ps[0].replace(max_outer=1, nz=20)], grad=False)
         torch.cuda.synchronize()
         with ClockSampler(0) as clk:
             t0 = time.perf_counter()
@@ -593,16 +618,15 @@ def run_thermal_batch(args) -> dict:
         runs = []
         for i, (p, st) in enumerate(zip(ps, stats)):
             r = {"oven_c": round(p.temp, 2), "sh_power_w": st.sh_power, "sweeps": st.jacobi_sweeps,
-                 "jacobi_ms": st.jacobi_ms, "optics_ms": st.optics_ms, "last_max_dT_K": st.last_residual}
+                 "outer_iterations": st.outer_iterations, "jacobi_ms": st.jacobi_ms, "optics_ms": st.optics_ms,
+                 "last_max_dT_K": st.last_residual}
             if dt is not None:
                 r["dJ_dToven_w_per_k"] = float(dt[i])
             runs.append(r)
         return {"metric": "thermal batch time", "value": stats[0].device_ms, "unit": "ms", "higher_is_better": False,
                 "timing": "device time of one shg_thermal_batch call (CUDA events)", "wall_ms": wall_ms,
-                "mode": "batch", "with_gradient": grad,
-                "workload": f"{len(ps)} x thermal 512x512x1000 FP32, {args.thermal_outer} outer x "
-                            f"{args.thermal_fixed_sweeps} Jacobi sweeps each",
-                "instances": runs, "clocks": clk.summary()}
+                "mode": "batch", "with_gradient": grad, "heat_solver": args.heat_solver, "workload": label,
+                "max_last_dT_K": max(st.last_residual for st in stats), "instances": runs, "clocks": clk.summary()}
     os.environ.setdefault("SHG_POOL_KEEP_MB", "16384")
     shg.reserve_device_memory(12 << 30)
 
@@ -646,8 +670,7 @@ def run_thermal_batch(args) -> dict:
             "timing": ("wall clock of the whole batch, instances overlapping" if args.thermal_concurrency > 1
                        else "sum of the instances' device times, one at a time"),
             "concurrency": args.thermal_concurrency, "sum_device_ms": total_ms, "wall_ms": wall_ms,
-            "workload": f"{len(ps)} x thermal 512x512x1000 FP32, {args.thermal_outer} outer x "
-                        f"{args.thermal_fixed_sweeps} Jacobi sweeps each",
+            "workload": label, "heat_solver": args.heat_solver,
             "instances": runs, "voxel_sweeps": jac_vox, "optical_point_steps": opt_pts,
             "clocks": clk.summary()}
 
@@ -750,6 +773,9 @@ def main() -> int:
     ap.add_argument("--thermal-max-sweeps", type=int, default=0)
     ap.add_argument("--thermal-precision", type=int, default=64, choices=[32, 64])
     ap.add_argument("--jacobi-block", type=int, default=0, help="sweeps per launch (0 = automatic)")
+    ap.add_argument("--heat-solver", default="jacobi", choices=["jacobi", "direct"],
+                    help="thermal workloads: Jacobi sweeps as the reference runs them, or their fixed point "
+                         "solved directly each outer iteration")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank = int(os.environ.get("RANK", "0"))

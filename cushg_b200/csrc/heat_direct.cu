@@ -1,0 +1,619 @@
+// heat_direct.cu — the steady temperature of the heat equation that the reference's Jacobi
+// sweeps converge to (kernelHeatEquationTopOpen / OvenSurrounded, src/headers/Tfield.h:93-240;
+// the loop Solver.h:339-355), computed directly instead of one sweep at a time.  No counterpart
+// in the reference.
+//
+// The linear system.  Every update of Tfield.h:93-240 is one row of A T = b once the row is
+// multiplied by its own scale: inner points by 1/L2 (Tfield.h:113-115), faces by 2/d^2 of their
+// normal direction (Tfield.h:119-137, 229-236), edges by 4/(d_a d_b) (Tfield.h:143-177) and
+// vertices by 2/(dx dy dz) (Tfield.h:181-196).  In that form every row is the sum of three
+// one-dimensional parts, one per direction, each of which is
+//   (2 u_i - u_{i-1} - u_{i+1}) / d^2                  inside the direction,
+//   (2 (1 + Bi) u_0 - 2 u_1) / d^2  (right-hand 2 Bi T_inf / d^2)   at a Robin face,
+//   and, next to a Dirichlet voxel g, the inside form with g moved to the right-hand side,
+// plus Q / kappa on inner points only.  (The face, edge and vertex coefficients ax .. GV of
+// the reference reduce exactly to these: e.g. the vertical edge's 0.5 (Bix + Biz) times
+// 4/(dx dz) is 2 Bix / dx^2 + 2 Biz / dz^2.)  So A = Ax (+) Ay (+) Az, a Kronecker sum.
+//
+// The solve.  Ax and Ay are tridiagonal and similar to symmetric matrices (a diagonal scaling
+// of the Robin end rows), whose eigendecomposition the host computes once per operator and
+// device (implicit QL).  With the forward transforms F = V^T S and the inverse G = S^{-1} V:
+//   1. b (FP64) from Q, the Dirichlet voxels and T_inf                        rhs_kernel
+//   2. b <- b Fx^T (along x), then Fy b (along y)                            dgemm_kernel x2
+//   3. for every mode (ky, kx): (Az + lambda_x + lambda_y) v = b along z       thomas_kernel
+//   4. v <- Gy v, then v Gx^T                                                dgemm_kernel x2
+//   5. T <- v, with the FP64 residual of one Jacobi sweep of v and the change  finish_kernel
+// Unknowns: TOP_OPEN, x 0..n-1 (Robin both ends), y 1..n-1 (y = 0 Dirichlet, Robin at n-1),
+// z 0..nz-1 (Robin); OVEN_SURROUNDED, x and y 1..n-2 (Dirichlet both ends), z as above.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "jacobi_point.cuh"
+#include "shg_host.h"
+#include "thermal.h"
+
+namespace shg {
+
+namespace {
+
+// One direction's operator: m unknowns at spacing d, each end Robin (with Biot number bi) or
+// next to a Dirichlet voxel.
+struct Op1D {
+    int m = 0;
+    double d = 0.0;
+    int lo_robin = 0, hi_robin = 0;
+    double bi = 0.0;
+    bool operator==(const Op1D& o) const {
+        return m == o.m && d == o.d && lo_robin == o.lo_robin && hi_robin == o.hi_robin && bi == o.bi;
+    }
+};
+
+// Rows of the scaled operator: diagonal a, below-diagonal l (l[0] unused), above-diagonal r
+// (r[m-1] unused).
+void op_rows(const Op1D& op, std::vector<double>& a, std::vector<double>& l, std::vector<double>& r) {
+    const int m = op.m;
+    const double i2 = 1.0 / (op.d * op.d);
+    a.assign(m, 2.0 * i2);
+    l.assign(m, -i2);
+    r.assign(m, -i2);
+    l[0] = 0.0;
+    r[m - 1] = 0.0;
+    if (op.lo_robin) {
+        a[0] = 2.0 * (1.0 + op.bi) * i2;
+        if (m > 1) r[0] = -2.0 * i2;
+    }
+    if (op.hi_robin) {
+        a[m - 1] = 2.0 * (1.0 + op.bi) * i2;
+        if (m > 1) l[m - 1] = -2.0 * i2;
+    }
+}
+
+// Eigenvalues and eigenvectors of the symmetric tridiagonal matrix with diagonal d[0..m) and
+// off-diagonal e[0..m-1) (e[i] couples i and i+1): implicit QL iterations with Wilkinson
+// shifts (Bowdler, Martin, Reinsch and Wilkinson, Numer. Math. 11, 293-306 (1968)).  On
+// return d holds the eigenvalues and z (column-major: vector k is z[k*m .. k*m+m)) the
+// orthonormal eigenvectors.  False if an eigenvalue took more than 64 iterations.
+bool tridiag_eigen(int m, std::vector<double>& d, std::vector<double> e, std::vector<double>& z) {
+    z.assign((size_t)m * m, 0.0);
+    for (int k = 0; k < m; ++k) z[(size_t)k * m + k] = 1.0;
+    e.resize(m);
+    e[m - 1] = 0.0;
+    for (int l = 0; l < m; ++l) {
+        for (int iter = 0;; ++iter) {
+            int j = l;
+            for (; j < m - 1; ++j)  // first negligible off-diagonal at or after l
+                if (std::fabs(e[j]) <= DBL_EPSILON * (std::fabs(d[j]) + std::fabs(d[j + 1]))) break;
+            if (j == l) break;  // d[l] converged
+            if (iter >= 64) return false;
+            // shift: the eigenvalue of the leading 2x2 block nearer to d[l]
+            double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+            double r = std::hypot(g, 1.0);
+            g = d[j] - d[l] + e[l] / (g + std::copysign(r, g));
+            double s = 1.0, c = 1.0, p = 0.0;
+            bool split = false;
+            for (int i = j - 1; i >= l; --i) {  // chase the bulge from the bottom of the block up
+                const double f = s * e[i], b = c * e[i];
+                r = std::hypot(f, g);
+                e[i + 1] = r;
+                if (r == 0.0) {  // the block split: restart on the smaller one
+                    d[i + 1] -= p;
+                    e[j] = 0.0;
+                    split = true;
+                    break;
+                }
+                s = f / r;
+                c = g / r;
+                g = d[i + 1] - p;
+                r = (d[i] - g) * s + 2.0 * c * b;
+                p = s * r;
+                d[i + 1] = g + p;
+                g = c * r - b;
+                double* zi = &z[(size_t)i * m];
+                double* zj = &z[(size_t)(i + 1) * m];
+                for (int k = 0; k < m; ++k) {
+                    const double t = zj[k];
+                    zj[k] = s * zi[k] + c * t;
+                    zi[k] = c * zi[k] - s * t;
+                }
+            }
+            if (split) continue;
+            d[l] -= p;
+            e[l] = g;
+            e[j] = 0.0;
+        }
+    }
+    return true;
+}
+
+// Eigenvalues, forward transform F (row k: mode k) and inverse G (row i: point i) of one
+// operator, all row-major m x m.  The operator M is similar to the symmetric B = S M S^{-1}
+// with S = diag(s), s[i+1] = s[i] sqrt(r[i] / l[i+1]); B = V diag(lambda) V^T gives
+// F = V^T S and G = S^{-1} V.
+bool op_modes(const Op1D& op, std::vector<double>& lam, std::vector<double>& F, std::vector<double>& G) {
+    const int m = op.m;
+    std::vector<double> a, l, r;
+    op_rows(op, a, l, r);
+    std::vector<double> s(m, 1.0), e(m, 0.0);
+    for (int i = 0; i + 1 < m; ++i) {
+        s[i + 1] = s[i] * std::sqrt(r[i] / l[i + 1]);
+        e[i] = -std::sqrt(r[i] * l[i + 1]);
+    }
+    lam = a;
+    std::vector<double> V;
+    if (!tridiag_eigen(m, lam, e, V)) return false;
+    F.assign((size_t)m * m, 0.0);
+    G.assign((size_t)m * m, 0.0);
+    for (int k = 0; k < m; ++k)
+        for (int i = 0; i < m; ++i) {
+            const double v = V[(size_t)k * m + i];  // component i of eigenvector k
+            F[(size_t)k * m + i] = v * s[i];
+            G[(size_t)i * m + k] = v / s[i];
+        }
+    return true;
+}
+
+// Device copies of one operator's transforms: F and G row-major, their transposes, lambda.
+struct OpMats {
+    Op1D op;
+    int dev = -1;
+    double *F = nullptr, *G = nullptr, *FT = nullptr, *GT = nullptr, *lam = nullptr;
+};
+
+// Process-wide cache of operator transforms, per device (an operator's eigendecomposition
+// costs O(m^3) on the host: about 0.3 s at m = 512).
+std::mutex g_ops_mu;
+std::vector<OpMats*> g_ops;
+constexpr size_t kMaxCachedOps = 64;
+
+shg_status get_op(const Op1D& op, const OpMats** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    std::lock_guard<std::mutex> lk(g_ops_mu);
+    for (const OpMats* c : g_ops)
+        if (c->dev == dev && c->op == op) {
+            *out = c;
+            return SHG_OK;
+        }
+    std::vector<double> lam, F, G;
+    if (!op_modes(op, lam, F, G)) return fail(SHG_ERR_NOT_CONVERGED, "heat operator eigendecomposition (m = %d)", op.m);
+    const int m = op.m;
+    const size_t mm = (size_t)m * m;
+    std::vector<double> FT(mm), GT(mm);
+    for (int i = 0; i < m; ++i)
+        for (int k = 0; k < m; ++k) {
+            FT[(size_t)i * m + k] = F[(size_t)k * m + i];
+            GT[(size_t)k * m + i] = G[(size_t)i * m + k];
+        }
+    if (g_ops.size() >= kMaxCachedOps) return fail(SHG_ERR_UNSUPPORTED, "more than %d heat operators cached", (int)kMaxCachedOps);
+    double* buf = nullptr;
+    if ((e = cudaMalloc((void**)&buf, sizeof(double) * (4 * mm + m))) != cudaSuccess) return cuda_fail(e, "cudaMalloc");
+    OpMats* c = new OpMats;
+    c->op = op;
+    c->dev = dev;
+    c->F = buf;
+    c->G = buf + mm;
+    c->FT = buf + 2 * mm;
+    c->GT = buf + 3 * mm;
+    c->lam = buf + 4 * mm;
+    const double* src[5] = {F.data(), G.data(), FT.data(), GT.data(), lam.data()};
+    double* dst[5] = {c->F, c->G, c->FT, c->GT, c->lam};
+    for (int k = 0; k < 5 && e == cudaSuccess; ++k)
+        e = cudaMemcpy(dst[k], src[k], sizeof(double) * (k == 4 ? (size_t)m : mm), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        cudaFree(buf);
+        delete c;
+        return cuda_fail(e, "heat operator upload");
+    }
+    g_ops.push_back(c);
+    *out = c;
+    return SHG_OK;
+}
+
+// The grid's three directions: unknown ranges and operators.
+struct HeatGrid {
+    int n = 0, nz = 0;
+    int x0 = 0, y0 = 0, mx = 0, my = 0;  // first unknown and count along x and y
+    Op1D ox, oy;
+    double dx = 0, dy = 0, dz = 0, biz = 0;
+};
+
+HeatGrid heat_grid(const shg_params& p) {
+    HeatGrid g;
+    g.n = p.nx;
+    g.nz = p.nz;
+    g.dx = p.lx / (p.nx - 1);
+    g.dy = p.ly / (p.ny - 1);
+    g.dz = p.lz / (p.nz - 1);
+    const double bix = p.h_conv * g.dx / p.kappa, biy = p.h_conv * g.dy / p.kappa;
+    g.biz = p.h_conv * g.dz / p.kappa;
+    if (p.boundary == SHG_BOUNDARY_TOP_OPEN) {
+        g.x0 = 0;
+        g.mx = g.n;
+        g.ox = {g.mx, g.dx, 1, 1, bix};
+        g.y0 = 1;
+        g.my = g.n - 1;
+        g.oy = {g.my, g.dy, 0, 1, biy};
+    } else {
+        g.x0 = g.y0 = 1;
+        g.mx = g.my = g.n - 2;
+        g.ox = {g.mx, g.dx, 0, 0, bix};
+        g.oy = {g.my, g.dy, 0, 0, biy};
+    }
+    return g;
+}
+
+// What the kernels need of the grid and the model, in FP64.
+struct HeatArgs {
+    int n, nz, x0, y0, mx, my;
+    int lo_x_robin, hi_x_robin, lo_y_robin, hi_y_robin;
+    double idx2, idy2, idz2, iK, tinf, bix, biy, biz;
+};
+
+// Compact volume index c = (z * my + j) * mx + i of unknown (x0 + i, y0 + j, z).
+// 1. Right-hand side of the scaled system: Q / kappa on inner points, 2 Bi T_inf / d^2 at each
+//    Robin end, g / d^2 for each Dirichlet neighbour g (read from T).
+template <typename R>
+__global__ void rhs_kernel(const R* __restrict__ T, const R* __restrict__ Q, double* __restrict__ b, const HeatArgs a) {
+    const size_t plane = (size_t)a.mx * a.my, total = plane * a.nz;
+    const size_t nn = (size_t)a.n;
+    for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < total; c += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(c % a.mx), j = (int)((c / a.mx) % a.my), z = (int)(c / plane);
+        const int x = a.x0 + i, y = a.y0 + j;
+        const size_t v = ((size_t)z * nn + y) * nn + x;
+        double s = 0.0;
+        if (Q && x > 0 && x < a.n - 1 && y > 0 && y < a.n - 1 && z > 0 && z < a.nz - 1) s = (double)Q[v] * a.iK;
+        if (i == 0) s += a.lo_x_robin ? 2.0 * a.bix * a.tinf * a.idx2 : (double)T[v - 1] * a.idx2;
+        if (i == a.mx - 1) s += a.hi_x_robin ? 2.0 * a.bix * a.tinf * a.idx2 : (double)T[v + 1] * a.idx2;
+        if (j == 0) s += a.lo_y_robin ? 2.0 * a.biy * a.tinf * a.idy2 : (double)T[v - nn] * a.idy2;
+        if (j == a.my - 1) s += a.hi_y_robin ? 2.0 * a.biy * a.tinf * a.idy2 : (double)T[v + nn] * a.idy2;
+        if (z == 0) s += 2.0 * a.biz * a.tinf * a.idz2;
+        if (z == a.nz - 1) s += 2.0 * a.biz * a.tinf * a.idz2;
+        b[c] = s;
+    }
+}
+
+constexpr int kGemmBM = 128, kGemmBN = 64, kGemmBK = 8, kGemmThreads = 256;
+
+// 2, 4. C[b] = A[b] B[b] in FP64 for row-major A (M x K, lda), B (K x N, ldb) and C (M x N, ldc),
+// batch b = blockIdx.z at element strides sA, sB, sC.  A 128 x 64 tile per block, an 8 x 4
+// block of it per thread in registers; the A and B tiles pass through shared memory, double
+// buffered (the next tile's loads are in flight during the current tile's products).  Each
+// output is one FMA chain over k in order.
+__global__ void __launch_bounds__(kGemmThreads, 2) dgemm_kernel(const double* __restrict__ A, const double* __restrict__ B,
+                                                             double* __restrict__ C, int M, int N, int K, int lda,
+                                                             int ldb, int ldc, long long sA, long long sB, long long sC) {
+    __shared__ __align__(16) double As[2][kGemmBK][kGemmBM];
+    __shared__ __align__(16) double Bs[2][kGemmBK][kGemmBN];
+    A += blockIdx.z * sA;
+    B += blockIdx.z * sB;
+    C += blockIdx.z * sC;
+    const int m0 = blockIdx.y * kGemmBM, n0 = blockIdx.x * kGemmBN;
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int ar = tid >> 1, ac = (tid & 1) * 4;   // loads: A row ar, columns ac..ac+3 of the tile
+    const int bk = tid >> 5, bn = (tid & 31) * 2;  // B row bk, columns bn, bn+1
+    double ra[4], rb[2];
+    auto load = [&](int k0) {
+        const int row = m0 + ar;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int col = k0 + ac + q;
+            ra[q] = (row < M && col < K) ? A[(size_t)row * lda + col] : 0.0;
+        }
+        const int krow = k0 + bk;
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int col = n0 + bn + q;
+            rb[q] = (krow < K && col < N) ? B[(size_t)krow * ldb + col] : 0.0;
+        }
+    };
+    auto stash = [&](int buf) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) As[buf][ac + q][ar] = ra[q];
+        Bs[buf][bk][bn] = rb[0];
+        Bs[buf][bk][bn + 1] = rb[1];
+    };
+    double acc[8][4];
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[r][c] = 0.0;
+    load(0);
+    stash(0);
+    __syncthreads();
+    const int tiles = (K + kGemmBK - 1) / kGemmBK;
+    for (int t = 0; t < tiles; ++t) {
+        const int buf = t & 1;
+        if (t + 1 < tiles) load((t + 1) * kGemmBK);
+#pragma unroll
+        for (int kk = 0; kk < kGemmBK; ++kk) {
+            double av[8], bv[4];
+            const double2* ap = reinterpret_cast<const double2*>(&As[buf][kk][ty * 8]);
+            const double2* bp = reinterpret_cast<const double2*>(&Bs[buf][kk][tx * 4]);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const double2 w = ap[q];
+                av[2 * q] = w.x;
+                av[2 * q + 1] = w.y;
+            }
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const double2 w = bp[q];
+                bv[2 * q] = w.x;
+                bv[2 * q + 1] = w.y;
+            }
+#pragma unroll
+            for (int r = 0; r < 8; ++r)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) acc[r][c] = fma(av[r], bv[c], acc[r][c]);
+        }
+        if (t + 1 < tiles) stash(buf ^ 1);  // the other buffer was last read before the previous barrier
+        __syncthreads();
+    }
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        const int row = m0 + ty * 8 + r;
+        if (row >= M) break;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int col = n0 + tx * 4 + c;
+            if (col < N) C[(size_t)row * ldc + col] = acc[r][c];
+        }
+    }
+}
+
+// 3. For every mode t = j * mx + i: (Az + lambda_x[i] + lambda_y[j]) u = f along z, Thomas
+// elimination (the system is diagonally dominant: lambda_x + lambda_y > 0 whenever a direction
+// has a Dirichlet end or a Robin end with Bi > 0, which every boundary model has).  f and then
+// u in v; the eliminated upper diagonal in cp.
+__global__ void thomas_kernel(double* __restrict__ v, double* __restrict__ cp, const double* __restrict__ lx,
+                              const double* __restrict__ ly, int mx, int my, int nz, double idz2, double biz) {
+    const size_t plane = (size_t)mx * my;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < plane; t += (size_t)gridDim.x * blockDim.x) {
+        const double lam = lx[t % mx] + ly[t / mx];
+        const double a_end = 2.0 * (1.0 + biz) * idz2 + lam;  // Robin rows z = 0, nz - 1
+        const double a_in = 2.0 * idz2 + lam;
+        double c = -2.0 * idz2 / a_end;
+        double d = v[t] / a_end;
+        cp[t] = c;
+        v[t] = d;
+        for (int z = 1; z < nz; ++z) {
+            const size_t o = (size_t)z * plane + t;
+            const bool last = z == nz - 1;
+            const double lo = last ? -2.0 * idz2 : -idz2;
+            const double den = (last ? a_end : a_in) - lo * c;
+            c = last ? 0.0 : -idz2 / den;
+            d = (v[o] - lo * d) / den;
+            cp[o] = c;
+            v[o] = d;
+        }
+        double u = d;
+        for (int z = nz - 2; z >= 0; --z) {
+            const size_t o = (size_t)z * plane + t;
+            u = v[o] - cp[o] * u;
+            v[o] = u;
+        }
+    }
+}
+
+__device__ __forceinline__ double nan_max(double a, double b) { return (b > a || b != b) ? b : a; }
+
+// 5. T <- u (rounded to R) for every unknown, with four sums into out: [0] max |J(u) - u| and
+// [1] sum (J(u) - u)^2 for one FP64 Jacobi sweep J of u (jacobi_point, coefficients in FP64),
+// [2] max |u - T_before| and [3] sum (u - T_before)^2.  Maxima are kept as the bits of
+// non-negative doubles (ordered like unsigned integers; a NaN wins).  Neighbours outside the
+// unknowns are Dirichlet voxels of T, which nothing writes.
+template <typename R, int BOUND>
+__global__ void __launch_bounds__(256) finish_kernel(R* __restrict__ T, const R* __restrict__ Q, const double* __restrict__ u,
+                                                     const HeatArgs a, const JacobiCoef<double> k, double* __restrict__ out) {
+    const size_t plane = (size_t)a.mx * a.my, total = plane * a.nz;
+    const size_t nn = (size_t)a.n;
+    double rmax = 0.0, rsum = 0.0, cmax = 0.0, csum = 0.0;
+    for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < total; c += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(c % a.mx), j = (int)((c / a.mx) % a.my), z = (int)(c / plane);
+        const int x = a.x0 + i, y = a.y0 + j;
+        const size_t v = ((size_t)z * nn + y) * nn + x;
+        const double uc = u[c];
+        auto get = [&](int ddx, int ddy, int ddz) -> double {
+            const int ii = i + ddx, jj = j + ddy, zz = z + ddz;
+            if (ii >= 0 && ii < a.mx && jj >= 0 && jj < a.my) return u[((size_t)zz * a.my + jj) * a.mx + ii];
+            return (double)T[((size_t)zz * nn + (a.y0 + jj)) * nn + (a.x0 + ii)];
+        };
+        double w = uc;
+        jacobi_point<double, BOUND>(x, y, z, k, Q ? (double)Q[v] : 0.0, get, &w);
+        const double r = fabs(w - uc), dc = fabs(uc - (double)T[v]);
+        rmax = nan_max(rmax, r);
+        rsum += r * r;
+        cmax = nan_max(cmax, dc);
+        csum += dc * dc;
+        T[v] = (R)uc;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        rmax = nan_max(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
+        rsum += __shfl_xor_sync(0xffffffffu, rsum, o);
+        cmax = nan_max(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
+        csum += __shfl_xor_sync(0xffffffffu, csum, o);
+    }
+    __shared__ double red[4][8];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) {
+        red[0][wid] = rmax;
+        red[1][wid] = rsum;
+        red[2][wid] = cmax;
+        red[3][wid] = csum;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w2 = 1; w2 < (int)(blockDim.x >> 5); ++w2) {
+            rmax = nan_max(rmax, red[0][w2]);
+            rsum += red[1][w2];
+            cmax = nan_max(cmax, red[2][w2]);
+            csum += red[3][w2];
+        }
+        atomicMax(reinterpret_cast<unsigned long long*>(out), (unsigned long long)__double_as_longlong(rmax));
+        atomicAdd(out + 1, rsum);
+        atomicMax(reinterpret_cast<unsigned long long*>(out + 2), (unsigned long long)__double_as_longlong(cmax));
+        atomicAdd(out + 3, csum);
+    }
+}
+
+// C = A B over `batch` matrices (see dgemm_kernel); M is split into launches of at most 65535
+// row tiles.
+cudaError_t gemm(const double* A, const double* B, double* C, int M, int N, int K, int lda, int ldb, int ldc, int batch,
+                 long long sA, long long sB, long long sC, cudaStream_t s) {
+    const int max_rows = 65535 * kGemmBM;
+    for (int r0 = 0; r0 < M; r0 += max_rows) {
+        const int rows = std::min(M - r0, max_rows);
+        const dim3 grid((unsigned)((N + kGemmBN - 1) / kGemmBN), (unsigned)((rows + kGemmBM - 1) / kGemmBM), (unsigned)batch);
+        dgemm_kernel<<<grid, kGemmThreads, 0, s>>>(A + (size_t)r0 * lda, B, C + (size_t)r0 * ldc, rows, N, K, lda, ldb,
+                                                   ldc, sA, sB, sC);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+int grid_for(size_t work, int threads) {
+    return (int)std::max<size_t>(1, std::min<size_t>((work + threads - 1) / threads, (size_t)148 * 16));
+}
+
+}  // namespace
+
+HeatDirect::~HeatDirect() {
+    if (ws_) cudaFree(ws_);  // synchronous: nothing queued may still use it
+}
+
+void HeatDirect::release(cudaStream_t s) {
+    if (ws_) cudaFreeAsync(ws_, s);
+    ws_ = nullptr;
+    cap_ = 0;
+}
+
+template <typename R>
+shg_status HeatDirect::solve(const shg_params& p, R* T, const R* Q, double t_inf, cudaStream_t s) {
+    const HeatGrid g = heat_grid(p);
+    if (g.nz > 65535) return fail(SHG_ERR_UNSUPPORTED, "direct heat solve: nz = %d above 65535", g.nz);
+    const OpMats *ox = nullptr, *oy = nullptr;
+    shg_status rc;
+    if ((rc = get_op(g.ox, &ox)) != SHG_OK || (rc = get_op(g.oy, &oy)) != SHG_OK) return rc;
+    const size_t vol = (size_t)g.mx * g.my * g.nz;
+    cudaError_t e;
+    if (vol > cap_) {
+        release(s);
+        if ((e = dev_alloc((void**)&ws_, sizeof(double) * (2 * vol + 4), s)) != cudaSuccess) {
+            ws_ = nullptr;
+            return cuda_fail(e, "cudaMallocAsync");
+        }
+        cap_ = vol;
+    }
+    nt_ = (size_t)g.n * g.n * g.nz;
+    double* X = ws_;
+    double* Y = ws_ + cap_;
+    double* out = ws_ + 2 * cap_;
+    HeatArgs a;
+    a.n = g.n;
+    a.nz = g.nz;
+    a.x0 = g.x0;
+    a.y0 = g.y0;
+    a.mx = g.mx;
+    a.my = g.my;
+    a.lo_x_robin = g.ox.lo_robin;
+    a.hi_x_robin = g.ox.hi_robin;
+    a.lo_y_robin = g.oy.lo_robin;
+    a.hi_y_robin = g.oy.hi_robin;
+    a.idx2 = 1.0 / (g.dx * g.dx);
+    a.idy2 = 1.0 / (g.dy * g.dy);
+    a.idz2 = 1.0 / (g.dz * g.dz);
+    a.iK = 1.0 / p.kappa;
+    a.tinf = t_inf;
+    a.bix = g.ox.bi;
+    a.biy = g.oy.bi;
+    a.biz = g.biz;
+    shg_params pk = p;
+    pk.t_inf = t_inf;
+    const JacobiCoef<double> k = make_jacobi_coef<double>(pk);
+    const int mx = g.mx, my = g.my, nz = g.nz;
+    const long long pl = (long long)mx * my;
+    if ((e = cudaMemsetAsync(out, 0, 4 * sizeof(double), s)) != cudaSuccess) return cuda_fail(e, "memset");
+    rhs_kernel<R><<<grid_for(vol, 256), 256, 0, s>>>(T, Q, X, a);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "heat right-hand side");
+    // into mode space: along x (rows of X), then along y (one product per z plane)
+    if ((e = gemm(X, ox->FT, Y, nz * my, mx, mx, mx, mx, mx, 1, 0, 0, 0, s)) != cudaSuccess ||
+        (e = gemm(oy->F, Y, X, my, mx, my, my, mx, mx, nz, 0, pl, pl, s)) != cudaSuccess)
+        return cuda_fail(e, "heat transform");
+    thomas_kernel<<<grid_for((size_t)pl, 128), 128, 0, s>>>(X, Y, ox->lam, oy->lam, mx, my, nz, a.idz2, a.biz);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "heat tridiagonal solve");
+    // back to voxels: along y, then along x
+    if ((e = gemm(oy->G, X, Y, my, mx, my, my, mx, mx, nz, 0, pl, pl, s)) != cudaSuccess ||
+        (e = gemm(Y, ox->GT, X, nz * my, mx, mx, mx, mx, mx, 1, 0, 0, 0, s)) != cudaSuccess)
+        return cuda_fail(e, "heat transform");
+    if (p.boundary == SHG_BOUNDARY_TOP_OPEN)
+        finish_kernel<R, SHG_BOUNDARY_TOP_OPEN><<<grid_for(vol, 256), 256, 0, s>>>(T, Q, X, a, k, out);
+    else
+        finish_kernel<R, SHG_BOUNDARY_OVEN_SURROUNDED><<<grid_for(vol, 256), 256, 0, s>>>(T, Q, X, a, k, out);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "heat solution");
+    return SHG_OK;
+}
+
+shg_status HeatDirect::result(int rule, double* residual, double* change, cudaStream_t s) {
+    if (!ws_) return fail(SHG_ERR_INVALID, "no heat solve to read");
+    double h[4] = {0, 0, 0, 0};
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(h, ws_ + 2 * cap_, sizeof(h), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(s)) != cudaSuccess)
+        return cuda_fail(e, "heat solve result");
+    const double nt = (double)nt_;
+    if (residual) *residual = rule == SHG_CONV_REFERENCE ? std::sqrt(h[1]) / nt : h[0];
+    if (change) *change = rule == SHG_CONV_REFERENCE ? std::sqrt(h[3]) / nt : h[2];
+    return SHG_OK;
+}
+
+template shg_status HeatDirect::solve<float>(const shg_params&, float*, const float*, double, cudaStream_t);
+template shg_status HeatDirect::solve<double>(const shg_params&, double*, const double*, double, cudaStream_t);
+
+shg_status heat_steady_device(const shg_params& p, void* temperature, const void* q, double* residual,
+                              cudaStream_t s) {
+    HeatDirect h;
+    shg_status rc = p.precision == 32
+                        ? h.solve<float>(p, reinterpret_cast<float*>(temperature), reinterpret_cast<const float*>(q), p.t_inf, s)
+                        : h.solve<double>(p, reinterpret_cast<double*>(temperature), reinterpret_cast<const double*>(q),
+                                          p.t_inf, s);
+    double r = 0.0;
+    if (rc == SHG_OK) rc = h.result(SHG_CONV_MAXABS, &r, nullptr, s);
+    h.release(s);
+    const cudaError_t e = cudaStreamSynchronize(s);
+    if (rc == SHG_OK && e != cudaSuccess) rc = cuda_fail(e, "heat steady solve");
+    if (rc == SHG_OK && !std::isfinite(r)) rc = fail(SHG_ERR_NONFINITE, "heat steady solve: residual %g", r);
+    if (residual) *residual = r;
+    return rc;
+}
+
+}  // namespace shg
+
+extern "C" shg_status shg_heat_operator_modes(int32_t m, double d, int32_t lo_robin, int32_t hi_robin, double bi,
+                                              double* lambda_out, double* forward_out, double* inverse_out) {
+    using namespace shg;
+    clear_error();
+    if (m < 1 || m > 65536) return fail(SHG_ERR_INVALID, "m = %d must be in 1..65536", m);
+    if (!(d > 0) || !std::isfinite(d) || !(bi >= 0) || !std::isfinite(bi))
+        return fail(SHG_ERR_INVALID, "spacing must be > 0 and the Biot number >= 0, both finite");
+    if (!lambda_out || !forward_out || !inverse_out) return fail(SHG_ERR_INVALID, "output pointer is NULL");
+    Op1D op;
+    op.m = m;
+    op.d = d;
+    op.lo_robin = lo_robin ? 1 : 0;
+    op.hi_robin = hi_robin ? 1 : 0;
+    op.bi = bi;
+    std::vector<double> lam, F, G;
+    if (!op_modes(op, lam, F, G)) return fail(SHG_ERR_NOT_CONVERGED, "heat operator eigendecomposition (m = %d)", m);
+    std::memcpy(lambda_out, lam.data(), sizeof(double) * m);
+    std::memcpy(forward_out, F.data(), sizeof(double) * F.size());
+    std::memcpy(inverse_out, G.data(), sizeof(double) * G.size());
+    return SHG_OK;
+}

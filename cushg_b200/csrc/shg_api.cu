@@ -257,7 +257,7 @@ void shg_default_params(shg_params* p) {
     p->max_sweeps = 0;
     p->jacobi_block = 0;
     p->march = SHG_MARCH_AUTO;
-    p->reserved1 = 0;
+    p->heat_solver = SHG_HEAT_JACOBI;
     p->waist_y = 0.0;
     p->fp32_guard = 0.0;
 }
@@ -298,6 +298,8 @@ static shg_status check_params_impl(const shg_params* p, bool need_kernel) {
         if (p->nz < 3 || p->nx < 3) return fail(SHG_ERR_INVALID, "thermal grid needs nx, nz >= 3");
         if (p->jacobi_block < 0 || p->jacobi_block > 4)
             return fail(SHG_ERR_INVALID, "jacobi_block %d must be in 0..4", p->jacobi_block);
+        if (p->heat_solver != SHG_HEAT_JACOBI && p->heat_solver != SHG_HEAT_DIRECT)
+            return fail(SHG_ERR_INVALID, "unknown heat_solver %d", p->heat_solver);
     }
     if (p->march < SHG_MARCH_AUTO || p->march > SHG_MARCH_MULTIPASS)
         return fail(SHG_ERR_INVALID, "unknown march %d", p->march);
@@ -468,6 +470,21 @@ shg_status shg_heat_sweeps_device(const shg_params* p, void* temperature_dev, co
     if (sweeps < 0) return fail(SHG_ERR_INVALID, "sweeps must be >= 0");
     if (sweeps == 0) return SHG_OK;
     return heat_sweeps_device(q, temperature_dev, q_dev, sweeps, (cudaStream_t)stream);
+}
+
+shg_status shg_heat_steady_device(const shg_params* p, void* temperature_dev, const void* q_dev, double* residual_out,
+                                  void* stream) {
+    clear_error();
+    if (!p) return fail(SHG_ERR_INVALID, "params is NULL");
+    shg_params q = *p;
+    q.thermal = 1;
+    shg_status st = check_params_impl(&q, false);  // the heat solve needs no optical kernel
+    if (st != SHG_OK) return st;
+    if (!temperature_dev) return fail(SHG_ERR_INVALID, "temperature is NULL");
+    const uintptr_t al = (p->precision == 32 ? 4 : 8) - 1;
+    if (((uintptr_t)temperature_dev & al) || ((uintptr_t)q_dev & al))
+        return fail(SHG_ERR_INVALID, "temperature and Q must be aligned to %d bytes", (int)al + 1);
+    return heat_steady_device(q, temperature_dev, q_dev, residual_out, (cudaStream_t)stream);
 }
 
 shg_status shg_reserve_device_memory(int64_t bytes) {

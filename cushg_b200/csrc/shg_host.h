@@ -61,6 +61,8 @@ shg_status plain_solve_batch(const shg_params* params, int count, void* const* p
 // copy), the Jacobi sweeps of this outer iteration (from the previous temperature to this
 // one), the centre temperature T(NX/2, NY/2, 0), the pass index and whether it is the run's
 // last pass (the one whose fields are the outputs).
+class HeatDirect;
+
 struct ThermalState {
     const void* T;
     const void* np;
@@ -73,6 +75,9 @@ struct ThermalState {
     int pass;
     bool last;
     int index;  // the instance's position in its batch (0 for a single run)
+    // heat_solver DIRECT: the run's solver (its workspace is free between the run's solves,
+    // so a hook may solve with it in stream order); NULL for Jacobi runs
+    HeatDirect* heat;
 };
 using ThermalHook = std::function<shg_status(const ThermalState&, cudaStream_t)>;
 
@@ -89,6 +94,9 @@ shg_status thermal_solve_batch(const shg_params* ps, int count, const void* cons
                                void* const* signal_out, void* const* temperature_out, shg_stats* stats,
                                cudaStream_t stream, void* slices_p = nullptr, void* slices_s = nullptr,
                                const ThermalBatchHook* hook = nullptr);
+// shg_heat_steady_device after validation (heat_direct.cu): *residual = max |J(T) - T|
+shg_status heat_steady_device(const shg_params& p, void* temperature, const void* q, double* residual,
+                              cudaStream_t stream);
 shg_status heat_sweeps_device(const shg_params& p, void* temperature, const void* q, int64_t sweeps,
                               cudaStream_t stream);
 

@@ -51,4 +51,31 @@ template <typename R>
 cudaError_t launch_jacobi_tb(const CUtensorMap& tmT, const CUtensorMap& tmQ, R* Tf, const JacobiCoef<R>& k,
                              int boundary, int depth, unsigned* err, cudaStream_t s, TbWait w = TbWait());
 
+// The fixed point of the Jacobi sweeps for a heat source, solved directly (heat_direct.cu).
+// One object holds the FP64 workspace of one grid size; its solves run in stream order, so
+// the instances of a batch and their tangents share it.
+class HeatDirect {
+  public:
+    HeatDirect() = default;
+    HeatDirect(const HeatDirect&) = delete;
+    HeatDirect& operator=(const HeatDirect&) = delete;
+    ~HeatDirect();
+    // T (n*n*nz): Dirichlet voxels keep their values, the others receive the fixed point for
+    // heat source Q (NULL: none) and environment temperature t_inf; p gives the grid,
+    // boundary, kappa and h_conv.
+    template <typename R>
+    shg_status solve(const shg_params& p, R* T, const R* Q, double t_inf, cudaStream_t s);
+    // Of the latest solve (synchronises s): the FP64 Jacobi-sweep residual of the solution and
+    // the change from the temperature T held before, each as the `rule` measures it
+    // (SHG_CONV_REFERENCE: sqrt(sum d^2) / voxels; otherwise max |d|).
+    shg_status result(int rule, double* residual, double* change, cudaStream_t s);
+    // Frees the workspace on s (which must outlive the call).
+    void release(cudaStream_t s);
+
+  private:
+    double* ws_ = nullptr;  // two compact FP64 volumes, then the four reduction slots
+    size_t cap_ = 0;        // doubles per volume
+    size_t nt_ = 0;         // voxels of the latest solve
+};
+
 }  // namespace shg

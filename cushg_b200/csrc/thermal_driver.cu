@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <utility>
 #include <vector>
 
@@ -92,6 +93,7 @@ struct ThermalInst {
     int64_t total = 0, counter = 0;  // sweeps of the run, of the current outer iteration
     int outer = 0;
     double last = 0.0, Tc = 0.0;
+    double change = 0.0;  // heat_solver DIRECT: how far the latest solve moved T (the rule's measure)
     bool done = false;
     InstDesc d;  // descriptor of the latest optical pass
     double jacobi_ms = 0.0, optics_ms = 0.0;
@@ -211,9 +213,29 @@ shg_status ti_init(ThermalInst<R>& t, cudaStream_t s) {
 // the first sweep of every window of check_every sweeps; a value equal to the previous check
 // counts as converged; the rest of each window runs unchecked, `depth` sweeps per launch.
 // FIXED rule: exactly max_sweeps sweeps, the last one reporting max |Tf - Ti|.
+// DIRECT heat solver: the loop's fixed point in one solve, with the FP64 residual of one sweep
+// of it (t.last) and how far it moved the temperature (t.change).
 template <typename R>
-shg_status ti_jacobi(ThermalInst<R>& t, cudaStream_t s) {
+shg_status ti_direct(ThermalInst<R>& t, HeatDirect* heat, cudaStream_t s) {
     const shg_params& p = *t.p;
+    if (!heat) return fail(SHG_ERR_INVALID, "direct heat solve without a workspace");
+    shg_status rc = heat->solve<R>(p, t.cur, t.Q, p.t_inf, s);
+    if (rc != SHG_OK) return rc;
+    double resid = 0.0, change = 0.0;
+    const int rule = p.conv_rule == SHG_CONV_REFERENCE ? SHG_CONV_REFERENCE : SHG_CONV_MAXABS;
+    if ((rc = heat->result(rule, &resid, &change, s)) != SHG_OK) return rc;
+    if (!std::isfinite(resid) || !std::isfinite(change))
+        return fail(SHG_ERR_NONFINITE, "heat solve: residual %g, change %g", resid, change);
+    t.counter = 0;
+    t.last = resid;
+    t.change = change;
+    return SHG_OK;
+}
+
+template <typename R>
+shg_status ti_jacobi(ThermalInst<R>& t, HeatDirect* heat, cudaStream_t s) {
+    const shg_params& p = *t.p;
+    if (p.heat_solver == SHG_HEAT_DIRECT) return ti_direct<R>(t, heat, s);
     const size_t nt = (size_t)p.nx * p.nx * p.nz;
     cudaError_t e;
     double red = 1.0, aux = -1.0;
@@ -322,6 +344,9 @@ shg_status thermal_batch_run(const shg_params* ps, int count, const void* const*
     std::vector<ThermalState> states(count);
     std::vector<int> act(count);
     InstDesc* dd = nullptr;
+    std::unique_ptr<HeatDirect> heat;  // one FP64 workspace for the batch's direct heat solves
+    for (int i = 0; i < count; ++i)
+        if (ps[i].heat_solver == SHG_HEAT_DIRECT && !heat) heat.reset(new HeatDirect);
     shg_status rc = SHG_OK;
     cudaError_t e;
     cudaEvent_t t0 = nullptr, t1 = nullptr;
@@ -359,7 +384,7 @@ shg_status thermal_batch_run(const shg_params* ps, int count, const void* const*
             for (int a = 0; a < na && rc == SHG_OK; ++a) {
                 ThermalInst<R>& t = ti[act[a]];
                 cudaEventRecord(ej[0], s);
-                if ((rc = ti_jacobi<R>(t, s)) != SHG_OK) break;
+                if ((rc = ti_jacobi<R>(t, heat.get(), s)) != SHG_OK) break;
                 cudaEventRecord(ej[1], s);
                 if ((e = cudaEventSynchronize(ej[1])) != cudaSuccess) { rc = cuda_fail(e, "jacobi"); break; }
                 float ms = 0.f;
@@ -386,9 +411,11 @@ shg_status thermal_batch_run(const shg_params* ps, int count, const void* const*
                 ThermalInst<R>& t = ti[act[a]];
                 ++t.outer;
                 t.optics_ms += ms;
-                // Solver.h:367: the last pass is the one whose Jacobi loop converged at its first sweep
-                t.done = t.outer == t.max_outer || (t.p->conv_rule != SHG_CONV_FIXED && t.counter == 1 && g != 0);
-                states[a] = {t.cur, t.NP, t.NS, t.DK, &hd[a], dd + a, t.counter, t.Tc, g, t.done, act[a]};
+                // Solver.h:367: the last pass is the one whose Jacobi loop converged at its first
+                // sweep; with the direct solver, the one whose solve moved T by less than tol
+                const bool settled = t.p->heat_solver == SHG_HEAT_DIRECT ? t.change < t.tol : t.counter == 1;
+                t.done = t.outer == t.max_outer || (t.p->conv_rule != SHG_CONV_FIXED && settled && g != 0);
+                states[a] = {t.cur, t.NP, t.NS, t.DK, &hd[a], dd + a, t.counter, t.Tc, g, t.done, act[a], heat.get()};
             }
             if (hook && (rc = (*hook)(states.data(), na, s)) != SHG_OK) break;
         }
@@ -430,6 +457,7 @@ shg_status thermal_batch_run(const shg_params* ps, int count, const void* const*
         }
     } while (0);
     cudaStreamSynchronize(s);  // the graphs' launches are done before their release
+    if (heat) heat->release(s);
     for (auto& t : ti) {
         ti_release<R>(t);
         if (t.buf) cudaFreeAsync(t.buf, s);

@@ -21,6 +21,8 @@
 //      of the fields on the temperature (absorbed power changes with the phase matching) is
 //      carried through every outer iteration: the result is the derivative of the whole
 //      computed procedure, for its sweep counts.
+//   With heat_solver DIRECT each outer iteration's temperature is the exact solution of the
+//   sweep's linear system, so step 1 is that solve applied to u's sources instead of sweeps.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -120,8 +122,15 @@ class ThermalTangent {
         shg_params q = p_;
         q.t_inf = 0.0;
         shg_status rc;
-        if (st.sweeps > 0 && (rc = heat_sweeps_device(q, u_, st.pass > 0 ? q_ : nullptr, st.sweeps, s)) != SHG_OK)
+        if (p_.heat_solver == SHG_HEAT_DIRECT) {
+            // the direct solve is linear in (Q, faces, T_inf): its tangent is the same solve of
+            // the tangent source with faces at 1 (u's initial value there) and T_inf = 0
+            if (!st.heat) return fail(SHG_ERR_INVALID, "direct heat tangent without a workspace");
+            if ((rc = st.heat->solve<R>(q, u_, st.pass > 0 ? q_ : nullptr, 0.0, s)) != SHG_OK) return rc;
+        } else if (st.sweeps > 0 &&
+                   (rc = heat_sweeps_device(q, u_, st.pass > 0 ? q_ : nullptr, st.sweeps, s)) != SHG_OK) {
             return rc;
+        }
         // 2. per-voxel tangents of the optics
         if ((e = launch_optics_tangent<R>(reinterpret_cast<const R*>(st.T), u_, ddk_, dnp_, dns_, p_, s)) != cudaSuccess)
             return cuda_fail(e, "optics tangent");

@@ -28,6 +28,8 @@ SHG_BOUNDARY_OVEN_SURROUNDED = 1
 SHG_CONV_REFERENCE = 0
 SHG_CONV_MAXABS = 1
 SHG_CONV_FIXED = 2
+SHG_HEAT_JACOBI = 0
+SHG_HEAT_DIRECT = 1
 SHG_MARCH_AUTO = 0
 SHG_MARCH_FUSED = 1
 SHG_MARCH_MULTIPASS = 2
@@ -57,7 +59,7 @@ class ShgParams(ctypes.Structure):
         ("conv_rule", ctypes.c_int32), ("crystal", ctypes.c_int32),
         ("jacobi_tol", ctypes.c_double), ("max_sweeps", ctypes.c_int64),
         ("jacobi_block", ctypes.c_int32), ("march", ctypes.c_int32),
-        ("reserved1", ctypes.c_int32), ("waist_y", ctypes.c_double),
+        ("heat_solver", ctypes.c_int32), ("waist_y", ctypes.c_double),
         ("fp32_guard", ctypes.c_double),
     ]
 

@@ -29,7 +29,7 @@ EXPORTS = (
     "shg_batch_plan_powers", "shg_batch_plan_destroy", "shg_autotune", "shg_grad_batch", "shg_solve_batch",
     "shg_thermal_grad", "shg_autotune_batch", "shg_autotune_reset", "shg_set_schedule",
     "shg_reserve_device_memory", "shg_fp32_error_estimate", "shg_selftest_bounded_wait",
-    "shg_thermal_batch",
+    "shg_thermal_batch", "shg_heat_steady_device", "shg_heat_operator_modes",
 )
 
 
@@ -113,6 +113,11 @@ def lib() -> ctypes.CDLL:
         L.shg_sh_power.restype = ctypes.c_int
         L.shg_heat_sweeps_device.argtypes = [P, vp, vp, ctypes.c_int64, vp]
         L.shg_heat_sweeps_device.restype = ctypes.c_int
+        L.shg_heat_steady_device.argtypes = [P, vp, vp, ctypes.POINTER(ctypes.c_double), vp]
+        L.shg_heat_steady_device.restype = ctypes.c_int
+        L.shg_heat_operator_modes.argtypes = [ctypes.c_int32, ctypes.c_double, ctypes.c_int32, ctypes.c_int32,
+                                              ctypes.c_double] + [ctypes.POINTER(ctypes.c_double)] * 3
+        L.shg_heat_operator_modes.restype = ctypes.c_int
         L.shg_batch_plan_create.argtypes = [P, ctypes.c_int32, ctypes.POINTER(vp), ctypes.POINTER(vp),
                                             ctypes.POINTER(vp)]
         L.shg_batch_plan_create.restype = ctypes.c_int
@@ -257,6 +262,32 @@ def heat_sweeps_device(p: ShgParams, temperature, q, sweeps: int, stream=None) -
     s = None if stream is None else ctypes.c_void_p(stream)
     _check(lib().shg_heat_sweeps_device(ctypes.byref(p), ctypes.c_void_p(temperature.data_ptr()),
                                         ctypes.c_void_p(q.data_ptr()), int(sweeps), s))
+
+
+def heat_steady_device(p: ShgParams, temperature, q=None, stream=None) -> float:
+    """The temperature the Jacobi sweeps converge to, in place on a device tensor
+    (shg_heat_steady_device): temperature and q are contiguous real tensors of shape
+    (nz, ny, nx) in the precision of p (q None: no heat source); the Dirichlet voxels of
+    temperature keep their values.  Returns max |J(T) - T| of one FP64 Jacobi sweep J of the
+    FP64 solution."""
+    s = None if stream is None else ctypes.c_void_p(stream)
+    r = ctypes.c_double(0.0)
+    qp = ctypes.c_void_p(q.data_ptr()) if q is not None else None
+    _check(lib().shg_heat_steady_device(ctypes.byref(p), ctypes.c_void_p(temperature.data_ptr()), qp,
+                                        ctypes.byref(r), s))
+    return r.value
+
+
+def heat_operator_modes(m: int, d: float, lo_robin: bool, hi_robin: bool, bi: float):
+    """Eigenvalues, forward and inverse transforms (m x m) of one direction's operator of the
+    direct heat solve (shg_heat_operator_modes; host only)."""
+    lam = np.zeros(m)
+    F = np.zeros((m, m))
+    G = np.zeros((m, m))
+    dp = ctypes.POINTER(ctypes.c_double)
+    _check(lib().shg_heat_operator_modes(int(m), float(d), int(bool(lo_robin)), int(bool(hi_robin)), float(bi),
+                                         lam.ctypes.data_as(dp), F.ctypes.data_as(dp), G.ctypes.data_as(dp)))
+    return lam, F, G
 
 
 def _host_ptr(a):

@@ -119,7 +119,10 @@ typedef struct shg_params {
      * one is built for the grid side (planes in shared memory, sides <= 256) and the
      * multi-pass march otherwise (planes in global memory, side 512). */
     int32_t march;
-    int32_t reserved1;      /* zero */
+    /* How each outer iteration of a thermal run solves the heat equation (SHG_HEAT_*):
+     * Jacobi sweeps as the reference runs them (default), or the sweeps' fixed point computed
+     * directly.  No counterpart in the reference. */
+    int32_t heat_solver;
     /* Beam waist radius in y [µm].  <= 0 (default): a round beam of radius `waist`, setPump
      * as the reference runs it (Efields.h:94, waistY = waistX).  Otherwise the elliptical beam
      * of the reference's commented-out variant (Efields.h:113-115), with its own Rayleigh
@@ -137,8 +140,22 @@ typedef struct shg_params {
     double fp32_guard;
 } shg_params;
 
+/* Heat solvers of a thermal run. */
 enum {
-    SHG_MARCH_AUTO = 0,      /* fused where built (the autotuner's choice if it ran), else multi-pass */
+    SHG_HEAT_JACOBI = 0, /* Jacobi sweeps under conv_rule (Solver.h:335-355); bit-identical to the
+                            reference */
+    SHG_HEAT_DIRECT = 1  /* the temperature the sweeps converge to, solved directly for every
+                            outer iteration (shg_heat_steady_device), in FP64.  jacobi_block,
+                            check_every and max_sweeps are ignored; jacobi_sweeps reports 0;
+                            last_residual is the conv_rule value (max |ΔT| for MAXABS and
+                            FIXED) of one FP64 Jacobi sweep applied to the solution.  The outer
+                            loop stops after max_outer iterations, or (conv_rule REFERENCE or
+                            MAXABS) after the first iteration g > 0 whose solution moved by less
+                            than the Jacobi tolerance, by the rule's own measure. */
+};
+
+enum {
+    SHG_MARCH_AUTO = 0,     /* fused where built (the autotuner's choice if it ran), else multi-pass */
     SHG_MARCH_FUSED = 1,     /* one thread-block cluster per instance, fields in shared memory */
     SHG_MARCH_MULTIPASS = 2  /* fields in global memory, a row and a column launch per step */
 };
@@ -339,6 +356,39 @@ SHG_API shg_status shg_solve_batch_device_noalloc(const shg_params* params, int3
  */
 SHG_API shg_status shg_heat_sweeps_device(const shg_params* p, void* temperature_dev, const void* q_dev,
                                           int64_t sweeps, void* stream);
+
+/*
+ * The temperature that shg_heat_sweeps_device's sweeps converge to, computed directly: the
+ * fixed point T = J(T) of one Jacobi sweep J for the heat source Q.  No counterpart in the
+ * reference, whose Jacobi loop (Solver.h:339-355) approaches it one sweep at a time.
+ * With the faces' coefficients of Tfield.h:93-240 scaled to a common form the sweep's linear
+ * system is the sum of three one-dimensional operators (Robin, or next to a Dirichlet face,
+ * at each end); the solve diagonalises the x and y operators (FP64 transforms cached per
+ * device and operator) and solves a tridiagonal system along z for every (x, y) mode.
+ *   temperature_dev  nx*ny*nz reals: the Dirichlet voxels hold their values on entry and keep
+ *                    them; every other voxel receives the solution (rounded to the precision).
+ *   q_dev            nx*ny*nz reals: the heat source Q, or NULL for none.
+ *   residual_out     optional: max |J(T) - T| of one FP64 Jacobi sweep applied to the FP64
+ *                    solution (the sweep's own measure of how far T is from its fixed point).
+ * Uses the grid, precision, kappa, h_conv, t_inf and boundary of *p.  Works in FP64 with two
+ * workspace buffers of nx*ny*nz doubles from the stream's pool.  Stream-ordered on `stream`;
+ * synchronises once at the end.
+ */
+SHG_API shg_status shg_heat_steady_device(const shg_params* p, void* temperature_dev, const void* q_dev,
+                                          double* residual_out, void* stream);
+
+/*
+ * The one-dimensional operator of the direct heat solve for one grid direction, and its
+ * eigendecomposition (host only; no device needed).  m unknowns at spacing d; each end is
+ * next to a Dirichlet voxel (robin = 0) or a Robin face with Biot number bi (robin = 1).  In the
+ * scaled form each row reads (2u_i - u_{i-1} - u_{i+1}) / d^2, and a Robin end row
+ * (2(1 + bi) u_0 - 2 u_1) / d^2.  On return lambda_out[k] (m) are its eigenvalues,
+ * forward_out (m x m, row-major, row k) maps values to mode amplitudes and inverse_out
+ * (m x m, row-major, row i) maps them back: M = inverse * diag(lambda) * forward and
+ * forward * inverse = I.
+ */
+SHG_API shg_status shg_heat_operator_modes(int32_t m, double d, int32_t lo_robin, int32_t hi_robin, double bi,
+                                           double* lambda_out, double* forward_out, double* inverse_out);
 
 /*
  * A batch of thermal runs: the -DTHERMAL outer loop of Solver::run (Solver.h:321-373) for each

@@ -532,7 +532,7 @@ def run_thermal(args) -> dict:
     if args.thermal_max_sweeps:
         p = p.replace(max_sweeps=args.thermal_max_sweeps)
     direct = args.heat_solver == "direct"
-    p = p.replace(jacobi_block=args.jacobi_block, precision=args.thermal_precision,
+    p = p.replace(jacobi_block=args.jacobi_block, precision=args.thermal_precision or 64,
                   heat_solver=P.SHG_HEAT_DIRECT if direct else P.SHG_HEAT_JACOBI)
     cdt = torch.complex128 if p.precision == 64 else torch.complex64
     if direct:  # operator transforms (computed once per process) and kernels before timing
@@ -675,6 +675,69 @@ def run_thermal_batch(args) -> dict:
             "clocks": clk.summary()}
 
 
+def run_heat_direct(args) -> dict:
+    """Direct heat-solve workload (outside the default sweep line): shg_heat_steady_device on
+    the large thermal batch's grid (512 x 512 x 1000, FP32 storage, FP64 solve, top-open
+    boundary; --thermal-side / --thermal-nz / --thermal-precision change it) with a random heat
+    source, timed with CUDA events on the launching stream.  Its four transform GEMMs carry
+    2 (mx + my) 2 mx my nz FP64 flops; for scale, cuBLAS's FP64 matmul (torch.matmul) is timed
+    on the x-transform's shape, the same flops in one call."""
+    import torch
+    from cushg_b200 import shg
+
+    p = P.config_thermal_512(1)[0]
+    if args.thermal_side:
+        p = p.replace(nx=args.thermal_side, ny=args.thermal_side)
+    if args.thermal_nz:
+        p = p.replace(nz=args.thermal_nz)
+    p = p.replace(precision=args.thermal_precision or 32)
+    n, nz = p.nx, p.nz
+    tdt = torch.float64 if p.precision == 64 else torch.float32
+    g = torch.Generator(device="cuda").manual_seed(0)
+    Q = (torch.rand((nz, n, n), dtype=torch.float64, device="cuda", generator=g) * (60.0 * p.kappa / p.lx ** 2)).to(tdt)
+    T0 = torch.full((nz, n, n), p.temp, dtype=tdt, device="cuda")
+    T0[:, 0, :] = p.t_peltier  # top-open: the y = 0 face at the oven temperature
+    T = T0.clone()
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+    for _ in range(max(1, args.warmup)):
+        T.copy_(T0)
+        resid = shg.heat_steady_device(p, T, Q, stream=sptr)
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(0) as clk:
+        for a, b in evs:
+            a.record(stream)
+            shg.heat_steady_device(p, T, Q, stream=sptr)
+            b.record(stream)
+        torch.cuda.synchronize()
+    ms = statistics.median(x.elapsed_time(y) for x, y in evs)
+    mx, my = n, n - 1
+    flops = 2.0 * (mx + my) * 2.0 * mx * my * nz
+    # cuBLAS FP64 on the x-transform's shape (nz*my x mx) @ (mx x mx), scaled to all four GEMMs
+    A = torch.rand((nz * my, mx), dtype=torch.float64, device="cuda", generator=g)
+    B = torch.rand((mx, mx), dtype=torch.float64, device="cuda", generator=g)
+    for _ in range(3):
+        C = A @ B
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(5):
+        C = A @ B
+    e1.record(stream)
+    torch.cuda.synchronize()
+    cublas_tflops = 5 * 2.0 * A.shape[0] * mx * mx / (e0.elapsed_time(e1) * 1e-3) / 1e12
+    del A, B, C
+    return {"metric": "direct heat solve time", "value": ms, "unit": "ms", "higher_is_better": False,
+            "workload": f"shg_heat_steady_device {n}x{n}x{nz} FP{p.precision} storage, FP64 solve",
+            "residual_max_dT_K": resid, "gemm_tflop_per_solve": flops / 1e12,
+            "gemm_tflops_if_all_time": flops / (ms * 1e-3) / 1e12,
+            "cublas_fp64_matmul_tflops_same_shape": cublas_tflops,
+            "note": "gemm_tflops_if_all_time divides the transform flops by the whole solve's time "
+                    "(right-hand side, tridiagonal pass and finish included)",
+            "clocks": clk.summary()}
+
+
 def run_jacobi(args) -> dict:
     """Heat-solve workload (outside the default sweep line): `--jacobi-sweeps` Jacobi sweeps
     of the heat equation per step through shg_heat_sweeps_device on the thermal grid (default
@@ -688,7 +751,7 @@ def run_jacobi(args) -> dict:
         p = p.replace(nx=args.thermal_side, ny=args.thermal_side)
     if args.thermal_nz:
         p = p.replace(nz=args.thermal_nz)
-    p = p.replace(jacobi_block=args.jacobi_block, precision=args.thermal_precision)
+    p = p.replace(jacobi_block=args.jacobi_block, precision=args.thermal_precision or 64)
     tdt = torch.float64 if p.precision == 64 else torch.float32
     vox = p.nx * p.ny * p.nz
     T = torch.full((p.nz, p.ny, p.nx), 40.0, dtype=tdt, device="cuda")
@@ -754,7 +817,8 @@ def main() -> int:
     ap.add_argument("--class-nz", type=int, default=24)
     ap.add_argument("--class-schedule", default="",
                     help="with --class-side: the compiled split to use, as CLUSTER,THREADS (shg_set_schedule)")
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "thermal", "adjoint", "jacobi", "thermal-batch"])
+    ap.add_argument("--workload", default="sweep",
+                    choices=["sweep", "thermal", "adjoint", "jacobi", "thermal-batch", "heat-direct"])
     ap.add_argument("--thermal-count", type=int, default=8)
     ap.add_argument("--thermal-fixed-sweeps", type=int, default=200)
     ap.add_argument("--thermal-outer", type=int, default=2)
@@ -771,7 +835,8 @@ def main() -> int:
     ap.add_argument("--adjoint-nz", type=int, default=0, help="adjoint workload with this nz (profiling case)")
     ap.add_argument("--adjoint-batch", type=int, default=18, help="instances of the batched gradient")
     ap.add_argument("--thermal-max-sweeps", type=int, default=0)
-    ap.add_argument("--thermal-precision", type=int, default=64, choices=[32, 64])
+    ap.add_argument("--thermal-precision", type=int, default=None, choices=[32, 64],
+                    help="thermal, jacobi: default 64; heat-direct: default 32")
     ap.add_argument("--jacobi-block", type=int, default=0, help="sweeps per launch (0 = automatic)")
     ap.add_argument("--heat-solver", default="jacobi", choices=["jacobi", "direct"],
                     help="thermal workloads: Jacobi sweeps as the reference runs them, or their fixed point "
@@ -789,6 +854,8 @@ def main() -> int:
         out = run_jacobi(args) if rank == 0 else None
     elif args.workload == "thermal-batch":
         out = run_thermal_batch(args) if rank == 0 else None
+    elif args.workload == "heat-direct":
+        out = run_heat_direct(args) if rank == 0 else None
     elif args.impl == "reference":
         out = run_reference(args, rank, world)
     else:

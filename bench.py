@@ -692,6 +692,10 @@ def run_heat_direct(args) -> dict:
         p = p.replace(nz=args.thermal_nz)
     p = p.replace(precision=args.thermal_precision or 32)
     n, nz = p.nx, p.nz
+    # the solve's two FP64 volumes stay in the library's pool from call to call
+    work = 2 * 8 * n * n * nz + (64 << 20)
+    os.environ.setdefault("SHG_POOL_KEEP_MB", str((work >> 20) + 1024))
+    shg.reserve_device_memory(work)
     tdt = torch.float64 if p.precision == 64 else torch.float32
     g = torch.Generator(device="cuda").manual_seed(0)
     Q = (torch.rand((nz, n, n), dtype=torch.float64, device="cuda", generator=g) * (60.0 * p.kappa / p.lx ** 2)).to(tdt)

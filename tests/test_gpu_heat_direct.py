@@ -7,7 +7,10 @@
   reference), max |J(T) - T| <= 1e-10 K, and the FP64 residual the solve reports agrees.
 * A thermal run with the direct solver equals the Jacobi thermal run converged to 1e-12 K
   (fields relative L2 <= 1e-8, T <= 1e-7 K), and its dJ/dT_oven equals central finite
-  differences of direct runs to 1e-6 relative."""
+  differences of direct runs to 1e-5 relative (measured 1.0e-7 at sides 256 and 512).
+* The FP32 thermal path (FP32 fields, FP64 heat solve), which the large 512 x 512 x 1000 batch
+  runs, against FP64 runs with the same solver: at one full-size instance of that batch,
+  T <= 2e-5 K, SH field relative L2 <= 5e-5 and SH power <= 2e-5."""
 import os
 
 import numpy as np
@@ -142,9 +145,10 @@ def test_thermal_fp32_direct_against_fp64_direct():
     """The FP32 thermal path with the FP64 heat solve against the FP64 run with the same
     solver: the temperature differs by the FP32 optics' effect on Q and the final rounding."""
     dT, sig, pw = fp32_vs_fp64(thermal_case(P.SHG_HEAT_DIRECT))
+    # measured: 1.2e-5 K, 3.1e-6, 7.3e-7
     assert dT <= 1e-4
-    assert sig <= 1e-4
-    assert pw <= 1e-4
+    assert sig <= 3e-5
+    assert pw <= 1e-5
 
 
 def test_large_thermal_instance_fp32_against_fp64():
@@ -153,9 +157,10 @@ def test_large_thermal_instance_fp32_against_fp64():
     against FP64 fields, both with the direct heat solve."""
     p = P.config_thermal_512(1)[0].replace(heat_solver=P.SHG_HEAT_DIRECT)
     dT, sig, pw = fp32_vs_fp64(p)
-    assert dT <= 1e-3
-    assert sig <= 1e-3
-    assert pw <= 1e-4
+    # measured: 2.2e-6 K, 5.7e-6, 3.8e-6
+    assert dT <= 2e-5
+    assert sig <= 5e-5
+    assert pw <= 2e-5
 
 
 def test_configuration_2_direct_against_reference_jacobi():
@@ -175,4 +180,5 @@ def test_configuration_2_direct_against_reference_jacobi():
           f"FP64 sweep residual {r.stats.last_residual:.3g} K")
     assert r.stats.jacobi_sweeps == 0
     assert r.stats.last_residual < 1e-9
+    # measured: 8.45e-3 K of a 0.322 K span
     assert dT < 0.05 * span

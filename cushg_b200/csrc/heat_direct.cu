@@ -158,10 +158,13 @@ bool op_modes(const Op1D& op, std::vector<double>& lam, std::vector<double>& F, 
     return true;
 }
 
-// Device copies of one operator's transforms: F and G row-major, their transposes, lambda.
+// Device copies of one operator's transforms: F and G row-major, their transposes, lambda.  The
+// matrices' rows are ld = m rounded up to even doubles (zero-padded), so that every row starts
+// on 16 bytes for the GEMM's copies.
 struct OpMats {
     Op1D op;
     int dev = -1;
+    int ld = 0;
     double *F = nullptr, *G = nullptr, *FT = nullptr, *GT = nullptr, *lam = nullptr;
 };
 
@@ -183,13 +186,15 @@ shg_status get_op(const Op1D& op, const OpMats** out) {
         }
     std::vector<double> lam, F, G;
     if (!op_modes(op, lam, F, G)) return fail(SHG_ERR_NOT_CONVERGED, "heat operator eigendecomposition (m = %d)", op.m);
-    const int m = op.m;
-    const size_t mm = (size_t)m * m;
-    std::vector<double> FT(mm), GT(mm);
+    const int m = op.m, ld = m + (m & 1);
+    const size_t mm = (size_t)m * ld;
+    std::vector<double> Fp(mm, 0.0), Gp(mm, 0.0), FT(mm, 0.0), GT(mm, 0.0);
     for (int i = 0; i < m; ++i)
         for (int k = 0; k < m; ++k) {
-            FT[(size_t)i * m + k] = F[(size_t)k * m + i];
-            GT[(size_t)k * m + i] = G[(size_t)i * m + k];
+            Fp[(size_t)k * ld + i] = F[(size_t)k * m + i];
+            Gp[(size_t)i * ld + k] = G[(size_t)i * m + k];
+            FT[(size_t)i * ld + k] = F[(size_t)k * m + i];
+            GT[(size_t)k * ld + i] = G[(size_t)i * m + k];
         }
     if (g_ops.size() >= kMaxCachedOps) return fail(SHG_ERR_UNSUPPORTED, "more than %d heat operators cached", (int)kMaxCachedOps);
     double* buf = nullptr;
@@ -197,12 +202,13 @@ shg_status get_op(const Op1D& op, const OpMats** out) {
     OpMats* c = new OpMats;
     c->op = op;
     c->dev = dev;
+    c->ld = ld;
     c->F = buf;
     c->G = buf + mm;
     c->FT = buf + 2 * mm;
     c->GT = buf + 3 * mm;
     c->lam = buf + 4 * mm;
-    const double* src[5] = {F.data(), G.data(), FT.data(), GT.data(), lam.data()};
+    const double* src[5] = {Fp.data(), Gp.data(), FT.data(), GT.data(), lam.data()};
     double* dst[5] = {c->F, c->G, c->FT, c->GT, c->lam};
     for (int k = 0; k < 5 && e == cudaSuccess; ++k)
         e = cudaMemcpy(dst[k], src[k], sizeof(double) * (k == 4 ? (size_t)m : mm), cudaMemcpyHostToDevice);
@@ -279,90 +285,97 @@ __global__ void rhs_kernel(const R* __restrict__ T, const R* __restrict__ Q, dou
     }
 }
 
-constexpr int kGemmBM = 128, kGemmBN = 64, kGemmBK = 8, kGemmThreads = 256;
+constexpr int kGemmBM = 128, kGemmBN = 128, kGemmBK = 16, kGemmThreads = 256, kGemmStages = 3;
+constexpr int kGemmALd = kGemmBK + 2;  // A tile row pitch: 144 B (16-byte rows, adjacent rows 4 banks apart)
+constexpr int kGemmStageDoubles = kGemmBM * kGemmALd + kGemmBK * kGemmBN;
+constexpr size_t kGemmSmem = sizeof(double) * kGemmStageDoubles * kGemmStages;
+
+// 16 bytes from global to shared memory, asynchronously; the bytes past `valid` (0..16) are
+// zero-filled and not read.
+__device__ __forceinline__ void cp_async16(double* dst, const double* src, int valid) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(valid) : "memory");
+}
 
 // 2, 4. C[b] = A[b] B[b] in FP64 for row-major A (M x K, lda), B (K x N, ldb) and C (M x N, ldc),
-// batch b = blockIdx.z at element strides sA, sB, sC.  A 128 x 64 tile per block, an 8 x 4
-// block of it per thread in registers; the A and B tiles pass through shared memory, double
-// buffered (the next tile's loads are in flight during the current tile's products).  Each
-// output is one FMA chain over k in order.
-__global__ void __launch_bounds__(kGemmThreads, 2) dgemm_kernel(const double* __restrict__ A, const double* __restrict__ B,
+// batch b = blockIdx.z at element strides sA, sB, sC.  lda, ldb, the strides and the three base
+// addresses are even (16-byte rows).  A 128 x 128 tile per block; thread (tx, ty) accumulates
+// rows ty + 16 r and columns tx + 16 c (r, c < 8) in registers, so that a warp's reads of the
+// A tile are two broadcast rows and of the B tile 16 consecutive doubles.  The tiles stream
+// through a three-stage ring of cp.async copies (zero-filled past M, N and K).  Each output is
+// one FMA chain over k in order.
+__global__ void __launch_bounds__(kGemmThreads, 1) dgemm_kernel(const double* __restrict__ A, const double* __restrict__ B,
                                                              double* __restrict__ C, int M, int N, int K, int lda,
                                                              int ldb, int ldc, long long sA, long long sB, long long sC) {
-    __shared__ __align__(16) double As[2][kGemmBK][kGemmBM];
-    __shared__ __align__(16) double Bs[2][kGemmBK][kGemmBN];
+    extern __shared__ __align__(16) double gsm[];
     A += blockIdx.z * sA;
     B += blockIdx.z * sB;
     C += blockIdx.z * sC;
     const int m0 = blockIdx.y * kGemmBM, n0 = blockIdx.x * kGemmBN;
     const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-    const int ar = tid >> 1, ac = (tid & 1) * 4;   // loads: A row ar, columns ac..ac+3 of the tile
-    const int bk = tid >> 5, bn = (tid & 31) * 2;  // B row bk, columns bn, bn+1
-    double ra[4], rb[2];
-    auto load = [&](int k0) {
-        const int row = m0 + ar;
+    // tile t into stage st: A 128 x 16 and B 16 x 128, each 1024 chunks of 16 bytes, 4 per thread
+    auto load = [&](int t, int st) {
+        double* As = gsm + st * kGemmStageDoubles;
+        double* Bs = As + kGemmBM * kGemmALd;
+        const int k0 = t * kGemmBK;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int col = k0 + ac + q;
-            ra[q] = (row < M && col < K) ? A[(size_t)row * lda + col] : 0.0;
+        for (int j = 0; j < 4; ++j) {
+            const int c = tid + j * kGemmThreads;
+            const int row = c >> 3, col = (c & 7) * 2;
+            const int gr = m0 + row, gc = k0 + col;
+            const int valid = gr < M ? 8 * max(0, min(2, K - gc)) : 0;
+            cp_async16(As + row * kGemmALd + col, valid ? A + (size_t)gr * lda + gc : A, valid);
         }
-        const int krow = k0 + bk;
 #pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            const int col = n0 + bn + q;
-            rb[q] = (krow < K && col < N) ? B[(size_t)krow * ldb + col] : 0.0;
+        for (int j = 0; j < 4; ++j) {
+            const int c = tid + j * kGemmThreads;
+            const int row = c >> 6, col = (c & 63) * 2;
+            const int gr = k0 + row, gc = n0 + col;
+            const int valid = gr < K ? 8 * max(0, min(2, N - gc)) : 0;
+            cp_async16(Bs + row * kGemmBN + col, valid ? B + (size_t)gr * ldb + gc : B, valid);
         }
     };
-    auto stash = [&](int buf) {
-#pragma unroll
-        for (int q = 0; q < 4; ++q) As[buf][ac + q][ar] = ra[q];
-        Bs[buf][bk][bn] = rb[0];
-        Bs[buf][bk][bn + 1] = rb[1];
-    };
-    double acc[8][4];
+    double acc[8][8];
 #pragma unroll
     for (int r = 0; r < 8; ++r)
 #pragma unroll
-        for (int c = 0; c < 4; ++c) acc[r][c] = 0.0;
-    load(0);
-    stash(0);
-    __syncthreads();
+        for (int c = 0; c < 8; ++c) acc[r][c] = 0.0;
     const int tiles = (K + kGemmBK - 1) / kGemmBK;
+#pragma unroll
+    for (int st = 0; st < kGemmStages - 1; ++st) {
+        if (st < tiles) load(st, st);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    }
     for (int t = 0; t < tiles; ++t) {
-        const int buf = t & 1;
-        if (t + 1 < tiles) load((t + 1) * kGemmBK);
+        // this thread's copies of tile t have landed; the barrier makes everyone's visible and
+        // ends every read of the stage the next load overwrites (tile t - 1's)
+        asm volatile("cp.async.wait_group %0;" ::"n"(kGemmStages - 2) : "memory");
+        __syncthreads();
+        if (t + kGemmStages - 1 < tiles) load(t + kGemmStages - 1, (t + kGemmStages - 1) % kGemmStages);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        const double* As = gsm + (t % kGemmStages) * kGemmStageDoubles;
+        const double* Bs = As + kGemmBM * kGemmALd;
 #pragma unroll
         for (int kk = 0; kk < kGemmBK; ++kk) {
-            double av[8], bv[4];
-            const double2* ap = reinterpret_cast<const double2*>(&As[buf][kk][ty * 8]);
-            const double2* bp = reinterpret_cast<const double2*>(&Bs[buf][kk][tx * 4]);
+            double av[8], bv[8];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const double2 w = ap[q];
-                av[2 * q] = w.x;
-                av[2 * q + 1] = w.y;
-            }
+            for (int r = 0; r < 8; ++r) av[r] = As[(ty + 16 * r) * kGemmALd + kk];
 #pragma unroll
-            for (int q = 0; q < 2; ++q) {
-                const double2 w = bp[q];
-                bv[2 * q] = w.x;
-                bv[2 * q + 1] = w.y;
-            }
+            for (int c = 0; c < 8; ++c) bv[c] = Bs[kk * kGemmBN + tx + 16 * c];
 #pragma unroll
             for (int r = 0; r < 8; ++r)
 #pragma unroll
-                for (int c = 0; c < 4; ++c) acc[r][c] = fma(av[r], bv[c], acc[r][c]);
+                for (int c = 0; c < 8; ++c) acc[r][c] = fma(av[r], bv[c], acc[r][c]);
         }
-        if (t + 1 < tiles) stash(buf ^ 1);  // the other buffer was last read before the previous barrier
-        __syncthreads();
     }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
-        const int row = m0 + ty * 8 + r;
+        const int row = m0 + ty + 16 * r;
         if (row >= M) break;
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            const int col = n0 + tx * 4 + c;
+        for (int c = 0; c < 8; ++c) {
+            const int col = n0 + tx + 16 * c;
             if (col < N) C[(size_t)row * ldc + col] = acc[r][c];
         }
     }
@@ -371,7 +384,10 @@ __global__ void __launch_bounds__(kGemmThreads, 2) dgemm_kernel(const double* __
 // 3. For every mode t = j * mx + i: (Az + lambda_x[i] + lambda_y[j]) u = f along z, Thomas
 // elimination (the system is diagonally dominant: lambda_x + lambda_y > 0 whenever a direction
 // has a Dirichlet end or a Robin end with Bi > 0, which every boundary model has).  f and then
-// u in v; the eliminated upper diagonal in cp.
+// u in v; the eliminated upper diagonal in cp.  Both sweeps load kThomasChunk planes ahead of
+// the dependent recurrence, so each thread keeps that many loads in flight.
+constexpr int kThomasChunk = 4;
+
 __global__ void thomas_kernel(double* __restrict__ v, double* __restrict__ cp, const double* __restrict__ lx,
                               const double* __restrict__ ly, int mx, int my, int nz, double idz2, double biz) {
     const size_t plane = (size_t)mx * my;
@@ -379,25 +395,45 @@ __global__ void thomas_kernel(double* __restrict__ v, double* __restrict__ cp, c
         const double lam = lx[t % mx] + ly[t / mx];
         const double a_end = 2.0 * (1.0 + biz) * idz2 + lam;  // Robin rows z = 0, nz - 1
         const double a_in = 2.0 * idz2 + lam;
-        double c = -2.0 * idz2 / a_end;
-        double d = v[t] / a_end;
-        cp[t] = c;
-        v[t] = d;
-        for (int z = 1; z < nz; ++z) {
-            const size_t o = (size_t)z * plane + t;
-            const bool last = z == nz - 1;
-            const double lo = last ? -2.0 * idz2 : -idz2;
-            const double den = (last ? a_end : a_in) - lo * c;
-            c = last ? 0.0 : -idz2 / den;
-            d = (v[o] - lo * d) / den;
-            cp[o] = c;
-            v[o] = d;
+        double c = 0.0, d = 0.0;
+        for (int z0 = 0; z0 < nz; z0 += kThomasChunk) {
+            double f[kThomasChunk];
+#pragma unroll
+            for (int q = 0; q < kThomasChunk; ++q)
+                if (z0 + q < nz) f[q] = v[(size_t)(z0 + q) * plane + t];
+#pragma unroll
+            for (int q = 0; q < kThomasChunk; ++q) {
+                const int z = z0 + q;
+                if (z >= nz) break;
+                const bool first = z == 0, last = z == nz - 1;
+                const double lo = first ? 0.0 : (last ? -2.0 * idz2 : -idz2);
+                const double up = last ? 0.0 : (first ? -2.0 * idz2 : -idz2);
+                const double r = 1.0 / ((first || last ? a_end : a_in) - lo * c);
+                c = up * r;
+                d = (f[q] - lo * d) * r;
+                const size_t o = (size_t)z * plane + t;
+                cp[o] = c;
+                v[o] = d;
+            }
         }
-        double u = d;
-        for (int z = nz - 2; z >= 0; --z) {
-            const size_t o = (size_t)z * plane + t;
-            u = v[o] - cp[o] * u;
-            v[o] = u;
+        double u = d;  // u at z = nz - 1
+        for (int z1 = nz - 1; z1 > 0; z1 -= kThomasChunk) {  // z = z1 - 1 down to z1 - kThomasChunk
+            double dv[kThomasChunk], cv[kThomasChunk];
+#pragma unroll
+            for (int q = 0; q < kThomasChunk; ++q) {
+                const int z = z1 - 1 - q;
+                if (z >= 0) {
+                    dv[q] = v[(size_t)z * plane + t];
+                    cv[q] = cp[(size_t)z * plane + t];
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < kThomasChunk; ++q) {
+                const int z = z1 - 1 - q;
+                if (z < 0) break;
+                u = dv[q] - cv[q] * u;
+                v[(size_t)z * plane + t] = u;
+            }
         }
     }
 }
@@ -467,11 +503,16 @@ __global__ void __launch_bounds__(256) finish_kernel(R* __restrict__ T, const R*
 // row tiles.
 cudaError_t gemm(const double* A, const double* B, double* C, int M, int N, int K, int lda, int ldb, int ldc, int batch,
                  long long sA, long long sB, long long sC, cudaStream_t s) {
+    static PerDevice<int> attr;  // the kernel's dynamic shared memory, once per device
+    const cudaError_t ae = attr.get([](int, int&) {
+        return cudaFuncSetAttribute(dgemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem);
+    });
+    if (ae != cudaSuccess) return ae;
     const int max_rows = 65535 * kGemmBM;
     for (int r0 = 0; r0 < M; r0 += max_rows) {
         const int rows = std::min(M - r0, max_rows);
         const dim3 grid((unsigned)((N + kGemmBN - 1) / kGemmBN), (unsigned)((rows + kGemmBM - 1) / kGemmBM), (unsigned)batch);
-        dgemm_kernel<<<grid, kGemmThreads, 0, s>>>(A + (size_t)r0 * lda, B, C + (size_t)r0 * ldc, rows, N, K, lda, ldb,
+        dgemm_kernel<<<grid, kGemmThreads, kGemmSmem, s>>>(A + (size_t)r0 * lda, B, C + (size_t)r0 * ldc, rows, N, K, lda, ldb,
                                                    ldc, sA, sB, sC);
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
@@ -544,14 +585,14 @@ shg_status HeatDirect::solve(const shg_params& p, R* T, const R* Q, double t_inf
     rhs_kernel<R><<<grid_for(vol, 256), 256, 0, s>>>(T, Q, X, a);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "heat right-hand side");
     // into mode space: along x (rows of X), then along y (one product per z plane)
-    if ((e = gemm(X, ox->FT, Y, nz * my, mx, mx, mx, mx, mx, 1, 0, 0, 0, s)) != cudaSuccess ||
-        (e = gemm(oy->F, Y, X, my, mx, my, my, mx, mx, nz, 0, pl, pl, s)) != cudaSuccess)
+    if ((e = gemm(X, ox->FT, Y, nz * my, mx, mx, mx, ox->ld, mx, 1, 0, 0, 0, s)) != cudaSuccess ||
+        (e = gemm(oy->F, Y, X, my, mx, my, oy->ld, mx, mx, nz, 0, pl, pl, s)) != cudaSuccess)
         return cuda_fail(e, "heat transform");
     thomas_kernel<<<grid_for((size_t)pl, 128), 128, 0, s>>>(X, Y, ox->lam, oy->lam, mx, my, nz, a.idz2, a.biz);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "heat tridiagonal solve");
     // back to voxels: along y, then along x
-    if ((e = gemm(oy->G, X, Y, my, mx, my, my, mx, mx, nz, 0, pl, pl, s)) != cudaSuccess ||
-        (e = gemm(Y, ox->GT, X, nz * my, mx, mx, mx, mx, mx, 1, 0, 0, 0, s)) != cudaSuccess)
+    if ((e = gemm(oy->G, X, Y, my, mx, my, oy->ld, mx, mx, nz, 0, pl, pl, s)) != cudaSuccess ||
+        (e = gemm(Y, ox->GT, X, nz * my, mx, mx, mx, ox->ld, mx, 1, 0, 0, 0, s)) != cudaSuccess)
         return cuda_fail(e, "heat transform");
     if (p.boundary == SHG_BOUNDARY_TOP_OPEN)
         finish_kernel<R, SHG_BOUNDARY_TOP_OPEN><<<grid_for(vol, 256), 256, 0, s>>>(T, Q, X, a, k, out);

@@ -443,32 +443,55 @@ __device__ __forceinline__ double nan_max(double a, double b) { return (b > a ||
 // 5. T <- u (rounded to R) for every unknown, with four sums into out: [0] max |J(u) - u| and
 // [1] sum (J(u) - u)^2 for one FP64 Jacobi sweep J of u (jacobi_point, coefficients in FP64),
 // [2] max |u - T_before| and [3] sum (u - T_before)^2.  Maxima are kept as the bits of
-// non-negative doubles (ordered like unsigned integers; a NaN wins).  Neighbours outside the
-// unknowns are Dirichlet voxels of T, which nothing writes.
+// non-negative doubles (ordered like unsigned integers; a NaN wins).  A thread walks
+// kFinishZ planes of one (x, y) column with u's z neighbours in registers, so every load of a
+// plane is independent of the arithmetic; neighbours outside the unknowns are Dirichlet
+// voxels of T, which nothing writes.
+constexpr int kFinishZ = 16;
+
 template <typename R, int BOUND>
 __global__ void __launch_bounds__(256) finish_kernel(R* __restrict__ T, const R* __restrict__ Q, const double* __restrict__ u,
                                                      const HeatArgs a, const JacobiCoef<double> k, double* __restrict__ out) {
-    const size_t plane = (size_t)a.mx * a.my, total = plane * a.nz;
-    const size_t nn = (size_t)a.n;
+    const size_t plane = (size_t)a.mx * a.my, nn = (size_t)a.n, tplane = nn * nn;
+    const int chunks = (a.nz + kFinishZ - 1) / kFinishZ;
+    const size_t items = plane * chunks;
     double rmax = 0.0, rsum = 0.0, cmax = 0.0, csum = 0.0;
-    for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < total; c += (size_t)gridDim.x * blockDim.x) {
-        const int i = (int)(c % a.mx), j = (int)((c / a.mx) % a.my), z = (int)(c / plane);
+    for (size_t it = blockIdx.x * (size_t)blockDim.x + threadIdx.x; it < items; it += (size_t)gridDim.x * blockDim.x) {
+        const size_t t = it % plane;
+        const int z0 = (int)(it / plane) * kFinishZ, z1 = min(a.nz, z0 + kFinishZ);
+        const int i = (int)(t % a.mx), j = (int)(t / a.mx);
         const int x = a.x0 + i, y = a.y0 + j;
-        const size_t v = ((size_t)z * nn + y) * nn + x;
-        const double uc = u[c];
-        auto get = [&](int ddx, int ddy, int ddz) -> double {
-            const int ii = i + ddx, jj = j + ddy, zz = z + ddz;
-            if (ii >= 0 && ii < a.mx && jj >= 0 && jj < a.my) return u[((size_t)zz * a.my + jj) * a.mx + ii];
-            return (double)T[((size_t)zz * nn + (a.y0 + jj)) * nn + (a.x0 + ii)];
-        };
-        double w = uc;
-        jacobi_point<double, BOUND>(x, y, z, k, Q ? (double)Q[v] : 0.0, get, &w);
-        const double r = fabs(w - uc), dc = fabs(uc - (double)T[v]);
-        rmax = nan_max(rmax, r);
-        rsum += r * r;
-        cmax = nan_max(cmax, dc);
-        csum += dc * dc;
-        T[v] = (R)uc;
+        const bool uxm = i > 0, uxp = i + 1 < a.mx, uym = j > 0, uyp = j + 1 < a.my;
+        const bool gxm = x > 0, gxp = x + 1 < a.n, gym = y > 0, gyp = y + 1 < a.n;
+        size_t c = (size_t)z0 * plane + t;
+        size_t v = (size_t)z0 * tplane + (size_t)y * nn + x;
+        double below = z0 > 0 ? u[c - plane] : 0.0;
+        double cur = u[c];
+#pragma unroll 2
+        for (int z = z0; z < z1; ++z, c += plane, v += tplane) {
+            const double above = z + 1 < a.nz ? u[c + plane] : 0.0;
+            const double xm = uxm ? u[c - 1] : (gxm ? (double)T[v - 1] : 0.0);
+            const double xp = uxp ? u[c + 1] : (gxp ? (double)T[v + 1] : 0.0);
+            const double ym = uym ? u[c - a.mx] : (gym ? (double)T[v - nn] : 0.0);
+            const double yp = uyp ? u[c + a.mx] : (gyp ? (double)T[v + nn] : 0.0);
+            const double q = Q ? (double)Q[v] : 0.0;
+            const double before = (double)T[v];
+            auto get = [&](int dx, int dy, int dz) -> double {
+                if (dz) return dz > 0 ? above : below;
+                if (dy) return dy > 0 ? yp : ym;
+                return dx > 0 ? xp : xm;
+            };
+            double w = cur;
+            jacobi_point<double, BOUND>(x, y, z, k, q, get, &w);
+            const double r = fabs(w - cur), dc = fabs(cur - before);
+            rmax = nan_max(rmax, r);
+            rsum += r * r;
+            cmax = nan_max(cmax, dc);
+            csum += dc * dc;
+            T[v] = (R)cur;
+            below = cur;
+            cur = above;
+        }
     }
     for (int o = 16; o > 0; o >>= 1) {
         rmax = nan_max(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
@@ -594,10 +617,11 @@ shg_status HeatDirect::solve(const shg_params& p, R* T, const R* Q, double t_inf
     if ((e = gemm(oy->G, X, Y, my, mx, my, oy->ld, mx, mx, nz, 0, pl, pl, s)) != cudaSuccess ||
         (e = gemm(Y, ox->GT, X, nz * my, mx, mx, mx, ox->ld, mx, 1, 0, 0, 0, s)) != cudaSuccess)
         return cuda_fail(e, "heat transform");
+    const size_t fitems = (size_t)pl * ((nz + kFinishZ - 1) / kFinishZ);
     if (p.boundary == SHG_BOUNDARY_TOP_OPEN)
-        finish_kernel<R, SHG_BOUNDARY_TOP_OPEN><<<grid_for(vol, 256), 256, 0, s>>>(T, Q, X, a, k, out);
+        finish_kernel<R, SHG_BOUNDARY_TOP_OPEN><<<grid_for(fitems, 256), 256, 0, s>>>(T, Q, X, a, k, out);
     else
-        finish_kernel<R, SHG_BOUNDARY_OVEN_SURROUNDED><<<grid_for(vol, 256), 256, 0, s>>>(T, Q, X, a, k, out);
+        finish_kernel<R, SHG_BOUNDARY_OVEN_SURROUNDED><<<grid_for(fitems, 256), 256, 0, s>>>(T, Q, X, a, k, out);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "heat solution");
     return SHG_OK;
 }

@@ -113,7 +113,7 @@ extern "C" shg_status shg_autotune(int32_t precision, int32_t n, shg_tune_result
     return SHG_OK;
 }
 
-// shg_autotune_batch: the schedule of every grid-size class judged by the time of the whole
+// shg_autotune_batch: the schedule of every grid-size class scored by the time of the whole
 // given batch.  The classes of a mixed batch run side by side on forked streams and share
 // the SMs, so the variant that is fastest for a class alone can slow the batch (a class that
 // fills every SM with its own CTAs holds back the clusters of the larger classes).

@@ -122,7 +122,7 @@ def test_autotune_keeps_results(precision, n, default_schedules):
 
 @pytest.mark.parametrize("precision", [32, 64])
 def test_batch_autotune_keeps_results(precision, default_schedules):
-    """The batch tuner judges each class's compiled variants by the time of the whole batch and
+    """The batch tuner scores each class's compiled variants by the time of the whole batch and
     keeps a change only when the batch gets faster.  The fields agree with the default
     schedule's to the multi-pass-against-fused tolerances (FP64 relative L2 <= 1e-13, FP32
     <= 1e-5): a fused split gives the same bits, the multi-pass march (a candidate at 256 x

@@ -135,6 +135,12 @@ bool tridiag_eigen(int m, std::vector<double>& d, std::vector<double> e, std::ve
 // operator, all row-major m x m.  The operator M is similar to the symmetric B = S M S^{-1}
 // with S = diag(s), s[i+1] = s[i] sqrt(r[i] / l[i+1]); B = V diag(lambda) V^T gives
 // F = V^T S and G = S^{-1} V.
+// An operator with the same kind of end at both sides and m even is symmetric under
+// i -> m-1-i (B and S alike), and B splits into an even and an odd block of half size: for
+// v = (w, +-J w) / sqrt(2) (J the reversal), B v = lambda v exactly when w is an eigenvector of
+// the leading h x h block of B with its last diagonal entry d[h-1] +- e[h-1].  The modes are
+// then built from the blocks' eigenvectors, even modes first (k < h), so that their parity is
+// exact, which the folded transforms rely on; and the QL work is a quarter.
 bool op_modes(const Op1D& op, std::vector<double>& lam, std::vector<double>& F, std::vector<double>& G) {
     const int m = op.m;
     std::vector<double> a, l, r;
@@ -144,9 +150,31 @@ bool op_modes(const Op1D& op, std::vector<double>& lam, std::vector<double>& F, 
         s[i + 1] = s[i] * std::sqrt(r[i] / l[i + 1]);
         e[i] = -std::sqrt(r[i] * l[i + 1]);
     }
-    lam = a;
-    std::vector<double> V;
-    if (!tridiag_eigen(m, lam, e, V)) return false;
+    std::vector<double> V;  // column-major: vector k at V[k*m .. k*m+m)
+    if (op.lo_robin == op.hi_robin && m % 2 == 0 && m >= 2) {
+        const int h = m / 2;
+        V.assign((size_t)m * m, 0.0);
+        lam.assign(m, 0.0);
+        const double r2 = 1.0 / std::sqrt(2.0);
+        for (int par = 0; par < 2; ++par) {  // 0: even, 1: odd
+            std::vector<double> d(a.begin(), a.begin() + h), eh(e.begin(), e.begin() + h), W;
+            d[h - 1] += par == 0 ? e[h - 1] : -e[h - 1];
+            eh[h - 1] = 0.0;
+            if (!tridiag_eigen(h, d, eh, W)) return false;
+            for (int q = 0; q < h; ++q) {
+                const int k = par * h + q;
+                lam[k] = d[q];
+                for (int i = 0; i < h; ++i) {
+                    const double w = W[(size_t)q * h + i] * r2;
+                    V[(size_t)k * m + i] = w;
+                    V[(size_t)k * m + (m - 1 - i)] = par == 0 ? w : -w;
+                }
+            }
+        }
+    } else {
+        lam = a;
+        if (!tridiag_eigen(m, lam, e, V)) return false;
+    }
     F.assign((size_t)m * m, 0.0);
     G.assign((size_t)m * m, 0.0);
     for (int k = 0; k < m; ++k)
@@ -166,6 +194,14 @@ struct OpMats {
     int dev = -1;
     int ld = 0;
     double *F = nullptr, *G = nullptr, *FT = nullptr, *GT = nullptr, *lam = nullptr;
+    // Folded form, for an operator symmetric under i -> m-1-i (the same kind at both ends) with
+    // m a multiple of 4: its modes are even or odd, so with s_i = b_i + b_{m-1-i} and
+    // d_i = b_i - b_{m-1-i} (i < h = m/2) the even amplitudes are FeT-products of s and the odd
+    // ones FoT-products of d, and back, P = GeT-products and Q = GoT-products give
+    // u_i = P_i + Q_i, u_{m-1-i} = P_i - Q_i.  Half matrices h x h, row-major (ld = h, even),
+    // laid out for C = A B like FT and GT; lamf the eigenvalues, even modes first.
+    bool fold = false;
+    double *FeT = nullptr, *FoT = nullptr, *GeT = nullptr, *GoT = nullptr, *lamf = nullptr;
 };
 
 // Process-wide cache of operator transforms, per device (an operator's eigendecomposition
@@ -196,9 +232,27 @@ shg_status get_op(const Op1D& op, const OpMats** out) {
             FT[(size_t)i * ld + k] = F[(size_t)k * m + i];
             GT[(size_t)k * ld + i] = G[(size_t)i * m + k];
         }
+    // the folded form (op_modes gives a symmetric operator's even modes first, then its odd
+    // ones, each of exact parity); m a multiple of 4 keeps the half rows 16-byte aligned
+    const int h = m / 2;
+    const bool fold = op.lo_robin == op.hi_robin && m % 4 == 0;
+    const size_t hh = fold ? (size_t)h * h : 0;
+    std::vector<double> FeT(hh), FoT(hh), GeT(hh), GoT(hh), lamf(fold ? m : 0);
+    for (int a = 0; fold && a < h; ++a) {
+        const int ke = a, ko = h + a;
+        lamf[a] = lam[ke];
+        lamf[h + a] = lam[ko];
+        for (int i = 0; i < h; ++i) {
+            FeT[(size_t)i * h + a] = F[(size_t)ke * m + i];  // B operand: rows i, columns modes
+            FoT[(size_t)i * h + a] = F[(size_t)ko * m + i];
+            GeT[(size_t)a * h + i] = G[(size_t)i * m + ke];  // B operand: rows modes, columns i
+            GoT[(size_t)a * h + i] = G[(size_t)i * m + ko];
+        }
+    }
     if (g_ops.size() >= kMaxCachedOps) return fail(SHG_ERR_UNSUPPORTED, "more than %d heat operators cached", (int)kMaxCachedOps);
     double* buf = nullptr;
-    if ((e = cudaMalloc((void**)&buf, sizeof(double) * (4 * mm + m))) != cudaSuccess) return cuda_fail(e, "cudaMalloc");
+    if ((e = cudaMalloc((void**)&buf, sizeof(double) * (4 * mm + (m + (m & 1)) + 4 * hh + lamf.size()))) != cudaSuccess)
+        return cuda_fail(e, "cudaMalloc");
     OpMats* c = new OpMats;
     c->op = op;
     c->dev = dev;
@@ -208,10 +262,21 @@ shg_status get_op(const Op1D& op, const OpMats** out) {
     c->FT = buf + 2 * mm;
     c->GT = buf + 3 * mm;
     c->lam = buf + 4 * mm;
-    const double* src[5] = {Fp.data(), Gp.data(), FT.data(), GT.data(), lam.data()};
-    double* dst[5] = {c->F, c->G, c->FT, c->GT, c->lam};
-    for (int k = 0; k < 5 && e == cudaSuccess; ++k)
-        e = cudaMemcpy(dst[k], src[k], sizeof(double) * (k == 4 ? (size_t)m : mm), cudaMemcpyHostToDevice);
+    c->fold = fold;
+    double* fb = c->lam + (m + (m & 1));  // 16-byte aligned (4 mm and the padded m are even)
+    if (fold) {
+        c->FeT = fb;
+        c->FoT = fb + hh;
+        c->GeT = fb + 2 * hh;
+        c->GoT = fb + 3 * hh;
+        c->lamf = fb + 4 * hh;
+    }
+    const double* src[10] = {Fp.data(), Gp.data(), FT.data(), GT.data(), lam.data(),
+                             FeT.data(), FoT.data(), GeT.data(), GoT.data(), lamf.data()};
+    double* dst[10] = {c->F, c->G, c->FT, c->GT, c->lam, c->FeT, c->FoT, c->GeT, c->GoT, c->lamf};
+    const size_t cnt[10] = {mm, mm, mm, mm, (size_t)m, hh, hh, hh, hh, lamf.size()};
+    for (int k = 0; k < 10 && e == cudaSuccess; ++k)
+        if (cnt[k]) e = cudaMemcpy(dst[k], src[k], sizeof(double) * cnt[k], cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
         cudaFree(buf);
         delete c;
@@ -266,22 +331,37 @@ struct HeatArgs {
 // 1. Right-hand side of the scaled system: Q / kappa on inner points, 2 Bi T_inf / d^2 at each
 //    Robin end, g / d^2 for each Dirichlet neighbour g (read from T).
 template <typename R>
-__global__ void rhs_kernel(const R* __restrict__ T, const R* __restrict__ Q, double* __restrict__ b, const HeatArgs a) {
-    const size_t plane = (size_t)a.mx * a.my, total = plane * a.nz;
+__device__ __forceinline__ double rhs_value(const R* __restrict__ T, const R* __restrict__ Q, const HeatArgs& a, int i,
+                                            int j, int z) {
     const size_t nn = (size_t)a.n;
+    const int x = a.x0 + i, y = a.y0 + j;
+    const size_t v = ((size_t)z * nn + y) * nn + x;
+    double s = 0.0;
+    if (Q && x > 0 && x < a.n - 1 && y > 0 && y < a.n - 1 && z > 0 && z < a.nz - 1) s = (double)Q[v] * a.iK;
+    if (i == 0) s += a.lo_x_robin ? 2.0 * a.bix * a.tinf * a.idx2 : (double)T[v - 1] * a.idx2;
+    if (i == a.mx - 1) s += a.hi_x_robin ? 2.0 * a.bix * a.tinf * a.idx2 : (double)T[v + 1] * a.idx2;
+    if (j == 0) s += a.lo_y_robin ? 2.0 * a.biy * a.tinf * a.idy2 : (double)T[v - nn] * a.idy2;
+    if (j == a.my - 1) s += a.hi_y_robin ? 2.0 * a.biy * a.tinf * a.idy2 : (double)T[v + nn] * a.idy2;
+    if (z == 0) s += 2.0 * a.biz * a.tinf * a.idz2;
+    if (z == a.nz - 1) s += 2.0 * a.biz * a.tinf * a.idz2;
+    return s;
+}
+
+// FOLD: each row holds s_i = b_i + b_{mx-1-i} at i < mx/2 and d_i = b_i - b_{mx-1-i} at mx/2 + i.
+template <typename R, bool FOLD>
+__global__ void rhs_kernel(const R* __restrict__ T, const R* __restrict__ Q, double* __restrict__ b, const HeatArgs a) {
+    const int w = FOLD ? a.mx / 2 : a.mx;  // work items per row
+    const size_t plane = (size_t)w * a.my, total = plane * a.nz;
     for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < total; c += (size_t)gridDim.x * blockDim.x) {
-        const int i = (int)(c % a.mx), j = (int)((c / a.mx) % a.my), z = (int)(c / plane);
-        const int x = a.x0 + i, y = a.y0 + j;
-        const size_t v = ((size_t)z * nn + y) * nn + x;
-        double s = 0.0;
-        if (Q && x > 0 && x < a.n - 1 && y > 0 && y < a.n - 1 && z > 0 && z < a.nz - 1) s = (double)Q[v] * a.iK;
-        if (i == 0) s += a.lo_x_robin ? 2.0 * a.bix * a.tinf * a.idx2 : (double)T[v - 1] * a.idx2;
-        if (i == a.mx - 1) s += a.hi_x_robin ? 2.0 * a.bix * a.tinf * a.idx2 : (double)T[v + 1] * a.idx2;
-        if (j == 0) s += a.lo_y_robin ? 2.0 * a.biy * a.tinf * a.idy2 : (double)T[v - nn] * a.idy2;
-        if (j == a.my - 1) s += a.hi_y_robin ? 2.0 * a.biy * a.tinf * a.idy2 : (double)T[v + nn] * a.idy2;
-        if (z == 0) s += 2.0 * a.biz * a.tinf * a.idz2;
-        if (z == a.nz - 1) s += 2.0 * a.biz * a.tinf * a.idz2;
-        b[c] = s;
+        const int i = (int)(c % w), j = (int)((c / w) % a.my), z = (int)(c / plane);
+        const size_t row = ((size_t)z * a.my + j) * a.mx;
+        if (FOLD) {
+            const double b1 = rhs_value<R>(T, Q, a, i, j, z), b2 = rhs_value<R>(T, Q, a, a.mx - 1 - i, j, z);
+            b[row + i] = b1 + b2;
+            b[row + w + i] = b1 - b2;
+        } else {
+            b[row + i] = rhs_value<R>(T, Q, a, i, j, z);
+        }
     }
 }
 
@@ -446,12 +526,21 @@ __device__ __forceinline__ double nan_max(double a, double b) { return (b > a ||
 // non-negative doubles (ordered like unsigned integers; a NaN wins).  A thread walks
 // kFinishZ planes of one (x, y) column with u's z neighbours in registers, so every load of a
 // plane is independent of the arithmetic; neighbours outside the unknowns are Dirichlet
-// voxels of T, which nothing writes.
+// voxels of T, which nothing writes.  FOLD: each row of u holds P at i < mx/2 and Q at
+// mx/2 + i, and u_i = P_i + Q_i, u_{mx-1-i} = P_i - Q_i.
 constexpr int kFinishZ = 16;
 
-template <typename R, int BOUND>
-__global__ void __launch_bounds__(256) finish_kernel(R* __restrict__ T, const R* __restrict__ Q, const double* __restrict__ u,
+template <typename R, int BOUND, bool FOLD>
+__global__ void __launch_bounds__(256, 2) finish_kernel(R* __restrict__ T, const R* __restrict__ Q, const double* __restrict__ u,
                                                      const HeatArgs a, const JacobiCoef<double> k, double* __restrict__ out) {
+    const int h = a.mx / 2;
+    auto U = [&](size_t rowbase, int col) -> double {  // the solution at column col of a row
+        if (!FOLD) return u[rowbase + col];
+        const bool lo = col < h;
+        const int p = lo ? col : a.mx - 1 - col;
+        const double pv = u[rowbase + p], qv = u[rowbase + h + p];
+        return lo ? pv + qv : pv - qv;
+    };
     const size_t plane = (size_t)a.mx * a.my, nn = (size_t)a.n, tplane = nn * nn;
     const int chunks = (a.nz + kFinishZ - 1) / kFinishZ;
     const size_t items = plane * chunks;
@@ -463,17 +552,17 @@ __global__ void __launch_bounds__(256) finish_kernel(R* __restrict__ T, const R*
         const int x = a.x0 + i, y = a.y0 + j;
         const bool uxm = i > 0, uxp = i + 1 < a.mx, uym = j > 0, uyp = j + 1 < a.my;
         const bool gxm = x > 0, gxp = x + 1 < a.n, gym = y > 0, gyp = y + 1 < a.n;
-        size_t c = (size_t)z0 * plane + t;
+        size_t rb = (size_t)z0 * plane + (size_t)j * a.mx;  // this column's row in plane z
         size_t v = (size_t)z0 * tplane + (size_t)y * nn + x;
-        double below = z0 > 0 ? u[c - plane] : 0.0;
-        double cur = u[c];
+        double below = z0 > 0 ? U(rb - plane, i) : 0.0;
+        double cur = U(rb, i);
 #pragma unroll 2
-        for (int z = z0; z < z1; ++z, c += plane, v += tplane) {
-            const double above = z + 1 < a.nz ? u[c + plane] : 0.0;
-            const double xm = uxm ? u[c - 1] : (gxm ? (double)T[v - 1] : 0.0);
-            const double xp = uxp ? u[c + 1] : (gxp ? (double)T[v + 1] : 0.0);
-            const double ym = uym ? u[c - a.mx] : (gym ? (double)T[v - nn] : 0.0);
-            const double yp = uyp ? u[c + a.mx] : (gyp ? (double)T[v + nn] : 0.0);
+        for (int z = z0; z < z1; ++z, rb += plane, v += tplane) {
+            const double above = z + 1 < a.nz ? U(rb + plane, i) : 0.0;
+            const double xm = uxm ? U(rb, i - 1) : (gxm ? (double)T[v - 1] : 0.0);
+            const double xp = uxp ? U(rb, i + 1) : (gxp ? (double)T[v + 1] : 0.0);
+            const double ym = uym ? U(rb - a.mx, i) : (gym ? (double)T[v - nn] : 0.0);
+            const double yp = uyp ? U(rb + a.mx, i) : (gyp ? (double)T[v + nn] : 0.0);
             const double q = Q ? (double)Q[v] : 0.0;
             const double before = (double)T[v];
             auto get = [&](int dx, int dy, int dz) -> double {
@@ -605,23 +694,44 @@ shg_status HeatDirect::solve(const shg_params& p, R* T, const R* Q, double t_inf
     const int mx = g.mx, my = g.my, nz = g.nz;
     const long long pl = (long long)mx * my;
     if ((e = cudaMemsetAsync(out, 0, 4 * sizeof(double), s)) != cudaSuccess) return cuda_fail(e, "memset");
-    rhs_kernel<R><<<grid_for(vol, 256), 256, 0, s>>>(T, Q, X, a);
+    const bool fold = ox->fold;
+    const int h = mx / 2;
+    if (fold) rhs_kernel<R, true><<<grid_for(vol / 2, 256), 256, 0, s>>>(T, Q, X, a);
+    else rhs_kernel<R, false><<<grid_for(vol, 256), 256, 0, s>>>(T, Q, X, a);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "heat right-hand side");
-    // into mode space: along x (rows of X), then along y (one product per z plane)
-    if ((e = gemm(X, ox->FT, Y, nz * my, mx, mx, mx, ox->ld, mx, 1, 0, 0, 0, s)) != cudaSuccess ||
-        (e = gemm(oy->F, Y, X, my, mx, my, oy->ld, mx, mx, nz, 0, pl, pl, s)) != cudaSuccess)
+    // into mode space: along x (rows of X; folded, the even modes from the sums and the odd
+    // ones from the differences, half the work), then along y (one product per z plane)
+    if (fold) {
+        if ((e = gemm(X, ox->FeT, Y, nz * my, h, h, mx, h, mx, 1, 0, 0, 0, s)) == cudaSuccess)
+            e = gemm(X + h, ox->FoT, Y + h, nz * my, h, h, mx, h, mx, 1, 0, 0, 0, s);
+    } else {
+        e = gemm(X, ox->FT, Y, nz * my, mx, mx, mx, ox->ld, mx, 1, 0, 0, 0, s);
+    }
+    if (e != cudaSuccess || (e = gemm(oy->F, Y, X, my, mx, my, oy->ld, mx, mx, nz, 0, pl, pl, s)) != cudaSuccess)
         return cuda_fail(e, "heat transform");
-    thomas_kernel<<<grid_for((size_t)pl, 128), 128, 0, s>>>(X, Y, ox->lam, oy->lam, mx, my, nz, a.idz2, a.biz);
+    thomas_kernel<<<grid_for((size_t)pl, 128), 128, 0, s>>>(X, Y, fold ? ox->lamf : ox->lam, oy->lam, mx, my, nz, a.idz2,
+                                                             a.biz);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "heat tridiagonal solve");
-    // back to voxels: along y, then along x
-    if ((e = gemm(oy->G, X, Y, my, mx, my, oy->ld, mx, mx, nz, 0, pl, pl, s)) != cudaSuccess ||
-        (e = gemm(Y, ox->GT, X, nz * my, mx, mx, mx, ox->ld, mx, 1, 0, 0, 0, s)) != cudaSuccess)
+    // back to voxels: along y, then along x (folded: P from the even modes, Q from the odd;
+    // the finishing pass combines them)
+    if ((e = gemm(oy->G, X, Y, my, mx, my, oy->ld, mx, mx, nz, 0, pl, pl, s)) != cudaSuccess)
         return cuda_fail(e, "heat transform");
+    if (fold) {
+        if ((e = gemm(Y, ox->GeT, X, nz * my, h, h, mx, h, mx, 1, 0, 0, 0, s)) == cudaSuccess)
+            e = gemm(Y + h, ox->GoT, X + h, nz * my, h, h, mx, h, mx, 1, 0, 0, 0, s);
+    } else {
+        e = gemm(Y, ox->GT, X, nz * my, mx, mx, mx, ox->ld, mx, 1, 0, 0, 0, s);
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "heat transform");
     const size_t fitems = (size_t)pl * ((nz + kFinishZ - 1) / kFinishZ);
-    if (p.boundary == SHG_BOUNDARY_TOP_OPEN)
-        finish_kernel<R, SHG_BOUNDARY_TOP_OPEN><<<grid_for(fitems, 256), 256, 0, s>>>(T, Q, X, a, k, out);
-    else
-        finish_kernel<R, SHG_BOUNDARY_OVEN_SURROUNDED><<<grid_for(fitems, 256), 256, 0, s>>>(T, Q, X, a, k, out);
+    const int fb = grid_for(fitems, 256);
+    if (p.boundary == SHG_BOUNDARY_TOP_OPEN) {
+        if (fold) finish_kernel<R, SHG_BOUNDARY_TOP_OPEN, true><<<fb, 256, 0, s>>>(T, Q, X, a, k, out);
+        else finish_kernel<R, SHG_BOUNDARY_TOP_OPEN, false><<<fb, 256, 0, s>>>(T, Q, X, a, k, out);
+    } else {
+        if (fold) finish_kernel<R, SHG_BOUNDARY_OVEN_SURROUNDED, true><<<fb, 256, 0, s>>>(T, Q, X, a, k, out);
+        else finish_kernel<R, SHG_BOUNDARY_OVEN_SURROUNDED, false><<<fb, 256, 0, s>>>(T, Q, X, a, k, out);
+    }
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "heat solution");
     return SHG_OK;
 }

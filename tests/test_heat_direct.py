@@ -63,3 +63,17 @@ def test_heat_solver_is_validated():
     assert shg.check_params(p) == P.SHG_ERR_INVALID
     p.heat_solver = P.SHG_HEAT_DIRECT
     assert shg.check_params(p) == P.SHG_OK
+
+
+@pytest.mark.parametrize("m,robin,bi", [(2, 1, 0.5), (8, 0, 0.0), (128, 1, 1.4e-6), (510, 0, 0.0), (512, 1, 1.4e-6)])
+def test_symmetric_operator_modes_have_exact_parity(m, robin, bi):
+    """An operator with the same kind of end at both sides: its modes come even first, then
+    odd, each exactly symmetric or antisymmetric under i -> m-1-i (the folded transforms of
+    the direct solve rely on it)."""
+    lam, F, G = shg.heat_operator_modes(m, 1.17, robin, robin, bi)
+    h = m // 2
+    scale = np.abs(F).max()
+    assert np.abs(F[:h] - F[:h, ::-1]).max() <= 1e-15 * scale
+    assert np.abs(F[h:] + F[h:, ::-1]).max() <= 1e-15 * scale
+    assert np.abs(G[:, :h] - G[::-1, :h]).max() <= 1e-15 * np.abs(G).max()
+    assert np.abs(F @ G - np.eye(m)).max() < 1e-12 * m

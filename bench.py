@@ -618,16 +618,18 @@ def run_thermal_batch(args) -> dict:
     # library's pool from one instance to the next (read when the pool is first created), and
     # grow the pool to it before the timed runs (set-up, as an application would at start)
     ps = P.config_thermal_512(args.thermal_count)
+    if args.thermal_nz:  # a shorter crystal grid, e.g. for a launch list
+        ps = [p.replace(nz=args.thermal_nz) for p in ps]
     direct = args.heat_solver == "direct"
     if direct:  # the stated rule: max|ΔT| < 1e-6 K every outer iteration, at most 5 of them
         ps = [p.replace(precision=32, heat_solver=P.SHG_HEAT_DIRECT) for p in ps]
-        label = (f"{len(ps)} x thermal 512x512x1000 FP32, heat equation solved to the Jacobi fixed point "
+        label = (f"{len(ps)} x thermal 512x512x{ps[0].nz} FP32, heat equation solved to the Jacobi fixed point "
                  f"(direct, FP64) every outer iteration, <= {ps[0].max_outer} outer iterations, "
                  f"max|ΔT| < {ps[0].jacobi_tol:g} K")
     else:
         ps = [p.replace(conv_rule=P.SHG_CONV_FIXED, max_sweeps=args.thermal_fixed_sweeps,
                         max_outer=args.thermal_outer, precision=32) for p in ps]
-        label = (f"{len(ps)} x thermal 512x512x1000 FP32, {args.thermal_outer} outer x "
+        label = (f"{len(ps)} x thermal 512x512x{ps[0].nz} FP32, {args.thermal_outer} outer x "
                  f"{args.thermal_fixed_sweeps} Jacobi sweeps each")
     if args.thermal_mode == "batch":
         # all instances in one shg_thermal_batch call: every instance's buffers and tangent at

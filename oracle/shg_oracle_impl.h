@@ -601,6 +601,16 @@ static int SFX(solve_thermal)(const shg_params* p, const R* signal_in, R* pump_o
         /* Jacobi loop, Solver.h:335-355 */
         double red = 1.0, aux = -1.0;
         int64_t counter = 0;
+        if (p->conv_rule == SHG_CONV_FIXED) {
+            /* the library's fixed rule (no counterpart in the reference): exactly max_sweeps
+               sweeps per outer iteration and exactly max_outer outer iterations */
+            for (; counter < p->max_sweeps; ++counter) {
+                if (p->boundary == SHG_BOUNDARY_OVEN_SURROUNDED) SFX(jacobi_oven)(&c, Ti, Tf, Q);
+                else SFX(jacobi_top_open)(&c, Ti, Tf, Q);
+                memcpy(Ti, Tf, sizeof(R) * nt);
+            }
+            red = 0.0;
+        }
         while (red >= tol) {
             if (counter >= max_sweeps) { status = SHG_ERR_NOT_CONVERGED; break; }
             if (p->boundary == SHG_BOUNDARY_OVEN_SURROUNDED) SFX(jacobi_oven)(&c, Ti, Tf, Q);
@@ -635,7 +645,7 @@ static int SFX(solve_thermal)(const shg_params* p, const R* signal_in, R* pump_o
             SFX(set_q)(&c, Tf, P, S, s, Q);
         }
         ++outer;
-        if (counter == 1 && g != 0) break; /* Solver.h:367 */
+        if (p->conv_rule != SHG_CONV_FIXED && counter == 1 && g != 0) break; /* Solver.h:367 */
     }
     if (pump_out) memcpy(pump_out, Pout, sizeof(CPX) * n);
     if (signal_out) memcpy(signal_out, Sout, sizeof(CPX) * n);

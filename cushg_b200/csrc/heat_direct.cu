@@ -365,10 +365,15 @@ __global__ void rhs_kernel(const R* __restrict__ T, const R* __restrict__ Q, dou
     }
 }
 
-constexpr int kGemmBM = 128, kGemmBN = 128, kGemmBK = 16, kGemmThreads = 256, kGemmStages = 3;
-constexpr int kGemmALd = kGemmBK + 2;  // A tile row pitch: 144 B (16-byte rows, adjacent rows 4 banks apart)
-constexpr int kGemmStageDoubles = kGemmBM * kGemmALd + kGemmBK * kGemmBN;
-constexpr size_t kGemmSmem = sizeof(double) * kGemmStageDoubles * kGemmStages;
+// A block computes a 128 x 128 tile of C with eight warps, each a 64 x 32 part of it as 4 x 4
+// FP64 tensor-core products (mma.sync m16n8k4); k runs in 32-wide slices through a
+// three-stage ring of cp.async copies.  Row pitches: A slices 36 doubles, B slices 132, so
+// that the fragment reads of a half-warp (4 rows x 4 columns of A, 4 rows x 4 columns of B)
+// fall in 16 different 8-byte bank pairs; every row starts on 16 bytes.
+constexpr int kGemmBM = 128, kGemmBN = 128, kGemmBK = 32, kGemmThreads = 256, kGemmStages = 3;
+constexpr int kGemmALd = kGemmBK + 4, kGemmBLd = kGemmBN + 4;
+constexpr int kGemmStageDoubles = kGemmBM * kGemmALd + kGemmBK * kGemmBLd;
+constexpr size_t kGemmSmem = sizeof(double) * kGemmStageDoubles * kGemmStages;  // 207 KB
 
 // 16 bytes from global to shared memory, asynchronously; the bytes past `valid` (0..16) are
 // zero-filled and not read.
@@ -377,13 +382,18 @@ __device__ __forceinline__ void cp_async16(double* dst, const double* src, int v
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(valid) : "memory");
 }
 
+// c += A B for one 16 x 8 x 4 FP64 product held in the fragments of mma.sync m16n8k4: with
+// g = lane / 4 and t = lane % 4, a0 = A[g][t], a1 = A[g + 8][t], b = B[t][g], and c = C[g][2t],
+// C[g][2t + 1], C[g + 8][2t], C[g + 8][2t + 1].
+__device__ __forceinline__ void mma_f64(double (&c)[4], double a0, double a1, double b) {
+    asm volatile("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};"
+                 : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+                 : "d"(a0), "d"(a1), "d"(b));
+}
+
 // 2, 4. C[b] = A[b] B[b] in FP64 for row-major A (M x K, lda), B (K x N, ldb) and C (M x N, ldc),
-// batch b = blockIdx.z at element strides sA, sB, sC.  lda, ldb, the strides and the three base
-// addresses are even (16-byte rows).  A 128 x 128 tile per block; thread (tx, ty) accumulates
-// rows ty + 16 r and columns tx + 16 c (r, c < 8) in registers, so that a warp's reads of the
-// A tile are two broadcast rows and of the B tile 16 consecutive doubles.  The tiles stream
-// through a three-stage ring of cp.async copies (zero-filled past M, N and K).  Each output is
-// one FMA chain over k in order.
+// batch b = blockIdx.z at element strides sA, sB, sC.  lda, ldb, ldc, the strides and the three
+// base addresses are even (16-byte rows).  Copies past M, N and K are zero-filled.
 __global__ void __launch_bounds__(kGemmThreads, 1) dgemm_kernel(const double* __restrict__ A, const double* __restrict__ B,
                                                              double* __restrict__ C, int M, int N, int K, int lda,
                                                              int ldb, int ldc, long long sA, long long sB, long long sC) {
@@ -392,73 +402,84 @@ __global__ void __launch_bounds__(kGemmThreads, 1) dgemm_kernel(const double* __
     B += blockIdx.z * sB;
     C += blockIdx.z * sC;
     const int m0 = blockIdx.y * kGemmBM, n0 = blockIdx.x * kGemmBN;
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-    // tile t into stage st: A 128 x 16 and B 16 x 128, each 1024 chunks of 16 bytes, 4 per thread
-    auto load = [&](int t, int st) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int wm = (warp & 1) * 64, wn = (warp >> 1) * 32;  // this warp's 64 x 32 part of the tile
+    // k slice `tile` into stage st: A 128 x 32 and B 32 x 128, 2048 chunks of 16 bytes each
+    auto load = [&](int tile, int st) {
         double* As = gsm + st * kGemmStageDoubles;
         double* Bs = As + kGemmBM * kGemmALd;
-        const int k0 = t * kGemmBK;
+        const int k0 = tile * kGemmBK;
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
+        for (int j = 0; j < kGemmBM * kGemmBK / 2 / kGemmThreads; ++j) {
             const int c = tid + j * kGemmThreads;
-            const int row = c >> 3, col = (c & 7) * 2;
+            const int row = c / (kGemmBK / 2), col = (c % (kGemmBK / 2)) * 2;
             const int gr = m0 + row, gc = k0 + col;
             const int valid = gr < M ? 8 * max(0, min(2, K - gc)) : 0;
             cp_async16(As + row * kGemmALd + col, valid ? A + (size_t)gr * lda + gc : A, valid);
         }
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
+        for (int j = 0; j < kGemmBK * kGemmBN / 2 / kGemmThreads; ++j) {
             const int c = tid + j * kGemmThreads;
-            const int row = c >> 6, col = (c & 63) * 2;
+            const int row = c / (kGemmBN / 2), col = (c % (kGemmBN / 2)) * 2;
             const int gr = k0 + row, gc = n0 + col;
             const int valid = gr < K ? 8 * max(0, min(2, N - gc)) : 0;
-            cp_async16(Bs + row * kGemmBN + col, valid ? B + (size_t)gr * ldb + gc : B, valid);
+            cp_async16(Bs + row * kGemmBLd + col, valid ? B + (size_t)gr * ldb + gc : B, valid);
         }
     };
-    double acc[8][8];
+    double acc[4][4][4];
 #pragma unroll
-    for (int r = 0; r < 8; ++r)
+    for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int c = 0; c < 8; ++c) acc[r][c] = 0.0;
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.0;
     const int tiles = (K + kGemmBK - 1) / kGemmBK;
 #pragma unroll
     for (int st = 0; st < kGemmStages - 1; ++st) {
         if (st < tiles) load(st, st);
         asm volatile("cp.async.commit_group;" ::: "memory");
     }
-    for (int t = 0; t < tiles; ++t) {
-        // this thread's copies of tile t have landed; the barrier makes everyone's visible and
-        // ends every read of the stage the next load overwrites (tile t - 1's)
+    for (int tl = 0; tl < tiles; ++tl) {
+        // this thread's copies of slice tl have landed; the barrier makes everyone's visible and
+        // ends every read of the stage the next load overwrites (slice tl - 1's)
         asm volatile("cp.async.wait_group %0;" ::"n"(kGemmStages - 2) : "memory");
         __syncthreads();
-        if (t + kGemmStages - 1 < tiles) load(t + kGemmStages - 1, (t + kGemmStages - 1) % kGemmStages);
+        if (tl + kGemmStages - 1 < tiles) load(tl + kGemmStages - 1, (tl + kGemmStages - 1) % kGemmStages);
         asm volatile("cp.async.commit_group;" ::: "memory");
-        const double* As = gsm + (t % kGemmStages) * kGemmStageDoubles;
+        const double* As = gsm + (tl % kGemmStages) * kGemmStageDoubles;
         const double* Bs = As + kGemmBM * kGemmALd;
 #pragma unroll
-        for (int kk = 0; kk < kGemmBK; ++kk) {
-            double av[8], bv[8];
+        for (int kk = 0; kk < kGemmBK; kk += 4) {
+            double a[4][2], b[4];
 #pragma unroll
-            for (int r = 0; r < 8; ++r) av[r] = As[(ty + 16 * r) * kGemmALd + kk];
+            for (int i = 0; i < 4; ++i) {
+                a[i][0] = As[(wm + 16 * i + g) * kGemmALd + kk + t];
+                a[i][1] = As[(wm + 16 * i + g + 8) * kGemmALd + kk + t];
+            }
 #pragma unroll
-            for (int c = 0; c < 8; ++c) bv[c] = Bs[kk * kGemmBN + tx + 16 * c];
+            for (int j = 0; j < 4; ++j) b[j] = Bs[(kk + t) * kGemmBLd + wn + 8 * j + g];
 #pragma unroll
-            for (int r = 0; r < 8; ++r)
+            for (int i = 0; i < 4; ++i)
 #pragma unroll
-                for (int c = 0; c < 8; ++c) acc[r][c] = fma(av[r], bv[c], acc[r][c]);
+                for (int j = 0; j < 4; ++j) mma_f64(acc[i][j], a[i][0], a[i][1], b[j]);
         }
     }
     asm volatile("cp.async.wait_group 0;" ::: "memory");
 #pragma unroll
-    for (int r = 0; r < 8; ++r) {
-        const int row = m0 + ty + 16 * r;
-        if (row >= M) break;
+    for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            const int col = n0 + tx + 16 * c;
-            if (col < N) C[(size_t)row * ldc + col] = acc[r][c];
+        for (int h = 0; h < 2; ++h) {
+            const int row = m0 + wm + 16 * i + g + 8 * h;
+            if (row >= M) continue;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int col = n0 + wn + 8 * j + 2 * t;  // even: 16-byte aligned in C
+                double* out = C + (size_t)row * ldc + col;
+                if (col + 1 < N) *reinterpret_cast<double2*>(out) = make_double2(acc[i][j][2 * h], acc[i][j][2 * h + 1]);
+                else if (col < N) out[0] = acc[i][j][2 * h];
+            }
         }
-    }
 }
 
 // 3. For every mode t = j * mx + i: (Az + lambda_x[i] + lambda_y[j]) u = f along z, Thomas
@@ -701,9 +722,10 @@ shg_status HeatDirect::solve(const shg_params& p, R* T, const R* Q, double t_inf
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "heat right-hand side");
     // into mode space: along x (rows of X; folded, the even modes from the sums and the odd
     // ones from the differences, half the work), then along y (one product per z plane)
+    // (folded: the even and odd halves as a batch of two, FoT = FeT + h*h)
+    const long long hh = (long long)h * h;
     if (fold) {
-        if ((e = gemm(X, ox->FeT, Y, nz * my, h, h, mx, h, mx, 1, 0, 0, 0, s)) == cudaSuccess)
-            e = gemm(X + h, ox->FoT, Y + h, nz * my, h, h, mx, h, mx, 1, 0, 0, 0, s);
+        e = gemm(X, ox->FeT, Y, nz * my, h, h, mx, h, mx, 2, h, hh, h, s);
     } else {
         e = gemm(X, ox->FT, Y, nz * my, mx, mx, mx, ox->ld, mx, 1, 0, 0, 0, s);
     }
@@ -717,8 +739,7 @@ shg_status HeatDirect::solve(const shg_params& p, R* T, const R* Q, double t_inf
     if ((e = gemm(oy->G, X, Y, my, mx, my, oy->ld, mx, mx, nz, 0, pl, pl, s)) != cudaSuccess)
         return cuda_fail(e, "heat transform");
     if (fold) {
-        if ((e = gemm(Y, ox->GeT, X, nz * my, h, h, mx, h, mx, 1, 0, 0, 0, s)) == cudaSuccess)
-            e = gemm(Y + h, ox->GoT, X + h, nz * my, h, h, mx, h, mx, 1, 0, 0, 0, s);
+        e = gemm(Y, ox->GeT, X, nz * my, h, h, mx, h, mx, 2, h, hh, h, s);
     } else {
         e = gemm(Y, ox->GT, X, nz * my, mx, mx, mx, ox->ld, mx, 1, 0, 0, 0, s);
     }

@@ -22,6 +22,7 @@
 //   2. b <- b Fx^T (along x), then Fy b (along y)                            dgemm_kernel x2
 //   3. for every mode (ky, kx): (Az + lambda_x + lambda_y) v = b along z       thomas_kernel
 //   4. v <- Gy v, then v Gx^T                                                dgemm_kernel x2
+//      (folded x transform: v's rows from their even and odd halves)           unfold_kernel
 //   5. T <- v, with the FP64 residual of one Jacobi sweep of v and the change  finish_kernel
 // Unknowns: TOP_OPEN, x 0..n-1 (Robin both ends), y 1..n-1 (y = 0 Dirichlet, Robin at n-1),
 // z 0..nz-1 (Robin); OVEN_SURROUNDED, x and y 1..n-2 (Dirichlet both ends), z as above.
@@ -541,27 +542,36 @@ __global__ void thomas_kernel(double* __restrict__ v, double* __restrict__ cp, c
 
 __device__ __forceinline__ double nan_max(double a, double b) { return (b > a || b != b) ? b : a; }
 
+// 4'. Folded x transform: each row of the inverse transform's output holds P at i < mx/2 and Q
+// at mx/2 + i; the solution row is u_i = P_i + Q_i, u_{mx-1-i} = P_i - Q_i.  One streaming pass
+// into the other volume, so that the finishing pass reads one value per neighbour.
+__global__ void unfold_kernel(const double* __restrict__ pq, double* __restrict__ u, size_t rows, int mx) {
+    const int h = mx / 2;
+    const size_t items = rows * (size_t)h;
+    for (size_t it = blockIdx.x * (size_t)blockDim.x + threadIdx.x; it < items; it += (size_t)gridDim.x * blockDim.x) {
+        const size_t r = it / h;
+        const int i = (int)(it % h);
+        const double* src = pq + r * mx;
+        double* dst = u + r * mx;
+        const double pv = src[i], qv = src[h + i];
+        dst[i] = pv + qv;
+        dst[mx - 1 - i] = pv - qv;
+    }
+}
+
 // 5. T <- u (rounded to R) for every unknown, with four sums into out: [0] max |J(u) - u| and
 // [1] sum (J(u) - u)^2 for one FP64 Jacobi sweep J of u (jacobi_point, coefficients in FP64),
 // [2] max |u - T_before| and [3] sum (u - T_before)^2.  Maxima are kept as the bits of
 // non-negative doubles (ordered like unsigned integers; a NaN wins).  A thread walks
 // kFinishZ planes of one (x, y) column with u's z neighbours in registers, so every load of a
 // plane is independent of the arithmetic; neighbours outside the unknowns are Dirichlet
-// voxels of T, which nothing writes.  FOLD: each row of u holds P at i < mx/2 and Q at
-// mx/2 + i, and u_i = P_i + Q_i, u_{mx-1-i} = P_i - Q_i.
+// voxels of T, which nothing writes.
 constexpr int kFinishZ = 16;
 
-template <typename R, int BOUND, bool FOLD>
+template <typename R, int BOUND>
 __global__ void __launch_bounds__(256, 2) finish_kernel(R* __restrict__ T, const R* __restrict__ Q, const double* __restrict__ u,
                                                      const HeatArgs a, const JacobiCoef<double> k, double* __restrict__ out) {
-    const int h = a.mx / 2;
-    auto U = [&](size_t rowbase, int col) -> double {  // the solution at column col of a row
-        if (!FOLD) return u[rowbase + col];
-        const bool lo = col < h;
-        const int p = lo ? col : a.mx - 1 - col;
-        const double pv = u[rowbase + p], qv = u[rowbase + h + p];
-        return lo ? pv + qv : pv - qv;
-    };
+    auto U = [&](size_t rowbase, int col) -> double { return u[rowbase + col]; };  // the solution
     const size_t plane = (size_t)a.mx * a.my, nn = (size_t)a.n, tplane = nn * nn;
     const int chunks = (a.nz + kFinishZ - 1) / kFinishZ;
     const size_t items = plane * chunks;
@@ -746,13 +756,16 @@ shg_status HeatDirect::solve(const shg_params& p, R* T, const R* Q, double t_inf
     if (e != cudaSuccess) return cuda_fail(e, "heat transform");
     const size_t fitems = (size_t)pl * ((nz + kFinishZ - 1) / kFinishZ);
     const int fb = grid_for(fitems, 256);
-    if (p.boundary == SHG_BOUNDARY_TOP_OPEN) {
-        if (fold) finish_kernel<R, SHG_BOUNDARY_TOP_OPEN, true><<<fb, 256, 0, s>>>(T, Q, X, a, k, out);
-        else finish_kernel<R, SHG_BOUNDARY_TOP_OPEN, false><<<fb, 256, 0, s>>>(T, Q, X, a, k, out);
-    } else {
-        if (fold) finish_kernel<R, SHG_BOUNDARY_OVEN_SURROUNDED, true><<<fb, 256, 0, s>>>(T, Q, X, a, k, out);
-        else finish_kernel<R, SHG_BOUNDARY_OVEN_SURROUNDED, false><<<fb, 256, 0, s>>>(T, Q, X, a, k, out);
+    const double* u = X;
+    if (fold) {
+        unfold_kernel<<<grid_for((size_t)nz * my * h, 256), 256, 0, s>>>(X, Y, (size_t)nz * my, mx);
+        if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "heat solution");
+        u = Y;
     }
+    if (p.boundary == SHG_BOUNDARY_TOP_OPEN)
+        finish_kernel<R, SHG_BOUNDARY_TOP_OPEN><<<fb, 256, 0, s>>>(T, Q, u, a, k, out);
+    else
+        finish_kernel<R, SHG_BOUNDARY_OVEN_SURROUNDED><<<fb, 256, 0, s>>>(T, Q, u, a, k, out);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "heat solution");
     return SHG_OK;
 }

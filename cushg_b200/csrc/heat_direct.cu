@@ -569,7 +569,7 @@ __global__ void unfold_kernel(const double* __restrict__ pq, double* __restrict_
 constexpr int kFinishZ = 16;
 
 template <typename R, int BOUND>
-__global__ void __launch_bounds__(256, 2) finish_kernel(R* __restrict__ T, const R* __restrict__ Q, const double* __restrict__ u,
+__global__ void __launch_bounds__(256, 3) finish_kernel(R* __restrict__ T, const R* __restrict__ Q, const double* __restrict__ u,
                                                      const HeatArgs a, const JacobiCoef<double> k, double* __restrict__ out) {
     auto U = [&](size_t rowbase, int col) -> double { return u[rowbase + col]; };  // the solution
     const size_t plane = (size_t)a.mx * a.my, nn = (size_t)a.n, tplane = nn * nn;

@@ -138,7 +138,7 @@ template <> struct pair_t<float> { using type = float2; };
 template <> struct pair_t<double> { using type = double2; };
 
 template <typename R, int BOUND>
-__global__ void __launch_bounds__(256) jacobi_zb2_kernel(const R* __restrict__ Ti, R* __restrict__ Tf,
+__global__ void __launch_bounds__(256, 5) jacobi_zb2_kernel(const R* __restrict__ Ti, R* __restrict__ Tf,
                                                          const R* __restrict__ Q, JacobiCoef<R> k) {
     using R2 = typename pair_t<R>::type;
     const int n = k.n, nz = k.nz;

@@ -364,6 +364,10 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
             out["thermal_c5"] = thermal_c5_figures()
         except Exception as e:  # the sweep line stands without it
             out["thermal_c5"] = {"error": str(e)[:300]}
+        try:
+            out["thermal_c2"] = thermal_c2_figures()
+        except Exception as e:
+            out["thermal_c2"] = {"error": str(e)[:300]}
     if args.class_side:
         out["config"]["workload"] = f"{len(ps)} instances of {args.class_side}x{args.class_side}, nz = {args.class_nz}"
     if not args.no_cpu_baseline:
@@ -396,6 +400,30 @@ def thermal_c5_figures() -> dict:
             "optical_passes_ms": stats[0].optics_ms,
             "sh_power_w": [st.sh_power for st in stats],
             "dJ_dToven_w_per_k": [float(x) for x in dt]}
+
+
+def thermal_c2_figures() -> dict:
+    """The thermal configuration as stated (128 x 128 x 200 FP64, 20 mm, 20 W, w0 = 40 µm, oven
+    40 °C, max|ΔT| < 1e-6 K inside <= 5 outer iterations), one shg_solve_device call each way:
+    with the reference's Jacobi sweeps (its bits and sweep counts) and with the direct heat
+    solve (each outer iteration at the sweeps' fixed point).  Device times by CUDA events,
+    after an untimed run of each."""
+    import torch
+    from cushg_b200 import shg
+
+    p = P.config_thermal_128()
+    pump = torch.empty((p.ny, p.nx), dtype=torch.complex128, device="cuda")
+    sig = torch.empty_like(pump)
+    out = {"workload": "thermal 128x128x200 FP64, max|dT| < 1e-6 K, <= 5 outer iterations"}
+    for name, q in (("jacobi", p), ("direct", p.replace(heat_solver=P.SHG_HEAT_DIRECT))):
+        shg.solve_device(q, pump, sig)
+        torch.cuda.synchronize()
+        st = shg.solve_device(q, pump, sig)
+        torch.cuda.synchronize()
+        out[name] = {"device_ms": st.device_ms, "heat_ms": st.jacobi_ms, "optics_ms": st.optics_ms,
+                     "jacobi_sweeps": st.jacobi_sweeps, "outer_iterations": st.outer_iterations,
+                     "sh_power_w": st.sh_power}
+    return out
 
 
 def fp64_per_instance(ps, fp32_batch_value: float, count: int = 32) -> dict:

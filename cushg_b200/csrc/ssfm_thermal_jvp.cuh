@@ -276,23 +276,43 @@ __global__ void __launch_bounds__(MpCfg<T, N>::RNT * kJvpPX)
             const size_t gi = (size_t)(y0 + lr) * N + x;
             V p = F4[0][o], q = F4[1][o], pd = F4[2][o], qd = F4[3][o];
             const int h0 = mode == 0 ? 1 : 0, h1 = mode == 2 ? 1 : 2;
+            // the per-voxel optics and their tangents of both half steps and the running
+            // prefixes, read before any arithmetic so that the loads are in flight together
+            // (the march never writes the optics)
+            R pnp[2] = {0, 0}, pns[2] = {0, 0}, pdnp[2] = {0, 0}, pdns[2] = {0, 0}, pdk = 0, pddk = 0;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                if (h < h0 || h >= h1) continue;
+                const size_t gz = (size_t)(s + h) * nn + gi;
+                pnp[h] = __ldg(tnp + gz);
+                pns[h] = __ldg(tns + gz);
+                pdnp[h] = __ldg(dnp + gz);
+                pdns[h] = __ldg(dns + gz);
+                if (h == 1) {
+                    pdk = __ldg(tdk + gz);
+                    pddk = __ldg(ddk + gz);
+                }
+            }
+            double dki = mode == 0 ? 0.0 : dkint[gi], dkid = mode == 0 ? 0.0 : dkind[gi];
 #pragma unroll 1
             for (int h = h0; h < h1; ++h) {
                 const int sl = s + h;
                 const size_t gz = (size_t)sl * nn + gi;
                 if (h == 1) {
-                    dkint[gi] = (mode == 0 ? 0.0 : dkint[gi]) + (double)tdk[gz];
-                    dkind[gi] = (mode == 0 ? 0.0 : dkind[gi]) + (double)ddk[gz];
+                    dki += (double)pdk;
+                    dkid += (double)pddk;
+                    dkint[gi] = dki;
+                    dkind[gi] = dkid;
                 }
-                const double np = (double)tnp[gz], ns = (double)tns[gz];
+                const double np = (double)pnp[h], ns = (double)pns[h];
                 V cf[6], cfd[6];
-                thermal_coef_jvp<T>(d, dkint[gi], dkind[gi], sl, np, ns, (double)dnp[gz], (double)dns[gz], cf, cfd);
-                rk4_jvp<T>(p, q, pd, qd, cf, cfd, hap, has, (T)(0.5 * (d.bf_s * ns)), (T)(0.5 * (d.bf_s * (double)dns[gz])),
+                thermal_coef_jvp<T>(d, dki, dkid, sl, np, ns, (double)pdnp[h], (double)pdns[h], cf, cfd);
+                rk4_jvp<T>(p, q, pd, qd, cf, cfd, hap, has, (T)(0.5 * (d.bf_s * ns)), (T)(0.5 * (d.bf_s * (double)pdns[h])),
                            dz6);
                 if (h == 0 && jd.q_dot) {
                     // tangent of kernelSetQ for slice s after its step:
                     // Q = q_p n_p |P|^2 + q_s n_s |S|^2 + βs (q_h n_s |S|^2)^2
-                    const double npd = (double)dnp[gz], nsd = (double)dns[gz];
+                    const double npd = (double)pdnp[h], nsd = (double)pdns[h];
                     const double ap2 = (double)p.x * p.x + (double)p.y * p.y;
                     const double as2 = (double)q.x * q.x + (double)q.y * q.y;
                     const double ap2d = 2.0 * ((double)p.x * pd.x + (double)p.y * pd.y);

@@ -269,31 +269,46 @@ __global__ void __launch_bounds__(MpCfg<T, N>::RNT * kJvpPX)
         const int f0 = part * 4 / PX, f1 = (part + 1) * 4 / PX;
         if (mode != 0) r2_pass(n1, lr, true, f0, f1);
         __syncthreads();
+        const int h0 = mode == 0 ? 1 : 0, h1 = mode == 2 ? 1 : 2;
+        // the per-voxel optics and their tangents of both half steps and the running prefixes
+        // of point k, read before any arithmetic so that the loads are in flight together
+        // (the march never writes the optics); the next point's are read before this one's
+        // arithmetic starts
+        struct Pre {
+            R np[2], ns[2], dnp[2], dns[2], dk, ddk;
+            double dki, dkid;
+        };
+        auto fetch = [&](int k) {
+            Pre f;
+            const size_t gi = (size_t)(y0 + lr) * N + n1 + 16 * k;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                f.np[h] = f.ns[h] = f.dnp[h] = f.dns[h] = 0;
+                if (h < h0 || h >= h1) continue;
+                const size_t gz = (size_t)(s + h) * nn + gi;
+                f.np[h] = __ldg(tnp + gz);
+                f.ns[h] = __ldg(tns + gz);
+                f.dnp[h] = __ldg(dnp + gz);
+                f.dns[h] = __ldg(dns + gz);
+            }
+            f.dk = h1 == 2 ? __ldg(tdk + (size_t)(s + 1) * nn + gi) : (R)0;
+            f.ddk = h1 == 2 ? __ldg(ddk + (size_t)(s + 1) * nn + gi) : (R)0;
+            f.dki = mode == 0 ? 0.0 : dkint[gi];
+            f.dkid = mode == 0 ? 0.0 : dkind[gi];
+            return f;
+        };
+        Pre nxt;
+        if (part < R2) nxt = fetch(part);
 #pragma unroll 1
         for (int k = part; k < R2; k += PX) {
             const int x = n1 + 16 * k;
             const int o = sidx<N, R2, SW>(lr, x);
             const size_t gi = (size_t)(y0 + lr) * N + x;
+            const Pre cur = nxt;
+            if (k + PX < R2) nxt = fetch(k + PX);
             V p = F4[0][o], q = F4[1][o], pd = F4[2][o], qd = F4[3][o];
-            const int h0 = mode == 0 ? 1 : 0, h1 = mode == 2 ? 1 : 2;
-            // the per-voxel optics and their tangents of both half steps and the running
-            // prefixes, read before any arithmetic so that the loads are in flight together
-            // (the march never writes the optics)
-            R pnp[2] = {0, 0}, pns[2] = {0, 0}, pdnp[2] = {0, 0}, pdns[2] = {0, 0}, pdk = 0, pddk = 0;
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                if (h < h0 || h >= h1) continue;
-                const size_t gz = (size_t)(s + h) * nn + gi;
-                pnp[h] = __ldg(tnp + gz);
-                pns[h] = __ldg(tns + gz);
-                pdnp[h] = __ldg(dnp + gz);
-                pdns[h] = __ldg(dns + gz);
-                if (h == 1) {
-                    pdk = __ldg(tdk + gz);
-                    pddk = __ldg(ddk + gz);
-                }
-            }
-            double dki = mode == 0 ? 0.0 : dkint[gi], dkid = mode == 0 ? 0.0 : dkind[gi];
+            const R pdk = cur.dk, pddk = cur.ddk;
+            double dki = cur.dki, dkid = cur.dkid;
 #pragma unroll 1
             for (int h = h0; h < h1; ++h) {
                 const int sl = s + h;
@@ -304,15 +319,15 @@ __global__ void __launch_bounds__(MpCfg<T, N>::RNT * kJvpPX)
                     dkint[gi] = dki;
                     dkind[gi] = dkid;
                 }
-                const double np = (double)pnp[h], ns = (double)pns[h];
+                // this half step's values (selects, so that the rolled loop indexes no array)
+                const double np = (double)(h ? cur.np[1] : cur.np[0]), ns = (double)(h ? cur.ns[1] : cur.ns[0]);
+                const double npd = (double)(h ? cur.dnp[1] : cur.dnp[0]), nsd = (double)(h ? cur.dns[1] : cur.dns[0]);
                 V cf[6], cfd[6];
-                thermal_coef_jvp<T>(d, dki, dkid, sl, np, ns, (double)pdnp[h], (double)pdns[h], cf, cfd);
-                rk4_jvp<T>(p, q, pd, qd, cf, cfd, hap, has, (T)(0.5 * (d.bf_s * ns)), (T)(0.5 * (d.bf_s * (double)pdns[h])),
-                           dz6);
+                thermal_coef_jvp<T>(d, dki, dkid, sl, np, ns, npd, nsd, cf, cfd);
+                rk4_jvp<T>(p, q, pd, qd, cf, cfd, hap, has, (T)(0.5 * (d.bf_s * ns)), (T)(0.5 * (d.bf_s * nsd)), dz6);
                 if (h == 0 && jd.q_dot) {
                     // tangent of kernelSetQ for slice s after its step:
                     // Q = q_p n_p |P|^2 + q_s n_s |S|^2 + βs (q_h n_s |S|^2)^2
-                    const double npd = (double)pdnp[h], nsd = (double)pdns[h];
                     const double ap2 = (double)p.x * p.x + (double)p.y * p.y;
                     const double as2 = (double)q.x * q.x + (double)q.y * q.y;
                     const double ap2d = 2.0 * ((double)p.x * pd.x + (double)p.y * pd.y);

@@ -273,14 +273,23 @@ __global__ void __launch_bounds__(MpCfg<T, N>::row_threads(THERM))
                 k0 = R2 & ~1;
             }
         }
+        // thermal: each point's optics and Δk prefix are loaded before the previous point's
+        // arithmetic (thermal_pre one point ahead)
+        auto pre_of = [&](int k) {
+            const size_t g = (size_t)(y0 + lr) * N + n1 + 16 * k;
+            return thermal_pre<T, THERM>(d, mode, s, g, (size_t)N * N, THERM ? dkint + g : nullptr);
+        };
+        ThermPre<T> nxt = pre_of(k0 + part < R2 ? k0 + part : 0);
 #pragma unroll 1
         for (int k = k0 + part; k < R2; k += PX) {
             const int x = n1 + 16 * k;
             const int o = sidx<N, R2, SW>(lr, x);
             const size_t g = (size_t)(y0 + lr) * N + x;
+            const ThermPre<T> cur = nxt;
+            if (k + PX < R2) nxt = pre_of(k + PX);
             V p = Ps[o], q = Ss[o];
             boundary_point<T, THERM>(d, mode, s, g, (size_t)N * N, p, q, coef, coef + 6, hap, has, qs, dz6,
-                                     THERM ? dkint + g : nullptr, acc_s, acc_p);
+                                     THERM ? dkint + g : nullptr, acc_s, acc_p, cur);
             if (mode != 2) {
                 Ps[o] = p;
                 Ss[o] = q;

@@ -317,43 +317,72 @@ __device__ __forceinline__ void thermal_coef(const InstDesc& d, double dki, int 
     }
 }
 
+// The per-voxel values a thermal boundary_point reads from global memory, fetched apart from
+// its arithmetic so that a caller can issue the next point's loads before this point's work:
+// n_p and n_s of the slices of both half steps, Δk of slice s + 1 (when the second half step
+// runs), and the point's running Δk prefix through slice s.
+template <typename R>
+struct ThermPre {
+    R np[2], ns[2], dk;
+    double dki;
+};
+
+template <typename T, bool THERM>
+__device__ __forceinline__ ThermPre<T> thermal_pre(const InstDesc& d, int mode, int s, size_t g, size_t nn,
+                                                   const double* dki) {
+    ThermPre<T> t;
+    t.np[0] = t.np[1] = t.ns[0] = t.ns[1] = t.dk = (T)0;
+    t.dki = 0.0;
+    if constexpr (THERM) {
+        const T* tnp = reinterpret_cast<const T*>(d.t_np);
+        const T* tns = reinterpret_cast<const T*>(d.t_ns);
+        const T* tdk = reinterpret_cast<const T*>(d.t_dk);
+        const int h0 = mode == 0 ? 1 : 0, h1 = mode == 2 ? 1 : 2;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            if (h < h0 || h >= h1) continue;
+            const size_t gz = (size_t)(s + h) * nn + g;
+            t.np[h] = __ldg(tnp + gz);
+            t.ns[h] = __ldg(tns + gz);
+        }
+        if (h1 == 2) t.dk = __ldg(tdk + (size_t)(s + 1) * nn + g);
+        if (mode != 0) t.dki = *dki;
+    }
+    return t;
+}
+
 // The pointwise work of a row pass at grid point g (index y*n + x in the plane): the RK4
 // applications around a step boundary, h = 0 the second half of step s and h = 1 the first
 // half of step s+1 (Solver.h:267-273); mode 0 (s = -1, the first pass) runs h = 1 only, mode
 // 2 (the last step) h = 0 only.  With them: the heat source of slice s (thermal), the
 // per-slice record of the fields before step s+1 and the outputs after step out_after with
-// their power sums.  dki: this point's running Δk prefix (thermal), else unused.
+// their power sums.  Thermal: pre holds the point's optics and running Δk prefix
+// (thermal_pre), and dki receives the prefix through slice s + 1.
 template <typename T, bool THERM>
 __device__ __forceinline__ void boundary_point(const InstDesc& d, int mode, int s, size_t g, size_t nn, cx<T>& p,
                                                cx<T>& q, const cx<T>* cf_prev, const cx<T>* cf_next, T hap, T has,
-                                               T qs, T dz6, double* dki, double& acc_s, double& acc_p) {
+                                               T qs, T dz6, double* dki, double& acc_s, double& acc_p,
+                                               const ThermPre<T>& pre) {
     using V = cx<T>;
     using R = T;  // real type of the thermal 3D arrays
     const R* tnp = reinterpret_cast<const R*>(d.t_np);
     const R* tns = reinterpret_cast<const R*>(d.t_ns);
-    const R* tdk = reinterpret_cast<const R*>(d.t_dk);
     R* tq = reinterpret_cast<R*>(d.t_q);
     const int h0 = mode == 0 ? 1 : 0, h1 = mode == 2 ? 1 : 2;
-    // thermal: the per-voxel optics of both half steps, read before any arithmetic through
-    // the read-only path (the march never writes them), so that they are in flight together
-    R pre_np[2] = {0, 0}, pre_ns[2] = {0, 0}, pre_dk = 0;
-    if constexpr (THERM) {
-        for (int h = h0; h < h1; ++h) {
-            const size_t gz = (size_t)(s + h) * nn + g;
-            pre_np[h] = __ldg(tnp + gz);
-            pre_ns[h] = __ldg(tns + gz);
-            if (h == 1) pre_dk = __ldg(tdk + gz);
-        }
-    }
+    double dk_run = pre.dki;  // thermal: the running Δk prefix through this half step's slice
 #pragma unroll 1
     for (int h = h0; h < h1; ++h) {
         const int sl = s + h;  // slice of this half step
         if constexpr (THERM) {
             const size_t gz = (size_t)sl * nn + g;
-            if (h == 1) *dki = (mode == 0 ? 0.0 : *dki) + (double)pre_dk;
-            const double np = (double)pre_np[h], ns = (double)pre_ns[h];
+            if (h == 1) {
+                dk_run += (double)pre.dk;
+                *dki = dk_run;
+            }
+            // this half step's optics (selects, so that the rolled loop indexes no array)
+            const double np = (double)(h ? pre.np[1] : pre.np[0]), ns = (double)(h ? pre.ns[1] : pre.ns[0]);
             V cf[6];
-            thermal_coef<T>(d, *dki, sl, np, ns, cf);
+            thermal_coef<T>(d, dk_run, sl, np, ns, cf);
             rk4_point<T>(p, q, cf, hap, has, (T)(0.5 * (d.bf_s * ns)), dz6);
             if (h == 0 && tq) {
                 // kernelSetQ (Tfield.h:260-276) for slice s, after its step
@@ -363,6 +392,7 @@ __device__ __forceinline__ void boundary_point(const InstDesc& d, int mode, int 
             }
         } else {
             (void)dki;
+            (void)pre;
             rk4_point<T>(p, q, h ? cf_next : cf_prev, hap, has, qs, dz6);
         }
         if (h == 0 && s + 1 < d.nslices) {
@@ -524,8 +554,10 @@ __global__ void __launch_bounds__(NT, MINB)
                             const int o = sidx<N, R2, SW>(lr, x);
                             const size_t g = (size_t)(crank + C * lr) * N + x;
                             V p = Ps[o], q = Ss[o];
+                            double* dkp = THERM ? &dkint[lr * N + x] : nullptr;
+                            const ThermPre<T> pre = thermal_pre<T, THERM>(d, mode, s, g, (size_t)N * N, dkp);
                             boundary_point<T, THERM>(d, mode, s, g, (size_t)N * N, p, q, cf_prev, cf_next, hap, has,
-                                                     qs, dz6, THERM ? &dkint[lr * N + x] : nullptr, acc_s, acc_p);
+                                                     qs, dz6, dkp, acc_s, acc_p, pre);
                             if (mode != 2) {
                                 Ps[o] = p;
                                 Ss[o] = q;

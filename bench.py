@@ -592,7 +592,9 @@ def run_thermal(args) -> dict:
         p = p.replace(max_sweeps=args.thermal_max_sweeps)
     direct = args.heat_solver == "direct"
     p = p.replace(jacobi_block=args.jacobi_block, precision=args.thermal_precision or 64,
-                  heat_solver=P.SHG_HEAT_DIRECT if direct else P.SHG_HEAT_JACOBI)
+                  heat_solver=P.SHG_HEAT_DIRECT if direct else P.SHG_HEAT_JACOBI,
+                  march={"auto": P.SHG_MARCH_AUTO, "fused": P.SHG_MARCH_FUSED,
+                         "multipass": P.SHG_MARCH_MULTIPASS}[args.march])
     cdt = torch.complex128 if p.precision == 64 else torch.complex64
     if direct:  # operator transforms (computed once per process) and kernels before timing
         wp = torch.empty((p.ny, p.nx), dtype=cdt, device="cuda")
@@ -899,6 +901,8 @@ def main() -> int:
     ap.add_argument("--jacobi-sweeps", type=int, default=400)
     ap.add_argument("--thermal-side", type=int, default=0)
     ap.add_argument("--thermal-nz", type=int, default=0)
+    ap.add_argument("--march", default="auto", choices=["auto", "fused", "multipass"],
+                    help="optical march of the thermal workload")
     ap.add_argument("--checkpoint-every", type=int, default=0,
                     help="adjoint checkpoint interval (0: the library's choice)")
     ap.add_argument("--adjoint-nz", type=int, default=0, help="adjoint workload with this nz (profiling case)")

@@ -1,6 +1,7 @@
 // ssfm_multipass.cu — variants and host sequence of the multi-pass SSFM march
-// (ssfm_multipass.cuh): N = 512 (plain and thermal, FP32 and FP64) and N = 256 (plain and
-// thermal, the side where it can be checked against the fused cluster march).
+// (ssfm_multipass.cuh): N = 512 (plain and thermal, FP32 and FP64), N = 256 (plain and
+// thermal, the side where it can be checked against the fused cluster march) and N = 128
+// (thermal).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -57,6 +58,7 @@ const PlainVariant kTable[] = {
     SHG_MP_VARIANT(float, 32, 256, false),  SHG_MP_VARIANT(double, 64, 256, false),
     SHG_MP_VARIANT(float, 32, 512, true),   SHG_MP_VARIANT(double, 64, 512, true),
     SHG_MP_VARIANT(float, 32, 256, true),   SHG_MP_VARIANT(double, 64, 256, true),
+    SHG_MP_VARIANT(float, 32, 128, true),   SHG_MP_VARIANT(double, 64, 128, true),
 };
 
 }  // namespace

@@ -42,6 +42,12 @@ const PlainVariant* find_plain_variant(int precision, int n, int thermal, int ma
     });
     if (march == SHG_MARCH_FUSED) return fused;
     if (march == SHG_MARCH_MULTIPASS) return multi;
+    // automatic: a thermal run marches on the multi-pass kernels where they are built.  One
+    // thermal instance's fused cluster holds 1-16 SMs for every optical pass, which lies on the
+    // run's critical path between two heat solves; the multi-pass launches spread each step
+    // over the GPU (configuration 2's optical passes 47.6 -> 21.3 ms, FP64).  Plain runs, which
+    // come in batches that fill the GPU with clusters, keep the fused march.
+    if (th && multi) return multi;
     return fused ? fused : multi;
 }
 

@@ -115,9 +115,12 @@ typedef struct shg_params {
      * sweep per launch, 2..4 = that many through the TMA-staged blocked kernel.  Every setting gives the same
      * temperatures bit for bit; the checked sweep of each window always runs alone. */
     int32_t jacobi_block;
-    /* Which SSFM march to run (SHG_MARCH_*): automatic picks the fused cluster march where
-     * one is built for the grid side (planes in shared memory, sides <= 256) and the
-     * multi-pass march otherwise (planes in global memory, side 512). */
+    /* Which SSFM march to run (SHG_MARCH_*): automatic picks, for plain runs, the fused
+     * cluster march where one is built for the grid side (planes in shared memory, sides
+     * <= 256) and the multi-pass march otherwise (planes in global memory, side 512); for
+     * thermal runs, the multi-pass march where one is built (sides 128, 256, 512), since a
+     * single instance's optical pass then spreads over the GPU, and the fused march
+     * otherwise. */
     int32_t march;
     /* How each outer iteration of a thermal run solves the heat equation (SHG_HEAT_*):
      * Jacobi sweeps as the reference runs them (default), or the sweeps' fixed point computed
@@ -155,7 +158,8 @@ enum {
 };
 
 enum {
-    SHG_MARCH_AUTO = 0,     /* fused where built (the autotuner's choice if it ran), else multi-pass */
+    SHG_MARCH_AUTO = 0,     /* plain runs: fused where built (the autotuner's choice if it ran), else
+                               multi-pass; thermal runs: multi-pass where built, else fused */
     SHG_MARCH_FUSED = 1,     /* one thread-block cluster per instance, fields in shared memory */
     SHG_MARCH_MULTIPASS = 2  /* fields in global memory, a row and a column launch per step */
 };

@@ -41,9 +41,10 @@ def test_multipass_equals_fused(precision):
     assert abs(a.sh_power - b.sh_power) <= (1e-12 if precision == 64 else 1e-5) * a.sh_power
 
 
+@pytest.mark.parametrize("n", [256, 128])
 @pytest.mark.parametrize("precision", [64, 32])
-def test_multipass_thermal_equals_fused(precision):
-    p = P.workload(256, 10, 4000.0, 20.0, 25.0, 2000.0, 30.0, precision=precision, thermal=1)
+def test_multipass_thermal_equals_fused(precision, n):
+    p = P.workload(n, 10, 4000.0, 20.0, 25.0, 2000.0, 30.0, precision=precision, thermal=1)
     p.alpha_p, p.alpha_s, p.beta_s = 2e-5, 1e-4, 1e-3
     p.max_outer = 2
     p.check_every = 50

@@ -88,6 +88,18 @@ def test_march_selector_is_validated():
     assert shg.check_params(p64.replace(march=P.SHG_MARCH_FUSED)) == P.SHG_OK
 
 
+@pytest.mark.parametrize("n,fused,multipass", [(64, True, False), (128, True, True), (256, True, True),
+                                               (512, False, True)])
+def test_thermal_marches_built_per_side(n, fused, multipass):
+    """Thermal runs: fused cluster marches for sides up to 256, multi-pass marches at 128, 256
+    and 512 (the automatic choice where built); a side with neither is unsupported."""
+    p = P.workload(n, 9, 6000.0, 5.0, 30.0, 3000.0, 30.0, precision=64, thermal=1)
+    ok = lambda built: P.SHG_OK if built else P.SHG_ERR_UNSUPPORTED  # noqa: E731
+    assert shg.check_params(p.replace(march=P.SHG_MARCH_FUSED)) == ok(fused)
+    assert shg.check_params(p.replace(march=P.SHG_MARCH_MULTIPASS)) == ok(multipass)
+    assert shg.check_params(p) == P.SHG_OK
+
+
 def test_fixed_sweep_rule_needs_counts():
     p = P.config_thermal_128().replace(conv_rule=P.SHG_CONV_FIXED, max_sweeps=0)
     assert shg.check_params(p) == P.SHG_ERR_INVALID

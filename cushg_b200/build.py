@@ -14,6 +14,7 @@ import argparse
 import concurrent.futures as cf
 import glob
 import os
+import shutil
 import subprocess
 import sys
 
@@ -29,6 +30,12 @@ NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
          "-I", os.path.join(ROOT, "include")]
+
+
+def _cuda_root() -> str:
+    """The CUDA toolkit that holds nvcc (its include/ and lib64/ serve the command-line tool)."""
+    nvcc = shutil.which(NVCC) or "/usr/local/cuda/bin/nvcc"
+    return os.path.dirname(os.path.dirname(os.path.realpath(nvcc)))
 
 
 def _headers() -> list[str]:
@@ -65,8 +72,10 @@ def build(force: bool = False, verbose: bool = False) -> str:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
     if force or _stale(CLI, [CLI_SRC, LIB, os.path.join(ROOT, "include", "shg.h")]):
         cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
-        cmd = [cxx, "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), CLI_SRC, "-o", CLI, "-L", PKG,
-               "-lshg_b200", "-Wl,-rpath,$ORIGIN"]
+        cuda = _cuda_root()
+        cmd = [cxx, "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), "-I", os.path.join(cuda, "include"),
+               CLI_SRC, "-o", CLI, "-L", PKG, "-lshg_b200", "-L", os.path.join(cuda, "lib64"), "-lcudart",
+               "-Wl,-rpath,$ORIGIN"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"CLI build failed:\n{r.stdout}\n{r.stderr}")

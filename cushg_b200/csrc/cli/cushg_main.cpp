@@ -21,8 +21,10 @@
 // is the sweep script src/cuSHG.sh:43-105: the three comma-separated lists play ARG1, ARG2
 // and ARG3, every combination is a run, and each run's files go into the script's folder
 // sPPLT_P_<power>_W_T1_<temperature>_WAIST_<waist>/ with its report in <folder>/<folder>.txt.
-// Plain runs that keep only the last slice go through one batched call (shg_solve_batch);
-// the others run one after another.
+// Runs that keep only the last slice go through one batched call: shg_solve_batch for plain
+// runs, shg_thermal_batch for thermal runs (their outer iterations in lockstep; if the batch
+// does not fit in device memory the points run one after another).  With every slice kept,
+// the points run one after another.
 #include <sys/stat.h>
 #include <sys/time.h>
 
@@ -35,6 +37,8 @@
 #include <sstream>
 #include <string>
 #include <vector>
+
+#include <cuda_runtime.h>
 
 #include "../../../include/shg.h"
 
@@ -112,6 +116,67 @@ int run(const shg_params& p, bool save_only_last, bool save_temperature, const s
     }
     if (!T.empty()) save_tensor(T.data(), p.nx, p.ny, p.nz, dir + "Tfinal");
     *line = report(p, st);
+    return 0;
+}
+
+// The thermal points of a sweep that keeps only the last slice, as one shg_thermal_batch call
+// on device buffers; each point's files as run() writes them.  Returns 0, 1 on an error, or -1
+// when the batch's buffers or workspace do not fit in device memory (the caller then runs the
+// points one by one).
+template <typename R>
+int thermal_sweep_batch(const std::vector<shg_params>& ps, const std::vector<std::string>& dirs, bool save_temperature,
+                        std::vector<std::string>* lines) {
+    const size_t n = ps.size();
+    const shg_params& p0 = ps[0];
+    const size_t plane = (size_t)p0.nx * p0.ny, vol = plane * p0.nz;
+    std::vector<void*> bufs;
+    auto release = [&]() {
+        for (void* b : bufs) cudaFree(b);
+        bufs.clear();
+    };
+    auto alloc = [&](size_t bytes, void** out) {
+        if (cudaMalloc(out, bytes) != cudaSuccess) {
+            cudaGetLastError();  // clear the allocation error; the caller falls back
+            return false;
+        }
+        bufs.push_back(*out);
+        return true;
+    };
+    std::vector<void*> pp(n, nullptr), sp(n, nullptr), tp(n, nullptr);
+    for (size_t i = 0; i < n; ++i) {
+        if (!alloc(2 * sizeof(R) * plane, &pp[i]) || !alloc(2 * sizeof(R) * plane, &sp[i]) ||
+            (save_temperature && !alloc(sizeof(R) * vol, &tp[i]))) {
+            release();
+            return -1;
+        }
+    }
+    std::vector<shg_stats> st(n);
+    const shg_status rc = shg_thermal_batch(ps.data(), (int32_t)n, pp.data(), sp.data(),
+                                            save_temperature ? tp.data() : nullptr, st.data(), nullptr, nullptr);
+    if (rc == SHG_ERR_NOMEM) {
+        release();
+        return -1;
+    }
+    if (rc != SHG_OK) {
+        std::cerr << "cushg: " << shg_status_string(rc) << ": " << shg_last_error() << std::endl;
+        release();
+        return 1;
+    }
+    std::vector<R> pump(2 * plane), sig(2 * plane), T(save_temperature ? vol : 0);
+    for (size_t i = 0; i < n; ++i) {
+        if (cudaMemcpy(pump.data(), pp[i], 2 * sizeof(R) * plane, cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(sig.data(), sp[i], 2 * sizeof(R) * plane, cudaMemcpyDeviceToHost) != cudaSuccess ||
+            (save_temperature && cudaMemcpy(T.data(), tp[i], sizeof(R) * vol, cudaMemcpyDeviceToHost) != cudaSuccess)) {
+            std::cerr << "cushg: copying the results back failed" << std::endl;
+            release();
+            return 1;
+        }
+        save_complex(pump.data(), p0.nx, p0.ny, dirs[i] + "Pump_out");
+        save_complex(sig.data(), p0.nx, p0.ny, dirs[i] + "Signal_out");
+        if (save_temperature) save_tensor(T.data(), p0.nx, p0.ny, p0.nz, dirs[i] + "Tfinal");
+        (*lines)[i] = report(ps[i], st[i]) + " (batched thermal sweep of " + std::to_string(n) + " runs)";
+    }
+    release();
     return 0;
 }
 
@@ -249,7 +314,20 @@ int sweep(int argc, char** argv) {
             lines[i] = o.str();
         }
     } else {
-        for (size_t i = 0; i < pts.size(); ++i) {
+        int batched = -1;
+        if (save_only_last && base.thermal && !pts.empty()) {
+            std::vector<shg_params> ps;
+            std::vector<std::string> dirs;
+            for (const Point& pt : pts) {
+                mkdir(pt.folder.c_str(), 0755);
+                ps.push_back(pt.p);
+                dirs.push_back(pt.folder + "/");
+            }
+            batched = base.precision == 32 ? thermal_sweep_batch<float>(ps, dirs, save_temperature, &lines)
+                                           : thermal_sweep_batch<double>(ps, dirs, save_temperature, &lines);
+            if (batched > 0) return batched;
+        }
+        for (size_t i = 0; batched != 0 && i < pts.size(); ++i) {
             mkdir(pts[i].folder.c_str(), 0755);
             const int rc = base.precision == 32
                                ? run<float>(pts[i].p, save_only_last, save_temperature, pts[i].folder + "/", &lines[i])

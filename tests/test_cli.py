@@ -130,6 +130,33 @@ def test_cli_sweep_mode_writes_the_script_folders(tmp_path):
 
 
 @pytest.mark.gpu
+def test_cli_thermal_sweep_runs_as_one_batch(tmp_path):
+    """A thermal sweep that keeps only the last slice runs its points as one shg_thermal_batch
+    call (outer iterations in lockstep); every point's fields and temperature files equal the
+    single run of that point, and the report says the run was batched."""
+    base = P.workload(32, 12, 4000.0, 20.0, 25.0, 2000.0, 30.0, precision=64, thermal=1)
+    base.alpha_p, base.alpha_s, base.beta_s = 2e-5, 1e-4, 1e-3
+    base.max_outer = 2
+    base.check_every = 500
+    extra = cli_args(base)[6:]  # every option, as for a single run
+    r = subprocess.run([CLI, "--sweep", "10,20", "25", "30,33", "1", "1"] + extra, cwd=tmp_path,
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert "batched thermal sweep of 4 runs" in r.stdout
+    for pw in ("10", "20"):
+        for t in ("30", "33"):
+            folder = tmp_path / f"sPPLT_P_{pw}_W_T1_{t}_WAIST_25"
+            p = base.replace(power=float(pw), temp=float(t), t_peltier=float(t))
+            ref = shg.solve(p, want_temperature=True)
+            got = read_matrix(folder / "Signal_out_r.dat") + 1j * read_matrix(folder / "Signal_out_i.dat")
+            assert np.array_equal(got, ref.signal), (pw, t)
+            gotp = read_matrix(folder / "Pump_out_r.dat") + 1j * read_matrix(folder / "Pump_out_i.dat")
+            assert np.array_equal(gotp, ref.pump), (pw, t)
+            for z in (0, p.nz - 1):  # Tfinal files: 6 significant digits, as the reference writes them
+                assert np.allclose(read_matrix(folder / f"Tfinal_{z}.dat"), ref.temperature[z], rtol=1e-5, atol=0)
+
+
+@pytest.mark.gpu
 def test_cli_second_crystal_matches_the_library(tmp_path):
     """--crystal ppln selects MgO:PPLN: the .dat files hold the fields shg_solve gives for the
     same parameters (written at 20 significant digits)."""

@@ -45,7 +45,7 @@ const PlainVariant* find_plain_variant(int precision, int n, int thermal, int ma
     // automatic: a thermal run marches on the multi-pass kernels where they are built.  One
     // thermal instance's fused cluster holds 1-16 SMs for every optical pass, which lies on the
     // run's critical path between two heat solves; the multi-pass launches spread each step
-    // over the GPU (configuration 2's optical passes 47.6 -> 21.3 ms, FP64).  Plain runs, which
+    // over the GPU (the optical passes of a 128 x 128 x 200 FP64 run: 47.6 -> 21.3 ms).  Plain runs, which
     // come in batches that fill the GPU with clusters, keep the fused march.
     if (th && multi) return multi;
     return fused ? fused : multi;

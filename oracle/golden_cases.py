@@ -90,7 +90,7 @@ CASES = {
 
 
 def _thermal_c2() -> P.ShgParams:
-    # configuration 2 at its stated size: 128 x 128 x 200, 20 mm, 20 W, w0 = 40 µm, oven 40 °C,
+    # the thermal workload at its stated size: 128 x 128 x 200, 20 mm, 20 W, w0 = 40 µm, oven 40 °C,
     # 5 outer iterations, under the reference's own stopping rule (the reference binary has no
     # other): residual check every 5000 sweeps against 5e-4 / TSIZE, stagnation exit
     return P.config_thermal_128().replace(conv_rule=P.SHG_CONV_REFERENCE, jacobi_tol=0.0, check_every=5000,
@@ -98,13 +98,14 @@ def _thermal_c2() -> P.ShgParams:
 
 
 def _plain_c4() -> P.ShgParams:
-    # configuration 4's forward at its stated size: 256 x 256, nz = 400, 20 mm, 30 W, w0 = 35 µm,
+    # the gradient workload's forward at its stated size: 256 x 256, nz = 400, 20 mm, 30 W, w0 = 35 µm,
     # focus at 0.4 L, 30 °C (the reference has no per-slice poling phase: uniform grating)
     return P.config_adjoint().replace(precision=64)
 
 
-# Full-size configurations 2 and 4, kept apart from CASES because the CPU oracle needs
-# minutes for them.  Configuration 2's temperature grid (26 MB) is too large for a fixture,
+# The 128 x 128 x 200 thermal and 256 x 256 x 400 plain workloads at full size, kept apart from
+# CASES because the CPU oracle needs minutes for them.  The thermal run's temperature grid
+# (26 MB) is too large for a fixture,
 # so make_golden.py keeps the slices T_SLICES plus FP64 sums over all voxels.
 FULL_CASES = {
     "thermal64_c2": {"precision": 64, "params": _d(_thermal_c2())},

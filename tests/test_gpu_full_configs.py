@@ -1,21 +1,21 @@
 """The benchmark configurations at their stated sizes, through the C ABI.
 
-* Configuration 2 (thermal 128 x 128 x 200, FP64, 5 outer iterations under the reference's
-  stopping rule) and configuration 4's forward (256 x 256, nz = 400, FP64) against the
+* The thermal run (128 x 128 x 200, FP64, 5 outer iterations under the reference's
+  stopping rule) and the gradient workload's forward (256 x 256, nz = 400, FP64) against the
   reference's own outputs (tests/golden/thermal64_c2.npz, plain64_c4.npz, made by
   oracle/make_golden.py from the binaries of oracle/ref_build.py).  Tolerances: fields
   relative L2 <= 1e-10 and SH power <= 1e-12 (plain); temperatures |ΔT| <= 1e-9 K on the
   stored slices and identical Jacobi sweep and outer-iteration counts (thermal).  The thermal
-  SH output of configuration 2 (oven 13 K off phase matching) is a remainder of a field that
+  SH output of the 128 x 128 x 200 thermal run (oven 13 K off phase matching) is a remainder of a field that
   grew and cancelled along the crystal, 1e-15 of the pump's magnitude: it inherits the last-bit
   differences of 105 004 Jacobi sweeps (through n(T) and Δk(T)) and of cuFFT against this
   library's transform amplified by that cancellation, so its field and power are held to
   1e-9 (measured 2.2e-10), the pump to 1e-10.
-* Configuration 4's adjoint (256 x 256, nz = 400, 30 W, w0 = 35 µm, focus 0.4 L, 30 °C, a
+* The adjoint of the 256 x 256 x 400 gradient workload (nz = 400, 30 W, w0 = 35 µm, focus 0.4 L, 30 °C, a
   399-entry poling phase from N(0, 0.1 rad), checkpoints every 20 steps) against FP64
   central differences with h = 1e-6 relative, and the FP32 adjoint against the FP64 adjoint,
   each within 1e-4.
-* A stride sample of configuration 3's 256-instance sweep, in FP64 through the batched
+* A stride sample of the 256-instance sweep, in FP64 through the batched
   march, against the CPU oracle (fields <= 1e-10, SH power <= 1e-12).
 """
 import json
@@ -42,7 +42,7 @@ def load(name):
     return z, json.loads(str(z["meta"]))
 
 
-def test_configuration_4_forward_matches_reference():
+def test_plain_256x256x400_forward_matches_reference():
     z, meta = load("plain64_c4")
     p = G.params_of("plain64_c4")
     assert (p.nx, p.nz, p.precision) == (256, 400, 64)
@@ -54,7 +54,7 @@ def test_configuration_4_forward_matches_reference():
     assert abs(r.sh_power - ref_power) / ref_power <= 1e-12
 
 
-def test_configuration_2_thermal_matches_reference():
+def test_thermal_128x128x200_matches_reference():
     z, meta = load("thermal64_c2")
     p = G.params_of("thermal64_c2")
     assert (p.nx, p.nz, p.precision, p.thermal, p.max_outer) == (128, 200, 64, 1, 5)
@@ -90,7 +90,7 @@ def fd(f, x, h):
     return (f(x + h) - f(x - h)) / (2 * h)
 
 
-def test_configuration_4_adjoint_matches_finite_differences_and_fp64():
+def test_adjoint_256x256x400_matches_finite_differences_and_fp64():
     p = adjoint_case(64)
     pol = poling(p)
     g = shg.grad(p, pol, checkpoint_every=20)
@@ -118,7 +118,7 @@ def test_configuration_4_adjoint_matches_finite_differences_and_fp64():
     assert np.abs(np.asarray(g32["d_poling"]) - np.asarray(g["d_poling"])).max() <= 1e-4 * scale
 
 
-def test_configuration_3_fp64_stride_sample_matches_oracle():
+def test_sweep_fp64_stride_sample_matches_oracle():
     ps = [p.replace(precision=64) for p in P.config_sweep(256, seed=0)][::16]
     assert len(ps) == 16 and {p.nx for p in ps} == {64, 128, 192, 256}
     import torch

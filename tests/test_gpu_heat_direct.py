@@ -2,7 +2,7 @@
 
 * Against the fixed point of the oracle's Jacobi sweep (dense, small grids): max |ΔT| <= 1e-9 K
   in FP64; in FP32 the stored temperature is that fixed point rounded (<= 1e-5 K at 40 °C).
-* At configuration 2's grid (128 x 128 x 200, FP64) and at 512 x 512 x 64 FP32: the solution is
+* On the 128 x 128 x 200 FP64 thermal grid and at 512 x 512 x 64 FP32: the solution is
   a fixed point of the library's own Jacobi sweep (the kernel pinned bit for bit to the
   reference), max |J(T) - T| <= 1e-10 K, and the FP64 residual the solve reports agrees.
 * A thermal run with the direct solver equals the Jacobi thermal run converged to 1e-12 K
@@ -163,8 +163,8 @@ def test_large_thermal_instance_fp32_against_fp64():
     assert pw <= 2e-5
 
 
-def test_configuration_2_direct_against_reference_jacobi():
-    """Configuration 2 (128 x 128 x 200 FP64, 5 outer iterations, Jacobi to max |ΔT| < 1e-6 K)
+def test_thermal_128x128x200_direct_against_reference_jacobi():
+    """The 128 x 128 x 200 FP64 thermal run (5 outer iterations, Jacobi to max |ΔT| < 1e-6 K)
     with the direct heat solve, against the reference's own run (tests/golden/thermal64_c2.npz).
     They differ by the reference loop's stopping error: its last sweep moves T by less than
     1e-6 K, but the iterate is still that sweep's contraction factor away from the fixed
@@ -175,7 +175,7 @@ def test_configuration_2_direct_against_reference_jacobi():
     zs = [int(v) for v in z["T_z"]]
     dT = float(np.abs(r.temperature[zs] - z["T_slices"]).max())
     span = float(z["T_max"] - z["T_min"])
-    print(f"configuration 2, direct vs the reference's Jacobi: max |dT| {dT:.3g} K on the stored slices "
+    print(f"128 x 128 x 200 thermal run, direct vs the reference's Jacobi: max |dT| {dT:.3g} K on the stored slices "
           f"(T spans {span:.3g} K), {r.stats.outer_iterations} outer iterations, "
           f"FP64 sweep residual {r.stats.last_residual:.3g} K")
     assert r.stats.jacobi_sweeps == 0

@@ -82,7 +82,7 @@ def test_plain_fp32_error_against_fp64_oracle(n):
     assert abs(r.sh_power - st.sh_power) / st.sh_power <= 1e-5
 
 
-def test_c1_fp32_against_reference_fp64():
+def test_plain_64x64x100_fp32_against_reference_fp64():
     z = np.load(os.path.join(GOLDEN, "plain64_c1.npz"))
     p = G.params_of("plain64_c1").replace(precision=32)
     r = shg.solve(p)
@@ -91,9 +91,9 @@ def test_c1_fp32_against_reference_fp64():
     assert rel_l2(r.signal, z["signal"]) <= 1e-4
 
 
-def test_c1_fp32_is_closer_to_reference_fp64_than_reference_fp32():
-    """The reference's own float build (its default, cuSHG.cu:7-8, cuFFT in FP32) at
-    configuration 1 is 1.3e-3 (SH field, relative L2) and 6.2e-4 (SH power) from its FP64 build:
+def test_plain_64x64x100_fp32_is_closer_to_reference_fp64_than_reference_fp32():
+    """The reference's own float build (its default, cuSHG.cu:7-8, cuFFT in FP32) on the plain
+    64 x 64 x 100 case is 1.3e-3 (SH field, relative L2) and 6.2e-4 (SH power) from its FP64 build:
     it rounds Δk, κ and the propagator phases to float.  This library's FP32 march computes
     those scalars in FP64 and applies its constants compensated: at least 100x closer on both."""
     z64 = np.load(os.path.join(GOLDEN, "plain64_c1.npz"))

@@ -361,13 +361,13 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         out["fp64_plain_per_instance"] = fp64_per_instance(ps, value)
         out["adjoint"] = adjoint_figures(32, args.adjoint_batch, 5, 3, args.checkpoint_every)
         try:
-            out["thermal_c5"] = thermal_c5_figures()
+            out["thermal_batch_8x512x512x1000"] = thermal_batch_512_figures()
         except Exception as e:  # the sweep line stands without it
-            out["thermal_c5"] = {"error": str(e)[:300]}
+            out["thermal_batch_8x512x512x1000"] = {"error": str(e)[:300]}
         try:
-            out["thermal_c2"] = thermal_c2_figures()
+            out["thermal_128x128x200"] = thermal_128_figures()
         except Exception as e:
-            out["thermal_c2"] = {"error": str(e)[:300]}
+            out["thermal_128x128x200"] = {"error": str(e)[:300]}
     if args.class_side:
         out["config"]["workload"] = f"{len(ps)} instances of {args.class_side}x{args.class_side}, nz = {args.class_nz}"
     if not args.no_cpu_baseline:
@@ -375,7 +375,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     return out
 
 
-def thermal_c5_figures() -> dict:
+def thermal_batch_512_figures() -> dict:
     """The large thermal batch as stated: 8 thermal runs of 512x512 / nz = 1000 in FP32 (50 W,
     w0 = 50 µm, 20 mm, ovens evenly spaced 30-65 °C), each to max|ΔT| < 1e-6 K in every one of
     at most 5 outer iterations, with dJ/dT_oven through the temperature field, in one
@@ -402,7 +402,7 @@ def thermal_c5_figures() -> dict:
             "dJ_dToven_w_per_k": [float(x) for x in dt]}
 
 
-def thermal_c2_figures() -> dict:
+def thermal_128_figures() -> dict:
     """The thermal configuration as stated (128 x 128 x 200 FP64, 20 mm, 20 W, w0 = 40 µm, oven
     40 °C, max|ΔT| < 1e-6 K inside <= 5 outer iterations), one shg_solve_device call each way:
     with the reference's Jacobi sweeps (its bits and sweep counts) and with the direct heat
